@@ -1,0 +1,236 @@
+"""ctypes bindings for the in-tree sm_100a library (include/gerjoii_gpu.h).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+GJ_OK, GJ_EINVAL, GJ_ENOMEM, GJ_ENUMERIC, GJ_ETIMEOUT, GJ_ECUDA, GJ_EUNSUPPORTED = range(7)
+GJ_F32, GJ_F64 = 0, 1
+GJ_ADJ_REFERENCE, GJ_ADJ_EXACT = 0, 1
+GJ_MISFIT_L2, GJ_MISFIT_ENV_L2 = 0, 1
+
+STATUS_NAMES = {0: "GJ_OK", 1: "GJ_EINVAL", 2: "GJ_ENOMEM", 3: "GJ_ENUMERIC", 4: "GJ_ETIMEOUT",
+                5: "GJ_ECUDA", 6: "GJ_EUNSUPPORTED"}
+
+
+class GJError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class GridC(C.Structure):
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("pml", C.c_int), ("pml_top", C.c_int),
+                ("air", C.c_int), ("nt", C.c_int), ("dx", C.c_double), ("dy", C.c_double),
+                ("dt", C.c_double), ("eps0", C.c_double), ("mu0", C.c_double), ("order", C.c_int),
+                ("R0", C.c_double)]
+
+
+class ShotC(C.Structure):
+    _fields_ = [("src_i", C.c_int), ("src_j", C.c_int), ("wavelet", C.POINTER(C.c_double)),
+                ("nr", C.c_int), ("rec", C.POINTER(C.c_long))]
+
+
+class OptsC(C.Structure):
+    _fields_ = [("ckpt_every", C.c_int), ("mem_budget_bytes", C.c_size_t),
+                ("shots_per_launch", C.c_int), ("no_kahan", C.c_int), ("no_graph", C.c_int),
+                ("per_shot", C.c_int), ("plain", C.c_int)]
+
+
+# Every symbol the header declares, with its signature.
+_VP, _DP, _I, _L = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_long
+SIGNATURES = {
+    "gj_version": (C.c_char_p, []),
+    "gj_context_create": (_I, [C.POINTER(_VP), _I]),
+    "gj_context_destroy": (_I, [_VP]),
+    "gj_last_error": (C.c_char_p, [_VP]),
+    "gj_last_launch_count": (_L, [_VP]),
+    "gj_w_forward": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _DP, _DP]),
+    "gj_w_gradient": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _I,
+                           C.POINTER(OptsC), _DP, _DP, _DP, _DP, _DP]),
+    "gj_w_grad": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _DP, _DP, _DP, _DP]),
+    "gj_w_gradient_dev": (_I, [_VP, C.POINTER(GridC), _I, _VP, _VP, C.POINTER(ShotC), _I, _VP, _I, _I,
+                               C.POINTER(OptsC), _VP, _VP, _DP, _VP]),
+}
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = False):
+    """Loads libgerjoii_b200.so; raises if it is absent (no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if build_if_missing:
+            _build.build()
+        else:
+            raise ImportError(f"gerjoii_b200 CUDA library not built: {path} "
+                              "(run python -m gerjoii_b200.build)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(_DP) if a is not None else None
+
+
+def grid_c(g) -> GridC:
+    return GridC(g.m, g.n, g.pml, g.pml_top, g.air, g.nt, g.dx, g.dy, g.dt, g.eps0, g.mu0, g.order, g.R0)
+
+
+class _ShotPack:
+    """Keeps the numpy buffers behind a ShotC array alive."""
+
+    def __init__(self, shots, nt):
+        self.wav = [np.ascontiguousarray(np.asarray(s.wavelet, np.float64)[:nt]) for s in shots]
+        self.rec = [np.ascontiguousarray(np.asarray(s.rec, np.int64)) for s in shots]
+        arr = (ShotC * len(shots))()
+        for k, s in enumerate(shots):
+            if len(self.wav[k]) < nt:
+                raise ValueError(f"shot {k}: wavelet has {len(self.wav[k])} < nt samples")
+            arr[k].src_i = int(s.src_i)
+            arr[k].src_j = int(s.src_j)
+            arr[k].wavelet = self.wav[k].ctypes.data_as(_DP)
+            arr[k].nr = len(self.rec[k])
+            arr[k].rec = self.rec[k].ctypes.data_as(C.POINTER(C.c_long))
+        self.arr = arr
+        self.n = len(shots)
+
+
+def _f(a):
+    """Column-major float64 copy of a model / trace array."""
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+class Context:
+    """One gj_ctx on a device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = _VP()
+        st = self.lib.gj_context_create(C.byref(h), int(device))
+        if st != GJ_OK:
+            raise GJError(st, f"gj_context_create(device={device}) failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.gj_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != GJ_OK:
+            raise GJError(st, self.lib.gj_last_error(self.h).decode())
+
+    @property
+    def last_launch_count(self) -> int:
+        return int(self.lib.gj_last_launch_count(self.h))
+
+    # ------------------------------------------------------------------ radar
+    def w_forward(self, g, eps, sig, shots, precision=GJ_F32, want_jz=False, want_u=False):
+        """Traces per shot (nt x nr), optional Jz (nt) and u (m x n x nt)."""
+        sp = _ShotPack(shots, g.nt)
+        d = np.zeros(sum(g.nt * len(r) for r in sp.rec), np.float64)
+        jz = np.zeros(len(shots) * g.nt, np.float64) if want_jz else None
+        u = np.zeros(len(shots) * g.m * g.n * g.nt, np.float64) if want_u else None
+        gc = grid_c(g)
+        e, s = _f(eps), _f(sig)
+        self._check(self.lib.gj_w_forward(self.h, C.byref(gc), precision, _dp(e), _dp(s), sp.arr, sp.n,
+                                          _dp(d), _dp(jz), _dp(u)))
+        out, o = [], 0
+        for r in sp.rec:
+            out.append(d[o:o + g.nt * len(r)].reshape((g.nt, len(r)), order="F"))
+            o += g.nt * len(r)
+        res = {"d": out}
+        if want_jz:
+            res["jz"] = jz.reshape(len(shots), g.nt)
+        if want_u:
+            res["u"] = [u[k * g.m * g.n * g.nt:(k + 1) * g.m * g.n * g.nt].reshape((g.m, g.n, g.nt), order="F")
+                        for k in range(len(shots))]
+        return res
+
+    def w_gradient(self, g, eps, sig, shots, d_obs, mode=GJ_ADJ_REFERENCE, misfit=GJ_MISFIT_L2,
+                   precision=GJ_F32, opts=None, want_traces=False):
+        """Gradient (g_eps, g_sig) summed over shots (or per shot), misfits, optional d and e."""
+        sp = _ShotPack(shots, g.nt)
+        o = opts or OptsC()
+        per = len(shots) if o.per_shot else 1
+        ge = np.zeros(per * g.m * g.n, np.float64)
+        gs = np.zeros_like(ge)
+        mis = np.zeros(len(shots), np.float64)
+        dobs = np.concatenate([_f(x).ravel(order="F") for x in d_obs])
+        ntr = sum(g.nt * len(r) for r in sp.rec)
+        if dobs.size != ntr:
+            raise ValueError("d_obs does not match the shots' receivers")
+        dd = np.zeros(ntr) if want_traces else None
+        ee = np.zeros(ntr) if want_traces else None
+        gc = grid_c(g)
+        e, s = _f(eps), _f(sig)
+        self._check(self.lib.gj_w_gradient(self.h, C.byref(gc), precision, _dp(e), _dp(s), sp.arr, sp.n,
+                                           _dp(dobs), int(mode), int(misfit), C.byref(o), _dp(ge), _dp(gs),
+                                           _dp(mis), _dp(dd), _dp(ee)))
+        shape = (g.m, g.n) if per == 1 else (per, g.m, g.n)
+        res = {"g_eps": ge.reshape(shape, order="F") if per == 1 else
+               np.stack([ge[k * g.m * g.n:(k + 1) * g.m * g.n].reshape((g.m, g.n), order="F") for k in range(per)]),
+               "g_sig": gs.reshape(shape, order="F") if per == 1 else
+               np.stack([gs[k * g.m * g.n:(k + 1) * g.m * g.n].reshape((g.m, g.n), order="F") for k in range(per)]),
+               "misfit": mis}
+        if want_traces:
+            outd, oute, q = [], [], 0
+            for r in sp.rec:
+                n_ = g.nt * len(r)
+                outd.append(dd[q:q + n_].reshape((g.nt, len(r)), order="F"))
+                oute.append(ee[q:q + n_].reshape((g.nt, len(r)), order="F"))
+                q += n_
+            res["d"], res["e"] = outd, oute
+        return res
+
+    def w_grad(self, g, eps, sig, shot, e, u, precision=GJ_F32):
+        """w_grad.m for one shot: (g, a_max)."""
+        sp = _ShotPack([shot], g.nt)
+        out = np.zeros(g.m * g.n)
+        amax = np.zeros(g.m * g.n)
+        gc = grid_c(g)
+        ea, ua = _f(e), _f(u)
+        self._check(self.lib.gj_w_grad(self.h, C.byref(gc), precision, _dp(_f(eps)), _dp(_f(sig)), sp.arr,
+                                       _dp(ea), _dp(ua), _dp(out), _dp(amax)))
+        return out.reshape((g.m, g.n), order="F"), amax.reshape((g.m, g.n), order="F")
+
+    def w_gradient_dev(self, g, eps_t, sig_t, shots, dobs_t, ge_t, gs_t, mode=GJ_ADJ_REFERENCE,
+                       misfit=GJ_MISFIT_L2, opts=None, stream=0):
+        """Device-pointer gradient: arguments are torch CUDA tensors (float32 or float64)."""
+        import torch
+        prec = GJ_F64 if eps_t.dtype == torch.float64 else GJ_F32
+        sp = _ShotPack(shots, g.nt)
+        o = opts or OptsC()
+        mis = np.zeros(len(shots), np.float64)
+        gc = grid_c(g)
+        self._check(self.lib.gj_w_gradient_dev(self.h, C.byref(gc), prec, eps_t.data_ptr(), sig_t.data_ptr(),
+                                               sp.arr, sp.n, dobs_t.data_ptr(), int(mode), int(misfit),
+                                               C.byref(o), ge_t.data_ptr(), gs_t.data_ptr(), _dp(mis),
+                                               C.c_void_p(stream)))
+        return mis

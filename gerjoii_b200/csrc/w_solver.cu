@@ -1,0 +1,688 @@
+// Radar (GPR) solver: device plan, forward, checkpointed gradient, w_grad.
+//
+// Host orchestration of the kernels in w_kernels.cuh.  One plan holds the
+// padded grid, the coefficient arrays (built on the device from the model),
+// the per-shot source/receiver tables, the A/B state buffers of the forward
+// and adjoint fields, the checkpoints and the u-history ring.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+
+#include "gj_internal.h"
+#include "w_kernels.cuh"
+
+namespace gj {
+
+static inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// Graded PML profiles (w_cpml.m:47-55, 70-78, 110-118, 151-159), 0-based rows/cols.
+static void pml_profiles(const gj_w_grid& g, int NX, int NY, std::vector<double>& sex,
+                         std::vector<double>& smx, std::vector<double>& sey,
+                         std::vector<double>& smy) {
+  const double P = g.pml, c = 1.0 / std::sqrt(g.mu0 * g.eps0);
+  const double sx = -(g.order + 1) * g.eps0 * c * std::log(g.R0) / (2.0 * g.dx * g.pml);
+  const double sy = -(g.order + 1) * g.eps0 * c * std::log(g.R0) / (2.0 * g.dy * g.pml);
+  const double rm = g.mu0 / g.eps0;
+  sex.assign(NX + 2, 0.0); smx.assign(NX + 2, 0.0); sey.assign(NY + 2, 0.0); smy.assign(NY + 2, 0.0);
+  for (int I = 1; I <= g.pml_top; ++I) sex[I] = sx * std::pow((P - I + 0.25) / P, g.order);
+  for (int I = 0; I <= g.pml_top - 1; ++I) smx[I] = rm * sx * std::pow((P - I - 0.25) / P, g.order);
+  for (int I = NX - g.pml; I <= NX - 1; ++I) {
+    const double k = I - (NX - g.pml) + 1;
+    sex[I] = sx * std::pow((k - 0.75) / P, g.order);
+    smx[I] = rm * sx * std::pow((k - 0.25) / P, g.order);
+  }
+  for (int J = 1; J <= g.pml; ++J) sey[J] = sy * std::pow((P - J + 0.25) / P, g.order);
+  for (int J = 0; J <= g.pml - 1; ++J) smy[J] = rm * sy * std::pow((P - J - 0.25) / P, g.order);
+  for (int J = NY - g.pml; J <= NY - 1; ++J) {
+    const double k = J - (NY - g.pml) + 1;
+    sey[J] = sy * std::pow((k - 0.75) / P, g.order);
+    smy[J] = rm * sy * std::pow((k - 0.25) / P, g.order);
+  }
+}
+
+template <class TM>
+__global__ void k_cezj(const CoefBuild c, const TM* eps, const TM* sig, const int* si, const int* sj,
+                       int nshots, void* out, int is_double) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nshots) return;
+  double e = 1, sg = 0;
+  pad_model(c, eps, sig, si[s], sj[s], e, sg);
+  const double v = -(2 * c.dt) / (2 * e * c.eps0 + c.dt * sg);  // w_coeff.m:44-45
+  if (is_double) static_cast<double*>(out)[s] = v;
+  else static_cast<float*>(out)[s] = float(v);
+}
+
+// Residual e = d - d_obs and the two sums of the normalised L2 misfit
+// (w_bozdag.m:49, w_E.m:15-16, w_update_e.m:75-76).
+template <class T>
+__global__ void k_residual(const T* d, const T* dobs, T* e, size_t per_shot, double* sums) {
+  const int s = blockIdx.y;
+  double num = 0, den = 0;
+  const size_t base = size_t(s) * per_shot;
+  for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < per_shot; i += size_t(blockDim.x) * gridDim.x) {
+    const T r = d[base + i] - dobs[base + i];
+    e[base + i] = r;
+    num += double(r) * double(r);
+    den += double(dobs[base + i]) * double(dobs[base + i]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    num += __shfl_down_sync(0xffffffffu, num, o);
+    den += __shfl_down_sync(0xffffffffu, den, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(sums + 2 * s, num);
+    atomicAdd(sums + 2 * s + 1, den);
+  }
+}
+
+template <class TI, class TO>
+__global__ void k_convert(const TI* in, TO* out, size_t n) {
+  for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < n; i += size_t(blockDim.x) * gridDim.x)
+    out[i] = TO(in[i]);
+}
+
+template <class T>
+class WSolver : public WSolverBase {
+ public:
+  gj_w_grid g{};
+  int NX = 0, NY = 0, ld = 0, nshots = 0, nr = 0;  // nr = max receivers per shot
+  size_t fstride = 0, sstride = 0, mn = 0;
+  WDev<T> w{};   // forward coefficients
+  WDev<T> wr{};  // reference-adjoint coefficients (sigma -> -sigma in the interior)
+  DevBuf coef, model_d, prof, shotbuf, recbuf, selbuf, nrsbuf, nselbuf, sibuf, sjbuf;
+  DevBuf fwdA, fwdB, adjA, adjB, hist, ckpt, acc, dbuf, ebuf, dobsbuf, sums, scratch;
+  std::vector<ShotHost> sh;
+  std::vector<int> nrs, nsel;
+  // layout of shotbuf: src (long) | cezj (T) | wav (T, nshots*nt)
+  long* d_src = nullptr; T* d_cezj = nullptr; T* d_wav = nullptr;
+  double* eps_m = nullptr; double* sig_m = nullptr;
+  size_t hist_slots = 0, n_ckpt = 0;
+  int K = 0;
+  // launch shape
+  int bx = 128, tj = 16;
+
+  ~WSolver() override = default;
+
+  static std::string key(const gj_w_grid& g, const gj_w_shot* shots, int nshots) {
+    std::string k((const char*)&g, sizeof g);
+    k.append((const char*)&nshots, sizeof nshots);
+    for (int s = 0; s < nshots; ++s) {
+      k.append((const char*)&shots[s].src_i, 2 * sizeof(int));
+      k.append((const char*)&shots[s].nr, sizeof(int));
+      k.append((const char*)shots[s].rec, sizeof(long) * size_t(shots[s].nr));
+      k.append((const char*)shots[s].wavelet, sizeof(double) * size_t(g.nt));
+    }
+    return k;
+  }
+
+  gj_status setup(Err& err, const gj_w_grid& gg, const gj_w_shot* shots, int ns) {
+    g = gg;
+    if (g.m < 3 || g.n < 3 || g.pml < 1 || g.nt < 3)
+      return err.set(GJ_EINVAL, "grid too small: need m, n >= 3, pml >= 1, nt >= 3");
+    if (!(g.pml_top == 0 || g.pml_top == g.pml))
+      return err.set(GJ_EINVAL, "pml_top must be 0 (free top) or equal to pml");
+    if (g.air < 0 || (g.pml_top == 0 && g.air < 1))
+      return err.set(GJ_EINVAL, "air must be >= 0, and >= 1 with a free top");
+    if (!(g.dx > 0 && g.dy > 0 && g.dt > 0 && g.eps0 > 0 && g.mu0 > 0 && g.R0 > 0 && g.R0 < 1))
+      return err.set(GJ_EINVAL, "dx, dy, dt, eps0, mu0 must be positive and 0 < R0 < 1");
+    if (ns < 1 || !shots) return err.set(GJ_EINVAL, "need at least one shot");
+    NX = g.pml_top + g.air + g.m + g.pml;
+    NY = g.n + 2 * g.pml;
+    ld = round_up(NX + 2, 32);
+    fstride = size_t(ld) * size_t(NY + 3);
+    sstride = size_t(NFIELDS) * fstride;
+    mn = size_t(g.m) * size_t(g.n);
+    nshots = ns;
+    nr = 0;
+    sh.assign(ns, ShotHost{});
+    nrs.assign(ns, 0);
+    nsel.assign(ns, 0);
+    for (int s = 0; s < ns; ++s) {
+      const gj_w_shot& q = shots[s];
+      if (!q.wavelet) return err.set(GJ_EINVAL, "shot %d: null wavelet", s);
+      if (q.nr < 0 || (q.nr > 0 && !q.rec)) return err.set(GJ_EINVAL, "shot %d: bad receivers", s);
+      if (q.src_i < 1 || q.src_i > NX - 1 || q.src_j < 1 || q.src_j > NY - 1)
+        return err.set(GJ_EINVAL, "shot %d: source (%d,%d) must be an updated Ez node, 1..NX-1 x 1..NY-1", s,
+                       q.src_i, q.src_j);
+      const bool interior = q.src_i >= g.pml_top + 1 && q.src_i <= NX - g.pml - 1 &&
+                            q.src_j >= g.pml + 1 && q.src_j <= NY - g.pml - 1;
+      // A source in the PML band is overwritten by new_Ez_pml (w_solve.m:92-94): no effect.
+      sh[s].src = interior ? long(q.src_i) + long(q.src_j) * ld : -1;
+      sh[s].wav.assign(q.wavelet, q.wavelet + g.nt);
+      sh[s].rec.resize(q.nr);
+      std::map<long, int> last;
+      for (int r = 0; r < q.nr; ++r) {
+        const long L = q.rec[r];
+        if (L < 0 || L >= long(NX + 1) * long(NY + 1))
+          return err.set(GJ_EINVAL, "shot %d receiver %d: node %ld outside the (NX+1)x(NY+1) grid", s, r, L);
+        const long i = L % (NX + 1), j = L / (NX + 1);
+        sh[s].rec[r] = i + j * ld;
+        last[sh[s].rec[r]] = r;
+      }
+      for (int r = 0; r < q.nr; ++r)
+        if (last[sh[s].rec[r]] == r) sh[s].sel.push_back(r);
+      nrs[s] = q.nr;
+      nsel[s] = int(sh[s].sel.size());
+      nr = std::max(nr, q.nr);
+    }
+    // device geometry
+    w.NX = NX; w.NY = NY; w.ld = ld; w.P = g.pml; w.Pt = g.pml_top; w.m = g.m; w.n = g.n;
+    w.di0 = g.pml_top + g.air; w.dj0 = g.pml;
+    w.ei0 = g.pml_top + 1; w.ei1 = NX - g.pml - 1; w.ej0 = g.pml + 1; w.ej1 = NY - g.pml - 1;
+    w.hyi0 = g.pml_top; w.hyi1 = NX - g.pml - 1; w.hxj0 = g.pml; w.hxj1 = NY - g.pml - 1;
+    w.chxez = T(-(2 * g.dt / g.dy) / (2 * g.mu0));
+    w.chyez = T((2 * g.dt / g.dx) / (2 * g.mu0));
+    w.rxy = T(-g.dx / g.dy);
+    // coefficient arrays: 12 node arrays
+    GJ_TRY(coef.alloc(err, 12 * fstride * sizeof(T)));
+    GJ_CUDA(err, cudaMemset(coef.p, 0, 12 * fstride * sizeof(T)));
+    T* cb = coef.as<T>() + ld;  // base one column in
+    T* arr[12];
+    for (int q = 0; q < 12; ++q) arr[q] = cb + q * fstride;
+    w.ce = arr[0]; w.chy = arr[1]; w.ax = arr[2]; w.bx = arr[3]; w.ay = arr[4]; w.by = arr[5];
+    w.hxa = arr[6]; w.hxb = arr[7]; w.hya = arr[8]; w.hyb = arr[9];
+    wr = w;
+    wr.ce = arr[10]; wr.chy = arr[11];
+    GJ_TRY(model_d.alloc(err, 2 * mn * sizeof(double)));
+    eps_m = model_d.as<double>(); sig_m = eps_m + mn;
+    // PML profiles
+    std::vector<double> sex, smx, sey, smy;
+    pml_profiles(g, NX, NY, sex, smx, sey, smy);
+    GJ_TRY(prof.alloc(err, (2 * (NX + 2) + 2 * (NY + 2)) * sizeof(double)));
+    double* pp = prof.as<double>();
+    GJ_CUDA(err, cudaMemcpy(pp, sex.data(), (NX + 2) * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(pp + NX + 2, smx.data(), (NX + 2) * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(pp + 2 * (NX + 2), sey.data(), (NY + 2) * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(pp + 2 * (NX + 2) + NY + 2, smy.data(), (NY + 2) * sizeof(double), cudaMemcpyHostToDevice));
+    // shot tables
+    const size_t sb = ns * sizeof(long) + ns * sizeof(T) + size_t(ns) * g.nt * sizeof(T) + 64;
+    GJ_TRY(shotbuf.alloc(err, sb));
+    d_src = shotbuf.as<long>();
+    d_cezj = reinterpret_cast<T*>(d_src + ns);
+    d_wav = d_cezj + ns;
+    std::vector<long> hsrc(ns);
+    std::vector<T> hwav(size_t(ns) * g.nt);
+    std::vector<int> hsi(ns), hsj(ns);
+    for (int s = 0; s < ns; ++s) {
+      hsrc[s] = sh[s].src;
+      hsi[s] = shots[s].src_i; hsj[s] = shots[s].src_j;
+      for (int t = 0; t < g.nt; ++t) hwav[size_t(s) * g.nt + t] = T(sh[s].wav[t]);
+    }
+    GJ_CUDA(err, cudaMemcpy(d_src, hsrc.data(), ns * sizeof(long), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(d_wav, hwav.data(), hwav.size() * sizeof(T), cudaMemcpyHostToDevice));
+    GJ_TRY(sibuf.alloc(err, ns * sizeof(int)));
+    GJ_TRY(sjbuf.alloc(err, ns * sizeof(int)));
+    GJ_CUDA(err, cudaMemcpy(sibuf.p, hsi.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(sjbuf.p, hsj.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+    const int nrr = std::max(nr, 1);
+    std::vector<long> hrec(size_t(ns) * nrr, 0);
+    std::vector<int> hsel(size_t(ns) * nrr, 0);
+    for (int s = 0; s < ns; ++s) {
+      for (int r = 0; r < nrs[s]; ++r) hrec[size_t(s) * nrr + r] = sh[s].rec[r];
+      for (int q = 0; q < nsel[s]; ++q) hsel[size_t(s) * nrr + q] = sh[s].sel[q];
+    }
+    GJ_TRY(recbuf.alloc(err, hrec.size() * sizeof(long)));
+    GJ_TRY(selbuf.alloc(err, hsel.size() * sizeof(int)));
+    GJ_TRY(nrsbuf.alloc(err, ns * sizeof(int)));
+    GJ_TRY(nselbuf.alloc(err, ns * sizeof(int)));
+    GJ_CUDA(err, cudaMemcpy(recbuf.p, hrec.data(), hrec.size() * sizeof(long), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(selbuf.p, hsel.data(), hsel.size() * sizeof(int), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(nrsbuf.p, nrs.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(nselbuf.p, nsel.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+    // traces
+    GJ_TRY(dbuf.alloc(err, size_t(ns) * nrr * g.nt * sizeof(T)));
+    GJ_TRY(ebuf.alloc(err, size_t(ns) * nrr * g.nt * sizeof(T)));
+    GJ_TRY(dobsbuf.alloc(err, size_t(ns) * nrr * g.nt * sizeof(T)));
+    GJ_TRY(sums.alloc(err, 2 * ns * sizeof(double)));
+    GJ_TRY(fwdA.alloc(err, size_t(ns) * sstride * sizeof(T)));
+    GJ_TRY(fwdB.alloc(err, size_t(ns) * sstride * sizeof(T)));
+    // launch shape: 128 rows per block; columns per block sized for >= ~4 waves
+    bx = 128;
+    const long blocks_per_col = (ld + bx - 1) / bx;
+    tj = 64;
+    while (tj > 4 && blocks_per_col * ((NY + tj) / tj) * ns < 148L * 16) tj /= 2;
+    return GJ_OK;
+  }
+
+  // Coefficients from the model (host doubles or device T / double).
+  template <class TM>
+  gj_status build(Err& err, Ctx& c, const TM* eps_dev, const TM* sig_dev, cudaStream_t st) {
+    CoefBuild cb;
+    cb.NX = NX; cb.NY = NY; cb.ld = ld; cb.P = g.pml; cb.Pt = g.pml_top; cb.air = g.air; cb.m = g.m; cb.n = g.n;
+    cb.dx = g.dx; cb.dy = g.dy; cb.dt = g.dt; cb.eps0 = g.eps0; cb.mu0 = g.mu0;
+    const double* pp = prof.as<double>();
+    cb.sex = pp; cb.smx = pp + NX + 2; cb.sey = pp + 2 * (NX + 2); cb.smy = pp + 2 * (NX + 2) + NY + 2;
+    dim3 blk(32, 8), grd((NX + 1 + 31) / 32, (NY + 1 + 7) / 8);
+    k_build_coefs<T, TM><<<grd, blk, 0, st>>>(cb, eps_dev, sig_dev, const_cast<T*>(w.ce), const_cast<T*>(w.chy),
+                                            const_cast<T*>(w.ax), const_cast<T*>(w.bx), const_cast<T*>(w.ay),
+                                            const_cast<T*>(w.by), const_cast<T*>(w.hxa), const_cast<T*>(w.hxb),
+                                            const_cast<T*>(w.hya), const_cast<T*>(w.hyb), const_cast<T*>(wr.ce),
+                                            const_cast<T*>(wr.chy), eps_m, sig_m);
+    k_cezj<TM><<<(nshots + 127) / 128, 128, 0, st>>>(cb, eps_dev, sig_dev, sibuf.as<int>(), sjbuf.as<int>(), nshots,
+                                                   d_cezj, sizeof(T) == 8);
+    c.launches += 2;
+    GJ_CUDA(err, cudaGetLastError());
+    return GJ_OK;
+  }
+
+  StepArgs<T> step_args(const T* A, T* B, int it) const {
+    StepArgs<T> a{};
+    a.A = A; a.B = B; a.fstride = fstride; a.sstride = sstride; a.shot0 = 0; a.tj = tj; a.it = it;
+    a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.hist = nullptr; a.hstride = 0;
+    a.kahan = 1;
+    return a;
+  }
+
+  dim3 grid_dims() const { return dim3((ld + bx - 1) / bx, (NY + 1 + tj - 1) / tj, nshots); }
+
+  // Forward time loop over [it0, it1); state in A (swapped in place).  Optionally
+  // writes the history slot it+1 - hbase of every step and records traces.
+  gj_status run_forward(Err& err, Ctx& c, T*& A, T*& B, int it0, int it1, bool record, T* hring,
+                        long hbase, size_t hcap, size_t hstride, cudaStream_t st, T* ckpt_base,
+                        int ckK) {
+    const dim3 grd = grid_dims();
+    for (int it = it0; it < it1; ++it) {
+      if (ckpt_base && ckK > 0 && it % ckK == 0) {
+        GJ_CUDA(err, cudaMemcpyAsync(ckpt_base + size_t(it / ckK) * nshots * sstride, A - ld,
+                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
+      }
+      StepArgs<T> a = step_args(A, B, it);
+      if (hring) {
+        const long slot = long(it + 1) - hbase;
+        a.hist = hring + size_t(slot % long(hcap)) * nshots * hstride;
+        a.hstride = hstride;
+      }
+      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+      ++c.launches;
+      if (record) {
+        k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), std::max(nr, 1),
+                                                     nrsbuf.as<int>(), it, g.nt, dbuf.as<T>(), d_src,
+                                                     static_cast<T*>(nullptr), nshots);
+        ++c.launches;
+      }
+      std::swap(A, B);
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    return GJ_OK;
+  }
+
+  gj_status alloc_states(Err& err) {
+    GJ_TRY(fwdA.alloc(err, size_t(nshots) * sstride * sizeof(T)));
+    GJ_TRY(fwdB.alloc(err, size_t(nshots) * sstride * sizeof(T)));
+    return GJ_OK;
+  }
+
+  // ------------------------------------------------------------ forward
+  gj_status forward(Err& err, Ctx& c, const double* eps, const double* sig, double* d_out,
+                    double* jz_out, double* u_out) {
+    cudaStream_t st = 0;
+    DevBuf mh;
+    GJ_TRY(mh.alloc(err, 2 * mn * sizeof(double)));
+    GJ_CUDA(err, cudaMemcpy(mh.as<double>(), eps, mn * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(mh.as<double>() + mn, sig, mn * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_TRY(build<double>(err, c, mh.as<double>(), mh.as<double>() + mn, st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
+    T* A = fwdA.as<T>() + ld;
+    T* B = fwdB.as<T>() + ld;
+    const int nrr = std::max(nr, 1);
+    DevBuf jzb, ub;
+    if (jz_out) GJ_TRY(jzb.alloc(err, size_t(nshots) * g.nt * sizeof(T)));
+    if (u_out) GJ_TRY(ub.alloc(err, size_t(nshots) * mn * (g.nt + 1) * sizeof(T)));
+    const dim3 grd = grid_dims();
+    for (int it = 0; it < g.nt; ++it) {
+      StepArgs<T> a = step_args(A, B, it);
+      if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * mn; a.hstride = mn; }
+      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
+                                                   g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
+                                                   nshots);
+      c.launches += 2;
+      std::swap(A, B);
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    GJ_CUDA(err, cudaDeviceSynchronize());
+    // copy out (per shot nt x nr, time fastest)
+    std::vector<T> hd(size_t(nshots) * nrr * g.nt);
+    GJ_CUDA(err, cudaMemcpy(hd.data(), dbuf.p, hd.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    size_t o = 0;
+    for (int s = 0; s < nshots; ++s)
+      for (int r = 0; r < nrs[s]; ++r)
+        for (int t = 0; t < g.nt; ++t) d_out[o++] = double(hd[(size_t(s) * nrr + r) * g.nt + t]);
+    if (jz_out) {
+      std::vector<T> hj(size_t(nshots) * g.nt);
+      GJ_CUDA(err, cudaMemcpy(hj.data(), jzb.p, hj.size() * sizeof(T), cudaMemcpyDeviceToHost));
+      for (size_t i = 0; i < hj.size(); ++i) jz_out[i] = double(hj[i]);
+    }
+    if (u_out) {
+      std::vector<T> hu(size_t(nshots) * mn * g.nt);
+      GJ_CUDA(err, cudaMemcpy(hu.data(), ub.p, hu.size() * sizeof(T), cudaMemcpyDeviceToHost));
+      // device [t][shot][p] -> host [shot][t][p]
+      for (int s = 0; s < nshots; ++s)
+        for (int t = 0; t < g.nt; ++t)
+          for (size_t p = 0; p < mn; ++p)
+            u_out[(size_t(s) * g.nt + t) * mn + p] = double(hu[(size_t(t) * nshots + s) * mn + p]);
+    }
+    return GJ_OK;
+  }
+
+  // ------------------------------------------------------------ gradient
+  // Chooses K: the whole history when it fits, else checkpoints every K steps.
+  void choose_k(const gj_w_opts& o, size_t free_bytes) {
+    const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.8 * double(free_bytes));
+    const size_t per_slot = size_t(nshots) * mn * sizeof(T);
+    const size_t per_ck = size_t(nshots) * sstride * sizeof(T);
+    if (o.ckpt_every > 0) { K = std::min(std::max(o.ckpt_every, 2), g.nt); return; }
+    if (size_t(g.nt + 1) * per_slot <= budget) { K = g.nt; return; }
+    double k = std::sqrt(double(g.nt) * double(per_ck) / double(per_slot));
+    K = std::min(std::max(int(k), 2), g.nt);
+    while (K > 2 && (size_t(g.nt / K + 2) * per_ck + size_t(K + 3) * per_slot) > budget) K = K * 3 / 4;
+  }
+
+  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
+                     bool dev_dobs, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
+                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+    const int nrr = std::max(nr, 1);
+    const size_t tr = size_t(nrr) * g.nt;  // trace elements per shot
+    // model -> coefficients
+    DevBuf mh;
+    const double* eps_d = nullptr; const double* sig_d = nullptr;
+    if (!dev_in) {
+      GJ_TRY(mh.alloc(err, 2 * mn * sizeof(double)));
+      GJ_CUDA(err, cudaMemcpyAsync(mh.as<double>(), eps, mn * sizeof(double), cudaMemcpyHostToDevice, st));
+      GJ_CUDA(err, cudaMemcpyAsync(mh.as<double>() + mn, sig, mn * sizeof(double), cudaMemcpyHostToDevice, st));
+      eps_d = mh.as<double>(); sig_d = eps_d + mn;
+      GJ_TRY(build<double>(err, c, eps_d, sig_d, st));
+    } else {
+      GJ_TRY(build<T>(err, c, static_cast<const T*>(eps), static_cast<const T*>(sig), st));
+    }
+    // observed traces -> device T, layout per shot [r][t] (nt x nr, time fastest)
+    if (!dev_dobs) {
+      std::vector<T> hd(size_t(nshots) * tr, T(0));
+      size_t q = 0;
+      for (int s = 0; s < nshots; ++s)
+        for (int r = 0; r < nrs[s]; ++r)
+          for (int t = 0; t < g.nt; ++t) hd[(size_t(s) * nrr + r) * g.nt + t] = T(static_cast<const double*>(dobs)[q++]);
+      GJ_CUDA(err, cudaMemcpyAsync(dobsbuf.p, hd.data(), hd.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+      GJ_CUDA(err, cudaStreamSynchronize(st));
+    } else {
+      GJ_CUDA(err, cudaMemcpyAsync(dobsbuf.p, dobs, size_t(nshots) * tr * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    }
+    // memory plan
+    size_t free_b = 0, total_b = 0;
+    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
+    choose_k(o, free_b + hist.bytes + ckpt.bytes);
+    const bool full = (K >= g.nt);
+    // segments: [s0, s1) in steps; a remainder of one step joins the previous segment
+    std::vector<std::pair<int, int>> segs;
+    for (int s0 = 0; s0 < g.nt; s0 += K) segs.push_back({s0, std::min(g.nt, s0 + K)});
+    if (segs.size() > 1 && segs.back().second - segs.back().first < 2) {
+      segs[segs.size() - 2].second = segs.back().second;
+      segs.pop_back();
+    }
+    int maxlen = 0;
+    for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
+    hist_slots = full ? size_t(g.nt + 1) : size_t(maxlen + 3);
+    GJ_TRY(hist.alloc(err, hist_slots * nshots * mn * sizeof(T)));
+    n_ckpt = full ? 0 : segs.size();
+    if (!full) GJ_TRY(ckpt.alloc(err, n_ckpt * nshots * sstride * sizeof(T)));
+    GJ_TRY(adjA.alloc(err, size_t(nshots) * sstride * sizeof(T)));
+    GJ_TRY(adjB.alloc(err, size_t(nshots) * sstride * sizeof(T)));
+    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * mn * sizeof(T)));
+    T* H = hist.as<T>();
+    const size_t hs = mn;  // per-shot stride inside a slot
+    auto slot_ptr = [&](long k, long base) { return H + size_t(k - base) * nshots * hs; };
+
+    // ---- forward (with checkpoints at segment starts) ----
+    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
+    T* A = fwdA.as<T>() + ld;
+    T* B = fwdB.as<T>() + ld;
+    const dim3 grd = grid_dims();
+    if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, nshots * hs * sizeof(T), st));  // slot 0 = zero state
+    size_t segi = 0;
+    for (int it = 0; it < g.nt; ++it) {
+      if (!full && segi < segs.size() && it == segs[segi].first) {
+        GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * nshots * sstride, A - ld,
+                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        ++segi;
+      }
+      StepArgs<T> a = step_args(A, B, it);
+      if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
+      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
+                                                   g.nt, dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
+      c.launches += 2;
+      std::swap(A, B);
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    // ---- residual and misfit ----
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+    k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr, sums.as<double>());
+    ++c.launches;
+    std::vector<double> hsums(2 * nshots);
+    GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // ---- adjoint ----
+    GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * mn * sizeof(T), st));
+    T* LA = adjA.as<T>() + ld;
+    T* LB = adjB.as<T>() + ld;
+    const int nt = g.nt;
+    const double dt = g.dt;
+    for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
+      const int s0 = segs[sidx].first, s1 = segs[sidx].second;
+      long base = 0;
+      if (!full) {
+        // restore the checkpoint and recompute slots s0..min(s1+1, nt)
+        base = s0;
+        GJ_CUDA(err, cudaMemcpyAsync(A - ld, ckpt.as<T>() + size_t(sidx) * nshots * sstride,
+                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        k_domain_copy<T><<<dim3(64, nshots), 256, 0, st>>>(w, A, sstride, slot_ptr(s0, base), hs, nshots);
+        ++c.launches;
+        const int iend = std::min(s1 + 1, nt);
+        for (int it = s0; it < iend; ++it) {
+          StepArgs<T> a = step_args(A, B, it);
+          a.hist = slot_ptr(it + 1, base); a.hstride = hs;
+          k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+          ++c.launches;
+          std::swap(A, B);
+        }
+      }
+      for (int k = s1; k >= s0 + 1; --k) {  // k = history slot of forward step k-1
+        const int itf = k - 1;              // 0-based forward step
+        if (mode == GJ_ADJ_REFERENCE) {
+          if (nsel.size() && nr > 0)
+            k_inject_set<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), selbuf.as<int>(), nrr,
+                                                             nselbuf.as<int>(), ebuf.as<T>(), itf, nt, nshots);
+          StepArgs<T> a = step_args(LA, LB, itf);
+          a.src = d_src; a.hist = nullptr;
+          // d/dt u stencil (differentiate_cube.m:33-51); slots are 1-based in time
+          int k0, k1, k2; double c0, c1, c2;
+          if (k == 1) { k0 = 1; k1 = 2; k2 = 3; c0 = -1.5 / dt; c1 = 2.0 / dt; c2 = -0.5 / dt; }
+          else if (k == nt) { k0 = nt - 2; k1 = nt - 1; k2 = nt; c0 = 0.5 / dt; c1 = -2.0 / dt; c2 = 1.5 / dt; }
+          else { k0 = k - 1; k1 = k; k2 = k + 1; c0 = -0.5 / dt; c1 = 0.0; c2 = 0.5 / dt; }
+          a.u0 = slot_ptr(k0, base); a.u1 = slot_ptr(k1, base); a.u2 = slot_ptr(k2, base);
+          a.c0 = T(c0); a.c1 = T(c1); a.c2 = T(c2);
+          a.uk = slot_ptr(k, base);
+          a.hstride = hs;
+          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = o.no_kahan ? 0 : 1;
+          k_step<T, 1><<<grd, bx, 0, st>>>(wr, a);
+        } else {
+          if (nr > 0)
+            k_inject_add<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(),
+                                                             ebuf.as<T>(), itf, nt, nshots);
+          AdjArgs<T> a{};
+          a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = 0; a.tj = tj;
+          a.ek = slot_ptr(k, base); a.ekm1 = slot_ptr(k - 1, base); a.hstride = hs;
+          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = o.no_kahan ? 0 : 1;
+          k_adj_step<T><<<grd, bx, 0, st>>>(w, a);
+        }
+        c.launches += 2;
+        std::swap(LA, LB);
+      }
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    // ---- finish ----
+    const size_t gsz = (o.per_shot ? size_t(nshots) : 1) * mn;
+    DevBuf gout;
+    double* ge_d; double* gs_d;
+    if (dev_out && sizeof(T) == 8) { ge_d = static_cast<double*>(geps); gs_d = static_cast<double*>(gsig); }
+    else {
+      GJ_TRY(gout.alloc(err, 2 * gsz * sizeof(double)));
+      ge_d = gout.as<double>(); gs_d = ge_d + gsz;
+    }
+    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * mn, nshots, o.per_shot, mode == GJ_ADJ_EXACT ? 1 : 0,
+                                     g.dt, g.eps0, eps_m, sig_m, ge_d, gs_d);
+    ++c.launches;
+    if (dev_out && sizeof(T) == 4) {
+      k_convert<double, float><<<256, 256, 0, st>>>(ge_d, static_cast<float*>(geps), gsz);
+      k_convert<double, float><<<256, 256, 0, st>>>(gs_d, static_cast<float*>(gsig), gsz);
+      c.launches += 2;
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    if (!dev_out) {
+      GJ_CUDA(err, cudaMemcpyAsync(geps, ge_d, gsz * sizeof(double), cudaMemcpyDeviceToHost, st));
+      GJ_CUDA(err, cudaMemcpyAsync(gsig, gs_d, gsz * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    std::vector<T> hd, he;
+    if (d_out) { hd.resize(size_t(nshots) * tr); GJ_CUDA(err, cudaMemcpyAsync(hd.data(), dbuf.p, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, st)); }
+    if (e_out) { he.resize(size_t(nshots) * tr); GJ_CUDA(err, cudaMemcpyAsync(he.data(), ebuf.p, he.size() * sizeof(T), cudaMemcpyDeviceToHost, st)); }
+    GJ_CUDA(err, cudaStreamSynchronize(st));
+    if (misfit_out)
+      for (int s = 0; s < nshots; ++s)
+        misfit_out[s] = hsums[2 * s + 1] > 0 ? 0.5 * hsums[2 * s] / hsums[2 * s + 1] : 0.5 * hsums[2 * s];
+    auto unpack = [&](const std::vector<T>& v, double* out) {
+      size_t q = 0;
+      for (int s = 0; s < nshots; ++s)
+        for (int r = 0; r < nrs[s]; ++r)
+          for (int t = 0; t < g.nt; ++t) out[q++] = double(v[(size_t(s) * nrr + r) * g.nt + t]);
+    };
+    if (d_out) unpack(hd, d_out);
+    if (e_out) unpack(he, e_out);
+    return GJ_OK;
+  }
+
+  // ------------------------------------------------------------ w_grad only
+  gj_status grad_only(Err& err, Ctx& c, const double* eps, const double* sig, const double* e,
+                      const double* u, double* gout, double* amax) {
+    cudaStream_t st = 0;
+    DevBuf mh;
+    GJ_TRY(mh.alloc(err, 2 * mn * sizeof(double)));
+    GJ_CUDA(err, cudaMemcpy(mh.as<double>(), eps, mn * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_CUDA(err, cudaMemcpy(mh.as<double>() + mn, sig, mn * sizeof(double), cudaMemcpyHostToDevice));
+    GJ_TRY(build<double>(err, c, mh.as<double>(), mh.as<double>() + mn, st));
+    const int nrr = std::max(nr, 1), nt = g.nt;
+    // e: host nt x nr -> device [r][t]
+    std::vector<T> he(size_t(nrr) * nt, T(0));
+    for (int r = 0; r < nrs[0]; ++r)
+      for (int t = 0; t < nt; ++t) he[size_t(r) * nt + t] = T(e[size_t(r) * nt + t]);
+    GJ_CUDA(err, cudaMemcpy(ebuf.p, he.data(), he.size() * sizeof(T), cudaMemcpyHostToDevice));
+    // u: host m x n x nt -> device slots 1..nt (slot 0 unused)
+    GJ_TRY(hist.alloc(err, size_t(nt + 1) * mn * sizeof(T)));
+    {
+      std::vector<T> hu(size_t(nt) * mn);
+      for (size_t i = 0; i < hu.size(); ++i) hu[i] = T(u[i]);
+      GJ_CUDA(err, cudaMemcpy(hist.as<T>() + mn, hu.data(), hu.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    GJ_TRY(adjA.alloc(err, sstride * sizeof(T)));
+    GJ_TRY(adjB.alloc(err, sstride * sizeof(T)));
+    GJ_TRY(acc.alloc(err, 4 * mn * sizeof(T)));
+    GJ_CUDA(err, cudaMemset(adjA.p, 0, sstride * sizeof(T)));
+    GJ_CUDA(err, cudaMemset(adjB.p, 0, sstride * sizeof(T)));
+    GJ_CUDA(err, cudaMemset(acc.p, 0, 4 * mn * sizeof(T)));
+    T* LA = adjA.as<T>() + ld;
+    T* LB = adjB.as<T>() + ld;
+    const dim3 grd = grid_dims();
+    for (int k = nt; k >= 1; --k) {
+      if (nr > 0)
+        k_inject_set<T><<<dim3(1, 1), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), selbuf.as<int>(), nrr,
+                                                    nselbuf.as<int>(), ebuf.as<T>(), k - 1, nt, 1);
+      StepArgs<T> a = step_args(LA, LB, k - 1);
+      T* uk = hist.as<T>() + size_t(k) * mn;
+      a.u0 = uk; a.u1 = uk; a.u2 = uk; a.c0 = T(0); a.c1 = T(0); a.c2 = T(0);
+      a.uk = uk; a.hstride = mn;
+      a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = 1;
+      k_step<T, 1><<<grd, bx, 0, st>>>(wr, a);
+      c.launches += 2;
+      std::swap(LA, LB);
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    DevBuf gb;
+    GJ_TRY(gb.alloc(err, 2 * mn * sizeof(double)));
+    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * mn, 1, 0, 0, g.dt, g.eps0, eps_m, sig_m,
+                                     gb.as<double>(), gb.as<double>() + mn);
+    GJ_CUDA(err, cudaGetLastError());
+    GJ_CUDA(err, cudaDeviceSynchronize());
+    std::vector<double> tmp(2 * mn);
+    GJ_CUDA(err, cudaMemcpy(tmp.data(), gb.p, 2 * mn * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t p = 0; p < mn; ++p) gout[p] = tmp[mn + p];  // the u-correlation (sigma form)
+    if (amax) {
+      std::vector<T> hl(sstride);
+      GJ_CUDA(err, cudaMemcpy(hl.data(), LA - ld, sstride * sizeof(T), cudaMemcpyDeviceToHost));
+      for (int b = 0; b < g.n; ++b)
+        for (int a_ = 0; a_ < g.m; ++a_)
+          amax[size_t(a_) + size_t(b) * g.m] =
+              std::fabs(double(hl[size_t(ld) + size_t(w.di0 + a_) + size_t(w.dj0 + b) * ld]));
+    }
+    return GJ_OK;
+  }
+};
+
+template <class T>
+static gj_status get_solver(Ctx& c, const gj_w_grid& g, const gj_w_shot* shots, int ns, WSolver<T>*& out) {
+  std::string k = std::string(sizeof(T) == 8 ? "d" : "f") + WSolver<T>::key(g, shots, ns);
+  if (c.wsolver && c.wkey == k) {
+    out = static_cast<WSolver<T>*>(c.wsolver.get());
+    return GJ_OK;
+  }
+  c.wsolver.reset();
+  auto s = std::make_unique<WSolver<T>>();
+  GJ_TRY(s->setup(c.err, g, shots, ns));
+  out = s.get();
+  c.wsolver = std::move(s);
+  c.wkey = k;
+  return GJ_OK;
+}
+
+gj_status w_forward(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
+                    const gj_w_shot* shots, int nshots, double* d_out, double* jz_out, double* u_out) {
+  if (!eps || !sig || !d_out) return c.err.set(GJ_EINVAL, "null model or output pointer");
+  if (prec == GJ_F64) {
+    WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+    return s->forward(c.err, c, eps, sig, d_out, jz_out, u_out);
+  }
+  WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+  return s->forward(c.err, c, eps, sig, d_out, jz_out, u_out);
+}
+
+gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* eps, const void* sig,
+                     bool dev_in, const gj_w_shot* shots, int nshots, const void* dobs, bool dev_dobs,
+                     gj_adj_mode mode, gj_misfit_kind mk, const gj_w_opts& o, void* geps, void* gsig,
+                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+  if (!eps || !sig || !dobs || !geps || !gsig) return c.err.set(GJ_EINVAL, "null input or output pointer");
+  if (mode != GJ_ADJ_REFERENCE && mode != GJ_ADJ_EXACT) return c.err.set(GJ_EINVAL, "unknown adjoint mode");
+  if (mk != GJ_MISFIT_L2) return c.err.set(GJ_EUNSUPPORTED, "only the L2 misfit is built into this entry point");
+  if (prec == GJ_F64) {
+    WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+    return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, o, geps, gsig, dev_out, misfit_out, d_out,
+                       e_out, st);
+  }
+  WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+  return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, o, geps, gsig, dev_out, misfit_out, d_out,
+                     e_out, st);
+}
+
+gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
+                      const gj_w_shot& shot, const double* e, const double* u, double* gout, double* amax) {
+  if (!eps || !sig || !e || !u || !gout) return c.err.set(GJ_EINVAL, "null input or output pointer");
+  if (prec == GJ_F64) {
+    WSolver<double>* s; GJ_TRY(get_solver(c, g, &shot, 1, s));
+    return s->grad_only(c.err, c, eps, sig, e, u, gout, amax);
+  }
+  WSolver<float>* s; GJ_TRY(get_solver(c, g, &shot, 1, s));
+  return s->grad_only(c.err, c, eps, sig, e, u, gout, amax);
+}
+
+}  // namespace gj

@@ -1,0 +1,149 @@
+/*
+ * gerjoii_gpu.h — C ABI of the B200 (sm_100a) radar full-waveform gradient path
+ * and the 2.5D DC-resistivity solves.
+ *
+ * Every entry point replaces one MATLAB function of the reference
+ * (diegozain/gerjoii); the function it replaces is cited beside it as
+ * path:line inside that project.  A MEX gateway (mex/*.c) unpacks the
+ * reference's structs and calls these functions, so the reference's L2 layer
+ * (w_update_e.m, w_update_s.m, dc_update2_5d.m, ...) keeps its call sites.
+ *
+ * Conventions
+ *  - Arrays are column-major (MATLAB order); the fastest index is depth (i).
+ *  - The padded Yee grid has NX = pml_top + air + m + pml rows and
+ *    NY = n + 2*pml columns (wdc_geom.m:69-70); Ez nodes are (NX+1) x (NY+1).
+ *  - All node indices are 0-based (MATLAB index - 1).  A receiver is a linear
+ *    Ez node index i + j*(NX+1), i.e. gerjoii_.w.M - 1 (w_M.m:20).
+ *  - Host pointers are double precision; `precision` selects the arithmetic
+ *    (GJ_F32 fields and stencils, or GJ_F64).
+ *  - Every function returns a gj_status; gj_last_error(ctx) gives the text.
+ *  - A context is used by one host thread at a time; several contexts may
+ *    share a device.  There is no global mutable state.
+ */
+#ifndef GERJOII_GPU_H
+#define GERJOII_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gj_status {
+  GJ_OK = 0,
+  GJ_EINVAL = 1,      /* invalid argument (sizes, indices, null pointers) */
+  GJ_ENOMEM = 2,      /* device memory could not be allocated */
+  GJ_ENUMERIC = 3,    /* NaN or Inf detected in a result */
+  GJ_ETIMEOUT = 4,    /* a bounded device wait expired */
+  GJ_ECUDA = 5,       /* CUDA runtime error */
+  GJ_EUNSUPPORTED = 6 /* option not supported by this build */
+} gj_status;
+
+typedef enum gj_precision { GJ_F32 = 0, GJ_F64 = 1 } gj_precision;
+
+/* REFERENCE: w_grad.m semantics (sigma-flipped forward-type propagation of the
+ * time-reversed residual hard-set at the receivers; g_eps from d/dt u, g_sig
+ * from u).  EXACT: transpose of the discrete Yee/PML update, i.e. the true
+ * gradient of 0.5*sum (d - d_obs)^2 with respect to eps_r and sigma. */
+typedef enum gj_adj_mode { GJ_ADJ_REFERENCE = 0, GJ_ADJ_EXACT = 1 } gj_adj_mode;
+
+/* Objective / adjoint source (w_bozdag.m:48-60). */
+typedef enum gj_misfit_kind { GJ_MISFIT_L2 = 0, GJ_MISFIT_ENV_L2 = 1 } gj_misfit_kind;
+
+typedef struct gj_ctx gj_ctx;
+
+/* Padded Yee grid (wdc_geom.m:35-125, generalised with pml_top). */
+typedef struct gj_w_grid {
+  int m, n;      /* model rows (depth) and columns (lateral) */
+  int pml;       /* PML cells bottom/left/right (pml_w == pml_d) */
+  int pml_top;   /* PML rows on top: == pml (reference layout) or 0 (free top) */
+  int air;       /* air rows (eps_r = 1, sigma = 0) above the model; >= 1 for a free top */
+  int nt;        /* time steps */
+  double dx, dy, dt;
+  double eps0, mu0; /* parame_.w.eps_0, parame_.w.mu_0 (param_wdc.m:28-29) */
+  int order;        /* PML grading order, 2 in wdc_geom.m:98 */
+  double R0;        /* PML reflection, 1e-8 in wdc_geom.m:99 */
+} gj_w_grid;
+
+/* One shot (gerjoii_.w.s, gerjoii_.w.wvlet_, gerjoii_.w.M). */
+typedef struct gj_w_shot {
+  int src_i, src_j;       /* source Ez node, 0-based (gerjoii_.w.s - 1) */
+  const double* wavelet;  /* nt samples (w_wavelet.m) */
+  int nr;                 /* receivers */
+  const long* rec;        /* nr linear Ez node indices, 0-based (gerjoii_.w.M - 1) */
+} gj_w_shot;
+
+/* Options for the gradient; zero-initialise for the defaults. */
+typedef struct gj_w_opts {
+  int ckpt_every;        /* checkpoint interval K in steps; 0 = automatic: keep the whole
+                            u history when it fits mem_budget_bytes, else checkpoint */
+  size_t mem_budget_bytes; /* 0 = 80% of free device memory */
+  int shots_per_launch;  /* shots advanced together per kernel launch; 0 = automatic */
+  int no_kahan;          /* 1 = plain FP32 sums for the imaging condition */
+  int no_graph;          /* 1 = launch the time loop without CUDA graphs */
+  int per_shot;          /* 1 = g_eps/g_sig hold nshots gradients (m*n each), else their sum */
+  int plain;             /* 1 = the plain form: one half-step per launch, one shot at a time */
+} gj_w_opts;
+
+/* ---------------------------------------------------------------- context */
+gj_status gj_context_create(gj_ctx** ctx, int device);
+gj_status gj_context_destroy(gj_ctx* ctx);
+const char* gj_last_error(const gj_ctx* ctx);
+const char* gj_version(void);
+
+/* ------------------------------------------------------------ radar (GPR) */
+
+/* Forward model for nshots shots: replaces w_fwd.m:18-24 / w_solve.m:80-124
+ * (and w_solve_.m with is == 0 when u_out is NULL).
+ *   eps_r, sigma : m x n model (parame_.w.epsilon, parame_.w.sigma)
+ *   d_out        : per shot nt x nr traces, shots concatenated (gerjoii_.w.d_2d)
+ *   jz_out       : per shot nt samples of Ez at the source (gerjoii_.w.Jy), may be NULL
+ *   u_out        : per shot m x n x nt history (gerjoii_.w.u_2d), may be NULL */
+gj_status gj_w_forward(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision,
+                       const double* eps_r, const double* sigma, const gj_w_shot* shots,
+                       int nshots, double* d_out, double* jz_out, double* u_out);
+
+/* Whole gradient for nshots shots in one call: forward with checkpoints, the
+ * residual and misfit (w_fwd.m:34-35 via w_bozdag.m, w_E.m, w_update_e.m:74-76),
+ * then the adjoint and imaging condition.  In GJ_ADJ_REFERENCE mode this is
+ * w_update_es.m's pair of calls: g_eps = w_grad(d/dt u) (w_update_e.m:83-98)
+ * and g_sig = w_grad(u) (w_update_s.m:77).  In GJ_ADJ_EXACT mode g_eps and
+ * g_sig are dJ/d(eps_r) and dJ/d(sigma) of J = 0.5*sum (d - d_obs)^2 (or of the
+ * envelope misfit).
+ *   d_obs   : per shot nt x nr observed traces (parame_.natu.w.d_2d)
+ *   g_eps, g_sig : m x n (or nshots x m x n with opts->per_shot)
+ *   misfit  : nshots normalised misfits, may be NULL
+ *   d_out, e_out : per shot nt x nr modelled traces and adjoint sources, may be NULL */
+gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision,
+                        const double* eps_r, const double* sigma, const gj_w_shot* shots,
+                        int nshots, const double* d_obs, gj_adj_mode mode,
+                        gj_misfit_kind misfit, const gj_w_opts* opts, double* g_eps,
+                        double* g_sig, double* misfit_out, double* d_out, double* e_out);
+
+/* The adjoint half on its own: replaces [g, a_max] = w_grad(u, ...) (w_grad.m:1-115)
+ * for one shot.  u is the m x n x nt history (or its time derivative), e the
+ * nt x nr residual.  a_max may be NULL.  Reference semantics only. */
+gj_status gj_w_grad(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision,
+                    const double* eps_r, const double* sigma, const gj_w_shot* shot,
+                    const double* e, const double* u, double* g, double* a_max);
+
+/* Device-pointer gradient for callers that keep everything in HBM (the torch
+ * test harness and the benchmark).  Pointers are device memory of the chosen
+ * precision (float or double); d_obs is nshots x nr x nt... laid out per shot
+ * as nt x nr.  misfit_out is a host array of nshots doubles, may be NULL.
+ * stream is a cudaStream_t (NULL = legacy default stream). */
+gj_status gj_w_gradient_dev(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision,
+                            const void* eps_r_dev, const void* sigma_dev,
+                            const gj_w_shot* shots, int nshots, const void* d_obs_dev,
+                            gj_adj_mode mode, gj_misfit_kind misfit, const gj_w_opts* opts,
+                            void* g_eps_dev, void* g_sig_dev, double* misfit_out,
+                            void* stream);
+
+/* Number of kernel launches issued by the last call on this context (for the
+ * benchmark's launch count).  Graph launches count the kernels they contain. */
+long gj_last_launch_count(const gj_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GERJOII_GPU_H */

@@ -1,0 +1,109 @@
+"""Oracle self-consistency (CPU): the C++ restatement against the numpy twin
+that follows the MATLAB slicing, known-answer checks, and the exact adjoint
+against central finite differences."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gerjoii_b200 import synth
+from gerjoii_b200.geometry import Shot
+
+
+def _np_run(npo, p, shot):
+    g = p.grid
+    f = npo.w_layout(g.m, g.n, g.pml, g.air, g.pml_top)
+    er, sz = npo.w_exp2pml(p.eps0, p.sig0, g.pml, g.air, g.pml_top)
+    d, u, jz = npo.w_solve(er, sz, f, (shot.src_i + 1, shot.src_j + 1), shot.rec + 1, shot.wavelet, g.nt,
+                           g.dx, g.dy, g.dt, g.eps0, g.mu0)
+    return f, er, sz, d, u, jz
+
+
+@pytest.mark.parametrize("free_top", [True, False])
+def test_forward_and_reference_adjoint_match_numpy_twin(oracle, free_top):
+    import np_oracle as npo
+    p = synth.small(m=14, n=20, pml=6, nt=160, free_top=free_top, seed=3)
+    g, shot = p.grid, p.shots[1]
+    d, jz, u = oracle.forward(g, p.eps0, p.sig0, shot, store_u=True)
+    f, er, sz, d2, u2, jz2 = _np_run(npo, p, shot)
+    assert rel_l2(d, d2) < 1e-13 and rel_l2(u, u2) < 1e-13 and rel_l2(jz, jz2) < 1e-13
+    e = d - 0.5 * np.roll(d, 7, axis=0)
+    gr, am = oracle.grad_reference(g, p.eps0, p.sig0, shot, e, u)
+    gr2, am2 = npo.w_grad(u2, e, er, sz, f, (shot.src_i + 1, shot.src_j + 1), shot.rec + 1, g.nt, g.dx, g.dy,
+                          g.dt, g.eps0, g.mu0)
+    assert rel_l2(gr, gr2) < 1e-12 and rel_l2(am, am2) < 1e-12
+
+
+def test_differentiate_cube_known_answer(oracle):
+    # differentiate_line.m:52-56: derivative of sin is cos to second order.
+    import np_oracle as npo
+    nt, dt = 400, 1e-3
+    t = np.arange(nt) * dt
+    v = np.sin(2 * np.pi * 5 * t)[None, None, :] * np.ones((3, 2, 1))
+    dv = oracle.differentiate_cube(v, dt)
+    ref = 2 * np.pi * 5 * np.cos(2 * np.pi * 5 * t)
+    assert np.max(np.abs(dv[1, 1, 1:-1] - ref[1:-1])) < 2e-2 * np.max(np.abs(ref))
+    assert rel_l2(dv, npo.differentiate_cube(v, dt)) < 1e-14
+    # exact on quadratics in the interior and at both one-sided ends
+    q = (3 * t ** 2 - t)[None, None, :]
+    assert np.allclose(oracle.differentiate_cube(q, dt)[0, 0], 6 * t - 1, rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("free_top", [True, False])
+def test_exact_adjoint_matches_finite_differences(oracle, free_top):
+    p = synth.small(m=10, n=14, pml=5, nt=140, free_top=free_top, seed=11)
+    g = p.grid
+    sh = p.shots[1]
+    rec = np.concatenate([sh.rec, [g.node(*g.model_node(9, 0)), g.node(g.NX - 2, 3)]])
+    sh = Shot(sh.src_i, sh.src_j, sh.wavelet, rec)
+    dobs, _, _ = oracle.forward(g, p.eps_true, p.sig_true, sh)
+
+    def J(e_, s_):
+        d, _, _ = oracle.forward(g, e_, s_, sh)
+        return 0.5 * np.sum((d - dobs) ** 2)
+
+    d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+    ge, gs = oracle.grad_exact(g, p.eps0, p.sig0, sh, d - dobs)
+    # interior cell, model corners and edges (PML-replicated), first column (PML band)
+    for (a, b) in [(4, 6), (0, 0), (9, 13), (9, 0), (5, 0), (5, 13), (9, 7), (0, 8)]:
+        h = 1e-4 * p.eps0[a, b]
+        ep, em = p.eps0.copy(), p.eps0.copy()
+        ep[a, b] += h
+        em[a, b] -= h
+        fd = (J(ep, p.sig0) - J(em, p.sig0)) / (2 * h)
+        assert abs(ge[a, b] - fd) <= 1e-5 * abs(fd) + 1e-12 * np.abs(ge).max(), (a, b, ge[a, b], fd)
+        hs = 1e-3 * p.sig0[a, b]
+        sp, sm = p.sig0.copy(), p.sig0.copy()
+        sp[a, b] += hs
+        sm[a, b] -= hs
+        fds = (J(p.eps0, sp) - J(p.eps0, sm)) / (2 * hs)
+        assert abs(gs[a, b] - fds) <= 1e-5 * abs(fds) + 1e-9 * np.abs(gs).max(), (a, b, gs[a, b], fds)
+
+
+def test_exact_adjoint_dot_product(oracle):
+    """<J'(m) dm> from the adjoint equals the directional derivative."""
+    p = synth.small(m=10, n=14, pml=5, nt=120, seed=5)
+    g, sh = p.grid, p.shots[0]
+    rng = np.random.default_rng(0)
+    dm = rng.standard_normal(p.eps0.shape)
+    dobs, _, _ = oracle.forward(g, p.eps_true, p.sig_true, sh)
+    d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+    ge, _ = oracle.grad_exact(g, p.eps0, p.sig0, sh, d - dobs)
+    h = 1e-5
+    dp, _, _ = oracle.forward(g, p.eps0 + h * dm, p.sig0, sh)
+    dmn, _, _ = oracle.forward(g, p.eps0 - h * dm, p.sig0, sh)
+    fd = (0.5 * np.sum((dp - dobs) ** 2) - 0.5 * np.sum((dmn - dobs) ** 2)) / (2 * h)
+    assert abs(np.sum(ge * dm) - fd) < 1e-6 * abs(fd)
+
+
+def test_reference_adjoint_differs_from_exact_in_lossy_media(oracle):
+    """The reference adjoint (sigma flipped, hard-set residual) is not the
+    exact transpose; record the cosine between the two sigma gradients."""
+    p = synth.small(m=12, n=18, pml=6, nt=200, seed=9)
+    g, sh = p.grid, p.shots[1]
+    dobs, _, _ = oracle.forward(g, p.eps_true, p.sig_true, sh)
+    d, _, u = oracle.forward(g, p.eps0, p.sig0, sh, store_u=True)
+    e = d - dobs
+    ge, gs = oracle.grad_exact(g, p.eps0, p.sig0, sh, e)
+    gr, _ = oracle.grad_reference(g, p.eps0, p.sig0, sh, e, u)
+    c = float(np.sum(gr * gs) / (np.linalg.norm(gr) * np.linalg.norm(gs)))
+    assert np.isfinite(c)

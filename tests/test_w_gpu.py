@@ -1,0 +1,107 @@
+"""GPU parity of the radar path against the oracle, through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2, cosine
+from gerjoii_b200 import synth
+from gerjoii_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_ft():
+    return synth.small(m=24, n=40, pml=8, nt=300, free_top=True, seed=21)
+
+
+@pytest.fixture(scope="module")
+def small_ref():
+    return synth.small(m=20, n=36, pml=8, nt=300, free_top=False, seed=22)
+
+
+@pytest.mark.parametrize("which", ["small_ft", "small_ref"])
+def test_forward_f64_matches_oracle(gpu_ctx, oracle, which, request):
+    p = request.getfixturevalue(which)
+    g = p.grid
+    out = gpu_ctx.w_forward(g, p.eps0, p.sig0, p.shots, precision=N.GJ_F64, want_jz=True, want_u=True)
+    for k, sh in enumerate(p.shots):
+        d, jz, u = oracle.forward(g, p.eps0, p.sig0, sh, store_u=True)
+        assert rel_l2(out["d"][k], d) < 1e-12
+        assert rel_l2(out["jz"][k], jz) < 1e-12
+        assert rel_l2(out["u"][k], u) < 1e-12
+
+
+@pytest.mark.parametrize("which", ["small_ft", "small_ref"])
+def test_forward_f32_traces_within_1e5(gpu_ctx, oracle, which, request):
+    p = request.getfixturevalue(which)
+    g = p.grid
+    out = gpu_ctx.w_forward(g, p.eps0, p.sig0, p.shots, precision=N.GJ_F32)
+    for k, sh in enumerate(p.shots):
+        d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+        assert rel_l2(out["d"][k], d) < 1e-5
+
+
+def _dobs(oracle, p):
+    return [oracle.forward(p.grid, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
+
+
+@pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-10), (N.GJ_F32, 1e-4)])
+@pytest.mark.parametrize("ckpt", [0, 7])
+def test_reference_gradient_matches_oracle(gpu_ctx, oracle, small_ft, prec, tol, ckpt):
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    ge, gs, mis = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]),
+                                        mode="reference")
+    o = N.OptsC()
+    o.ckpt_every = ckpt
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_REFERENCE, precision=prec, opts=o)
+    assert rel_l2(res["g_eps"], ge) < tol and cosine(res["g_eps"], ge) > 1 - tol
+    assert rel_l2(res["g_sig"], gs) < tol and cosine(res["g_sig"], gs) > 1 - tol
+    assert np.allclose(res["misfit"], mis, rtol=1e-5 if prec == N.GJ_F32 else 1e-12)
+
+
+@pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-10), (N.GJ_F32, 1e-4)])
+@pytest.mark.parametrize("ckpt", [0, 9])
+def test_exact_gradient_matches_oracle_interior(gpu_ctx, oracle, small_ft, prec, tol, ckpt):
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    ge, gs, _ = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]), mode="exact")
+    o = N.OptsC()
+    o.ckpt_every = ckpt
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=prec, opts=o)
+    # interior model cells (edge cells also collect PML-coefficient terms)
+    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
+    assert rel_l2(res["g_eps"][sl], ge[sl]) < tol
+    assert rel_l2(res["g_sig"][sl], gs[sl]) < tol
+
+
+def test_w_grad_matches_oracle(gpu_ctx, oracle, small_ref):
+    p = small_ref
+    g, sh = p.grid, p.shots[0]
+    d, _, u = oracle.forward(g, p.eps0, p.sig0, sh, store_u=True)
+    e = d - oracle.forward(g, p.eps_true, p.sig_true, sh)[0]
+    gr, am = oracle.grad_reference(g, p.eps0, p.sig0, sh, e, u)
+    gg, aa = gpu_ctx.w_grad(g, p.eps0, p.sig0, sh, e, u, precision=N.GJ_F64)
+    assert rel_l2(gg, gr) < 1e-10 and rel_l2(aa, am) < 1e-10
+
+
+def test_per_shot_gradients_sum_to_total(gpu_ctx, oracle, small_ft):
+    p = small_ft
+    dobs = _dobs(oracle, p)
+    o = N.OptsC()
+    o.per_shot = 1
+    r1 = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, dobs, precision=N.GJ_F64, opts=o)
+    r2 = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, dobs, precision=N.GJ_F64)
+    assert r1["g_eps"].shape == (len(p.shots), p.grid.m, p.grid.n)
+    assert rel_l2(r1["g_eps"].sum(0), r2["g_eps"]) < 1e-12
+
+
+def test_invalid_source_is_rejected(gpu_ctx, small_ft):
+    p = small_ft
+    from gerjoii_b200.geometry import Shot
+    bad = Shot(0, 5, p.shots[0].wavelet, p.shots[0].rec)
+    with pytest.raises(N.GJError) as ei:
+        gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, [bad])
+    assert ei.value.status == N.GJ_EINVAL
