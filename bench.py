@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark: FWI shot-gradients/s on one B200 (FP32 + checkpointing + batched shots).
+
+Workload (one "step" = one whole FWI gradient over all shots): the 1000 x 400
+radar model at dx = 0.02 m with 30 PML cells and a free top (padded 431 x 1060
+Yee grid), 6000 time steps, 250 MHz Ricker source, 30 surface sources and 200
+receivers, five-layer + blob permittivity, layered conductivity; seeded
+synthetic data (no field data).  Each step runs, for all 30 shots at once, the
+forward solve with checkpoints every K steps, the residual and misfit, the
+segment-by-segment recompute and the exact adjoint with the imaging condition
+(Kahan-compensated FP32 sums), and returns the epsilon and sigma gradients.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs the same workload on its own GPU (weak
+scaling) and the gradients are summed with one NCCL all-reduce per step.
+The reference arm (--impl reference) times the CPU restatement of the
+reference (oracle/) on the host cores; rank 0 alone runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FWI shot-gradients/s & Gcell-upd/s, 1 B200: FP32+ckpt+batch vs plain FP64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gerjoii", choices=["gerjoii", "reference"])
+    ap.add_argument("--nt", type=int, default=6000)
+    ap.add_argument("--nshots", type=int, default=30)
+    ap.add_argument("--mode", default="exact", choices=["exact", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip the e2e, plain-FP64 and CPU legs")
+    return ap.parse_args()
+
+
+def workload(args):
+    from gerjoii_b200 import synth
+    p = synth.cfg2(nshots=args.nshots, nt=args.nt)
+    g = p.grid
+    cfg = {"workload": f"radar FWI gradient, {g.n}x{g.m} model (padded {g.NX}x{g.NY} Yee grid), "
+                       f"{args.nshots} shots x {len(p.shots[0].rec)} receivers, {g.nt} steps, FP32, "
+                       f"{args.mode} adjoint, checkpointed",
+           "grid": [g.NX, g.NY], "model": [g.m, g.n], "nt": g.nt, "shots": args.nshots,
+           "receivers": len(p.shots[0].rec), "adjoint": args.mode,
+           "l2": "working set (fields, checkpoints, history ring) larger than the 126 MB L2; no flush needed"}
+    return p, cfg
+
+
+def synth_dobs(p):
+    """Observed traces: the true model's forward response, from the library itself."""
+    from gerjoii_b200 import _native as N
+    ctx = N.Context(0)
+    out = ctx.w_forward(p.grid, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F32)
+    ctx.close()
+    return out["d"]
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def traffic_per_unit(kernel):
+    """dram bytes per (shot x cell) for `kernel` from the committed ncu summary, or None."""
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
+        e = t[kernel]
+        return e["dram_bytes_per_launch"] / e["units_per_launch"]
+    except Exception:
+        return None
+
+
+def _cpu_worker(job):
+    """One shot of the oracle in a worker process (the reference's parfor worker)."""
+    import copy
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from gerjoii_b200 import synth
+    from gerjoii_b200.geometry import Shot
+    nshots, nt_full, nt_sample, k, mode = job
+    p = synth.cfg2(nshots=nshots, nt=nt_full)
+    g = copy.copy(p.grid)
+    g.nt = nt_sample
+    s = p.shots[k % len(p.shots)]
+    shot = Shot(s.src_i, s.src_j, s.wavelet[:nt_sample], s.rec)
+    dobs = np.random.default_rng(k).standard_normal((1, shot.nr, nt_sample)) * 1e-3
+    t0 = time.perf_counter()
+    pyoracle.gradient_batch(g, p.eps0, p.sig0, [shot], dobs, mode=mode, precision="f32", threads=1)
+    return time.perf_counter() - t0
+
+
+class CpuPool:
+    """Spawned worker processes running the oracle, one shot each per round (the
+    reference's parfor pool).  Freed memory stays in each worker's heap, so
+    rounds after the first do not pay first-touch page faults again."""
+
+    def __init__(self, threads):
+        import multiprocessing as mp
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        pyoracle.build()
+        os.environ.setdefault("MALLOC_MMAP_MAX_", "0")
+        os.environ.setdefault("MALLOC_TRIM_THRESHOLD_", str(1 << 40))
+        self.threads = threads
+        self.pool = mp.get_context("spawn").Pool(threads)
+
+    def sample(self, p, mode, nt_sample):
+        """`threads` shots at nt_sample steps; returns (seconds, shot-gradients/s
+        scaled to the full nt)."""
+        jobs = [(len(p.shots), p.grid.nt, nt_sample, k, mode) for k in range(self.threads)]
+        t0 = time.perf_counter()
+        self.pool.map(_cpu_worker, jobs, chunksize=1)
+        dt = time.perf_counter() - t0
+        return dt, self.threads / dt * (nt_sample / p.grid.nt)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    p, cfg = workload(args)
+    threads = min(os.cpu_count() or 1, 32)
+    nt_sample = max(50, min(args.nt, 150))
+    vals = []
+    pool = CpuPool(threads)
+    for k in range(max(args.warmup, 1) + args.steps):
+        dt, v = pool.sample(p, args.mode, nt_sample)
+        if k >= max(args.warmup, 1):
+            vals.append((dt, v))
+    pool.close()
+    v = statistics.median([x[1] for x in vals])
+    ms = statistics.median([x[0] for x in vals]) * 1e3
+    sample = (f"{threads} shots x {nt_sample} of {args.nt} steps per step on {threads} threads "
+              f"(C++ oracle, FP32, {args.mode} adjoint); value scaled to the full step count")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "shot-gradients/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered model)", "config": cfg,
+            "cpu_baseline": {"value": v, "unit": "shot-gradients/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "shot-gradients/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from gerjoii_b200 import _native as N
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    p, cfg = workload(args)
+    g = p.grid
+    cfg["parallelism"] = f"shots replicated per GPU x{world} (weak), gradient all-reduce" if world > 1 else "1 GPU"
+    mode = N.GJ_ADJ_EXACT if args.mode == "exact" else N.GJ_ADJ_REFERENCE
+    dobs = synth_dobs(p)
+    nr = len(p.shots[0].rec)
+    dobs_t = torch.tensor(np.stack([d.T for d in dobs]), dtype=torch.float32, device=dev).contiguous()
+    eps_t = torch.tensor(np.asfortranarray(p.eps0).ravel(order="F"), dtype=torch.float32, device=dev)
+    sig_t = torch.tensor(np.asfortranarray(p.sig0).ravel(order="F"), dtype=torch.float32, device=dev)
+    ge_t = torch.zeros(g.m * g.n, dtype=torch.float32, device=dev)
+    gs_t = torch.zeros_like(ge_t)
+    ctx = N.Context(local)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.w_gradient_dev(g, eps_t, sig_t, p.shots, dobs_t, ge_t, gs_t, mode=mode, stream=stream.cuda_stream)
+        if world > 1:
+            dist.all_reduce(ge_t)
+            dist.all_reduce(gs_t)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    ctx.set_kernel_timing(True)
+    launches = 0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        launches += ctx.last_launch_count
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step")}
+    ctx.set_kernel_timing(False)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    shots_total = args.nshots * world * args.steps
+    value = shots_total / (ms / 1e3)
+    cells = g.NX * g.NY
+    # cell-updates per gradient: forward + recompute + adjoint
+    fwd_launches = ktimes["fwd_step"][1] / max(args.steps, 1)
+    adj_launches = (ktimes["adj_step"][1] + ktimes["ref_step"][1]) / max(args.steps, 1)
+    upd_per_step = (fwd_launches + adj_launches) * cells * args.nshots * world
+    gcell = upd_per_step * args.steps / (ms / 1e3) / 1e9
+
+    # roofline for the dominant kernel
+    pk, pk_src = peaks()
+    dom = max(ktimes, key=lambda k: ktimes[k][0])
+    tot_ms, nl = ktimes[dom]
+    mn = g.m * g.n
+    if dom == "fwd_step":
+        per_cell = 32.0
+        hist_launches = max(nl / args.steps - g.nt, 0)
+        bytes_total = nl * args.nshots * cells * per_cell + hist_launches * args.steps * args.nshots * mn * 4.0
+        unit_desc = "32 B per shot-cell (read Ez,Hx,Hy,Ceze,Cezhy; write Ez,Hx,Hy) + 4 B per history write"
+    elif dom == "adj_step":
+        bytes_total = nl * args.nshots * (cells * 32.0 + mn * 40.0)
+        unit_desc = "32 B per shot-cell stencil + 40 B per model cell (2 history reads, 4 Kahan accumulators r/w)"
+    else:
+        bytes_total = nl * args.nshots * (cells * 32.0 + mn * 44.0)
+        unit_desc = "32 B per shot-cell stencil + 44 B per model cell (3 history reads, 4 accumulators r/w)"
+    avg_s = tot_ms / 1e3 / max(nl, 1)
+    achieved = bytes_total / max(nl, 1) / avg_s / 1e9
+    kname = {"fwd_step": "k_step<float,0>", "adj_step": "k_adj_step<float>", "ref_step": "k_step<float,1>"}[dom]
+    tpu = traffic_per_unit(kname)
+    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
+            "traffic": (tpu * args.nshots * cells if tpu is not None else None),
+            "algorithmic_bytes_per_launch": bytes_total / max(nl, 1), "launches": nl,
+            "avg_launch_us": avg_s * 1e6, "units": unit_desc,
+            "kernel_share_of_step": tot_ms / ms}
+    line = {"metric": METRIC, "value": value, "unit": "shot-gradients/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded layered model, observed traces modelled on the device)",
+            "config": cfg, "gcell_updates_per_s": gcell, "gpu_launches": launches,
+            "clocks": clk, "roofline": roof,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()}}
+
+    if rank == 0 and not args.no_extras:
+        # e2e: the public C ABI with host (pinned) buffers, copies inside the timed region
+        import ctypes as C
+        eps_h = torch.empty(mn, dtype=torch.float64, pin_memory=True).numpy()
+        sig_h = torch.empty(mn, dtype=torch.float64, pin_memory=True).numpy()
+        eps_h[:] = np.asfortranarray(p.eps0).ravel(order="F")
+        sig_h[:] = np.asfortranarray(p.sig0).ravel(order="F")
+        dob_h = torch.empty(args.nshots * nr * g.nt, dtype=torch.float64, pin_memory=True).numpy()
+        dob_h[:] = np.concatenate([np.asfortranarray(d).ravel(order="F") for d in dobs])
+        ge_h = torch.empty(mn, dtype=torch.float64, pin_memory=True).numpy()
+        gs_h = torch.empty(mn, dtype=torch.float64, pin_memory=True).numpy()
+        mis_h = np.zeros(args.nshots)
+        sp = N._ShotPack(p.shots, g.nt)
+        gc = N.grid_c(g)
+        o = N.OptsC()
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+
+        def e2e_step():
+            st = ctx.lib.gj_w_gradient(ctx.h, C.byref(gc), N.GJ_F32, dp(eps_h), dp(sig_h), sp.arr, sp.n,
+                                       dp(dob_h), mode, N.GJ_MISFIT_L2, C.byref(o), dp(ge_h), dp(gs_h),
+                                       dp(mis_h), None, None)
+            if st != 0:
+                raise RuntimeError(ctx.lib.gj_last_error(ctx.h).decode())
+
+        e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        t_e2e = (time.perf_counter() - t0) / args.steps
+        line["e2e"] = {"value": args.nshots / t_e2e, "unit": "shot-gradients/s",
+                       "h2d_bytes_per_step": int(eps_h.nbytes + sig_h.nbytes + dob_h.nbytes),
+                       "d2h_bytes_per_step": int(ge_h.nbytes + gs_h.nbytes + mis_h.nbytes),
+                       "ms_per_step": t_e2e * 1e3,
+                       "path": "gj_w_gradient (C ABI, host float64 buffers in pinned memory)"}
+        # plain per-shot FP64 GPU form on 2 shots, same grid and step count
+        o_pl = N.OptsC()
+        o_pl.plain = 1
+        sub = p.shots[:2]
+        r_plain = ctx.w_gradient(g, p.eps0, p.sig0, sub, dobs[:2], mode=mode, precision=N.GJ_F64, opts=o_pl)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r_plain = ctx.w_gradient(g, p.eps0, p.sig0, sub, dobs[:2], mode=mode, precision=N.GJ_F64, opts=o_pl)
+        torch.cuda.synchronize()
+        t_pl = time.perf_counter() - t0
+        r32 = ctx.w_gradient(g, p.eps0, p.sig0, sub, dobs[:2], mode=mode, precision=N.GJ_F32)
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        line["plain_fp64"] = {"value": len(sub) / t_pl, "unit": "shot-gradients/s",
+                              "sample": f"{len(sub)} shots, full {g.nt} steps, one half-step per launch, FP64",
+                              "speedup_fp32_batched_over_plain_fp64": value / world / (len(sub) / t_pl),
+                              "g_eps_rel_l2_fp32_vs_fp64": rel(r32["g_eps"], r_plain["g_eps"]),
+                              "g_sig_rel_l2_fp32_vs_fp64": rel(r32["g_sig"], r_plain["g_sig"])}
+        # CPU baseline (oracle) on the host cores, bounded sample
+        threads = min(os.cpu_count() or 1, 32)
+        nt_s = max(50, min(args.nt, 150))
+        pool = CpuPool(threads)
+        pool.sample(p, args.mode, nt_s)  # first round: worker start-up and first-touch memory
+        dt_cpu, v_cpu = pool.sample(p, args.mode, nt_s)
+        pool.close()
+        line["cpu_baseline"] = {"value": v_cpu, "unit": "shot-gradients/s", "cores": threads, "kind": "port",
+                                "sample": f"{threads} shots x {nt_s} of {g.nt} steps ({dt_cpu:.1f} s, C++ oracle "
+                                          f"FP32 {args.mode} adjoint), scaled to the full step count"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -52,6 +52,8 @@ SIGNATURES = {
     "gj_context_destroy": (_I, [_VP]),
     "gj_last_error": (C.c_char_p, [_VP]),
     "gj_last_launch_count": (_L, [_VP]),
+    "gj_set_kernel_timing": (_I, [_VP, _I]),
+    "gj_kernel_time": (_I, [_VP, _I, _DP, C.POINTER(C.c_long)]),
     "gj_w_forward": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _DP, _DP]),
     "gj_w_gradient": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _I,
                            C.POINTER(OptsC), _DP, _DP, _DP, _DP, _DP]),
@@ -149,6 +151,18 @@ class Context:
     @property
     def last_launch_count(self) -> int:
         return int(self.lib.gj_last_launch_count(self.h))
+
+    KERNEL_KINDS = {"fwd_step": 0, "ref_step": 1, "adj_step": 2, "io": 3, "plain": 4, "dc": 5}
+
+    def set_kernel_timing(self, on: bool):
+        self._check(self.lib.gj_set_kernel_timing(self.h, int(bool(on))))
+
+    def kernel_time(self, kind: str):
+        """(milliseconds, launches) accumulated for a kernel kind while timing is on."""
+        ms = C.c_double(0)
+        n = C.c_long(0)
+        self._check(self.lib.gj_kernel_time(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(n)))
+        return ms.value, n.value
 
     # ------------------------------------------------------------------ radar
     def w_forward(self, g, eps, sig, shots, precision=GJ_F32, want_jz=False, want_u=False):

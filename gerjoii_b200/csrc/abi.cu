@@ -52,6 +52,20 @@ const char* gj_last_error(const gj_ctx* ctx) { return ctx ? ctx->c.err.msg.c_str
 
 long gj_last_launch_count(const gj_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
 
+gj_status gj_set_kernel_timing(gj_ctx* ctx, int on) {
+  if (!ctx) return GJ_EINVAL;
+  ctx->c.timer.on = on != 0;
+  ctx->c.timer.reset();
+  return GJ_OK;
+}
+
+gj_status gj_kernel_time(const gj_ctx* ctx, int kind, double* ms, long* launches) {
+  if (!ctx || kind < 0 || kind >= 8) return GJ_EINVAL;
+  if (ms) *ms = ctx->c.timer.ms[kind];
+  if (launches) *launches = ctx->c.timer.count[kind];
+  return GJ_OK;
+}
+
 gj_status gj_w_forward(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const double* eps_r,
                        const double* sigma, const gj_w_shot* shots, int nshots, double* d_out, double* jz_out,
                        double* u_out) {

@@ -79,10 +79,60 @@ class WSolverBase {
   virtual ~WSolverBase() = default;
 };
 
+// Optional per-kernel device timing: CUDA events around the launches of the
+// hot kernels, summed after each call's final synchronisation.
+struct KernelTimer {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<std::pair<int, size_t>> marks;  // (kind, first event index)
+  double ms[8] = {0};
+  long count[8] = {0};
+  ~KernelTimer() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(int kind, cudaStream_t st) {
+    if (!on) return;
+    marks.push_back({kind, used});
+    cudaEventRecord(next(), st);
+  }
+  void end(cudaStream_t st) {
+    if (!on) return;
+    cudaEventRecord(next(), st);
+  }
+  // Call after the stream is synchronised.
+  void collect() {
+    for (auto& mk : marks) {
+      float t = 0;
+      if (cudaEventElapsedTime(&t, pool[mk.second], pool[mk.second + 1]) == cudaSuccess) {
+        ms[mk.first] += t;
+        count[mk.first] += 1;
+      }
+    }
+    marks.clear();
+    used = 0;
+  }
+  void reset() {
+    for (int k = 0; k < 8; ++k) { ms[k] = 0; count[k] = 0; }
+  }
+};
+
+// Kernel kinds reported by gj_kernel_time().
+enum KernelKind { KK_FWD_STEP = 0, KK_REF_STEP = 1, KK_ADJ_STEP = 2, KK_IO = 3, KK_PLAIN = 4, KK_DC = 5 };
+
 struct Ctx {
   int device = 0;
   Err err;
   long launches = 0;
+  KernelTimer timer;
   std::unique_ptr<WSolverBase> wsolver;  // cached radar plan
   std::string wkey;
 };

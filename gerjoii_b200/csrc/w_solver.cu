@@ -91,7 +91,7 @@ class WSolver : public WSolverBase {
   WDev<T> w{};   // forward coefficients
   WDev<T> wr{};  // reference-adjoint coefficients (sigma -> -sigma in the interior)
   DevBuf coef, model_d, prof, shotbuf, recbuf, selbuf, nrsbuf, nselbuf, sibuf, sjbuf;
-  DevBuf fwdA, fwdB, adjA, adjB, hist, ckpt, acc, dbuf, ebuf, dobsbuf, sums, scratch;
+  DevBuf fwdA, fwdB, adjA, adjB, hist, ckpt, acc, dbuf, ebuf, dobsbuf, sums, scratch, stage, stage2, gout;
   std::vector<ShotHost> sh;
   std::vector<int> nrs, nsel;
   // layout of shotbuf: src (long) | cezj (T) | wav (T, nshots*nt)
@@ -380,153 +380,72 @@ class WSolver : public WSolverBase {
     while (K > 2 && (size_t(g.nt / K + 2) * per_ck + size_t(K + 3) * per_slot) > budget) K = K * 3 / 4;
   }
 
-  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
-                     bool dev_dobs, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
-                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+  // Inputs of a gradient call on the device: coefficients built from the model,
+  // observed traces converted to T in dobsbuf ([shot][r][t]).
+  gj_status stage_inputs(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
+                         bool dev_dobs, cudaStream_t st) {
     const int nrr = std::max(nr, 1);
-    const size_t tr = size_t(nrr) * g.nt;  // trace elements per shot
-    // model -> coefficients
-    DevBuf mh;
-    const double* eps_d = nullptr; const double* sig_d = nullptr;
+    const size_t tr = size_t(nrr) * g.nt;
     if (!dev_in) {
-      GJ_TRY(mh.alloc(err, 2 * mn * sizeof(double)));
-      GJ_CUDA(err, cudaMemcpyAsync(mh.as<double>(), eps, mn * sizeof(double), cudaMemcpyHostToDevice, st));
-      GJ_CUDA(err, cudaMemcpyAsync(mh.as<double>() + mn, sig, mn * sizeof(double), cudaMemcpyHostToDevice, st));
-      eps_d = mh.as<double>(); sig_d = eps_d + mn;
-      GJ_TRY(build<double>(err, c, eps_d, sig_d, st));
+      GJ_TRY(stage.alloc(err, 2 * mn * sizeof(double)));
+      GJ_CUDA(err, cudaMemcpyAsync(stage.as<double>(), eps, mn * sizeof(double), cudaMemcpyHostToDevice, st));
+      GJ_CUDA(err, cudaMemcpyAsync(stage.as<double>() + mn, sig, mn * sizeof(double), cudaMemcpyHostToDevice, st));
+      GJ_TRY(build<double>(err, c, stage.as<double>(), stage.as<double>() + mn, st));
     } else {
       GJ_TRY(build<T>(err, c, static_cast<const T*>(eps), static_cast<const T*>(sig), st));
     }
-    // observed traces -> device T, layout per shot [r][t] (nt x nr, time fastest)
-    if (!dev_dobs) {
-      std::vector<T> hd(size_t(nshots) * tr, T(0));
-      size_t q = 0;
-      for (int s = 0; s < nshots; ++s)
-        for (int r = 0; r < nrs[s]; ++r)
-          for (int t = 0; t < g.nt; ++t) hd[(size_t(s) * nrr + r) * g.nt + t] = T(static_cast<const double*>(dobs)[q++]);
-      GJ_CUDA(err, cudaMemcpyAsync(dobsbuf.p, hd.data(), hd.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-      GJ_CUDA(err, cudaStreamSynchronize(st));
-    } else {
+    if (dev_dobs) {
       GJ_CUDA(err, cudaMemcpyAsync(dobsbuf.p, dobs, size_t(nshots) * tr * sizeof(T), cudaMemcpyDeviceToDevice, st));
+      return GJ_OK;
     }
-    // memory plan
-    size_t free_b = 0, total_b = 0;
-    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
-    choose_k(o, free_b + hist.bytes + ckpt.bytes);
-    const bool full = (K >= g.nt);
-    // segments: [s0, s1) in steps; a remainder of one step joins the previous segment
+    bool uniform = true;
+    for (int s = 0; s < nshots; ++s) uniform = uniform && nrs[s] == nrr;
+    if (uniform) {
+      // host doubles straight to the device, converted there
+      GJ_TRY(stage2.alloc(err, size_t(nshots) * tr * sizeof(double)));
+      GJ_CUDA(err, cudaMemcpyAsync(stage2.p, dobs, size_t(nshots) * tr * sizeof(double), cudaMemcpyHostToDevice, st));
+      k_convert<double, T><<<1024, 256, 0, st>>>(stage2.as<double>(), dobsbuf.as<T>(), size_t(nshots) * tr);
+      ++c.launches;
+      GJ_CUDA(err, cudaGetLastError());
+      return GJ_OK;
+    }
+    std::vector<T> hd(size_t(nshots) * tr, T(0));
+    size_t q = 0;
+    for (int s = 0; s < nshots; ++s)
+      for (int r = 0; r < nrs[s]; ++r)
+        for (int t = 0; t < g.nt; ++t) hd[(size_t(s) * nrr + r) * g.nt + t] = T(static_cast<const double*>(dobs)[q++]);
+    GJ_CUDA(err, cudaMemcpyAsync(dobsbuf.p, hd.data(), hd.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    GJ_CUDA(err, cudaStreamSynchronize(st));
+    return GJ_OK;
+  }
+
+  // Segments [s0, s1) of the time axis; a remainder of one step joins the previous one.
+  std::vector<std::pair<int, int>> segments() const {
     std::vector<std::pair<int, int>> segs;
     for (int s0 = 0; s0 < g.nt; s0 += K) segs.push_back({s0, std::min(g.nt, s0 + K)});
     if (segs.size() > 1 && segs.back().second - segs.back().first < 2) {
       segs[segs.size() - 2].second = segs.back().second;
       segs.pop_back();
     }
-    int maxlen = 0;
-    for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
-    hist_slots = full ? size_t(g.nt + 1) : size_t(maxlen + 3);
-    GJ_TRY(hist.alloc(err, hist_slots * nshots * mn * sizeof(T)));
-    n_ckpt = full ? 0 : segs.size();
-    if (!full) GJ_TRY(ckpt.alloc(err, n_ckpt * nshots * sstride * sizeof(T)));
-    GJ_TRY(adjA.alloc(err, size_t(nshots) * sstride * sizeof(T)));
-    GJ_TRY(adjB.alloc(err, size_t(nshots) * sstride * sizeof(T)));
-    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * mn * sizeof(T)));
-    T* H = hist.as<T>();
-    const size_t hs = mn;  // per-shot stride inside a slot
-    auto slot_ptr = [&](long k, long base) { return H + size_t(k - base) * nshots * hs; };
+    return segs;
+  }
 
-    // ---- forward (with checkpoints at segment starts) ----
-    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
-    T* A = fwdA.as<T>() + ld;
-    T* B = fwdB.as<T>() + ld;
-    const dim3 grd = grid_dims();
-    if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, nshots * hs * sizeof(T), st));  // slot 0 = zero state
-    size_t segi = 0;
-    for (int it = 0; it < g.nt; ++it) {
-      if (!full && segi < segs.size() && it == segs[segi].first) {
-        GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * nshots * sstride, A - ld,
-                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        ++segi;
-      }
-      StepArgs<T> a = step_args(A, B, it);
-      if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
-      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
-      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
-                                                   g.nt, dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
-      c.launches += 2;
-      std::swap(A, B);
-    }
-    GJ_CUDA(err, cudaGetLastError());
-    // ---- residual and misfit ----
-    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
-    k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr, sums.as<double>());
-    ++c.launches;
-    std::vector<double> hsums(2 * nshots);
-    GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
-    // ---- adjoint ----
-    GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * mn * sizeof(T), st));
-    T* LA = adjA.as<T>() + ld;
-    T* LB = adjB.as<T>() + ld;
+  // d/dt u stencil of differentiate_cube.m:33-51 for 1-based history slot k.
+  void ddt_stencil(int k, int& k0, int& k1, int& k2, double& c0, double& c1, double& c2) const {
     const int nt = g.nt;
     const double dt = g.dt;
-    for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
-      const int s0 = segs[sidx].first, s1 = segs[sidx].second;
-      long base = 0;
-      if (!full) {
-        // restore the checkpoint and recompute slots s0..min(s1+1, nt)
-        base = s0;
-        GJ_CUDA(err, cudaMemcpyAsync(A - ld, ckpt.as<T>() + size_t(sidx) * nshots * sstride,
-                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        k_domain_copy<T><<<dim3(64, nshots), 256, 0, st>>>(w, A, sstride, slot_ptr(s0, base), hs, nshots);
-        ++c.launches;
-        const int iend = std::min(s1 + 1, nt);
-        for (int it = s0; it < iend; ++it) {
-          StepArgs<T> a = step_args(A, B, it);
-          a.hist = slot_ptr(it + 1, base); a.hstride = hs;
-          k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
-          ++c.launches;
-          std::swap(A, B);
-        }
-      }
-      for (int k = s1; k >= s0 + 1; --k) {  // k = history slot of forward step k-1
-        const int itf = k - 1;              // 0-based forward step
-        if (mode == GJ_ADJ_REFERENCE) {
-          if (nsel.size() && nr > 0)
-            k_inject_set<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), selbuf.as<int>(), nrr,
-                                                             nselbuf.as<int>(), ebuf.as<T>(), itf, nt, nshots);
-          StepArgs<T> a = step_args(LA, LB, itf);
-          a.src = d_src; a.hist = nullptr;
-          // d/dt u stencil (differentiate_cube.m:33-51); slots are 1-based in time
-          int k0, k1, k2; double c0, c1, c2;
-          if (k == 1) { k0 = 1; k1 = 2; k2 = 3; c0 = -1.5 / dt; c1 = 2.0 / dt; c2 = -0.5 / dt; }
-          else if (k == nt) { k0 = nt - 2; k1 = nt - 1; k2 = nt; c0 = 0.5 / dt; c1 = -2.0 / dt; c2 = 1.5 / dt; }
-          else { k0 = k - 1; k1 = k; k2 = k + 1; c0 = -0.5 / dt; c1 = 0.0; c2 = 0.5 / dt; }
-          a.u0 = slot_ptr(k0, base); a.u1 = slot_ptr(k1, base); a.u2 = slot_ptr(k2, base);
-          a.c0 = T(c0); a.c1 = T(c1); a.c2 = T(c2);
-          a.uk = slot_ptr(k, base);
-          a.hstride = hs;
-          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = o.no_kahan ? 0 : 1;
-          k_step<T, 1><<<grd, bx, 0, st>>>(wr, a);
-        } else {
-          if (nr > 0)
-            k_inject_add<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(),
-                                                             ebuf.as<T>(), itf, nt, nshots);
-          AdjArgs<T> a{};
-          a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = 0; a.tj = tj;
-          a.ek = slot_ptr(k, base); a.ekm1 = slot_ptr(k - 1, base); a.hstride = hs;
-          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = o.no_kahan ? 0 : 1;
-          k_adj_step<T><<<grd, bx, 0, st>>>(w, a);
-        }
-        c.launches += 2;
-        std::swap(LA, LB);
-      }
-    }
-    GJ_CUDA(err, cudaGetLastError());
-    // ---- finish ----
+    if (k == 1) { k0 = 1; k1 = 2; k2 = 3; c0 = -1.5 / dt; c1 = 2.0 / dt; c2 = -0.5 / dt; }
+    else if (k == nt) { k0 = nt - 2; k1 = nt - 1; k2 = nt; c0 = 0.5 / dt; c1 = -2.0 / dt; c2 = 1.5 / dt; }
+    else { k0 = k - 1; k1 = k; k2 = k + 1; c0 = -0.5 / dt; c1 = 0.0; c2 = 0.5 / dt; }
+  }
+
+  // Final scaling, shot reduction and outputs.
+  gj_status finish(Err& err, Ctx& c, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig, bool dev_out,
+                   double* misfit_out, double* d_out, double* e_out, const std::vector<double>& hsums,
+                   cudaStream_t st) {
+    const int nrr = std::max(nr, 1);
+    const size_t tr = size_t(nrr) * g.nt;
     const size_t gsz = (o.per_shot ? size_t(nshots) : 1) * mn;
-    DevBuf gout;
     double* ge_d; double* gs_d;
     if (dev_out && sizeof(T) == 8) { ge_d = static_cast<double*>(geps); gs_d = static_cast<double*>(gsig); }
     else {
@@ -550,6 +469,7 @@ class WSolver : public WSolverBase {
     if (d_out) { hd.resize(size_t(nshots) * tr); GJ_CUDA(err, cudaMemcpyAsync(hd.data(), dbuf.p, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, st)); }
     if (e_out) { he.resize(size_t(nshots) * tr); GJ_CUDA(err, cudaMemcpyAsync(he.data(), ebuf.p, he.size() * sizeof(T), cudaMemcpyDeviceToHost, st)); }
     GJ_CUDA(err, cudaStreamSynchronize(st));
+    c.timer.collect();
     if (misfit_out)
       for (int s = 0; s < nshots; ++s)
         misfit_out[s] = hsums[2 * s + 1] > 0 ? 0.5 * hsums[2 * s] / hsums[2 * s + 1] : 0.5 * hsums[2 * s];
@@ -562,6 +482,238 @@ class WSolver : public WSolverBase {
     if (d_out) unpack(hd, d_out);
     if (e_out) unpack(he, e_out);
     return GJ_OK;
+  }
+
+  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
+                     bool dev_dobs, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
+                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+    const int nrr = std::max(nr, 1);
+    const size_t tr = size_t(nrr) * g.nt;  // trace elements per shot
+    GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
+    if (o.plain) return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
+    // memory plan
+    size_t free_b = 0, total_b = 0;
+    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
+    choose_k(o, free_b + hist.bytes + ckpt.bytes);
+    const bool full = (K >= g.nt);
+    std::vector<std::pair<int, int>> segs = segments();
+    int maxlen = 0;
+    for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
+    hist_slots = full ? size_t(g.nt + 1) : size_t(maxlen + 3);
+    GJ_TRY(hist.alloc(err, hist_slots * nshots * mn * sizeof(T)));
+    n_ckpt = full ? 0 : segs.size();
+    if (!full) GJ_TRY(ckpt.alloc(err, n_ckpt * nshots * sstride * sizeof(T)));
+    GJ_TRY(adjA.alloc(err, size_t(nshots) * sstride * sizeof(T)));
+    GJ_TRY(adjB.alloc(err, size_t(nshots) * sstride * sizeof(T)));
+    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * mn * sizeof(T)));
+    T* H = hist.as<T>();
+    const size_t hs = mn;  // per-shot stride inside a slot
+    auto slot_ptr = [&](long k, long base) { return H + size_t(k - base) * nshots * hs; };
+    const int kahan = o.no_kahan ? 0 : 1;
+
+    // ---- forward (with checkpoints at segment starts) ----
+    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
+    T* A = fwdA.as<T>() + ld;
+    T* B = fwdB.as<T>() + ld;
+    const dim3 grd = grid_dims();
+    if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, nshots * hs * sizeof(T), st));  // slot 0 = zero state
+    size_t segi = 0;
+    for (int it = 0; it < g.nt; ++it) {
+      if (!full && segi < segs.size() && it == segs[segi].first) {
+        GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * nshots * sstride, A - ld,
+                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        ++segi;
+      }
+      StepArgs<T> a = step_args(A, B, it);
+      if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
+      c.timer.begin(KK_FWD_STEP, st);
+      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+      c.timer.end(st);
+      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
+                                                   g.nt, dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
+      c.launches += 2;
+      std::swap(A, B);
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    // ---- residual and misfit ----
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+    k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr, sums.as<double>());
+    ++c.launches;
+    std::vector<double> hsums(2 * nshots);
+    GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
+    // ---- adjoint ----
+    GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * mn * sizeof(T), st));
+    T* LA = adjA.as<T>() + ld;
+    T* LB = adjB.as<T>() + ld;
+    const int nt = g.nt;
+    for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
+      const int s0 = segs[sidx].first, s1 = segs[sidx].second;
+      long base = 0;
+      if (!full) {
+        // restore the checkpoint and recompute slots s0..min(s1+1, nt)
+        base = s0;
+        GJ_CUDA(err, cudaMemcpyAsync(A - ld, ckpt.as<T>() + size_t(sidx) * nshots * sstride,
+                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        k_domain_copy<T><<<dim3(64, nshots), 256, 0, st>>>(w, A, sstride, slot_ptr(s0, base), hs, nshots);
+        ++c.launches;
+        const int iend = std::min(s1 + 1, nt);
+        for (int it = s0; it < iend; ++it) {
+          StepArgs<T> a = step_args(A, B, it);
+          a.hist = slot_ptr(it + 1, base); a.hstride = hs;
+          c.timer.begin(KK_FWD_STEP, st);
+          k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+          c.timer.end(st);
+          ++c.launches;
+          std::swap(A, B);
+        }
+      }
+      for (int k = s1; k >= s0 + 1; --k) {  // k = history slot of forward step k-1
+        const int itf = k - 1;              // 0-based forward step
+        if (mode == GJ_ADJ_REFERENCE) {
+          if (nr > 0)
+            k_inject_set<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), selbuf.as<int>(), nrr,
+                                                             nselbuf.as<int>(), ebuf.as<T>(), itf, nt, nshots);
+          StepArgs<T> a = step_args(LA, LB, itf);
+          a.hist = nullptr;
+          int k0, k1, k2; double c0, c1, c2;
+          ddt_stencil(k, k0, k1, k2, c0, c1, c2);
+          a.u0 = slot_ptr(k0, base); a.u1 = slot_ptr(k1, base); a.u2 = slot_ptr(k2, base);
+          a.c0 = T(c0); a.c1 = T(c1); a.c2 = T(c2);
+          a.uk = slot_ptr(k, base);
+          a.hstride = hs;
+          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = kahan;
+          c.timer.begin(KK_REF_STEP, st);
+          k_step<T, 1><<<grd, bx, 0, st>>>(wr, a);
+          c.timer.end(st);
+        } else {
+          if (nr > 0)
+            k_inject_add<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(),
+                                                             ebuf.as<T>(), itf, nt, nshots);
+          AdjArgs<T> a{};
+          a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = 0; a.tj = tj;
+          a.ek = slot_ptr(k, base); a.ekm1 = slot_ptr(k - 1, base); a.hstride = hs;
+          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = kahan;
+          c.timer.begin(KK_ADJ_STEP, st);
+          k_adj_step<T><<<grd, bx, 0, st>>>(w, a);
+          c.timer.end(st);
+        }
+        c.launches += 2;
+        std::swap(LA, LB);
+      }
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    return finish(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, hsums, st);
+  }
+
+  // The plain form: one half-step per launch, one thread per node, one shot at a
+  // time, full u history in HBM when it fits (else the same checkpointing).
+  gj_status gradient_plain(Err& err, Ctx& c, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
+                           bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+    const int nrr = std::max(nr, 1), nt = g.nt;
+    const size_t tr = size_t(nrr) * nt;
+    size_t free_b = 0, total_b = 0;
+    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
+    // per-shot sizing: pretend a single shot
+    const int ns_save = nshots;
+    nshots = 1;
+    choose_k(o, free_b + hist.bytes + ckpt.bytes);
+    nshots = ns_save;
+    const bool full = (K >= nt);
+    std::vector<std::pair<int, int>> segs = segments();
+    int maxlen = 0;
+    for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
+    hist_slots = full ? size_t(nt + 1) : size_t(maxlen + 3);
+    GJ_TRY(hist.alloc(err, hist_slots * mn * sizeof(T)));
+    if (!full) GJ_TRY(ckpt.alloc(err, segs.size() * sstride * sizeof(T)));
+    GJ_TRY(adjA.alloc(err, sstride * sizeof(T)));
+    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * mn * sizeof(T)));
+    GJ_TRY(scratch.alloc(err, 5 * fstride * sizeof(T)));
+    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * mn * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(scratch.p, 0, 5 * fstride * sizeof(T), st));
+    T* px = scratch.as<T>() + ld; T* py = px + fstride; T* lm = py + fstride; T* qx = lm + fstride; T* qy = qx + fstride;
+    std::vector<T> hcezj(nshots), hwav(size_t(nshots) * nt);
+    GJ_CUDA(err, cudaMemcpyAsync(hcezj.data(), d_cezj, nshots * sizeof(T), cudaMemcpyDeviceToHost, st));
+    GJ_CUDA(err, cudaMemcpyAsync(hwav.data(), d_wav, hwav.size() * sizeof(T), cudaMemcpyDeviceToHost, st));
+    GJ_CUDA(err, cudaStreamSynchronize(st));
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+    const dim3 blk(32, 8), grd((NX + 1 + 31) / 32, (NY + 1 + 7) / 8);
+    T* H = hist.as<T>();
+    auto slot = [&](long k, long base) { return H + size_t(k - base) * mn; };
+    T* S = fwdA.as<T>() + ld;  // shot state (in place)
+    T* L = adjA.as<T>() + ld;
+    for (int s = 0; s < nshots; ++s) {
+      const long src = sh[s].src;
+      auto fwd_step = [&](int it, T* hslot) {
+        c.timer.begin(KK_PLAIN, st);
+        k_plain_h<T><<<grd, blk, 0, st>>>(w, S, fstride);
+        k_plain_e<T><<<grd, blk, 0, st>>>(w, S, fstride, src, hcezj[s] * hwav[size_t(s) * nt + it], hslot);
+        c.timer.end(st);
+        c.launches += 2;
+      };
+      GJ_CUDA(err, cudaMemsetAsync(S - ld, 0, sstride * sizeof(T), st));
+      if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, mn * sizeof(T), st));
+      size_t segi = 0;
+      for (int it = 0; it < nt; ++it) {
+        if (!full && segi < segs.size() && it == segs[segi].first) {
+          GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * sstride, S - ld, sstride * sizeof(T),
+                                       cudaMemcpyDeviceToDevice, st));
+          ++segi;
+        }
+        fwd_step(it, full ? slot(it + 1, 0) : nullptr);
+        k_record<T><<<dim3(1, 1), 128, 0, st>>>(S, sstride, recbuf.as<long>() + size_t(s) * nrr, nrr,
+                                                nrsbuf.as<int>() + s, it, nt, dbuf.as<T>() + size_t(s) * tr, d_src + s,
+                                                static_cast<T*>(nullptr), 1);
+        ++c.launches;
+      }
+      k_residual<T><<<dim3(64, 1), 256, 0, st>>>(dbuf.as<T>() + size_t(s) * tr, dobsbuf.as<T>() + size_t(s) * tr,
+                                                  ebuf.as<T>() + size_t(s) * tr, tr, sums.as<double>() + 2 * s);
+      ++c.launches;
+      GJ_CUDA(err, cudaMemsetAsync(L - ld, 0, sstride * sizeof(T), st));
+      T* A_ = acc.as<T>() + size_t(s) * 4 * mn;
+      for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
+        const int s0 = segs[sidx].first, s1 = segs[sidx].second;
+        long base = 0;
+        if (!full) {
+          base = s0;
+          GJ_CUDA(err, cudaMemcpyAsync(S - ld, ckpt.as<T>() + size_t(sidx) * sstride, sstride * sizeof(T),
+                                       cudaMemcpyDeviceToDevice, st));
+          k_domain_copy<T><<<dim3(64, 1), 256, 0, st>>>(w, S, sstride, slot(s0, base), mn, 1);
+          ++c.launches;
+          for (int it = s0; it < std::min(s1 + 1, nt); ++it) fwd_step(it, slot(it + 1, base));
+        }
+        for (int k = s1; k >= s0 + 1; --k) {
+          const int itf = k - 1;
+          c.timer.begin(KK_PLAIN, st);
+          if (mode == GJ_ADJ_REFERENCE) {
+            k_inject_set<T><<<dim3(1, 1), 128, 0, st>>>(L, sstride, recbuf.as<long>() + size_t(s) * nrr,
+                                                        selbuf.as<int>() + size_t(s) * nrr, nrr, nselbuf.as<int>() + s,
+                                                        ebuf.as<T>() + size_t(s) * tr, itf, nt, 1);
+            k_plain_h<T><<<grd, blk, 0, st>>>(wr, L, fstride);
+            k_plain_e<T><<<grd, blk, 0, st>>>(wr, L, fstride, -1, T(0), static_cast<T*>(nullptr));
+            int k0, k1, k2; double c0, c1, c2;
+            ddt_stencil(k, k0, k1, k2, c0, c1, c2);
+            k_plain_img_ref<T><<<256, 256, 0, st>>>(wr, L, slot(k0, base), slot(k1, base), slot(k2, base), T(c0),
+                                                    T(c1), T(c2), slot(k, base), A_);
+            c.launches += 4;
+          } else {
+            k_inject_add<T><<<dim3(1, 1), 128, 0, st>>>(L, sstride, recbuf.as<long>() + size_t(s) * nrr, nrr,
+                                                        nrsbuf.as<int>() + s, ebuf.as<T>() + size_t(s) * tr, itf, nt, 1);
+            k_plain_adj_e<T><<<grd, blk, 0, st>>>(w, L, fstride, px, py, lm, slot(k, base), slot(k - 1, base), A_);
+            k_plain_adj_h<T><<<grd, blk, 0, st>>>(w, L, fstride, px, py, qx, qy);
+            k_plain_adj_assemble<T><<<grd, blk, 0, st>>>(w, L, lm, qx, qy);
+            c.launches += 4;
+          }
+          c.timer.end(st);
+        }
+      }
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    std::vector<double> hsums(2 * nshots);
+    GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
+    return finish(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, hsums, st);
   }
 
   // ------------------------------------------------------------ w_grad only

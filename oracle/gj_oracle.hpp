@@ -387,13 +387,23 @@ struct AdjState {
 // Reverse of one step.  s1 = forward state after the step, s0 = before it.
 // ge/gs accumulate into padded-cell gradients (NX x NY, leading dimension NX).
 template <class T>
+struct AdjScratch {
+  std::vector<T> px, py, lEmid, qx, qy;
+  explicit AdjScratch(size_t N) : px(N), py(N), lEmid(N), qx(N), qy(N) {}
+};
+
+template <class T>
 inline void adjoint_step(const Grid& g, const Layout& L, const CoefT<T>& c, const Coefs& cd,
                          const std::vector<double>& epsr, const std::vector<double>& sigz,
                          const State<T>& s0, const State<T>& s1, AdjState<T>& a,
-                         std::vector<double>& ge, std::vector<double>& gs) {
+                         std::vector<double>& ge, std::vector<double>& gs, AdjScratch<T>& w) {
   const int NX = L.NX, NY = L.NY;
-  const size_t N = L.nodes();
-  std::vector<T> px(N, T(0)), py(N, T(0)), lEmid(N, T(0));
+  std::vector<T>& px = w.px;
+  std::vector<T>& py = w.py;
+  std::vector<T>& lEmid = w.lEmid;
+  std::fill(px.begin(), px.end(), T(0));
+  std::fill(py.begin(), py.end(), T(0));
+  std::fill(lEmid.begin(), lEmid.end(), T(0));
   const double e0 = g.eps0, u0 = g.mu0, dt = g.dt;
   auto cell = [&](int I, int J) { return size_t(I) + size_t(J) * NX; };
   // E part (transpose of new_Ez / new_Ez_pml)
@@ -432,7 +442,10 @@ inline void adjoint_step(const Grid& g, const Layout& L, const CoefT<T>& c, cons
       }
     }
   // H part (transpose of new_H / new_H_pml)
-  std::vector<T> qx(N, T(0)), qy(N, T(0));
+  std::vector<T>& qx = w.qx;
+  std::vector<T>& qy = w.qy;
+  std::fill(qx.begin(), qx.end(), T(0));
+  std::fill(qy.begin(), qy.end(), T(0));
   for (int J = 0; J <= NY - 1; ++J)
     for (int I = 0; I <= NX; ++I) {
       size_t k = L.at(I, J);
@@ -506,20 +519,19 @@ inline void grad_exact(const Grid& g, const double* eps, const double* sig, cons
   }
   std::vector<double> ge(size_t(L.NX) * L.NY, 0.0), gs(size_t(L.NX) * L.NY, 0.0);
   AdjState<T> a(L.nodes());
+  AdjScratch<T> scratch(L.nodes());
   const int nr = int(sh.rec.size());
+  std::vector<State<T>> buf(K + 1, State<T>(L.nodes()));  // reused by every segment
   for (int seg = int(ckpt.size()) - 1; seg >= 0; --seg) {
     const int k0 = seg * K, k1 = std::min(nt, k0 + K);
-    std::vector<State<T>> buf;
-    buf.reserve(k1 - k0 + 1);
-    buf.push_back(ckpt[seg]);
+    buf[0] = ckpt[seg];
     for (int it = k0; it < k1; ++it) {
-      State<T> nx = buf.back();
-      step<T>(L, c, nx, src, T(sh.wavelet[it]));
-      buf.push_back(std::move(nx));
+      buf[it - k0 + 1] = buf[it - k0];
+      step<T>(L, c, buf[it - k0 + 1], src, T(sh.wavelet[it]));
     }
     for (int it = k1 - 1; it >= k0; --it) {
       for (int r = 0; r < nr; ++r) a.lE[sh.rec[r]] += e[size_t(it) + size_t(r) * nt];
-      adjoint_step<T>(g, L, c, cd, epsr, sigz, buf[it - k0], buf[it - k0 + 1], a, ge, gs);
+      adjoint_step<T>(g, L, c, cd, epsr, sigz, buf[it - k0], buf[it - k0 + 1], a, ge, gs, scratch);
     }
   }
   pad_to_model(g, ge, gs, geps, gsig);

@@ -105,3 +105,19 @@ def test_invalid_source_is_rejected(gpu_ctx, small_ft):
     with pytest.raises(N.GJError) as ei:
         gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, [bad])
     assert ei.value.status == N.GJ_EINVAL
+
+
+@pytest.mark.parametrize("mode", [N.GJ_ADJ_REFERENCE, N.GJ_ADJ_EXACT])
+def test_plain_fp64_form_matches_fused(gpu_ctx, oracle, small_ft, mode):
+    p = small_ft
+    dobs = _dobs(oracle, p)
+    o = N.OptsC()
+    o.plain = 1
+    r1 = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64, opts=o)
+    r2 = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64)
+    assert rel_l2(r1["g_eps"], r2["g_eps"]) < 1e-11
+    assert rel_l2(r1["g_sig"], r2["g_sig"]) < 1e-11
+    assert np.allclose(r1["misfit"], r2["misfit"], rtol=1e-12)
+    o.ckpt_every = 11
+    r3 = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64, opts=o)
+    assert rel_l2(r3["g_eps"], r2["g_eps"]) < 1e-11
