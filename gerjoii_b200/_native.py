@@ -60,6 +60,8 @@ SIGNATURES = {
     "gj_w_grad": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _DP, _DP, _DP, _DP]),
     "gj_w_gradient_dev": (_I, [_VP, C.POINTER(GridC), _I, _VP, _VP, C.POINTER(ShotC), _I, _VP, _I, _I,
                                C.POINTER(OptsC), _VP, _VP, _DP, _VP]),
+    "gj_w_forward_noalloc": (_I, [C.POINTER(GridC), _VP, _VP, _I, _I, _VP, _I, _VP, _VP, _VP, C.c_char_p,
+                                  C.c_size_t]),
 }
 
 _lib = None

@@ -139,6 +139,34 @@ gj_status gj_w_gradient_dev(gj_ctx* ctx, const gj_w_grid* grid, gj_precision pre
                             void* g_eps_dev, void* g_sig_dev, double* misfit_out,
                             void* stream);
 
+/* Scratch limit of gj_w_forward_noalloc, in bytes (32 MiB): enough for a
+ * padded grid of about 380 000 Ez nodes (for example 600 x 600). */
+#define GJ_W_NOALLOC_SCRATCH_BYTES (32u << 20)
+
+/* Single-shot FP32 forward model that allocates no device memory.  It has no
+ * counterpart in the reference.  It is meant for callers that cannot allocate
+ * device memory when they call in: a MEX function inside MATLAB, whose GPU
+ * memory belongs to MATLAB's own pool, or an application that reserves the
+ * whole device up front and treats any later cudaMalloc as an error.
+ *   - All pointers except grid and errbuf are device pointers supplied by the
+ *     caller: eps_dev, sigma_dev (m x n floats, column-major), wavelet_dev
+ *     (nt floats), rec_dev (nr 0-based (NX+1)-linear Ez node indices) and
+ *     d_out_dev (nt x nr floats, written).
+ *   - Intermediate buffers live in one fixed array of
+ *     GJ_W_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the
+ *     library until the process exits.  Grids that need more are rejected with
+ *     GJ_EINVAL and a message in errbuf (may be NULL).
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Calls share the array: work is queued on `stream` (a cudaStream_t, NULL
+ *     = legacy default stream), and calls that overlap on the GPU, from any
+ *     thread or stream, race on it.  Each call clears the fields it needs. */
+gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* eps_dev, const float* sigma_dev,
+                               int src_i, int src_j, const float* wavelet_dev, int nr,
+                               const long* rec_dev, float* d_out_dev, void* stream, char* errbuf,
+                               size_t errlen);
+
 /* Number of kernel launches issued by the last call on this context (for the
  * benchmark's launch count).  Graph launches count the kernels they contain. */
 long gj_last_launch_count(const gj_ctx* ctx);
