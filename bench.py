@@ -268,6 +268,7 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step")}
+    ktimes = {k: v for k, v in ktimes.items() if v["launches"] > 0}
     ctx.set_kernel_timing(False)
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -276,45 +277,45 @@ def main():
     shots_total = args.nshots * world * args.steps
     value = shots_total / (ms / 1e3)
     cells = g.NX * g.NY
-    # cell-updates per gradient: forward + recompute + adjoint
-    fwd_launches = ktimes["fwd_step"][1] / max(args.steps, 1)
-    adj_launches = (ktimes["adj_step"][1] + ktimes["ref_step"][1]) / max(args.steps, 1)
-    upd_per_step = (fwd_launches + adj_launches) * cells * args.nshots * world
-    gcell = upd_per_step * args.steps / (ms / 1e3) / 1e9
-
-    # roofline for the dominant kernel
-    pk, pk_src = peaks()
-    dom = max(ktimes, key=lambda k: ktimes[k][0])
-    tot_ms, nl = ktimes[dom]
     mn = g.m * g.n
+    # cell-updates in the timed region: every forward, recompute and adjoint launch
+    upd = sum(k["shot_launches"] for k in ktimes.values()) * cells * world
+    gcell = upd / (ms / 1e3) / 1e9
+    # algorithmic bytes per shot for each kernel kind
+    per_shot_bytes = {
+        "fwd_step": cells * 32.0,             # read Ez,Hx,Hy,Ceze,Cezhy; write Ez,Hx,Hy
+        "adj_step": cells * 32.0 + mn * 40.0,  # + 2 history reads + 4 Kahan sums r/w
+        "ref_step": cells * 32.0 + mn * 48.0,  # + 4 history reads + 4 Kahan sums r/w
+    }
+    hist_launch_bytes = mn * 4.0               # history write of a forward launch that stores u
+    pk, pk_src = peaks()
+    dom = max(ktimes, key=lambda k: ktimes[k]["avg_us"] * ktimes[k]["launches"])
+    kt = ktimes[dom]
+    shots_per_launch = kt["shot_launches"] / max(kt["launches"], 1)
+    bytes_per_launch = shots_per_launch * per_shot_bytes[dom]
     if dom == "fwd_step":
-        per_cell = 32.0
-        hist_launches = max(nl / args.steps - g.nt, 0)
-        bytes_total = nl * args.nshots * cells * per_cell + hist_launches * args.steps * args.nshots * mn * 4.0
-        unit_desc = "32 B per shot-cell (read Ez,Hx,Hy,Ceze,Cezhy; write Ez,Hx,Hy) + 4 B per history write"
-    elif dom == "adj_step":
-        bytes_total = nl * args.nshots * (cells * 32.0 + mn * 40.0)
-        unit_desc = "32 B per shot-cell stencil + 40 B per model cell (2 history reads, 4 Kahan accumulators r/w)"
-    else:
-        bytes_total = nl * args.nshots * (cells * 32.0 + mn * 44.0)
-        unit_desc = "32 B per shot-cell stencil + 44 B per model cell (3 history reads, 4 accumulators r/w)"
-    avg_s = tot_ms / 1e3 / max(nl, 1)
-    achieved = bytes_total / max(nl, 1) / avg_s / 1e9
-    kname = {"fwd_step": "k_step<float,0>", "adj_step": "k_adj_step<float>", "ref_step": "k_step<float,1>"}[dom]
+        bytes_per_launch += shots_per_launch * hist_launch_bytes
+    avg_s = kt["avg_us"] / 1e6
+    achieved = bytes_per_launch / avg_s / 1e9 if avg_s > 0 else 0.0
+    kname = {"fwd_step": "k_stepv<float,0>", "adj_step": "k_adj_stepv<float>", "ref_step": "k_stepv<float,1>"}[dom]
     tpu = traffic_per_unit(kname)
     roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
-            "traffic": (tpu * args.nshots * cells if tpu is not None else None),
-            "algorithmic_bytes_per_launch": bytes_total / max(nl, 1), "launches": nl,
-            "avg_launch_us": avg_s * 1e6, "units": unit_desc,
-            "kernel_share_of_step": tot_ms / ms}
+            "traffic": (tpu * shots_per_launch * cells if tpu is not None else None),
+            "algorithmic_bytes_per_launch": bytes_per_launch, "shots_per_launch": shots_per_launch,
+            "launches": kt["launches"], "timed_launches": kt["sampled"], "avg_launch_us": kt["avg_us"],
+            "units": ("per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n history write" if dom == "fwd_step" else
+                      "per shot: 32 B x NX*NY cells (stencil) + 40 B x m*n (2 history reads, 4 Kahan sums r/w)"
+                      if dom == "adj_step" else
+                      "per shot: 32 B x NX*NY cells (stencil) + 48 B x m*n (4 history reads, 4 Kahan sums r/w)"),
+            "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / ms}
     line = {"metric": METRIC, "value": value, "unit": "shot-gradients/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded layered model, observed traces modelled on the device)",
             "config": cfg, "gcell_updates_per_s": gcell, "gpu_launches": launches,
             "clocks": clk, "roofline": roof,
-            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()}}
+            "kernel_ms_per_step": {k: v["avg_us"] * v["launches"] / 1e3 / args.steps for k, v in ktimes.items()}}
 
     if rank == 0 and not args.no_extras:
         # e2e: the public C ABI with host (pinned) buffers, copies inside the timed region

@@ -53,7 +53,7 @@ SIGNATURES = {
     "gj_last_error": (C.c_char_p, [_VP]),
     "gj_last_launch_count": (_L, [_VP]),
     "gj_set_kernel_timing": (_I, [_VP, _I]),
-    "gj_kernel_time": (_I, [_VP, _I, _DP, C.POINTER(C.c_long)]),
+    "gj_kernel_time": (_I, [_VP, _I, _DP, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long)]),
     "gj_w_forward": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _DP, _DP]),
     "gj_w_gradient": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _I,
                            C.POINTER(OptsC), _DP, _DP, _DP, _DP, _DP]),
@@ -76,7 +76,7 @@ def load(build_if_missing: bool = False):
     global _lib
     if _lib is not None:
         return _lib
-    path = _build.LIB
+    path = os.environ.get("GERJOII_B200_LIB", _build.LIB)
     if not os.path.exists(path):
         if build_if_missing:
             _build.build()
@@ -160,11 +160,15 @@ class Context:
         self._check(self.lib.gj_set_kernel_timing(self.h, int(bool(on))))
 
     def kernel_time(self, kind: str):
-        """(milliseconds, launches) accumulated for a kernel kind while timing is on."""
+        """Accumulated timing of a kernel kind while timing is on: dict with the
+        summed ms of the sampled launches, their number, all launches of the
+        kind and the sum of shots over those launches."""
         ms = C.c_double(0)
-        n = C.c_long(0)
-        self._check(self.lib.gj_kernel_time(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(n)))
-        return ms.value, n.value
+        smp, n, sl = C.c_long(0), C.c_long(0), C.c_long(0)
+        self._check(self.lib.gj_kernel_time(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(smp),
+                                            C.byref(n), C.byref(sl)))
+        return {"ms": ms.value, "sampled": smp.value, "launches": n.value, "shot_launches": sl.value,
+                "avg_us": 1e3 * ms.value / smp.value if smp.value else 0.0}
 
     # ------------------------------------------------------------------ radar
     def w_forward(self, g, eps, sig, shots, precision=GJ_F32, want_jz=False, want_u=False):

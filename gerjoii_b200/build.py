@@ -40,18 +40,20 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
+def build(force: bool = False, verbose: bool = False, out: str | None = None, defines=()) -> str:
+    """Compiles the library; `out` and `defines` build a tuning variant elsewhere."""
+    target = out or LIB
+    if out is None and not force and up_to_date():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
-    tmp = LIB + ".tmp"
+    os.makedirs(os.path.dirname(target), exist_ok=True)
+    tmp = target + ".tmp"
     cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-cudart", "static", "-o", tmp, *sources(), "-lcufft"]
+           "-cudart", "static", *[f"-D{d}" for d in defines], "-o", tmp, *sources(), "-lcufft"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True, cwd=CSRC)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":

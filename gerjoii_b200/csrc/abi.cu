@@ -59,10 +59,14 @@ gj_status gj_set_kernel_timing(gj_ctx* ctx, int on) {
   return GJ_OK;
 }
 
-gj_status gj_kernel_time(const gj_ctx* ctx, int kind, double* ms, long* launches) {
+gj_status gj_kernel_time(const gj_ctx* ctx, int kind, double* ms, long* sampled, long* launches,
+                         long* shot_launches) {
   if (!ctx || kind < 0 || kind >= 8) return GJ_EINVAL;
-  if (ms) *ms = ctx->c.timer.ms[kind];
-  if (launches) *launches = ctx->c.timer.count[kind];
+  const gj::KernelTimer& t = ctx->c.timer;
+  if (ms) *ms = t.ms[kind];
+  if (sampled) *sampled = t.sampled[kind];
+  if (launches) *launches = t.launches[kind];
+  if (shot_launches) *shot_launches = t.shot_launches[kind];
   return GJ_OK;
 }
 

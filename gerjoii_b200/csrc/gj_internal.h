@@ -79,49 +79,67 @@ class WSolverBase {
   virtual ~WSolverBase() = default;
 };
 
-// Optional per-kernel device timing: CUDA events around the launches of the
-// hot kernels, summed after each call's final synchronisation.
+// Optional per-kernel device timing: CUDA events around sampled launches of
+// the hot kernels (every `stride`-th launch of each kind), also inside captured
+// CUDA graphs (external event-record nodes).  A Marks list belongs to one
+// launch sequence (a direct enqueue, or one captured graph that is replayed);
+// collect() adds its elapsed times after the stream has been synchronised.
+struct Marks {
+  std::vector<cudaEvent_t> ev;            // owned events, in pairs
+  std::vector<int> kind;                  // per pair
+  long launches[8] = {0};                 // every launch of each kind in this sequence
+  long shot_launches[8] = {0};            // sum of shots over those launches
+  ~Marks() { for (auto e : ev) cudaEventDestroy(e); }
+};
+
 struct KernelTimer {
   bool on = false;
-  std::vector<cudaEvent_t> pool;
-  size_t used = 0;
-  std::vector<std::pair<int, size_t>> marks;  // (kind, first event index)
+  int stride = 8;
   double ms[8] = {0};
-  long count[8] = {0};
-  ~KernelTimer() {
-    for (auto e : pool) cudaEventDestroy(e);
+  long sampled[8] = {0};
+  long launches[8] = {0};
+  long shot_launches[8] = {0};
+  long seen[8] = {0};
+  Marks* cur = nullptr;  // list receiving new marks
+  static void rec(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else cudaEventRecord(e, st);
   }
-  cudaEvent_t next() {
-    if (used == pool.size()) {
-      cudaEvent_t e;
-      cudaEventCreate(&e);
-      pool.push_back(e);
-    }
-    return pool[used++];
+  // begin/end bracket one launch of `shots` shots; begin returns whether it is timed.
+  bool begin(int kind, cudaStream_t st, int shots = 1) {
+    if (!on || !cur) return false;
+    cur->launches[kind] += 1;
+    cur->shot_launches[kind] += shots;
+    if ((seen[kind]++ % stride) != 0) return false;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cur->ev.push_back(a);
+    cur->ev.push_back(b);
+    cur->kind.push_back(kind);
+    rec(a, st);
+    return true;
   }
-  void begin(int kind, cudaStream_t st) {
+  void end(bool timed, cudaStream_t st) {
+    if (timed) rec(cur->ev.back(), st);
+  }
+  // Adds one execution of the sequence `m` (after its stream has completed).
+  void collect(const Marks& m) {
     if (!on) return;
-    marks.push_back({kind, used});
-    cudaEventRecord(next(), st);
-  }
-  void end(cudaStream_t st) {
-    if (!on) return;
-    cudaEventRecord(next(), st);
-  }
-  // Call after the stream is synchronised.
-  void collect() {
-    for (auto& mk : marks) {
+    for (size_t q = 0; q < m.kind.size(); ++q) {
       float t = 0;
-      if (cudaEventElapsedTime(&t, pool[mk.second], pool[mk.second + 1]) == cudaSuccess) {
-        ms[mk.first] += t;
-        count[mk.first] += 1;
+      if (cudaEventElapsedTime(&t, m.ev[2 * q], m.ev[2 * q + 1]) == cudaSuccess) {
+        ms[m.kind[q]] += t;
+        sampled[m.kind[q]] += 1;
       }
     }
-    marks.clear();
-    used = 0;
+    for (int k = 0; k < 8; ++k) { launches[k] += m.launches[k]; shot_launches[k] += m.shot_launches[k]; }
+    cudaGetLastError();
   }
   void reset() {
-    for (int k = 0; k < 8; ++k) { ms[k] = 0; count[k] = 0; }
+    for (int k = 0; k < 8; ++k) { ms[k] = 0; sampled[k] = 0; launches[k] = 0; shot_launches[k] = 0; seen[k] = 0; }
   }
 };
 

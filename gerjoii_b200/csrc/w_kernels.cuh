@@ -54,7 +54,7 @@ struct StepArgs {
   const T* u0; const T* u1; const T* u2;  // three history slots for d/dt u
   T c0, c1, c2;                           // differentiation weights
   const T* uk;                            // u(k) slot
-  T* acc; size_t astride;                 // accumulators [shot][4][m*n]: sumE, compE, sumS, compS
+  T* acc; size_t astride;                 // accumulators [shot][4][dstride]: sumE, compE, sumS, compS
   int kahan;
 };
 
@@ -237,114 +237,6 @@ __device__ __forceinline__ void adj_p(const WDev<T>& w, int i, int j, size_t k, 
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_adj_step(const WDev<T> w, const AdjArgs<T> a) {
-  const int lane = threadIdx.x & 31;
-  const int i0w = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-  const int ld = w.ld, NX = w.NX, NY = w.NY;
-  if (i0w >= ld) return;
-  const int I = i0w + lane;
-  const int j0 = blockIdx.y * a.tj;
-  if (j0 > NY) return;
-  const int j1 = min(j0 + a.tj - 1, NY);
-  const int s = a.shot0 + blockIdx.z;
-  const size_t off = size_t(s) * a.sstride, fs = a.fstride;
-  const T* __restrict__ LA = a.A + off;
-  const T* __restrict__ LxA = LA + fs;   // lHx
-  const T* __restrict__ LyA = LA + 2 * fs;
-  const T* __restrict__ SxA = LA + 3 * fs;  // lEzx
-  const T* __restrict__ SyA = LA + 4 * fs;
-  T* __restrict__ LB = a.B + off;
-  T* __restrict__ LxB = LB + fs;
-  T* __restrict__ LyB = LB + 2 * fs;
-  T* __restrict__ SxB = LB + 3 * fs;
-  T* __restrict__ SyB = LB + 4 * fs;
-  const bool rowHx = I <= NX;
-  const bool rowHy = I <= NX - 1;
-  const bool rowE = I >= 1 && I <= NX - 1;
-  const bool rowDom = I >= w.di0 && I < w.di0 + w.m;
-
-  // node (I, j0): p-values; (I, j0-1): qx
-  T px_c, py_c, lm_c, lx_c, ly_c, l_c;
-  {
-    const size_t k = nidx(I, j0, ld);
-    l_c = LA[k];
-    adj_p(w, I, j0, k, l_c, SxA[k], SyA[k], px_c, py_c, lm_c, lx_c, ly_c);
-  }
-  T qx_prev = T(0);
-  if (j0 >= 1 && rowHx) {
-    const size_t k = nidx(I, j0 - 1, ld);
-    T px_m, py_m, lm_m, lx_m, ly_m;
-    adj_p(w, I, j0 - 1, k, LA[k], SxA[k], SyA[k], px_m, py_m, lm_m, lx_m, ly_m);
-    T ha, hb; hx_coef(w, I, j0 - 1, ha, hb);
-    qx_prev = hb * (LxA[k] + py_m - py_c);
-  }
-  for (int J = j0; J <= j1; ++J) {
-    const size_t k = nidx(I, J, ld);
-    // next node (I, J+1)
-    const size_t kn = k + ld;
-    const T l_n = LA[kn];
-    T px_n, py_n, lm_n, lx_n, ly_n;
-    adj_p(w, I, J + 1, kn, l_n, SxA[kn], SyA[kn], px_n, py_n, lm_n, lx_n, ly_n);
-    // px at (I+1, J) and (I-1, J)
-    T px_dn = __shfl_down_sync(0xffffffffu, px_c, 1);
-    T px_up = __shfl_up_sync(0xffffffffu, px_c, 1);
-    if (lane == 31) {
-      T a1, a2, a3, a4;
-      adj_p(w, I + 1, J, k + 1, LA[k + 1], SxA[k + 1], SyA[k + 1], px_dn, a1, a2, a3, a4);
-    }
-    if (lane == 0) {
-      T a1, a2, a3, a4;
-      adj_p(w, I - 1, J, k - 1, LA[k - 1], SxA[k - 1], SyA[k - 1], px_up, a1, a2, a3, a4);
-    }
-    // H-like half
-    T qx = T(0), qy = T(0);
-    if (rowHx && J <= NY - 1) {
-      T ha, hb; hx_coef(w, I, J, ha, hb);
-      const T lt = LxA[k] + py_c - py_n;
-      LxB[k] = ha * lt;
-      qx = hb * lt;
-    }
-    if (rowHy) {
-      T ha, hb; hy_coef(w, I, J, ha, hb);
-      const T lt = LyA[k] + px_c - px_dn;
-      LyB[k] = ha * lt;
-      qy = hb * lt;
-    }
-    T qy_up = __shfl_up_sync(0xffffffffu, qy, 1);
-    if (lane == 0) {
-      qy_up = T(0);
-      if (I >= 1) {
-        T ha, hb; hy_coef(w, I - 1, J, ha, hb);
-        qy_up = hb * (LyA[k - 1] + px_up - px_c);
-      }
-    }
-    // E-like half
-    if (rowE && J >= 1 && J <= NY - 1) {
-      LB[k] = lm_c + qx_prev - qx + qy_up - qy;
-      if (!(I >= w.ei0 && I <= w.ei1 && J >= w.ej0 && J <= w.ej1)) {
-        SxB[k] = w.ax[k] * lx_c;
-        SyB[k] = w.ay[k] * ly_c;
-      } else if (rowDom && J >= w.dj0 && J < w.dj0 + w.n) {
-        const size_t p = size_t(I - w.di0) + size_t(J - w.dj0) * size_t(w.m);
-        const size_t hs = size_t(s) * a.hstride;
-        const T e1 = a.ek[hs + p], e0 = a.ekm1[hs + p];
-        T* acc = a.acc + size_t(s) * a.astride;
-        const size_t mn = size_t(w.m) * size_t(w.n);
-        if (a.kahan) {
-          kahan_add(acc + p, acc + mn + p, l_c * (e1 - e0));
-          kahan_add(acc + 2 * mn + p, acc + 3 * mn + p, l_c * (e1 + e0));
-        } else {
-          acc[p] += l_c * (e1 - e0);
-          acc[2 * mn + p] += l_c * (e1 + e0);
-        }
-      }
-    }
-    qx_prev = qx;
-    px_c = px_n; py_c = py_n; lm_c = lm_n; lx_c = lx_n; ly_c = ly_n; l_c = l_n;
-  }
-}
-
 // --------------------------------------------------------------------------
 // Receiver I/O and small helpers
 // --------------------------------------------------------------------------
@@ -385,16 +277,24 @@ __global__ void k_inject_add(T* state, size_t sstride, const long* rec, int nr, 
     atomicAdd(L + rec[size_t(s) * nr + r], e[(size_t(s) * nr + r) * nt + k]);
 }
 
-// Copies the domain part of Ez (state) into a history slot (the checkpoint's u).
+// History slots and imaging accumulators use the "domain-node" layout: per
+// shot ld x n elements, element (i, j) of a model column j in [dj0, dj0+n) at
+// (j - dj0)*ld + i, so the marching kernels read and write them with the same
+// aligned vector accesses as the fields.  Rows outside the model are unused.
+__device__ __forceinline__ size_t dnode(int i, int j, int ld, int dj0) {
+  return size_t(j - dj0) * size_t(ld) + size_t(i);
+}
+
+// Copies the model columns of Ez (state) into a history slot (the checkpoint's u).
 template <class T>
 __global__ void k_domain_copy(const WDev<T> w, const T* state, size_t sstride, T* hist,
                               size_t hstride, int nshots) {
-  const size_t mn = size_t(w.m) * w.n;
+  const size_t dn = size_t(w.ld) * w.n;
   const int s = blockIdx.y;
   if (s >= nshots) return;
-  for (size_t p = threadIdx.x + size_t(blockIdx.x) * blockDim.x; p < mn; p += size_t(blockDim.x) * gridDim.x) {
-    const int a = int(p % w.m), b = int(p / w.m);
-    hist[size_t(s) * hstride + p] = state[size_t(s) * sstride + nidx(w.di0 + a, w.dj0 + b, w.ld)];
+  for (size_t q = threadIdx.x + size_t(blockIdx.x) * blockDim.x; q < dn; q += size_t(blockDim.x) * gridDim.x) {
+    const int I = int(q % w.ld), b = int(q / w.ld);
+    hist[size_t(s) * hstride + q] = state[size_t(s) * sstride + nidx(I, w.dj0 + b, w.ld)];
   }
 }
 
@@ -407,6 +307,7 @@ __global__ void k_finish(const WDev<T> w, const T* acc, size_t astride, int nsho
                          int kind, double dt, double eps0, const double* eps_m, const double* sig_m,
                          double* geps, double* gsig) {
   const size_t mn = size_t(w.m) * w.n;
+  const size_t dn = size_t(w.ld) * w.n;
   for (size_t p = threadIdx.x + size_t(blockIdx.x) * blockDim.x; p < mn; p += size_t(blockDim.x) * gridDim.x) {
     double fe, fs;
     if (kind == 0) { fe = dt; fs = dt; }
@@ -414,12 +315,13 @@ __global__ void k_finish(const WDev<T> w, const T* acc, size_t astride, int nsho
       const double D = 2.0 * eps_m[p] * eps0 + dt * sig_m[p];
       fe = -2.0 * eps0 / D; fs = -dt / D;
     }
+    const size_t q = dnode(w.di0 + int(p % w.m), w.dj0 + int(p / w.m), w.ld, w.dj0);
     double se = 0, ss = 0;
     for (int s = 0; s < nshots; ++s) {
       const T* A = acc + size_t(s) * astride;
       // Kahan: the compensation term holds the excess of the running sum.
-      const double ve = double(A[p]) - double(A[mn + p]);
-      const double vs = double(A[2 * mn + p]) - double(A[3 * mn + p]);
+      const double ve = double(A[q]) - double(A[dn + q]);
+      const double vs = double(A[2 * dn + q]) - double(A[3 * dn + q]);
       if (per_shot) {
         geps[size_t(s) * mn + p] = fe * ve;
         gsig[size_t(s) * mn + p] = fs * vs;
@@ -461,20 +363,21 @@ __global__ void k_plain_e(const WDev<T> w, T* st, size_t fs, long src, T sval, T
     Ex[k] = ex; Ey[k] = ey; e = ex + ey;
   }
   Ez[k] = e;
-  if (hist && I >= w.di0 && I < w.di0 + w.m && J >= w.dj0 && J < w.dj0 + w.n)
-    hist[size_t(I - w.di0) + size_t(J - w.dj0) * w.m] = e;
+  if (hist && J >= w.dj0 && J < w.dj0 + w.n) hist[dnode(I, J, w.ld, w.dj0)] = e;
 }
 
-// Plain reference-adjoint imaging: g -= du*a, g -= u*a (separate pass, FP64 sums).
+// Plain reference-adjoint imaging: g -= du*a, g -= u*a (separate pass).
 template <class T>
 __global__ void k_plain_img_ref(const WDev<T> w, const T* st, const T* u0, const T* u1, const T* u2,
                                 T c0, T c1, T c2, const T* uk, T* acc) {
   const size_t mn = size_t(w.m) * w.n;
+  const size_t dn = size_t(w.ld) * w.n;
   for (size_t p = threadIdx.x + size_t(blockIdx.x) * blockDim.x; p < mn; p += size_t(blockDim.x) * gridDim.x) {
-    const int a_ = int(p % w.m), b = int(p / w.m);
-    const T av = st[nidx(w.di0 + a_, w.dj0 + b, w.ld)];
-    acc[p] -= (c0 * u0[p] + c1 * u1[p] + c2 * u2[p]) * av;
-    acc[2 * mn + p] -= uk[p] * av;
+    const int I = w.di0 + int(p % w.m), J = w.dj0 + int(p / w.m);
+    const size_t q = dnode(I, J, w.ld, w.dj0);
+    const T av = st[nidx(I, J, w.ld)];
+    acc[q] -= (c0 * u0[q] + c1 * u1[q] + c2 * u2[q]) * av;
+    acc[2 * dn + q] -= uk[q] * av;
   }
 }
 
@@ -497,10 +400,10 @@ __global__ void k_plain_adj_e(const WDev<T> w, T* st, size_t fs, T* px, T* py, T
     Sx[k] = w.ax[k] * lx; Sy[k] = w.ay[k] * ly;
   }
   if (interior && I >= w.di0 && I < w.di0 + w.m && J >= w.dj0 && J < w.dj0 + w.n) {
-    const size_t p = size_t(I - w.di0) + size_t(J - w.dj0) * w.m;
-    const size_t mn = size_t(w.m) * w.n;
-    acc[p] += l * (ek[p] - ekm1[p]);
-    acc[2 * mn + p] += l * (ek[p] + ekm1[p]);
+    const size_t q = dnode(I, J, w.ld, w.dj0);
+    const size_t dn = size_t(w.ld) * w.n;
+    acc[q] += l * (ek[q] - ekm1[q]);
+    acc[2 * dn + q] += l * (ek[q] + ekm1[q]);
   }
 }
 // (2) H part: lH update, q into scratch.

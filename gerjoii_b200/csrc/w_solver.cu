@@ -11,6 +11,7 @@
 
 #include "gj_internal.h"
 #include "w_kernels.cuh"
+#include "w_kernels_vec.cuh"
 
 namespace gj {
 
@@ -87,7 +88,7 @@ class WSolver : public WSolverBase {
  public:
   gj_w_grid g{};
   int NX = 0, NY = 0, ld = 0, nshots = 0, nr = 0;  // nr = max receivers per shot
-  size_t fstride = 0, sstride = 0, mn = 0;
+  size_t fstride = 0, sstride = 0, mn = 0, dn = 0;  // dn: domain-node elements per shot (ld*n)
   WDev<T> w{};   // forward coefficients
   WDev<T> wr{};  // reference-adjoint coefficients (sigma -> -sigma in the interior)
   DevBuf coef, model_d, prof, shotbuf, recbuf, selbuf, nrsbuf, nselbuf, sibuf, sjbuf;
@@ -133,6 +134,7 @@ class WSolver : public WSolverBase {
     fstride = size_t(ld) * size_t(NY + 3);
     sstride = size_t(NFIELDS) * fstride;
     mn = size_t(g.m) * size_t(g.n);
+    dn = size_t(ld) * size_t(g.n);
     nshots = ns;
     nr = 0;
     sh.assign(ns, ShotHost{});
@@ -274,39 +276,6 @@ class WSolver : public WSolverBase {
     return a;
   }
 
-  dim3 grid_dims() const { return dim3((ld + bx - 1) / bx, (NY + 1 + tj - 1) / tj, nshots); }
-
-  // Forward time loop over [it0, it1); state in A (swapped in place).  Optionally
-  // writes the history slot it+1 - hbase of every step and records traces.
-  gj_status run_forward(Err& err, Ctx& c, T*& A, T*& B, int it0, int it1, bool record, T* hring,
-                        long hbase, size_t hcap, size_t hstride, cudaStream_t st, T* ckpt_base,
-                        int ckK) {
-    const dim3 grd = grid_dims();
-    for (int it = it0; it < it1; ++it) {
-      if (ckpt_base && ckK > 0 && it % ckK == 0) {
-        GJ_CUDA(err, cudaMemcpyAsync(ckpt_base + size_t(it / ckK) * nshots * sstride, A - ld,
-                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
-      }
-      StepArgs<T> a = step_args(A, B, it);
-      if (hring) {
-        const long slot = long(it + 1) - hbase;
-        a.hist = hring + size_t(slot % long(hcap)) * nshots * hstride;
-        a.hstride = hstride;
-      }
-      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
-      ++c.launches;
-      if (record) {
-        k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), std::max(nr, 1),
-                                                     nrsbuf.as<int>(), it, g.nt, dbuf.as<T>(), d_src,
-                                                     static_cast<T*>(nullptr), nshots);
-        ++c.launches;
-      }
-      std::swap(A, B);
-    }
-    GJ_CUDA(err, cudaGetLastError());
-    return GJ_OK;
-  }
-
   gj_status alloc_states(Err& err) {
     GJ_TRY(fwdA.alloc(err, size_t(nshots) * sstride * sizeof(T)));
     GJ_TRY(fwdB.alloc(err, size_t(nshots) * sstride * sizeof(T)));
@@ -329,12 +298,15 @@ class WSolver : public WSolverBase {
     const int nrr = std::max(nr, 1);
     DevBuf jzb, ub;
     if (jz_out) GJ_TRY(jzb.alloc(err, size_t(nshots) * g.nt * sizeof(T)));
-    if (u_out) GJ_TRY(ub.alloc(err, size_t(nshots) * mn * (g.nt + 1) * sizeof(T)));
-    const dim3 grd = grid_dims();
+    if (u_out) GJ_TRY(ub.alloc(err, size_t(nshots) * dn * (g.nt + 1) * sizeof(T)));
+    constexpr int V = VT<T>::V;
+    const int tjf = tj_for(nshots);
+    const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + tjf - 1) / tjf, nshots);
     for (int it = 0; it < g.nt; ++it) {
       StepArgs<T> a = step_args(A, B, it);
-      if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * mn; a.hstride = mn; }
-      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
+      a.tj = tjf;
+      if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * dn; a.hstride = dn; }
+      k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
       k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
                                                    g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
                                                    nshots);
@@ -356,13 +328,16 @@ class WSolver : public WSolverBase {
       for (size_t i = 0; i < hj.size(); ++i) jz_out[i] = double(hj[i]);
     }
     if (u_out) {
-      std::vector<T> hu(size_t(nshots) * mn * g.nt);
+      std::vector<T> hu(size_t(nshots) * dn * g.nt);
       GJ_CUDA(err, cudaMemcpy(hu.data(), ub.p, hu.size() * sizeof(T), cudaMemcpyDeviceToHost));
-      // device [t][shot][p] -> host [shot][t][p]
+      // device [t][shot][domain-node] -> host [shot][t][m x n]
+      const int di0 = w.di0;
       for (int s = 0; s < nshots; ++s)
         for (int t = 0; t < g.nt; ++t)
-          for (size_t p = 0; p < mn; ++p)
-            u_out[(size_t(s) * g.nt + t) * mn + p] = double(hu[(size_t(t) * nshots + s) * mn + p]);
+          for (int b = 0; b < g.n; ++b)
+            for (int a_ = 0; a_ < g.m; ++a_)
+              u_out[(size_t(s) * g.nt + t) * mn + size_t(b) * g.m + a_] =
+                  double(hu[(size_t(t) * nshots + s) * dn + size_t(b) * ld + di0 + a_]);
     }
     return GJ_OK;
   }
@@ -371,7 +346,7 @@ class WSolver : public WSolverBase {
   // Chooses K: the whole history when it fits, else checkpoints every K steps.
   void choose_k(const gj_w_opts& o, size_t free_bytes) {
     const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.8 * double(free_bytes));
-    const size_t per_slot = size_t(nshots) * mn * sizeof(T);
+    const size_t per_slot = size_t(nshots) * dn * sizeof(T);
     const size_t per_ck = size_t(nshots) * sstride * sizeof(T);
     if (o.ckpt_every > 0) { K = std::min(std::max(o.ckpt_every, 2), g.nt); return; }
     if (size_t(g.nt + 1) * per_slot <= budget) { K = g.nt; return; }
@@ -452,7 +427,7 @@ class WSolver : public WSolverBase {
       GJ_TRY(gout.alloc(err, 2 * gsz * sizeof(double)));
       ge_d = gout.as<double>(); gs_d = ge_d + gsz;
     }
-    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * mn, nshots, o.per_shot, mode == GJ_ADJ_EXACT ? 1 : 0,
+    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, nshots, o.per_shot, mode == GJ_ADJ_EXACT ? 1 : 0,
                                      g.dt, g.eps0, eps_m, sig_m, ge_d, gs_d);
     ++c.launches;
     if (dev_out && sizeof(T) == 4) {
@@ -469,7 +444,6 @@ class WSolver : public WSolverBase {
     if (d_out) { hd.resize(size_t(nshots) * tr); GJ_CUDA(err, cudaMemcpyAsync(hd.data(), dbuf.p, hd.size() * sizeof(T), cudaMemcpyDeviceToHost, st)); }
     if (e_out) { he.resize(size_t(nshots) * tr); GJ_CUDA(err, cudaMemcpyAsync(he.data(), ebuf.p, he.size() * sizeof(T), cudaMemcpyDeviceToHost, st)); }
     GJ_CUDA(err, cudaStreamSynchronize(st));
-    c.timer.collect();
     if (misfit_out)
       for (int s = 0; s < nshots; ++s)
         misfit_out[s] = hsums[2 * s + 1] > 0 ? 0.5 * hsums[2 * s] / hsums[2 * s + 1] : 0.5 * hsums[2 * s];
@@ -484,127 +458,244 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
-  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
-                     bool dev_dobs, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
-                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
-    const int nrr = std::max(nr, 1);
-    const size_t tr = size_t(nrr) * g.nt;  // trace elements per shot
-    GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
-    if (o.plain) return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
-    // memory plan
-    size_t free_b = 0, total_b = 0;
-    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
-    choose_k(o, free_b + hist.bytes + ckpt.bytes);
-    const bool full = (K >= g.nt);
-    std::vector<std::pair<int, int>> segs = segments();
-    int maxlen = 0;
-    for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
-    hist_slots = full ? size_t(g.nt + 1) : size_t(maxlen + 3);
-    GJ_TRY(hist.alloc(err, hist_slots * nshots * mn * sizeof(T)));
-    n_ckpt = full ? 0 : segs.size();
-    if (!full) GJ_TRY(ckpt.alloc(err, n_ckpt * nshots * sstride * sizeof(T)));
-    GJ_TRY(adjA.alloc(err, size_t(nshots) * sstride * sizeof(T)));
-    GJ_TRY(adjB.alloc(err, size_t(nshots) * sstride * sizeof(T)));
-    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * mn * sizeof(T)));
-    T* H = hist.as<T>();
-    const size_t hs = mn;  // per-shot stride inside a slot
-    auto slot_ptr = [&](long k, long base) { return H + size_t(k - base) * nshots * hs; };
-    const int kahan = o.no_kahan ? 0 : 1;
+  // ---------------------------------------------------------------- groups
+  // Shots are processed in groups of G: every group runs the whole gradient
+  // (forward, residual, recompute, adjoint) before the next starts, so the
+  // fields of one group can stay resident in L2.  State, checkpoint and
+  // history buffers are sized for one group; traces and accumulators hold all
+  // shots.
+  int G = 0;
+  struct GraphRec {
+    cudaGraphExec_t exec = nullptr;
+    std::unique_ptr<Marks> marks;
+    long launches = 0;
+    ~GraphRec() { if (exec) cudaGraphExecDestroy(exec); }
+  };
+  std::map<std::string, std::unique_ptr<GraphRec>> graphs;
 
-    // ---- forward (with checkpoints at segment starts) ----
-    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
+  void drop_graphs() { graphs.clear(); }
+
+  // Shot-group size.  Keeping the whole u history in HBM saves the recompute
+  // pass (about a third of the work), so the default is the largest group
+  // whose history fits the memory budget, as long as a group still fills the
+  // GPU (at least 8 shots, or all of them); otherwise all shots at once with
+  // checkpoints.
+  int choose_group(const gj_w_opts& o, size_t free_bytes) const {
+    if (o.shots_per_launch > 0) return std::min(o.shots_per_launch, nshots);
+    if (const char* e = getenv("GJ_SHOTS_PER_GROUP")) {
+      const int v = atoi(e);
+      if (v > 0) return std::min(v, nshots);
+    }
+    if (o.ckpt_every > 0) return nshots;
+    const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.8 * double(free_bytes));
+    const size_t per_shot = (size_t(g.nt + 1) * dn + 4 * sstride) * sizeof(T);
+    const int fit = int(std::min<size_t>(budget / std::max<size_t>(per_shot, 1), size_t(nshots)));
+    if (fit >= nshots) return nshots;
+    if (fit >= std::min(8, nshots)) {
+      const int ngroups = (nshots + fit - 1) / fit;  // balance the groups
+      return (nshots + ngroups - 1) / ngroups;
+    }
+    return nshots;
+  }
+
+  // Columns per block for a launch of `ns` shots: enough blocks for ~48 warps per SM.
+  int tj_for(int ns) const {
+    constexpr int V = VT<T>::V;
+    const long bxs = (NX + 1 + 128 * V - 1) / (128 * V);
+    int t = 64;
+    while (t > 2 && bxs * ((NY + t) / t) * ns < 148L * 12) t /= 2;
+    return t;
+  }
+
+  // Enqueues the whole gradient of shots [g0, g0+gn) on stream st.
+  gj_status enqueue_group(Err& err, Ctx& c, int g0, int gn, gj_adj_mode mode, int kahan,
+                          const std::vector<std::pair<int, int>>& segs, bool full, long& nl, cudaStream_t st) {
+    const int nrr = std::max(nr, 1), nt = g.nt;
+    const size_t tr = size_t(nrr) * nt;
+    constexpr int V = VT<T>::V;
+    const int tjg = tj_for(gn);
+    const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + tjg - 1) / tjg, gn);
+    T* H = hist.as<T>();
+    const size_t hs = dn;
+    auto slot_ptr = [&](long k, long base) { return H + size_t(k - base) * gn * hs; };
+    const long* rec = recbuf.as<long>() + size_t(g0) * nrr;
+    const int* nrs_d = nrsbuf.as<int>() + g0;
+    const int* sel = selbuf.as<int>() + size_t(g0) * nrr;
+    const int* nsel_d = nselbuf.as<int>() + g0;
+    T* dgrp = dbuf.as<T>() + size_t(g0) * tr;
+    T* egrp = ebuf.as<T>() + size_t(g0) * tr;
     T* A = fwdA.as<T>() + ld;
     T* B = fwdB.as<T>() + ld;
-    const dim3 grd = grid_dims();
-    if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, nshots * hs * sizeof(T), st));  // slot 0 = zero state
+    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, gn * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, gn * sstride * sizeof(T), st));
+    if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, gn * hs * sizeof(T), st));  // slot 0 = zero state
     size_t segi = 0;
-    for (int it = 0; it < g.nt; ++it) {
+    for (int it = 0; it < nt; ++it) {
       if (!full && segi < segs.size() && it == segs[segi].first) {
-        GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * nshots * sstride, A - ld,
-                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * gn * sstride, A - ld, gn * sstride * sizeof(T),
+                                     cudaMemcpyDeviceToDevice, st));
         ++segi;
       }
       StepArgs<T> a = step_args(A, B, it);
+      a.shot0 = g0; a.tj = tjg;
       if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
-      c.timer.begin(KK_FWD_STEP, st);
-      k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
-      c.timer.end(st);
-      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
-                                                   g.nt, dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
-      c.launches += 2;
+      const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
+      k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+      c.timer.end(tm, st);
+      k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, rec, nrr, nrs_d, it, nt, dgrp, d_src + g0,
+                                               static_cast<T*>(nullptr), gn);
+      nl += 2;
       std::swap(A, B);
     }
-    GJ_CUDA(err, cudaGetLastError());
-    // ---- residual and misfit ----
-    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
-    k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr, sums.as<double>());
-    ++c.launches;
-    std::vector<double> hsums(2 * nshots);
-    GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
-    // ---- adjoint ----
-    GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * mn * sizeof(T), st));
+    k_residual<T><<<dim3(64, gn), 256, 0, st>>>(dgrp, dobsbuf.as<T>() + size_t(g0) * tr, egrp, tr,
+                                                sums.as<double>() + 2 * g0);
+    ++nl;
     T* LA = adjA.as<T>() + ld;
     T* LB = adjB.as<T>() + ld;
-    const int nt = g.nt;
+    GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, gn * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, gn * sstride * sizeof(T), st));
     for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
       const int s0 = segs[sidx].first, s1 = segs[sidx].second;
       long base = 0;
       if (!full) {
-        // restore the checkpoint and recompute slots s0..min(s1+1, nt)
         base = s0;
-        GJ_CUDA(err, cudaMemcpyAsync(A - ld, ckpt.as<T>() + size_t(sidx) * nshots * sstride,
-                                     nshots * sstride * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        k_domain_copy<T><<<dim3(64, nshots), 256, 0, st>>>(w, A, sstride, slot_ptr(s0, base), hs, nshots);
-        ++c.launches;
+        GJ_CUDA(err, cudaMemcpyAsync(A - ld, ckpt.as<T>() + size_t(sidx) * gn * sstride, gn * sstride * sizeof(T),
+                                     cudaMemcpyDeviceToDevice, st));
+        k_domain_copy<T><<<dim3(64, gn), 256, 0, st>>>(w, A, sstride, slot_ptr(s0, base), hs, gn);
+        ++nl;
         const int iend = std::min(s1 + 1, nt);
         for (int it = s0; it < iend; ++it) {
           StepArgs<T> a = step_args(A, B, it);
+          a.shot0 = g0; a.tj = tjg;
           a.hist = slot_ptr(it + 1, base); a.hstride = hs;
-          c.timer.begin(KK_FWD_STEP, st);
-          k_step<T, 0><<<grd, bx, 0, st>>>(w, a);
-          c.timer.end(st);
-          ++c.launches;
+          const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
+          k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+          c.timer.end(tm, st);
+          ++nl;
           std::swap(A, B);
         }
       }
       for (int k = s1; k >= s0 + 1; --k) {  // k = history slot of forward step k-1
-        const int itf = k - 1;              // 0-based forward step
+        const int itf = k - 1;
         if (mode == GJ_ADJ_REFERENCE) {
           if (nr > 0)
-            k_inject_set<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), selbuf.as<int>(), nrr,
-                                                             nselbuf.as<int>(), ebuf.as<T>(), itf, nt, nshots);
+            k_inject_set<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, sel, nrr, nsel_d, egrp, itf, nt, gn);
           StepArgs<T> a = step_args(LA, LB, itf);
-          a.hist = nullptr;
+          a.shot0 = g0; a.tj = tjg; a.hist = nullptr;
           int k0, k1, k2; double c0, c1, c2;
           ddt_stencil(k, k0, k1, k2, c0, c1, c2);
           a.u0 = slot_ptr(k0, base); a.u1 = slot_ptr(k1, base); a.u2 = slot_ptr(k2, base);
           a.c0 = T(c0); a.c1 = T(c1); a.c2 = T(c2);
           a.uk = slot_ptr(k, base);
           a.hstride = hs;
-          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = kahan;
-          c.timer.begin(KK_REF_STEP, st);
-          k_step<T, 1><<<grd, bx, 0, st>>>(wr, a);
-          c.timer.end(st);
+          a.acc = acc.as<T>(); a.astride = 4 * dn; a.kahan = kahan;
+          const bool tm = c.timer.begin(KK_REF_STEP, st, gn);
+          k_stepv<T, 1><<<grd, 128, 0, st>>>(wr, a);
+          c.timer.end(tm, st);
         } else {
           if (nr > 0)
-            k_inject_add<T><<<dim3(1, nshots), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(),
-                                                             ebuf.as<T>(), itf, nt, nshots);
+            k_inject_add<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, nrr, nrs_d, egrp, itf, nt, gn);
           AdjArgs<T> a{};
-          a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = 0; a.tj = tj;
+          a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = g0; a.tj = tjg;
           a.ek = slot_ptr(k, base); a.ekm1 = slot_ptr(k - 1, base); a.hstride = hs;
-          a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = kahan;
-          c.timer.begin(KK_ADJ_STEP, st);
-          k_adj_step<T><<<grd, bx, 0, st>>>(w, a);
-          c.timer.end(st);
+          a.acc = acc.as<T>(); a.astride = 4 * dn; a.kahan = kahan;
+          const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
+          k_adj_stepv<T><<<grd, 128, 0, st>>>(w, a);
+          c.timer.end(tm, st);
         }
-        c.launches += 2;
+        nl += 2;
         std::swap(LA, LB);
       }
     }
     GJ_CUDA(err, cudaGetLastError());
+    return GJ_OK;
+  }
+
+  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
+                     bool dev_dobs, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
+                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+    GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
+    if (o.plain) return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
+    // memory plan for one group
+    size_t free_b = 0, total_b = 0;
+    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
+    const size_t owned = hist.bytes + ckpt.bytes + (G > 0 ? 4 * size_t(G) * sstride * sizeof(T) : 0);
+    const int Gnew = choose_group(o, free_b + owned);
+    const int ns_save = nshots;
+    nshots = Gnew;  // choose_k sizes buffers per group
+    const int Kold = K;
+    choose_k(o, free_b + owned);
+    nshots = ns_save;
+    if (Gnew != G || K != Kold) drop_graphs();
+    G = Gnew;
+    const bool full = (K >= g.nt);
+    std::vector<std::pair<int, int>> segs = segments();
+    int maxlen = 0;
+    for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
+    hist_slots = full ? size_t(g.nt + 1) : size_t(maxlen + 3);
+    const size_t hbytes = hist_slots * G * dn * sizeof(T);
+    const size_t cbytes = full ? 0 : segs.size() * G * sstride * sizeof(T);
+    void* old[5] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p};
+    GJ_TRY(hist.alloc(err, hbytes));
+    if (!full) GJ_TRY(ckpt.alloc(err, cbytes));
+    GJ_TRY(fwdA.alloc(err, size_t(G) * sstride * sizeof(T)));
+    GJ_TRY(fwdB.alloc(err, size_t(G) * sstride * sizeof(T)));
+    GJ_TRY(adjA.alloc(err, size_t(G) * sstride * sizeof(T)));
+    GJ_TRY(adjB.alloc(err, size_t(G) * sstride * sizeof(T)));
+    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
+    void* nw[5] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p};
+    for (int q = 0; q < 5; ++q)
+      if (old[q] != nw[q]) { drop_graphs(); break; }
+    const int kahan = o.no_kahan ? 0 : 1;
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
+    long nl = 0;
+    for (int g0 = 0; g0 < nshots; g0 += G) {
+      const int gn = std::min(G, nshots - g0);
+      if (o.no_graph) {
+        Marks m;
+        c.timer.cur = &m;
+        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st);
+        c.timer.cur = nullptr;
+        GJ_TRY(rs);
+        GJ_CUDA(err, cudaStreamSynchronize(st));
+        c.timer.collect(m);
+        continue;
+      }
+      char kb[96];
+      snprintf(kb, sizeof kb, "%d/%d/%d/%d/%d/%d/%d", g0, gn, int(mode), kahan, K, G, c.timer.on ? 1 : 0);
+      auto itg = graphs.find(kb);
+      if (itg == graphs.end()) {
+        auto rec = std::make_unique<GraphRec>();
+        rec->marks = std::make_unique<Marks>();
+        cudaStream_t cs;
+        GJ_CUDA(err, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        GJ_CUDA(err, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        c.timer.cur = rec->marks.get();
+        long cnt = 0;
+        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, cnt, cs);
+        c.timer.cur = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+        cudaStreamDestroy(cs);
+        GJ_TRY(rs);
+        if (ce != cudaSuccess) return err.set(GJ_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&rec->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return err.set(GJ_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+        rec->launches = cnt;
+        itg = graphs.emplace(kb, std::move(rec)).first;
+      }
+      GJ_CUDA(err, cudaGraphLaunch(itg->second->exec, st));
+      nl += itg->second->launches;
+      if (c.timer.on) {
+        GJ_CUDA(err, cudaStreamSynchronize(st));
+        c.timer.collect(*itg->second->marks);
+      }
+    }
+    c.launches += nl;
+    std::vector<double> hsums(2 * nshots);
+    GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
     return finish(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, hsums, st);
   }
 
@@ -626,12 +717,12 @@ class WSolver : public WSolverBase {
     int maxlen = 0;
     for (auto& q : segs) maxlen = std::max(maxlen, q.second - q.first);
     hist_slots = full ? size_t(nt + 1) : size_t(maxlen + 3);
-    GJ_TRY(hist.alloc(err, hist_slots * mn * sizeof(T)));
+    GJ_TRY(hist.alloc(err, hist_slots * dn * sizeof(T)));
     if (!full) GJ_TRY(ckpt.alloc(err, segs.size() * sstride * sizeof(T)));
     GJ_TRY(adjA.alloc(err, sstride * sizeof(T)));
-    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * mn * sizeof(T)));
+    GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
     GJ_TRY(scratch.alloc(err, 5 * fstride * sizeof(T)));
-    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * mn * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(scratch.p, 0, 5 * fstride * sizeof(T), st));
     T* px = scratch.as<T>() + ld; T* py = px + fstride; T* lm = py + fstride; T* qx = lm + fstride; T* qy = qx + fstride;
     std::vector<T> hcezj(nshots), hwav(size_t(nshots) * nt);
@@ -641,20 +732,22 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     const dim3 blk(32, 8), grd((NX + 1 + 31) / 32, (NY + 1 + 7) / 8);
     T* H = hist.as<T>();
-    auto slot = [&](long k, long base) { return H + size_t(k - base) * mn; };
+    auto slot = [&](long k, long base) { return H + size_t(k - base) * dn; };
     T* S = fwdA.as<T>() + ld;  // shot state (in place)
     T* L = adjA.as<T>() + ld;
+    Marks marks;
+    c.timer.cur = &marks;
     for (int s = 0; s < nshots; ++s) {
       const long src = sh[s].src;
       auto fwd_step = [&](int it, T* hslot) {
-        c.timer.begin(KK_PLAIN, st);
+        const bool tm = c.timer.begin(KK_PLAIN, st);
         k_plain_h<T><<<grd, blk, 0, st>>>(w, S, fstride);
         k_plain_e<T><<<grd, blk, 0, st>>>(w, S, fstride, src, hcezj[s] * hwav[size_t(s) * nt + it], hslot);
-        c.timer.end(st);
+        c.timer.end(tm, st);
         c.launches += 2;
       };
       GJ_CUDA(err, cudaMemsetAsync(S - ld, 0, sstride * sizeof(T), st));
-      if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, mn * sizeof(T), st));
+      if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, dn * sizeof(T), st));
       size_t segi = 0;
       for (int it = 0; it < nt; ++it) {
         if (!full && segi < segs.size() && it == segs[segi].first) {
@@ -672,7 +765,7 @@ class WSolver : public WSolverBase {
                                                   ebuf.as<T>() + size_t(s) * tr, tr, sums.as<double>() + 2 * s);
       ++c.launches;
       GJ_CUDA(err, cudaMemsetAsync(L - ld, 0, sstride * sizeof(T), st));
-      T* A_ = acc.as<T>() + size_t(s) * 4 * mn;
+      T* A_ = acc.as<T>() + size_t(s) * 4 * dn;
       for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
         const int s0 = segs[sidx].first, s1 = segs[sidx].second;
         long base = 0;
@@ -680,13 +773,13 @@ class WSolver : public WSolverBase {
           base = s0;
           GJ_CUDA(err, cudaMemcpyAsync(S - ld, ckpt.as<T>() + size_t(sidx) * sstride, sstride * sizeof(T),
                                        cudaMemcpyDeviceToDevice, st));
-          k_domain_copy<T><<<dim3(64, 1), 256, 0, st>>>(w, S, sstride, slot(s0, base), mn, 1);
+          k_domain_copy<T><<<dim3(64, 1), 256, 0, st>>>(w, S, sstride, slot(s0, base), dn, 1);
           ++c.launches;
           for (int it = s0; it < std::min(s1 + 1, nt); ++it) fwd_step(it, slot(it + 1, base));
         }
         for (int k = s1; k >= s0 + 1; --k) {
           const int itf = k - 1;
-          c.timer.begin(KK_PLAIN, st);
+          const bool tm = c.timer.begin(KK_PLAIN, st);
           if (mode == GJ_ADJ_REFERENCE) {
             k_inject_set<T><<<dim3(1, 1), 128, 0, st>>>(L, sstride, recbuf.as<long>() + size_t(s) * nrr,
                                                         selbuf.as<int>() + size_t(s) * nrr, nrr, nselbuf.as<int>() + s,
@@ -706,14 +799,17 @@ class WSolver : public WSolverBase {
             k_plain_adj_assemble<T><<<grd, blk, 0, st>>>(w, L, lm, qx, qy);
             c.launches += 4;
           }
-          c.timer.end(st);
+          c.timer.end(tm, st);
         }
       }
     }
+    c.timer.cur = nullptr;
     GJ_CUDA(err, cudaGetLastError());
     std::vector<double> hsums(2 * nshots);
     GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
-    return finish(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, hsums, st);
+    gj_status r = finish(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, hsums, st);
+    c.timer.collect(marks);
+    return r;
   }
 
   // ------------------------------------------------------------ w_grad only
@@ -732,38 +828,45 @@ class WSolver : public WSolverBase {
       for (int t = 0; t < nt; ++t) he[size_t(r) * nt + t] = T(e[size_t(r) * nt + t]);
     GJ_CUDA(err, cudaMemcpy(ebuf.p, he.data(), he.size() * sizeof(T), cudaMemcpyHostToDevice));
     // u: host m x n x nt -> device slots 1..nt (slot 0 unused)
-    GJ_TRY(hist.alloc(err, size_t(nt + 1) * mn * sizeof(T)));
+    GJ_TRY(hist.alloc(err, size_t(nt + 1) * dn * sizeof(T)));
     {
-      std::vector<T> hu(size_t(nt) * mn);
-      for (size_t i = 0; i < hu.size(); ++i) hu[i] = T(u[i]);
-      GJ_CUDA(err, cudaMemcpy(hist.as<T>() + mn, hu.data(), hu.size() * sizeof(T), cudaMemcpyHostToDevice));
+      // host m x n x nt -> device slots 1..nt in the domain-node layout
+      std::vector<T> hu(size_t(nt) * dn, T(0));
+      for (int t = 0; t < nt; ++t)
+        for (int b = 0; b < g.n; ++b)
+          for (int a_ = 0; a_ < g.m; ++a_)
+            hu[size_t(t) * dn + size_t(b) * ld + w.di0 + a_] = T(u[size_t(t) * mn + size_t(b) * g.m + a_]);
+      GJ_CUDA(err, cudaMemcpy(hist.as<T>() + dn, hu.data(), hu.size() * sizeof(T), cudaMemcpyHostToDevice));
     }
     GJ_TRY(adjA.alloc(err, sstride * sizeof(T)));
     GJ_TRY(adjB.alloc(err, sstride * sizeof(T)));
-    GJ_TRY(acc.alloc(err, 4 * mn * sizeof(T)));
+    GJ_TRY(acc.alloc(err, 4 * dn * sizeof(T)));
     GJ_CUDA(err, cudaMemset(adjA.p, 0, sstride * sizeof(T)));
     GJ_CUDA(err, cudaMemset(adjB.p, 0, sstride * sizeof(T)));
-    GJ_CUDA(err, cudaMemset(acc.p, 0, 4 * mn * sizeof(T)));
+    GJ_CUDA(err, cudaMemset(acc.p, 0, 4 * dn * sizeof(T)));
     T* LA = adjA.as<T>() + ld;
     T* LB = adjB.as<T>() + ld;
-    const dim3 grd = grid_dims();
+    constexpr int V = VT<T>::V;
+    const int tjf = tj_for(1);
+    const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + tjf - 1) / tjf, 1);
     for (int k = nt; k >= 1; --k) {
       if (nr > 0)
         k_inject_set<T><<<dim3(1, 1), 128, 0, st>>>(LA, sstride, recbuf.as<long>(), selbuf.as<int>(), nrr,
                                                     nselbuf.as<int>(), ebuf.as<T>(), k - 1, nt, 1);
       StepArgs<T> a = step_args(LA, LB, k - 1);
-      T* uk = hist.as<T>() + size_t(k) * mn;
+      T* uk = hist.as<T>() + size_t(k) * dn;
       a.u0 = uk; a.u1 = uk; a.u2 = uk; a.c0 = T(0); a.c1 = T(0); a.c2 = T(0);
-      a.uk = uk; a.hstride = mn;
-      a.acc = acc.as<T>(); a.astride = 4 * mn; a.kahan = 1;
-      k_step<T, 1><<<grd, bx, 0, st>>>(wr, a);
+      a.uk = uk; a.hstride = dn;
+      a.acc = acc.as<T>(); a.astride = 4 * dn; a.kahan = 1;
+      a.tj = tjf;
+      k_stepv<T, 1><<<grd, 128, 0, st>>>(wr, a);
       c.launches += 2;
       std::swap(LA, LB);
     }
     GJ_CUDA(err, cudaGetLastError());
     DevBuf gb;
     GJ_TRY(gb.alloc(err, 2 * mn * sizeof(double)));
-    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * mn, 1, 0, 0, g.dt, g.eps0, eps_m, sig_m,
+    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, 1, 0, 0, g.dt, g.eps0, eps_m, sig_m,
                                      gb.as<double>(), gb.as<double>() + mn);
     GJ_CUDA(err, cudaGetLastError());
     GJ_CUDA(err, cudaDeviceSynchronize());

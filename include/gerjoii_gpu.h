@@ -171,14 +171,17 @@ gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* eps_dev, cons
  * benchmark's launch count).  Graph launches count the kernels they contain. */
 long gj_last_launch_count(const gj_ctx* ctx);
 
-/* Per-kernel device timing (CUDA events around each launch of the hot
- * kernels), accumulated over calls while enabled.  kind: 0 forward Yee step,
- * 1 reference-adjoint step, 2 exact-adjoint step, 3 receiver I/O, 4 plain
- * kernels, 5 DC kernels.  gj_kernel_time returns the summed milliseconds and
- * the number of timed launches.  No counterpart in the reference (MATLAB
- * tic/toc around whole phases, w_begin_.m:74-76). */
+/* Per-kernel device timing, accumulated over calls while enabled: CUDA events
+ * around every 8th launch of each hot kernel (inside captured graphs too).
+ * kind: 0 forward Yee step, 1 reference-adjoint step, 2 exact-adjoint step,
+ * 3 receiver I/O, 4 plain kernels, 5 DC kernels.  gj_kernel_time returns the
+ * summed milliseconds of the timed launches (ms / sampled is the average
+ * launch duration), the number of launches of that kind, and the sum over
+ * those launches of the shots each one advanced.  No counterpart in the
+ * reference (MATLAB tic/toc around whole phases, w_begin_.m:74-76). */
 gj_status gj_set_kernel_timing(gj_ctx* ctx, int on);
-gj_status gj_kernel_time(const gj_ctx* ctx, int kind, double* ms, long* launches);
+gj_status gj_kernel_time(const gj_ctx* ctx, int kind, double* ms, long* sampled, long* launches,
+                         long* shot_launches);
 
 #ifdef __cplusplus
 }
