@@ -38,6 +38,26 @@ class ShotC(C.Structure):
                 ("nr", C.c_int), ("rec", C.POINTER(C.c_long))]
 
 
+class DcGridC(C.Structure):
+    _fields_ = [("n", C.c_int), ("m", C.c_int), ("robin", C.c_int), ("n_ky", C.c_int), ("dx", C.c_double),
+                ("dz", C.c_double)]
+
+
+class DcSrcC(C.Structure):
+    _fields_ = [("a", C.c_long), ("b", C.c_long), ("current", C.c_double), ("nd", C.c_int),
+                ("mn", C.POINTER(C.c_long)), ("ky", C.POINTER(C.c_double)), ("w", C.POINTER(C.c_double)),
+                ("alpha", C.POINTER(C.c_double)), ("d_obs", C.POINTER(C.c_double))]
+
+
+class DcOptsC(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("per_source", C.c_int),
+                ("sources_per_batch", C.c_int), ("mem_budget_bytes", C.c_size_t)]
+
+
+class DcStatsC(C.Structure):
+    _fields_ = [("max_iterations", C.c_int), ("max_rel_residual", C.c_double)]
+
+
 class OptsC(C.Structure):
     _fields_ = [("ckpt_every", C.c_int), ("mem_budget_bytes", C.c_size_t),
                 ("shots_per_launch", C.c_int), ("no_kahan", C.c_int), ("no_graph", C.c_int),
@@ -60,6 +80,10 @@ SIGNATURES = {
     "gj_w_grad": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _DP, _DP, _DP, _DP]),
     "gj_w_gradient_dev": (_I, [_VP, C.POINTER(GridC), _I, _VP, _VP, C.POINTER(ShotC), _I, _VP, _I, _I,
                                C.POINTER(OptsC), _VP, _VP, _DP, _VP]),
+    "gj_dc_forward": (_I, [_VP, C.POINTER(DcGridC), _DP, C.POINTER(DcSrcC), _I, C.POINTER(DcOptsC), _DP, _DP,
+                           C.POINTER(DcStatsC)]),
+    "gj_dc_gradient": (_I, [_VP, C.POINTER(DcGridC), _DP, C.POINTER(DcSrcC), _I, C.POINTER(DcOptsC), _DP, _DP, _DP,
+                            _DP, C.POINTER(DcStatsC)]),
     "gj_w_forward_noalloc": (_I, [C.POINTER(GridC), _VP, _VP, _I, _I, _VP, _I, _VP, _VP, _VP, C.c_char_p,
                                   C.c_size_t]),
 }
@@ -239,6 +263,67 @@ class Context:
         self._check(self.lib.gj_w_grad(self.h, C.byref(gc), precision, _dp(_f(eps)), _dp(_f(sig)), sp.arr,
                                        _dp(ea), _dp(ua), _dp(out), _dp(amax)))
         return out.reshape((g.m, g.n), order="F"), amax.reshape((g.m, g.n), order="F")
+
+    # --------------------------------------------------------------------- DC
+    @staticmethod
+    def _dc_pack(srcs, with_dobs):
+        keep, arr = [], (DcSrcC * len(srcs))()
+        for k, q in enumerate(srcs):
+            mn = np.ascontiguousarray(np.asarray(q.mn, np.int64).reshape(-1, 2))
+            ky = np.ascontiguousarray(q.ky_w[:, 0], np.float64)
+            w = np.ascontiguousarray(q.ky_w[:, 1], np.float64)
+            al = np.ascontiguousarray(q.alpha, np.float64)
+            do = np.ascontiguousarray(q.d_obs, np.float64) if (with_dobs and q.d_obs is not None) else None
+            keep += [mn, ky, w, al, do]
+            arr[k].a, arr[k].b, arr[k].current, arr[k].nd = int(q.a), int(q.b), float(q.current), len(mn)
+            arr[k].mn = mn.ctypes.data_as(C.POINTER(C.c_long))
+            arr[k].ky = ky.ctypes.data_as(_DP)
+            arr[k].w = w.ctypes.data_as(_DP)
+            arr[k].alpha = al.ctypes.data_as(_DP)
+            arr[k].d_obs = do.ctypes.data_as(_DP) if do is not None else None
+        return arr, keep
+
+    def dc_forward(self, sigma_robin, dx, dz, robin, srcs, opts=None, want_u=False):
+        """Data per source (list of nd arrays), optional stacked u (nsrc x n x m), stats."""
+        n, m = sigma_robin.shape
+        g = DcGridC(n, m, robin, len(srcs[0].ky_w), dx, dz)
+        arr, keep = self._dc_pack(srcs, False)
+        nd = sum(q.nd for q in srcs)
+        d = np.zeros(max(nd, 1))
+        u = np.zeros(len(srcs) * n * m) if want_u else None
+        st = DcStatsC()
+        sg = np.asfortranarray(sigma_robin, np.float64)
+        self._check(self.lib.gj_dc_forward(self.h, C.byref(g), _dp(sg), arr, len(srcs),
+                                           C.byref(opts) if opts else None, _dp(d), _dp(u), C.byref(st)))
+        out, o = [], 0
+        for q in srcs:
+            out.append(d[o:o + q.nd].copy())
+            o += q.nd
+        res = {"d": out, "iters": st.max_iterations, "rel_residual": st.max_rel_residual}
+        if want_u:
+            res["u"] = u.reshape((len(srcs), m, n)).transpose(0, 2, 1)
+        return res
+
+    def dc_gradient(self, sigma_robin, dx, dz, robin, srcs, opts=None):
+        """Gradient (n-2robin x m-robin, summed or per source), data, residuals, misfits, stats."""
+        n, m = sigma_robin.shape
+        g = DcGridC(n, m, robin, len(srcs[0].ky_w), dx, dz)
+        arr, keep = self._dc_pack(srcs, True)
+        nd = sum(q.nd for q in srcs)
+        per = len(srcs) if (opts is not None and opts.per_source) else 1
+        n0, m0 = n - 2 * robin, m - robin
+        gout = np.zeros(per * n0 * m0)
+        d = np.zeros(max(nd, 1))
+        e = np.zeros(max(nd, 1))
+        mis = np.zeros(len(srcs))
+        st = DcStatsC()
+        sg = np.asfortranarray(sigma_robin, np.float64)
+        self._check(self.lib.gj_dc_gradient(self.h, C.byref(g), _dp(sg), arr, len(srcs),
+                                            C.byref(opts) if opts else None, _dp(gout), _dp(d), _dp(e), _dp(mis),
+                                            C.byref(st)))
+        gg = gout.reshape((per, m0, n0)).transpose(0, 2, 1)
+        return {"g": gg[0] if per == 1 else gg, "d": d[:nd], "e": e[:nd], "misfit": mis,
+                "iters": st.max_iterations, "rel_residual": st.max_rel_residual}
 
     def w_gradient_dev(self, g, eps_t, sig_t, shots, dobs_t, ge_t, gs_t, mode=GJ_ADJ_REFERENCE,
                        misfit=GJ_MISFIT_L2, opts=None, stream=0):

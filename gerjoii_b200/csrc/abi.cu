@@ -111,4 +111,23 @@ gj_status gj_w_grad(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, 
   return gj::w_grad_only(ctx->c, *grid, precision, eps_r, sigma, *shot, e, u, g, a_max);
 }
 
+gj_status gj_dc_forward(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma, const gj_dc_src* srcs, int nsrc,
+                        const gj_dc_opts* opts, double* d_out, double* u_out, gj_dc_stats* stats) {
+  GJ_TRY(guard_ctx(ctx));
+  if (!grid) return ctx->c.err.set(GJ_EINVAL, "null grid");
+  gj_dc_opts o{};
+  if (opts) o = *opts;
+  return gj::dc_run(ctx->c, *grid, sigma, srcs, nsrc, false, o, d_out, nullptr, u_out, nullptr, nullptr, stats);
+}
+
+gj_status gj_dc_gradient(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma, const gj_dc_src* srcs, int nsrc,
+                         const gj_dc_opts* opts, double* g_out, double* d_out, double* e_out, double* misfit_out,
+                         gj_dc_stats* stats) {
+  GJ_TRY(guard_ctx(ctx));
+  if (!grid || !g_out) return ctx->c.err.set(GJ_EINVAL, "null grid or gradient output");
+  gj_dc_opts o{};
+  if (opts) o = *opts;
+  return gj::dc_run(ctx->c, *grid, sigma, srcs, nsrc, true, o, d_out, e_out, nullptr, g_out, misfit_out, stats);
+}
+
 }  // extern "C"

@@ -1,0 +1,339 @@
+// 2.5D DC-resistivity kernels for sm_100a.
+//
+// One "system" is the operator Lk of one (source, ky) pair (dc_Lk.m:809):
+//   Lk = -L + ky^2 diag(sigma), L the 5-point finite-volume operator with
+//   harmonic-mean face conductances, a Neumann top and Robin sides/bottom.
+// The off-diagonals are shared by all systems; the diagonal carries ky^2 sigma
+// and the source- and ky-dependent Robin ghost terms.
+//
+// Unknowns are ordered with the shorter grid direction fastest, so the matrix
+// is banded with half-bandwidth b = min(n, m).  The preconditioner is the FP32
+// LDL^T factor of that band (incomplete Cholesky with fill allowed inside the
+// band, i.e. complete within it), computed by one CTA per system with a
+// rolling (b+1) x (b+1) window in shared memory.  CG runs in FP64 with that
+// preconditioner, which is the FP64 iterative refinement of the FP32 solve.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gj {
+
+// Grid and ordering.  Node (l, h): l lateral in [0, n), h depth in [0, m)
+// (the reference's (l, h) minus one); vectorised reference index l + h*n.
+struct DcGrid {
+  int n, m, N;      // nodes per direction, total
+  int b;            // half-bandwidth = min(n, m)
+  int depth_fast;   // 1: band index q = h + l*m (b = m); 0: q = l + h*n (b = n)
+  double DX, DZ;    // DELTAS(:,:,1), DELTAS(:,:,2) as the reference computes them
+  int nb;           // compact Robin entries per system: 2(m-2) + (n-2) + 4
+};
+
+__device__ __forceinline__ int dc_q(const DcGrid& G, int l, int h) {
+  return G.depth_fast ? h + l * G.m : l + h * G.n;
+}
+
+// Face conductances of Lk (shared): ox(l,h) = Lk((l,h),(l+1,h)) = H*DZ/DX,
+// oz(l,h) = Lk((l,h),(l,h+1)) = H*DX/DZ, H = 2 s_i s_j / (s_i + s_j)
+// (dc_Lk.m:112-155 with -Lk), and dbase = -(sum of the node's offdiagonals).
+__global__ void k_dc_faces(const DcGrid G, const double* sig, double* ox, double* oz, double* dbase) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= G.n * G.m) return;
+  const int l = t % G.n, h = t / G.n;  // reference layout (lateral fastest)
+  const double s = sig[t];
+  double d = 0;
+  if (l + 1 < G.n) {
+    const double s2 = sig[t + 1];
+    const double v = 2.0 * s * s2 / (s + s2) * (G.DZ / G.DX);
+    ox[t] = v; d -= v;
+  } else ox[t] = 0;
+  if (l >= 1) {
+    const double s2 = sig[t - 1];
+    d -= 2.0 * s * s2 / (s + s2) * (G.DZ / G.DX);
+  }
+  if (h + 1 < G.m) {
+    const double s2 = sig[t + G.n];
+    const double v = 2.0 * s * s2 / (s + s2) * (G.DX / G.DZ);
+    oz[t] = v; d -= v;
+  } else oz[t] = 0;
+  if (h >= 1) {
+    const double s2 = sig[t - G.n];
+    d -= 2.0 * s * s2 / (s + s2) * (G.DX / G.DZ);
+  }
+  dbase[t] = d;
+}
+
+// Robin ghost coefficient "face * alpha" of node (l, h) for one system, from
+// the compact array [left h=1..m-2 | bottom l=1..n-2 | right h=1..m-2 |
+// c11 c21 c12 c22] (dc_Lk.m:236-520, alphas :945-960).  MM5 = -sigma * this.
+__device__ __forceinline__ double dc_robin_fa(const DcGrid& G, const double* al, int l, int h) {
+  const int n = G.n, m = G.m;
+  if (h >= 1 && h <= m - 2) {
+    if (l == 0) return G.DZ * al[h - 1];
+    if (l == n - 1) return G.DZ * al[(m - 2) + (n - 2) + (h - 1)];
+    return 0.0;
+  }
+  if (h == m - 1) {
+    const int c = 2 * (m - 2) + (n - 2);
+    if (l >= 1 && l <= n - 2) return G.DX * al[(m - 2) + (l - 1)];
+    if (l == 0) return G.DZ * al[c + 0] + G.DX * al[c + 1];
+    if (l == n - 1) return G.DZ * al[c + 2] + G.DX * al[c + 3];
+  }
+  return 0.0;
+}
+
+// Diagonal of Lk at node (l, h) for one system.
+__device__ __forceinline__ double dc_diag(const DcGrid& G, const double* dbase, const double* sig,
+                                          const double* al, double ky2, int l, int h) {
+  const int t = l + h * G.n;
+  return dbase[t] - sig[t] * dc_robin_fa(G, al, l, h) + ky2 * sig[t];
+}
+
+// Band entry A(q, q-off) for off in {1, b}: the coupling to the previous node
+// along the fast direction (off = 1) or the slow direction (off = b).
+__device__ __forceinline__ double dc_sub(const DcGrid& G, const double* ox, const double* oz, int q, int off) {
+  if (G.depth_fast) {
+    const int l = q / G.m, h = q % G.m;
+    if (off == 1) return h >= 1 ? oz[l + (h - 1) * G.n] : 0.0;
+    return l >= 1 ? ox[(l - 1) + h * G.n] : 0.0;
+  }
+  const int l = q % G.n, h = q / G.n;
+  if (off == 1) return l >= 1 ? ox[(l - 1) + h * G.n] : 0.0;
+  return h >= 1 ? oz[l + (h - 1) * G.n] : 0.0;
+}
+
+__device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
+  if (G.depth_fast) { l = q / G.m; h = q % G.m; }
+  else { l = q % G.n; h = q / G.n; }
+}
+
+// FP32 band LDL^T of every system: one CTA per system.  Output per system:
+// N columns of (b+1) floats: [d_q, l_{q+1,q}, ..., l_{q+b,q}].
+// Shared memory: (b+1)^2 floats (rolling window) + (b+1) floats.
+__global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, const double* dbase,
+                            const double* sig, const double* alpha, const double* ky2, int sys0,
+                            float* fac, int* status) {
+  extern __shared__ float sh[];
+  const int W = G.b + 1;
+  float* win = sh;            // W x W, row-major, circular in both indices
+  float* lc = sh + W * W;     // current column
+  const int sys = blockIdx.x;
+  const double* al = alpha + size_t(sys0 + sys) * G.nb;
+  const double k2 = ky2[sys0 + sys];
+  float* F = fac + size_t(sys) * size_t(G.N) * W;
+  const int N = G.N, b = G.b;
+  // initial window: rows/cols 0..b of A (lower triangle)
+  for (int e = threadIdx.x; e < W * W; e += blockDim.x) win[e] = 0.f;
+  __syncthreads();
+  for (int r = threadIdx.x; r < W && r < N; r += blockDim.x) {
+    int l, h; dc_lh(G, r, l, h);
+    win[r * W + r] = float(dc_diag(G, dbase, sig, al, k2, l, h));
+    if (r >= 1) win[r * W + (r - 1)] = float(dc_sub(G, ox, oz, r, 1));
+    if (r >= b) win[r * W + (r - b)] = float(dc_sub(G, ox, oz, r, b));
+  }
+  __syncthreads();
+  for (int q = 0; q < N; ++q) {
+    const int p0 = q % W;
+    const float d = win[p0 * W + p0];
+    if (threadIdx.x == 0) {
+      F[size_t(q) * W] = d;
+      if (!(d != 0.f) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
+    }
+    for (int i = threadIdx.x + 1; i <= b; i += blockDim.x) {
+      const int pi = (q + i) % W;
+      const float li = (q + i < N) ? win[pi * W + p0] / d : 0.f;
+      lc[i] = li;
+      F[size_t(q) * W + i] = li;
+    }
+    __syncthreads();
+    // rank-1 update of rows/cols q+1..q+b: A(i,j) -= l_i d l_j, j <= i
+    for (int i = 1; i <= b; ++i) {
+      const float ci = lc[i] * d;
+      if (ci != 0.f) {
+        const int pi = (q + i) % W;
+        for (int j = threadIdx.x + 1; j <= i; j += blockDim.x) win[pi * W + (q + j) % W] -= ci * lc[j];
+      }
+    }
+    __syncthreads();
+    // slide: row/col q+b+1 of A enters at the slot of q
+    const int nr = q + b + 1;
+    for (int c = threadIdx.x; c < W; c += blockDim.x) win[p0 * W + c] = 0.f;
+    for (int r = threadIdx.x; r < W; r += blockDim.x) win[r * W + p0] = 0.f;
+    __syncthreads();
+    if (threadIdx.x == 0 && nr < N) {
+      int l, h; dc_lh(G, nr, l, h);
+      win[p0 * W + p0] = float(dc_diag(G, dbase, sig, al, k2, l, h));
+      win[p0 * W + (nr - 1) % W] = float(dc_sub(G, ox, oz, nr, 1));
+      win[p0 * W + (nr - b) % W] = float(dc_sub(G, ox, oz, nr, b));
+    }
+    __syncthreads();
+  }
+}
+
+// z = (L D L^T)^{-1} r for every system, one warp per system, and rz = r.z.
+// r, z are FP64 vectors in the reference layout [sys][l + h*n].  The rolling
+// windows (b+1 values) live in shared memory per warp.
+__global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, double* z, double* rz,
+                             int nsys, const int* done) {
+  extern __shared__ float shp[];
+  const int W = G.b + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sys = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (sys >= nsys || (done && done[sys])) return;
+  float* win = shp + warp * W;
+  const float* F = fac + size_t(sys) * size_t(G.N) * W;
+  const double* R = r + size_t(sys) * G.N;
+  double* Z = z + size_t(sys) * G.N;
+  const int N = G.N, b = G.b;
+  auto ref = [&](int q) { int l, h; dc_lh(G, q, l, h); return l + h * G.n; };
+  // forward: L y = r (column oriented), window holds partially reduced r
+  for (int i = lane; i < W; i += 32) win[i] = (i < N) ? float(R[ref(i)]) : 0.f;
+  __syncwarp();
+  for (int q = 0; q < N; ++q) {
+    const int p0 = q % W;
+    const float y = win[p0];
+    const float* Fq = F + size_t(q) * W;
+    for (int i = lane + 1; i <= b; i += 32)
+      if (q + i < N) win[(q + i) % W] -= Fq[i] * y;
+    __syncwarp();
+    if (lane == 0) {
+      // y_q / d_q stored in Z (band order) temporarily via the reference index
+      Z[ref(q)] = double(y / Fq[0]);
+      const int nq = q + W;
+      win[p0] = (nq < N) ? float(R[ref(nq)]) : 0.f;
+    }
+    __syncwarp();
+  }
+  // backward: L^T x = z, x_q = z_q - sum_i l_{q+i,q} x_{q+i}
+  for (int i = lane; i < W; i += 32) win[i] = 0.f;
+  __syncwarp();
+  double acc = 0.0;
+  for (int q = N - 1; q >= 0; --q) {
+    const float* Fq = F + size_t(q) * W;
+    float s = 0.f;
+    for (int i = lane + 1; i <= b; i += 32)
+      if (q + i < N) s += Fq[i] * win[(q + i) % W];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      const int rq = ref(q);
+      const float x = float(Z[rq]) - s;
+      win[q % W] = x;
+      Z[rq] = double(x);
+      acc += R[rq] * double(x);
+    }
+    __syncwarp();
+  }
+  if (lane == 0) rz[sys] = acc;
+}
+
+// y = Lk x for every system (FP64), optional dot x.y into dot[sys].
+__global__ void k_dc_apply(const DcGrid G, const double* ox, const double* oz, const double* dbase,
+                           const double* sig, const double* alpha, const double* ky2, int sys0,
+                           const double* x, double* y, double* dot, int nsys, const int* done) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys || (done && done[sys])) return;
+  const double* al = alpha + size_t(sys0 + sys) * G.nb;
+  const double k2 = ky2[sys0 + sys];
+  const double* X = x + size_t(sys) * G.N;
+  double* Y = y + size_t(sys) * G.N;
+  double part = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < G.N; t += blockDim.x * gridDim.x) {
+    const int l = t % G.n, h = t / G.n;
+    double v = dc_diag(G, dbase, sig, al, k2, l, h) * X[t];
+    if (l + 1 < G.n) v += ox[t] * X[t + 1];
+    if (l >= 1) v += ox[t - 1] * X[t - 1];
+    if (h + 1 < G.m) v += oz[t] * X[t + G.n];
+    if (h >= 1) v += oz[t - G.n] * X[t - G.n];
+    Y[t] = v;
+    part += v * X[t];
+  }
+  if (dot) {
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(dot + sys, part);
+  }
+}
+
+// CG update: alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = r.r
+__global__ void k_dc_cg_xr(int N, const double* rz, const double* pap, double* x, double* r, const double* p,
+                           const double* ap, double* rr, int nsys, const int* done) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys || (done && done[sys])) return;
+  const double den = pap[sys];
+  const double a = (den != 0.0) ? rz[sys] / den : 0.0;
+  const size_t o = size_t(sys) * N;
+  double part = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += blockDim.x * gridDim.x) {
+    x[o + t] += a * p[o + t];
+    const double v = r[o + t] - a * ap[o + t];
+    r[o + t] = v;
+    part += v * v;
+  }
+  for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(rr + sys, part);
+}
+
+// p = z + beta p with beta = rz_new / rz_old (p = z when first).
+__global__ void k_dc_cg_p(int N, const double* rz_new, const double* rz_old, const double* z, double* p,
+                          int first, int nsys, const int* done) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys || (done && done[sys])) return;
+  const double beta = first ? 0.0 : (rz_old[sys] != 0.0 ? rz_new[sys] / rz_old[sys] : 0.0);
+  const size_t o = size_t(sys) * N;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += blockDim.x * gridDim.x)
+    p[o + t] = z[o + t] + beta * p[o + t];
+}
+
+// r = b - y (FP64), rr = r.r, bb = b.b
+__global__ void k_dc_residual(int N, const double* bvec, const double* y, double* r, double* rr, double* bb,
+                              int nsys) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys) return;
+  const size_t o = size_t(sys) * N;
+  double p1 = 0, p2 = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += blockDim.x * gridDim.x) {
+    const double v = bvec[o + t] - y[o + t];
+    r[o + t] = v;
+    p1 += v * v;
+    p2 += bvec[o + t] * bvec[o + t];
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    p1 += __shfl_down_sync(0xffffffffu, p1, off);
+    p2 += __shfl_down_sync(0xffffffffu, p2, off);
+  }
+  if ((threadIdx.x & 31) == 0) { atomicAdd(rr + sys, p1); if (bb) atomicAdd(bb + sys, p2); }
+}
+
+// Sensitivity of one system (dc_Sk.m with dc_gradient2_5d.m:37-38):
+// g += (2/pi) w [ sum_faces ratio 2 (s_j/(s_i+s_j))^2 (U_i-U_j)(a_i-a_j)
+//                 + face*alpha U_i a_i - ky^2 U_i a_i ].
+__global__ void k_dc_sens(const DcGrid G, const double* sig, const double* alpha, const double* ky2,
+                          const double* wts, int sys0, int nky, const double* U, const double* A, double* g,
+                          int nsys) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys) return;
+  const int gs = sys0 + sys;
+  const double* al = alpha + size_t(gs) * G.nb;
+  const double k2 = ky2[gs];
+  const double wq = (2.0 / 3.14159265358979323846) * wts[gs];
+  const double* Us = U + size_t(sys) * G.N;
+  const double* As = A + size_t(sys) * G.N;
+  double* gg = g + size_t(gs / nky) * G.N;  // one gradient per source
+  const double rx = G.DZ / G.DX, rzz = G.DX / G.DZ;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < G.N; t += blockDim.x * gridDim.x) {
+    const int l = t % G.n, h = t / G.n;
+    const double si = sig[t], ui = Us[t], ai = As[t];
+    double v = 0;
+    if (l + 1 < G.n) { const double sj = sig[t + 1]; const double q = sj / (si + sj);
+      v += rx * 2 * q * q * (ui - Us[t + 1]) * (ai - As[t + 1]); }
+    if (l >= 1) { const double sj = sig[t - 1]; const double q = sj / (si + sj);
+      v += rx * 2 * q * q * (ui - Us[t - 1]) * (ai - As[t - 1]); }
+    if (h + 1 < G.m) { const double sj = sig[t + G.n]; const double q = sj / (si + sj);
+      v += rzz * 2 * q * q * (ui - Us[t + G.n]) * (ai - As[t + G.n]); }
+    if (h >= 1) { const double sj = sig[t - G.n]; const double q = sj / (si + sj);
+      v += rzz * 2 * q * q * (ui - Us[t - G.n]) * (ai - As[t - G.n]); }
+    v += dc_robin_fa(G, al, l, h) * ui * ai;
+    v -= k2 * ui * ai;
+    atomicAdd(gg + t, wq * v);
+  }
+}
+
+}  // namespace gj

@@ -168,4 +168,9 @@ gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const doubl
                       const double* sig, const gj_w_shot& shot, const double* e, const double* u,
                       double* gout, double* amax);
 
+// DC entry point implemented in dc_solver.cu.
+gj_status dc_run(Ctx& c, const gj_dc_grid& g, const double* sigma, const gj_dc_src* srcs, int nsrc, bool grad,
+                 const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
+                 double* misfit_out, gj_dc_stats* stats);
+
 }  // namespace gj

@@ -150,3 +150,30 @@ def cfg4_problems(seed=2000, count=48):
         out.append(_problem(f"cfg4_{k}", m, n, dx, 20, nt, fo, ns, min(100, n // 4),
                             "blob" if k % 2 == 0 else "layer", seed + k))
     return out
+
+
+def cfg5(seed=1005, n_sources=200, n_ky=20):
+    """2.5D DC: 400 x 100 cells at 0.25 m, one Robin cell (402 x 101 nodes),
+    96 surface electrodes at 1 m, `n_sources` seeded dipole-dipole AB pairs x
+    6 MN levels, n_ky wavenumbers (grid units).  log10 sigma ~ N(log10 0.01,
+    0.5) smoothed over 1 m, plus 4 seeded resistive/conductive blocks."""
+    from . import dc
+    n0, m0, dx, robin = 400, 100, 0.25, 1
+    rng = np.random.default_rng(seed)
+    ls = np.log10(0.01) + 0.5 * rng.standard_normal((n0, m0))
+    ls = gaussian_smooth(ls, 1.0 / dx)
+    ls = np.log10(0.01) + (ls - ls.mean()) * (0.5 / max(ls.std(), 1e-12))
+    for _ in range(4):
+        l0, h0 = rng.integers(20, n0 - 60), rng.integers(4, m0 - 30)
+        L, H = rng.integers(12, 40), rng.integers(6, 20)
+        ls[l0:l0 + L, h0:h0 + H] += rng.choice([-1.0, 1.0]) * rng.uniform(0.5, 1.0)
+    sig = 10 ** ls
+    X = np.arange(n0) * dx
+    Z = np.arange(m0) * dx
+    DX, DZ = dc.deltas(X, Z, robin)
+    SIG = dc.dc_robin(sig, robin)
+    n, m = SIG.shape
+    kyw = dc.ky_weights(dx, n0 * dx, n_ky, dx=dx)
+    srcs = dc.dipole_dipole(n, m, robin, DX, DZ, n_electrodes=96, spacing_nodes=4, first_node=8,
+                            pairs=n_sources, levels=6, ky_w=kyw, rng=np.random.default_rng(seed + 1))
+    return dict(SIG=SIG, sig=sig, DX=DX, DZ=DZ, robin=robin, srcs=srcs, n=n, m=m, ky_w=kyw)

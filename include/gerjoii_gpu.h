@@ -139,6 +139,75 @@ gj_status gj_w_gradient_dev(gj_ctx* ctx, const gj_w_grid* grid, gj_precision pre
                             void* g_eps_dev, void* g_sig_dev, double* misfit_out,
                             void* stream);
 
+/* -------------------------------------------------- 2.5D DC resistivity */
+
+/* Finite-volume grid of dc_fwd2_5d.m: n = finite_.dc.nx lateral nodes and
+ * m = finite_.dc.nz depth nodes, both including the Robin padding
+ * (wdc_geom.m:76-77, dc_robin.m).  Arrays are n x m with the lateral index
+ * fastest; node (l, h) (0-based) is the vectorised unknown l + h*n
+ * (coordP.m).  dx and dz are DELTAS(:,:,1) and DELTAS(:,:,2) exactly as
+ * do_grid.m computes them (dx is negative for robin = 1 when the model starts
+ * at x = 0; the operator uses the value as given). */
+typedef struct gj_dc_grid {
+  int n, m;     /* nodes incl. Robin padding */
+  int robin;    /* Robin padding (parame_.dc.robin): the gradient drops robin
+                   columns on each side and robin rows at the bottom */
+  int n_ky;     /* wavenumbers per source */
+  double dx, dz;
+} gj_dc_grid;
+
+/* Number of compact Robin coefficients per (source, ky):
+ * [ALPHAS(1,2:m-1) | ALPHAS(2:n-1,m) | ALPHAS(n,2:m-1) | corners(1,1) corners(2,1)
+ *  corners(1,2) corners(2,2)] of dc_Lk.m's private alphas (:945-960). */
+#define GJ_DC_NALPHA(n, m) (2 * ((m) - 2) + ((n) - 2) + 4)
+
+/* One current dipole and its measurements (gerjoii_.dc.s, .r, dc_M.m). */
+typedef struct gj_dc_src {
+  long a, b;             /* +I and -I electrode nodes, 0-based, after binning, the
+                            parity clean and the Robin shift of dc_electrodes.m */
+  double current;        /* I (dc_electrodes.m:54) */
+  int nd;                /* measurements */
+  const long* mn;        /* nd pairs (M, N) of 0-based nodes: d = u(M) - u(N) (dc_M.m) */
+  const double* ky;      /* n_ky wavenumbers (finite_.dc.ky_w_(:,1)) */
+  const double* w;       /* n_ky weights (finite_.dc.ky_w_(:,2)) */
+  const double* alpha;   /* n_ky x GJ_DC_NALPHA(n, m) Robin coefficients, ky-major */
+  const double* d_obs;   /* nd observed data (parame_.natu.dc.d); needed by the gradient */
+} gj_dc_src;
+
+typedef struct gj_dc_opts {
+  double tol;              /* relative residual of every solve; 0 = 1e-10 */
+  int max_iter;            /* CG iterations; 0 = 50 */
+  int per_source;          /* 1 = one gradient per source, else their sum */
+  int sources_per_batch;   /* 0 = as many as fit mem_budget_bytes */
+  size_t mem_budget_bytes; /* 0 = 70% of free device memory */
+} gj_dc_opts;
+
+typedef struct gj_dc_stats {
+  int max_iterations;      /* largest CG iteration count over all solves */
+  double max_rel_residual; /* largest final FP64 relative residual */
+} gj_dc_stats;
+
+/* Forward: replaces [gerjoii_, finite_] = dc_fwd2_5d(parame_, finite_, gerjoii_)
+ * (dc_fwd2_5d.m:35-63) for nsrc sources at once.
+ *   sigma : n x m padded conductivity (parame_.dc.sigma_robin)
+ *   d_out : sum(nd) data, sources concatenated (gerjoii_.dc.d)
+ *   u_out : nsrc x n x m stacked potentials (gerjoii_.dc.u), may be NULL
+ *   stats : may be NULL */
+gj_status gj_dc_forward(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma,
+                        const gj_dc_src* srcs, int nsrc, const gj_dc_opts* opts,
+                        double* d_out, double* u_out, gj_dc_stats* stats);
+
+/* Sensitivity: replaces dc_fwd2_5d followed by
+ * gerjoii_ = dc_gradient2_5d(parame_, finite_, gerjoii_) (dc_gradient2_5d.m:18-41).
+ *   g_out  : (n - 2 robin) x (m - robin) gradient (sum over sources, or nsrc of
+ *            them with opts->per_source) (gerjoii_.dc.g)
+ *   d_out, e_out : sum(nd) data and residuals d - d_obs, may be NULL
+ *   misfit_out   : nsrc values 0.5 e'e, may be NULL */
+gj_status gj_dc_gradient(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma,
+                         const gj_dc_src* srcs, int nsrc, const gj_dc_opts* opts,
+                         double* g_out, double* d_out, double* e_out, double* misfit_out,
+                         gj_dc_stats* stats);
+
 /* Scratch limit of gj_w_forward_noalloc, in bytes (32 MiB): enough for a
  * padded grid of about 380 000 Ez nodes (for example 600 x 600). */
 #define GJ_W_NOALLOC_SCRATCH_BYTES (32u << 20)
