@@ -57,19 +57,31 @@ def alphas_compact(n: int, m: int, DX: float, DZ: float, a_node: int, b_node: in
     """Robin coefficients alpha = sum_e beta_e ky K1(ky r) (ca/r) / sum_e beta_e
     K0(ky r) for the two surface electrodes (beta = +1 at A, -1 at B), on the
     left side, bottom, right side and bottom corners, in the compact layout
-    [left h=2..m-1 | bottom l=2..n-1 | right h=2..m-1 | c11 c21 c12 c22]."""
-    beta = np.zeros(n)
-    beta[a_node % n] += 1.0
-    beta[b_node % n] -= 1.0
-    beta = np.sign(beta)
-    co_left = np.outer(np.arange(1, m) * DZ, np.ones(n))
-    idx = np.arange(n)
-    co_down = np.abs(idx[:, None] - idx[None, :]) * DX
-    co = np.vstack([co_left, co_down, co_left[::-1, ::-1]])
-    ca_left = np.outer(np.ones(m - 1), idx * DX)
-    ca = np.vstack([ca_left, (m - 1) * DZ * np.ones((n, n)), ca_left[::-1, ::-1]])
+    [left h=2..m-1 | bottom l=2..n-1 | right h=2..m-1 | c11 c21 c12 c22].
+
+    Distances follow dc_Lk.m's alphas (co/ca built from DELTAS, signs included).
+    Only the two electrode columns carry weight, so only they are evaluated,
+    and K0/K1 are taken exponentially scaled (k0e, k1e) relative to the nearer
+    electrode: where ky*r is large enough for besselk to underflow (0/0 in
+    the reference) this returns the limit of the same ratio."""
+    la, lb = a_node % n, b_node % n
+    cols = np.array([la, lb])
+    beta = np.array([1.0, -1.0])
+    hh = np.arange(1, m)
+    co_left = np.outer(hh * DZ, np.ones(2))
+    co_down = np.abs(np.arange(n)[:, None] - cols[None, :]) * DX
+    co_right = np.outer(hh[::-1] * DZ, np.ones(2))
+    co = np.vstack([co_left, co_down, co_right])
+    ca_left = np.outer(np.ones(m - 1), cols * DX)
+    ca_right = np.outer(np.ones(m - 1), (n - 1 - cols) * DX)
+    ca = np.vstack([ca_left, (m - 1) * DZ * np.ones((n, 2)), ca_right])
     r = np.sqrt(co ** 2 + ca ** 2)
-    a = ((ky * ss.k1(ky * r) * (ca / r)) @ beta) / (ss.k0(ky * r) @ beta)
+    x = ky * r
+    x0 = x.min(axis=1, keepdims=True)
+    sc = np.exp(-(x - x0))
+    numer = (ky * ss.k1e(x) * sc * (ca / r)) @ beta
+    denom = (ss.k0e(x) * sc) @ beta
+    a = numer / denom
     left = a[0:m - 2]
     bottom = a[m:m + n - 2]
     right = a[m + n:][::-1]
@@ -89,7 +101,7 @@ def ky_weights(r_min: float, r_max: float, n_ky: int, dx: float | None = None, n
     ky = np.geomspace(0.1 / r_max, 10.0 / r_min, n_ky)
     r = np.geomspace(r_min, r_max, n_fit)
     A = (2 / np.pi) * ss.k0(np.outer(r, ky)) * r[:, None]  # relative: times r
-    w, _ = nnls(A, np.ones(n_fit))
+    w, _ = nnls(A, np.ones(n_fit), maxiter=50 * n_ky * n_fit)
     if dx is not None:
         ky = ky * abs(dx)
     return np.column_stack([ky, w])

@@ -52,8 +52,6 @@ def alphas(n, m, DX, DZ, s_surface, ky):
     co_left = np.outer(np.arange(1, m) * DZ, np.ones(n))               # (m-1, n)
     idx = np.arange(n)
     co_down = np.abs(idx[:, None] - idx[None, :]) * DX                  # (n, n), DX may be negative
-    co_down = np.where(idx[:, None] < idx[None, :], (idx[None, :] - idx[:, None]) * DX,
-                       (idx[:, None] - idx[None, :]) * DX)
     co_right = co_left[::-1, ::-1]
     co = np.vstack([co_left, co_down, co_right])
     ca_left = np.outer(np.ones(m - 1), np.arange(n) * DX)
@@ -61,8 +59,15 @@ def alphas(n, m, DX, DZ, s_surface, ky):
     ca_right = ca_left[::-1, ::-1]
     ca = np.vstack([ca_left, ca_down, ca_right])
     r = np.sqrt(co ** 2 + ca ** 2)
-    numer = (ky * ss.k1(ky * r) * (ca / r)) @ beta
-    denom = ss.k0(ky * r) @ beta
+    # K0/K1 exponentially scaled relative to the nearest electrode of each row:
+    # identical to besselk where it does not underflow, and its limit where
+    # the reference's besselk would give 0/0.
+    x = ky * r
+    on = beta != 0
+    x0 = np.min(np.where(on[None, :], x, np.inf), axis=1, keepdims=True)
+    sc = np.where(on[None, :], np.exp(-np.where(on[None, :], x - x0, 0.0)), 0.0)
+    numer = (ky * ss.k1e(x) * sc * (ca / r)) @ beta
+    denom = (ss.k0e(x) * sc) @ beta
     a = numer / denom
     AL = np.zeros((n, m))
     AL[0, 1:m - 1] = a[0:m - 2]
