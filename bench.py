@@ -281,7 +281,7 @@ def main():
     # cell-updates in the timed region: every forward, recompute and adjoint launch
     upd = sum(k["shot_launches"] for k in ktimes.values()) * cells * world
     gcell = upd / (ms / 1e3) / 1e9
-    # algorithmic bytes per shot for each kernel kind (see DESIGN.md)
+    # algorithmic bytes per shot for each kernel kind
     per_shot_bytes = {
         "fwd_step": cells * 32.0,             # read Ez,Hx,Hy,Ceze,Cezhy; write Ez,Hx,Hy
         "adj_step": cells * 32.0 + mn * 40.0,  # + 2 history reads + 4 Kahan sums r/w

@@ -4,7 +4,7 @@
  *
  * Every entry point replaces one MATLAB function of the reference
  * (diegozain/gerjoii); the function it replaces is cited beside it as
- * path:line inside that project.  A MEX gateway (mex/*.c) unpacks the
+ * path:line inside that project.  A MEX gateway (mex/gj_mex.c) unpacks the
  * reference's structs and calls these functions, so the reference's L2 layer
  * (w_update_e.m, w_update_s.m, dc_update2_5d.m, ...) keeps its call sites.
  *

@@ -8,9 +8,8 @@
 // Each function names the reference file:line it restates (paths inside the
 // diegozain/gerjoii project).  Parity status: the reference is MATLAB and cannot
 // run here; this restatement is pinned against the numpy twin (oracle/np_oracle.py,
-// which follows the MATLAB strip-by-strip slicing literally) and against the
-// outputs of the reference .m files executed by the MATLAB-subset interpreter in
-// oracle/msub (fixtures in tests/golden).
+// which follows the MATLAB strip-by-strip slicing literally), against the
+// reference's known answers, and (exact adjoint) against central differences.
 //
 // Conventions (0-based, column-major, fastest index = depth i, as in MATLAB):
 //   NX = pml_top + air + m + pml   (depth incl. PML; "nx" in wdc_geom.m:70)

@@ -121,3 +121,26 @@ def test_plain_fp64_form_matches_fused(gpu_ctx, oracle, small_ft, mode):
     o.ckpt_every = 11
     r3 = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64, opts=o)
     assert rel_l2(r3["g_eps"], r2["g_eps"]) < 1e-11
+
+
+def test_autograd_harness_gradient_matches_finite_difference(gpu_ctx, oracle, small_ft):
+    import torch
+    from gerjoii_b200.autograd import WGradient
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    dev = torch.device("cuda", 0)
+    do_t = torch.tensor(np.stack([d.T for d in dobs]), dtype=torch.float64, device=dev)
+    eps = torch.tensor(p.eps0, dtype=torch.float64, device=dev, requires_grad=True)
+    sig = torch.tensor(p.sig0, dtype=torch.float64, device=dev, requires_grad=True)
+    J = WGradient.apply(eps, sig, g, p.shots, do_t, gpu_ctx)
+    J.backward()
+    for (a, b) in [(5, 10), (12, 20)]:
+        h = 1e-5 * p.eps0[a, b]
+        ep, em = p.eps0.copy(), p.eps0.copy()
+        ep[a, b] += h
+        em[a, b] -= h
+        Jp = WGradient.apply(torch.tensor(ep, dtype=torch.float64, device=dev), sig.detach(), g, p.shots, do_t, gpu_ctx)
+        Jm = WGradient.apply(torch.tensor(em, dtype=torch.float64, device=dev), sig.detach(), g, p.shots, do_t, gpu_ctx)
+        fd = (Jp.item() - Jm.item()) / (2 * h)
+        assert abs(eps.grad[a, b].item() - fd) <= 1e-5 * abs(fd), (a, b, eps.grad[a, b].item(), fd)
