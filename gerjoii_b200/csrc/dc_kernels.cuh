@@ -108,20 +108,33 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
 
 // FP32 band LDL^T of every system: one CTA per system.  Output per system:
 // N columns of (b+1) floats: [d_q, l_{q+1,q}, ..., l_{q+b,q}].
-// Shared memory: (b+1)^2 floats (rolling window) + (b+1) floats.
+// Shared memory: (b+1)^2 floats (rolling window, circular in both indices)
+// + (b+1) floats (current column).  The b(b+1)/2 updates of each step are
+// split into equal contiguous runs over all threads (row-major packed order),
+// and the next band row's entries are fetched from global memory while the
+// update runs.
 __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, const double* dbase,
                             const double* sig, const double* alpha, const double* ky2, int sys0,
                             float* fac, int* status) {
   extern __shared__ float sh[];
   const int W = G.b + 1;
-  float* win = sh;            // W x W, row-major, circular in both indices
-  float* lc = sh + W * W;     // current column
+  float* win = sh;
+  float* lc = sh + W * W;
   const int sys = blockIdx.x;
   const double* al = alpha + size_t(sys0 + sys) * G.nb;
   const double k2 = ky2[sys0 + sys];
   float* F = fac + size_t(sys) * size_t(G.N) * W;
   const int N = G.N, b = G.b;
-  // initial window: rows/cols 0..b of A (lower triangle)
+  // this thread's run of the packed lower triangle (rows i = 1..b, cols 1..i)
+  const int T = b * (b + 1) / 2;
+  const int chunk = (T + blockDim.x - 1) / blockDim.x;
+  const int e0 = min(int(threadIdx.x) * chunk, T), e1 = min(e0 + chunk, T);
+  int i0 = 1, j0 = 1;
+  {
+    int e = e0, i = 1;
+    while (e >= i) { e -= i; ++i; }
+    i0 = i; j0 = e + 1;
+  }
   for (int e = threadIdx.x; e < W * W; e += blockDim.x) win[e] = 0.f;
   __syncthreads();
   for (int r = threadIdx.x; r < W && r < N; r += blockDim.x) {
@@ -131,39 +144,54 @@ __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, 
     if (r >= b) win[r * W + (r - b)] = float(dc_sub(G, ox, oz, r, b));
   }
   __syncthreads();
+  const bool loader = threadIdx.x == blockDim.x - 1;
   for (int q = 0; q < N; ++q) {
     const int p0 = q % W;
+    // prefetch the entries of band row q+b+1 (enters the window after this step)
+    const int nr = q + b + 1;
+    float nd = 0.f, n1 = 0.f, nb_ = 0.f;
+    if (loader && nr < N) {
+      int l, h; dc_lh(G, nr, l, h);
+      nd = float(dc_diag(G, dbase, sig, al, k2, l, h));
+      n1 = float(dc_sub(G, ox, oz, nr, 1));
+      nb_ = float(dc_sub(G, ox, oz, nr, b));
+    }
     const float d = win[p0 * W + p0];
     if (threadIdx.x == 0) {
       F[size_t(q) * W] = d;
       if (!(d != 0.f) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
     }
     for (int i = threadIdx.x + 1; i <= b; i += blockDim.x) {
-      const int pi = (q + i) % W;
+      int pi = p0 + i; if (pi >= W) pi -= W;
       const float li = (q + i < N) ? win[pi * W + p0] / d : 0.f;
       lc[i] = li;
       F[size_t(q) * W + i] = li;
     }
     __syncthreads();
-    // rank-1 update of rows/cols q+1..q+b: A(i,j) -= l_i d l_j, j <= i
-    for (int i = 1; i <= b; ++i) {
-      const float ci = lc[i] * d;
-      if (ci != 0.f) {
-        const int pi = (q + i) % W;
-        for (int j = threadIdx.x + 1; j <= i; j += blockDim.x) win[pi * W + (q + j) % W] -= ci * lc[j];
+    // rank-1 update A(i, j) -= (l_i d) l_j for 1 <= j <= i <= b
+    {
+      int i = i0, j = j0;
+      int pi = p0 + i; if (pi >= W) pi -= W;
+      int pj = p0 + j; if (pj >= W) pj -= W;
+      float ci = (i <= b) ? lc[i] * d : 0.f;
+      for (int e = e0; e < e1; ++e) {
+        win[pi * W + pj] -= ci * lc[j];
+        if (++j > i) {
+          ++i; j = 1;
+          if (++pi >= W) pi -= W;
+          pj = p0 + 1; if (pj >= W) pj -= W;
+          ci = (i <= b) ? lc[i] * d : 0.f;
+        } else if (++pj >= W) pj -= W;
       }
     }
     __syncthreads();
-    // slide: row/col q+b+1 of A enters at the slot of q
-    const int nr = q + b + 1;
-    for (int c = threadIdx.x; c < W; c += blockDim.x) win[p0 * W + c] = 0.f;
-    for (int r = threadIdx.x; r < W; r += blockDim.x) win[r * W + p0] = 0.f;
+    // slide: row/col q+b+1 enters at the slot of q
+    for (int c = threadIdx.x; c < W; c += blockDim.x) { win[p0 * W + c] = 0.f; win[c * W + p0] = 0.f; }
     __syncthreads();
-    if (threadIdx.x == 0 && nr < N) {
-      int l, h; dc_lh(G, nr, l, h);
-      win[p0 * W + p0] = float(dc_diag(G, dbase, sig, al, k2, l, h));
-      win[p0 * W + (nr - 1) % W] = float(dc_sub(G, ox, oz, nr, 1));
-      win[p0 * W + (nr - b) % W] = float(dc_sub(G, ox, oz, nr, b));
+    if (loader && nr < N) {
+      win[p0 * W + p0] = nd;
+      win[p0 * W + (nr - 1) % W] = n1;
+      win[p0 * W + (nr - b) % W] = nb_;
     }
     __syncthreads();
   }
@@ -171,7 +199,8 @@ __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, 
 
 // z = (L D L^T)^{-1} r for every system, one warp per system, and rz = r.z.
 // r, z are FP64 vectors in the reference layout [sys][l + h*n].  The rolling
-// windows (b+1 values) live in shared memory per warp.
+// windows (b+1 values) live in shared memory per warp; factor columns are
+// loaded one step ahead, and r / z values 32 steps at a time (one per lane).
 __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, double* z, double* rz,
                              int nsys, const int* done) {
   extern __shared__ float shp[];
@@ -184,43 +213,80 @@ __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, 
   const double* R = r + size_t(sys) * G.N;
   double* Z = z + size_t(sys) * G.N;
   const int N = G.N, b = G.b;
+  constexpr int MAXI = 7;  // b <= 200 -> at most 7 entries of a column per lane
   auto ref = [&](int q) { int l, h; dc_lh(G, q, l, h); return l + h * G.n; };
-  // forward: L y = r (column oriented), window holds partially reduced r
+  auto load_col = [&](int q, float (&c)[MAXI]) {
+#pragma unroll
+    for (int u = 0; u < MAXI; ++u) {
+      const int i = lane + 1 + 32 * u;
+      c[u] = (q < N && i <= b) ? F[size_t(q) * W + i] : 0.f;
+    }
+  };
+  // forward: L y = r
   for (int i = lane; i < W; i += 32) win[i] = (i < N) ? float(R[ref(i)]) : 0.f;
   __syncwarp();
+  float col[MAXI], nxt[MAXI];
+  load_col(0, col);
+  float dq = F[0];
+  double rpre = 0.0;
   for (int q = 0; q < N; ++q) {
+    if ((q & 31) == 0) {  // r values entering the window over the next 32 steps
+      const int nq = q + W + lane;
+      rpre = (nq < N) ? R[ref(nq)] : 0.0;
+    }
+    load_col(q + 1, nxt);
+    const float dn = (q + 1 < N) ? F[size_t(q + 1) * W] : 1.f;
     const int p0 = q % W;
     const float y = win[p0];
-    const float* Fq = F + size_t(q) * W;
-    for (int i = lane + 1; i <= b; i += 32)
-      if (q + i < N) win[(q + i) % W] -= Fq[i] * y;
+#pragma unroll
+    for (int u = 0; u < MAXI; ++u) {
+      const int i = lane + 1 + 32 * u;
+      if (i <= b && q + i < N) { int pi = p0 + i; if (pi >= W) pi -= W; win[pi] -= col[u] * y; }
+    }
+    const double rin = __shfl_sync(0xffffffffu, rpre, q & 31);
     __syncwarp();
     if (lane == 0) {
-      // y_q / d_q stored in Z (band order) temporarily via the reference index
-      Z[ref(q)] = double(y / Fq[0]);
-      const int nq = q + W;
-      win[p0] = (nq < N) ? float(R[ref(nq)]) : 0.f;
+      Z[ref(q)] = double(y / dq);
+      win[p0] = (q + W < N) ? float(rin) : 0.f;
     }
     __syncwarp();
+#pragma unroll
+    for (int u = 0; u < MAXI; ++u) col[u] = nxt[u];
+    dq = dn;
   }
+  __threadfence_block();
   // backward: L^T x = z, x_q = z_q - sum_i l_{q+i,q} x_{q+i}
   for (int i = lane; i < W; i += 32) win[i] = 0.f;
   __syncwarp();
   double acc = 0.0;
+  load_col(N - 1, col);
+  double zpre = 0.0, rpre2 = 0.0;
   for (int q = N - 1; q >= 0; --q) {
-    const float* Fq = F + size_t(q) * W;
+    const int k = (N - 1 - q) & 31;
+    if (k == 0) {  // z and r values of the next 32 steps (descending)
+      const int qq = q - lane;
+      zpre = (qq >= 0) ? Z[ref(qq)] : 0.0;
+      rpre2 = (qq >= 0) ? R[ref(qq)] : 0.0;
+    }
+    load_col(q - 1 >= 0 ? q - 1 : N, nxt);
     float s = 0.f;
-    for (int i = lane + 1; i <= b; i += 32)
-      if (q + i < N) s += Fq[i] * win[(q + i) % W];
+#pragma unroll
+    for (int u = 0; u < MAXI; ++u) {
+      const int i = lane + 1 + 32 * u;
+      if (i <= b && q + i < N) { int pi = q % W + i; if (pi >= W) pi -= W; s += col[u] * win[pi]; }
+    }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double zq = __shfl_sync(0xffffffffu, zpre, k);
+    const double rq = __shfl_sync(0xffffffffu, rpre2, k);
     if (lane == 0) {
-      const int rq = ref(q);
-      const float x = float(Z[rq]) - s;
+      const float x = float(zq) - s;
       win[q % W] = x;
-      Z[rq] = double(x);
-      acc += R[rq] * double(x);
+      Z[ref(q)] = double(x);
+      acc += rq * double(x);
     }
     __syncwarp();
+#pragma unroll
+    for (int u = 0; u < MAXI; ++u) col[u] = nxt[u];
   }
   if (lane == 0) rz[sys] = acc;
 }

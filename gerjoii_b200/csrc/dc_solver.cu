@@ -172,6 +172,9 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
   P.nky = gg.n_ky; P.nsrc = nsrc; P.robin = gg.robin;
   const int N = G.N, nky = P.nky, nsys_all = nsrc * nky;
   cudaStream_t st = 0;
+  Marks marks;
+  c.timer.cur = &marks;
+  struct Unset { Ctx& c; ~Unset() { c.timer.cur = nullptr; } } unset{c};
   // ---- inputs
   std::vector<double> hky2(nsys_all), hw(nsys_all), hal(size_t(nsys_all) * G.nb), hcur(nsrc);
   std::vector<long> hab(2 * nsrc), hmn;
@@ -300,6 +303,7 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
   }
   GJ_CUDA(err, cudaGetLastError());
   GJ_CUDA(err, cudaDeviceSynchronize());
+  c.timer.collect(marks);
   std::vector<int> hst(nsys_all);
   GJ_CUDA(err, cudaMemcpy(hst.data(), P.status.p, nsys_all * sizeof(int), cudaMemcpyDeviceToHost));
   for (int s = 0; s < nsys_all; ++s)

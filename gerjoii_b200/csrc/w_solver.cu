@@ -12,6 +12,7 @@
 #include "gj_internal.h"
 #include "w_kernels.cuh"
 #include "w_kernels_vec.cuh"
+#include "w_misfit.cuh"
 
 namespace gj {
 
@@ -103,7 +104,6 @@ class WSolver : public WSolverBase {
   // launch shape
   int bx = 128, tj = 16;
 
-  ~WSolver() override = default;
 
   static std::string key(const gj_w_grid& g, const gj_w_shot* shots, int nshots) {
     std::string k((const char*)&g, sizeof g);
@@ -458,6 +458,61 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
+  // ------------------------------------------------------------ envelope
+  DevBuf envA, envAo, envG, envF;
+  cufftHandle fftplan = 0;
+  int fft_batch = 0;
+  ~WSolver() override {
+    if (fftplan) cufftDestroy(fftplan);
+  }
+
+  gj_status analytic(Err& err, typename CplxT<T>::type* X, cudaStream_t st) {
+    using C = typename CplxT<T>::type;
+    cufftResult r;
+    cufftSetStream(fftplan, st);
+    if (sizeof(T) == 8) r = cufftExecZ2Z(fftplan, (cufftDoubleComplex*)X, (cufftDoubleComplex*)X, CUFFT_FORWARD);
+    else r = cufftExecC2C(fftplan, (cufftComplex*)X, (cufftComplex*)X, CUFFT_FORWARD);
+    if (r != CUFFT_SUCCESS) return err.set(GJ_ECUDA, "cufft forward failed (%d)", int(r));
+    k_env_mask<T, C><<<512, 256, 0, st>>>(X, g.nt, size_t(fft_batch));
+    if (sizeof(T) == 8) r = cufftExecZ2Z(fftplan, (cufftDoubleComplex*)X, (cufftDoubleComplex*)X, CUFFT_INVERSE);
+    else r = cufftExecC2C(fftplan, (cufftComplex*)X, (cufftComplex*)X, CUFFT_INVERSE);
+    if (r != CUFFT_SUCCESS) return err.set(GJ_ECUDA, "cufft inverse failed (%d)", int(r));
+    return GJ_OK;
+  }
+
+  // env_L2 residual and misfit sums for shots [g0, g0+gn) (w_bozdag.m:51-60).
+  gj_status env_residual(Err& err, Ctx& c, int g0, int gn, cudaStream_t st) {
+    using C = typename CplxT<T>::type;
+    const int nrr = std::max(nr, 1), nt = g.nt;
+    const size_t tr = size_t(nrr) * nt, n = size_t(gn) * tr;
+    const int batch = gn * nrr;
+    if (fftplan && fft_batch != batch) { cufftDestroy(fftplan); fftplan = 0; }
+    if (!fftplan) {
+      int dims[1] = {nt};
+      if (cufftPlanMany(&fftplan, 1, dims, nullptr, 1, nt, nullptr, 1, nt, sizeof(T) == 8 ? CUFFT_Z2Z : CUFFT_C2C,
+                        batch) != CUFFT_SUCCESS)
+        return err.set(GJ_ENOMEM, "cufftPlanMany(nt=%d, batch=%d) failed", nt, batch);
+      fft_batch = batch;
+    }
+    GJ_TRY(envA.alloc(err, n * sizeof(C)));
+    GJ_TRY(envAo.alloc(err, n * sizeof(C)));
+    GJ_TRY(envG.alloc(err, n * sizeof(C)));
+    GJ_TRY(envF.alloc(err, n * sizeof(T)));
+    const T* d = dbuf.as<T>() + size_t(g0) * tr;
+    const T* dob = dobsbuf.as<T>() + size_t(g0) * tr;
+    k_env_to_complex<T, C><<<512, 256, 0, st>>>(d, envA.as<C>(), n);
+    k_env_to_complex<T, C><<<512, 256, 0, st>>>(dob, envAo.as<C>(), n);
+    GJ_TRY(analytic(err, envA.as<C>(), st));
+    GJ_TRY(analytic(err, envAo.as<C>(), st));
+    k_env_mid<T, C><<<dim3(64, gn), 256, 0, st>>>(envA.as<C>(), envAo.as<C>(), envF.as<T>(), envG.as<C>(), nt, nrr,
+                                                 gn, sums.as<double>() + 2 * g0);
+    GJ_TRY(analytic(err, envG.as<C>(), st));
+    k_env_final<T, C><<<512, 256, 0, st>>>(d, envF.as<T>(), envG.as<C>(), ebuf.as<T>() + size_t(g0) * tr, n);
+    c.launches += 10;
+    GJ_CUDA(err, cudaGetLastError());
+    return GJ_OK;
+  }
+
   // ---------------------------------------------------------------- groups
   // Shots are processed in groups of G: every group runs the whole gradient
   // (forward, residual, recompute, adjoint) before the next starts, so the
@@ -508,8 +563,10 @@ class WSolver : public WSolverBase {
   }
 
   // Enqueues the whole gradient of shots [g0, g0+gn) on stream st.
+  // phase: 1 = forward (+ the L2 residual when l2), 2 = adjoint, 3 = both.
   gj_status enqueue_group(Err& err, Ctx& c, int g0, int gn, gj_adj_mode mode, int kahan,
-                          const std::vector<std::pair<int, int>>& segs, bool full, long& nl, cudaStream_t st) {
+                          const std::vector<std::pair<int, int>>& segs, bool full, long& nl, cudaStream_t st,
+                          int phase = 3, bool l2 = true) {
     const int nrr = std::max(nr, 1), nt = g.nt;
     const size_t tr = size_t(nrr) * nt;
     constexpr int V = VT<T>::V;
@@ -526,6 +583,7 @@ class WSolver : public WSolverBase {
     T* egrp = ebuf.as<T>() + size_t(g0) * tr;
     T* A = fwdA.as<T>() + ld;
     T* B = fwdB.as<T>() + ld;
+    if (phase & 1) {
     GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, gn * sstride * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, gn * sstride * sizeof(T), st));
     if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, gn * hs * sizeof(T), st));  // slot 0 = zero state
@@ -547,9 +605,15 @@ class WSolver : public WSolverBase {
       nl += 2;
       std::swap(A, B);
     }
-    k_residual<T><<<dim3(64, gn), 256, 0, st>>>(dgrp, dobsbuf.as<T>() + size_t(g0) * tr, egrp, tr,
-                                                sums.as<double>() + 2 * g0);
-    ++nl;
+    if (l2) {
+      k_residual<T><<<dim3(64, gn), 256, 0, st>>>(dgrp, dobsbuf.as<T>() + size_t(g0) * tr, egrp, tr,
+                                                  sums.as<double>() + 2 * g0);
+      ++nl;
+    }
+    }  // phase 1
+    if (!(phase & 2)) { GJ_CUDA(err, cudaGetLastError()); return GJ_OK; }
+    A = fwdA.as<T>() + ld;
+    B = fwdB.as<T>() + ld;
     T* LA = adjA.as<T>() + ld;
     T* LB = adjB.as<T>() + ld;
     GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, gn * sstride * sizeof(T), st));
@@ -612,10 +676,14 @@ class WSolver : public WSolverBase {
   }
 
   gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
-                     bool dev_dobs, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
-                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+                     bool dev_dobs, gj_adj_mode mode, gj_misfit_kind mk, const gj_w_opts& o, void* geps,
+                     void* gsig, bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
     GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
-    if (o.plain) return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
+    if (o.plain) {
+      if (mk != GJ_MISFIT_L2) return err.set(GJ_EUNSUPPORTED, "the plain form supports the L2 misfit only");
+      return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
+    }
+    const bool env = (mk == GJ_MISFIT_ENV_L2);
     // memory plan for one group
     size_t free_b = 0, total_b = 0;
     GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
@@ -652,6 +720,19 @@ class WSolver : public WSolverBase {
     long nl = 0;
     for (int g0 = 0; g0 < nshots; g0 += G) {
       const int gn = std::min(G, nshots - g0);
+      if (env) {
+        // forward, envelope residual (cuFFT), adjoint: launched directly
+        Marks m;
+        c.timer.cur = &m;
+        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 1, false);
+        if (rs == GJ_OK) rs = env_residual(err, c, g0, gn, st);
+        if (rs == GJ_OK) rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 2, false);
+        c.timer.cur = nullptr;
+        GJ_TRY(rs);
+        GJ_CUDA(err, cudaStreamSynchronize(st));
+        c.timer.collect(m);
+        continue;
+      }
       if (o.no_graph) {
         Marks m;
         c.timer.cur = &m;
@@ -918,15 +999,15 @@ gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* 
                      bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
   if (!eps || !sig || !dobs || !geps || !gsig) return c.err.set(GJ_EINVAL, "null input or output pointer");
   if (mode != GJ_ADJ_REFERENCE && mode != GJ_ADJ_EXACT) return c.err.set(GJ_EINVAL, "unknown adjoint mode");
-  if (mk != GJ_MISFIT_L2) return c.err.set(GJ_EUNSUPPORTED, "only the L2 misfit is built into this entry point");
+  if (mk != GJ_MISFIT_L2 && mk != GJ_MISFIT_ENV_L2) return c.err.set(GJ_EINVAL, "unknown misfit kind");
   if (prec == GJ_F64) {
     WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
-    return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, o, geps, gsig, dev_out, misfit_out, d_out,
-                       e_out, st);
+    return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, mk, o, geps, gsig, dev_out, misfit_out,
+                       d_out, e_out, st);
   }
   WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
-  return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, o, geps, gsig, dev_out, misfit_out, d_out,
-                     e_out, st);
+  return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, mk, o, geps, gsig, dev_out, misfit_out,
+                     d_out, e_out, st);
 }
 
 gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,

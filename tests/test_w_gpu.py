@@ -144,3 +144,29 @@ def test_autograd_harness_gradient_matches_finite_difference(gpu_ctx, oracle, sm
         Jm = WGradient.apply(torch.tensor(em, dtype=torch.float64, device=dev), sig.detach(), g, p.shots, do_t, gpu_ctx)
         fd = (Jp.item() - Jm.item()) / (2 * h)
         assert abs(eps.grad[a, b].item() - fd) <= 1e-5 * abs(fd), (a, b, eps.grad[a, b].item(), fd)
+
+
+@pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-9), (N.GJ_F32, 2e-4)])
+def test_envelope_residual_and_exact_gradient_match_oracle(gpu_ctx, oracle, small_ft, prec, tol):
+    """env_L2 (w_bozdag.m:51-60): residual against the numpy twin, misfit of the
+    envelopes (w_E.m after w_fwd.m:34-35), exact gradient against the oracle's
+    exact adjoint driven by the same adjoint source (interior cells)."""
+    import np_oracle as npo
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, misfit=N.GJ_MISFIT_ENV_L2,
+                             precision=prec, want_traces=True)
+    ge = np.zeros((g.m, g.n))
+    gs = np.zeros((g.m, g.n))
+    for k, sh in enumerate(p.shots):
+        d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+        e, de, doe = npo.w_bozdag(dobs[k], d, "env_L2")
+        assert rel_l2(res["e"][k], e) < tol
+        assert abs(res["misfit"][k] - npo.w_E(doe, de)) <= tol * npo.w_E(doe, de)
+        a, b = oracle.grad_exact(g, p.eps0, p.sig0, sh, e)
+        ge += a
+        gs += b
+    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
+    assert rel_l2(res["g_eps"][sl], ge[sl]) < 10 * tol
+    assert rel_l2(res["g_sig"][sl], gs[sl]) < 10 * tol
