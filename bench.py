@@ -45,7 +45,8 @@ def parse():
     ap.add_argument("--nt", type=int, default=6000)
     ap.add_argument("--nshots", type=int, default=30)
     ap.add_argument("--mode", default="exact", choices=["exact", "reference"])
-    ap.add_argument("--no-extras", action="store_true", help="skip the e2e, plain-FP64 and CPU legs")
+    ap.add_argument("--no-extras", action="store_true", help="skip the e2e, plain-FP64, DC and CPU legs")
+    ap.add_argument("--no-dc", action="store_true", help="skip the DC leg")
     return ap.parse_args()
 
 
@@ -179,6 +180,45 @@ class CpuPool:
     def close(self):
         self.pool.close()
         self.pool.join()
+
+
+def dc_leg(ctx):
+    """Timed DC forward + sensitivity on the full survey; accuracy on one source."""
+    import torch
+    from gerjoii_b200 import synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import np_dc_oracle as dco
+    c = synth.cfg5()
+    srcs = c["srcs"]
+    fw = ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], srcs)  # warm-up and observed data
+    rng = np.random.default_rng(5)
+    for q, d in zip(srcs, fw["d"]):
+        q.d_obs = d * (1 + 0.02 * rng.standard_normal(d.shape))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fw = ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], srcs)
+    t_f = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    gr = ctx.dc_gradient(c["SIG"], c["DX"], c["DZ"], c["robin"], srcs)
+    t_g = time.perf_counter() - t0
+    nky = len(srcs[0].ky_w)
+    q = srcs[0]
+    n, m = c["n"], c["m"]
+    al = []
+    for ky in q.ky_w[:, 0]:
+        s_ = dco.source_vector(n, m, q.a, q.b)
+        al.append(dco.alphas(n, m, c["DX"], c["DZ"], s_[:n], ky))
+    _, _, d_ref, _ = dco.dc_fwd2_5d(c["SIG"], c["DX"], c["DZ"], dco.source_vector(n, m, q.a, q.b), al, q.ky_w,
+                                    dco.measuring_operator(n, m, q.mn))
+    rel = float(np.linalg.norm(fw["d"][0] - d_ref) / np.linalg.norm(d_ref))
+    return {"workload": f"2.5D DC, {n - 2}x{m - 1} cells (+Robin), {len(srcs)} sources x {nky} ky, "
+                        f"{sum(x.nd for x in srcs)} data",
+            "forward_solves_per_s": len(srcs) * nky / t_f, "forward_s": t_f,
+            "gradient_solves_per_s": 2 * len(srcs) * nky / t_g, "gradient_s": t_g,
+            "cg_iterations_max": max(fw["iters"], gr["iters"]),
+            "max_rel_residual": max(fw["rel_residual"], gr["rel_residual"]),
+            "data_rel_err_vs_fp64_direct_solve": rel,
+            "path": "gj_dc_forward / gj_dc_gradient, host buffers"}
 
 
 def run_reference(args):
@@ -370,6 +410,11 @@ def main():
                               "speedup_fp32_batched_over_plain_fp64": value / world / (len(sub) / t_pl),
                               "g_eps_rel_l2_fp32_vs_fp64": rel(r32["g_eps"], r_plain["g_eps"]),
                               "g_sig_rel_l2_fp32_vs_fp64": rel(r32["g_sig"], r_plain["g_sig"])}
+        # 2.5D DC leg: the full 200-source x 20-ky survey (400 x 100 cells), forward and
+        # sensitivity, FP64 CG with FP32 band factors; accuracy against the FP64 direct
+        # solve of the oracle on one source
+        if not args.no_dc:
+            line["dc"] = dc_leg(ctx)
         # CPU baseline (oracle) on the host cores, bounded sample
         threads = min(os.cpu_count() or 1, 32)
         nt_s = max(50, min(args.nt, 150))

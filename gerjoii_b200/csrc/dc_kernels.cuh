@@ -106,24 +106,26 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
   else { l = q % G.n; h = q / G.n; }
 }
 
-// FP32 band LDL^T of every system: one CTA per system.  Output per system:
+// Band LDL^T of every system (TF = double by default, float on request): one CTA per system.  Output per system:
 // N columns of (b+1) floats: [d_q, l_{q+1,q}, ..., l_{q+b,q}].
 // Shared memory: (b+1)^2 floats (rolling window, circular in both indices)
 // + (b+1) floats (current column).  The b(b+1)/2 updates of each step are
 // split into equal contiguous runs over all threads (row-major packed order),
 // and the next band row's entries are fetched from global memory while the
 // update runs.
+template <class TF>
 __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, const double* dbase,
                             const double* sig, const double* alpha, const double* ky2, int sys0,
-                            float* fac, int* status) {
-  extern __shared__ float sh[];
+                            TF* fac, int* status) {
+  extern __shared__ __align__(16) unsigned char shraw[];
+  TF* sh = reinterpret_cast<TF*>(shraw);
   const int W = G.b + 1;
-  float* win = sh;
-  float* lc = sh + W * W;
+  TF* win = sh;
+  TF* lc = sh + W * W;
   const int sys = blockIdx.x;
   const double* al = alpha + size_t(sys0 + sys) * G.nb;
   const double k2 = ky2[sys0 + sys];
-  float* F = fac + size_t(sys) * size_t(G.N) * W;
+  TF* F = fac + size_t(sys) * size_t(G.N) * W;
   const int N = G.N, b = G.b;
   // this thread's run of the packed lower triangle (rows i = 1..b, cols 1..i)
   const int T = b * (b + 1) / 2;
@@ -135,13 +137,13 @@ __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, 
     while (e >= i) { e -= i; ++i; }
     i0 = i; j0 = e + 1;
   }
-  for (int e = threadIdx.x; e < W * W; e += blockDim.x) win[e] = 0.f;
+  for (int e = threadIdx.x; e < W * W; e += blockDim.x) win[e] = TF(0);
   __syncthreads();
   for (int r = threadIdx.x; r < W && r < N; r += blockDim.x) {
     int l, h; dc_lh(G, r, l, h);
-    win[r * W + r] = float(dc_diag(G, dbase, sig, al, k2, l, h));
-    if (r >= 1) win[r * W + (r - 1)] = float(dc_sub(G, ox, oz, r, 1));
-    if (r >= b) win[r * W + (r - b)] = float(dc_sub(G, ox, oz, r, b));
+    win[r * W + r] = TF(dc_diag(G, dbase, sig, al, k2, l, h));
+    if (r >= 1) win[r * W + (r - 1)] = TF(dc_sub(G, ox, oz, r, 1));
+    if (r >= b) win[r * W + (r - b)] = TF(dc_sub(G, ox, oz, r, b));
   }
   __syncthreads();
   const bool loader = threadIdx.x == blockDim.x - 1;
@@ -149,21 +151,21 @@ __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, 
     const int p0 = q % W;
     // prefetch the entries of band row q+b+1 (enters the window after this step)
     const int nr = q + b + 1;
-    float nd = 0.f, n1 = 0.f, nb_ = 0.f;
+    TF nd = 0, n1 = 0, nb_ = 0;
     if (loader && nr < N) {
       int l, h; dc_lh(G, nr, l, h);
-      nd = float(dc_diag(G, dbase, sig, al, k2, l, h));
-      n1 = float(dc_sub(G, ox, oz, nr, 1));
-      nb_ = float(dc_sub(G, ox, oz, nr, b));
+      nd = TF(dc_diag(G, dbase, sig, al, k2, l, h));
+      n1 = TF(dc_sub(G, ox, oz, nr, 1));
+      nb_ = TF(dc_sub(G, ox, oz, nr, b));
     }
-    const float d = win[p0 * W + p0];
+    const TF d = win[p0 * W + p0];
     if (threadIdx.x == 0) {
       F[size_t(q) * W] = d;
-      if (!(d != 0.f) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
+      if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
     }
     for (int i = threadIdx.x + 1; i <= b; i += blockDim.x) {
       int pi = p0 + i; if (pi >= W) pi -= W;
-      const float li = (q + i < N) ? win[pi * W + p0] / d : 0.f;
+      const TF li = (q + i < N) ? win[pi * W + p0] / d : TF(0);
       lc[i] = li;
       F[size_t(q) * W + i] = li;
     }
@@ -173,20 +175,20 @@ __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, 
       int i = i0, j = j0;
       int pi = p0 + i; if (pi >= W) pi -= W;
       int pj = p0 + j; if (pj >= W) pj -= W;
-      float ci = (i <= b) ? lc[i] * d : 0.f;
+      TF ci = (i <= b) ? lc[i] * d : TF(0);
       for (int e = e0; e < e1; ++e) {
         win[pi * W + pj] -= ci * lc[j];
         if (++j > i) {
           ++i; j = 1;
           if (++pi >= W) pi -= W;
           pj = p0 + 1; if (pj >= W) pj -= W;
-          ci = (i <= b) ? lc[i] * d : 0.f;
+          ci = (i <= b) ? lc[i] * d : TF(0);
         } else if (++pj >= W) pj -= W;
       }
     }
     __syncthreads();
     // slide: row/col q+b+1 enters at the slot of q
-    for (int c = threadIdx.x; c < W; c += blockDim.x) { win[p0 * W + c] = 0.f; win[c * W + p0] = 0.f; }
+    for (int c = threadIdx.x; c < W; c += blockDim.x) { win[p0 * W + c] = TF(0); win[c * W + p0] = TF(0); }
     __syncthreads();
     if (loader && nr < N) {
       win[p0 * W + p0] = nd;
@@ -201,33 +203,35 @@ __global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, 
 // r, z are FP64 vectors in the reference layout [sys][l + h*n].  The rolling
 // windows (b+1 values) live in shared memory per warp; factor columns are
 // loaded one step ahead, and r / z values 32 steps at a time (one per lane).
-__global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, double* z, double* rz,
+template <class TF>
+__global__ void k_dc_precond(const DcGrid G, const TF* fac, const double* r, double* z, double* rz,
                              int nsys, const int* done) {
-  extern __shared__ float shp[];
+  extern __shared__ __align__(16) unsigned char shpraw[];
+  TF* shp = reinterpret_cast<TF*>(shpraw);
   const int W = G.b + 1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sys = blockIdx.x * (blockDim.x >> 5) + warp;
   if (sys >= nsys || (done && done[sys])) return;
-  float* win = shp + warp * W;
-  const float* F = fac + size_t(sys) * size_t(G.N) * W;
+  TF* win = shp + warp * W;
+  const TF* F = fac + size_t(sys) * size_t(G.N) * W;
   const double* R = r + size_t(sys) * G.N;
   double* Z = z + size_t(sys) * G.N;
   const int N = G.N, b = G.b;
   constexpr int MAXI = 7;  // b <= 200 -> at most 7 entries of a column per lane
   auto ref = [&](int q) { int l, h; dc_lh(G, q, l, h); return l + h * G.n; };
-  auto load_col = [&](int q, float (&c)[MAXI]) {
+  auto load_col = [&](int q, TF (&c)[MAXI]) {
 #pragma unroll
     for (int u = 0; u < MAXI; ++u) {
       const int i = lane + 1 + 32 * u;
-      c[u] = (q < N && i <= b) ? F[size_t(q) * W + i] : 0.f;
+      c[u] = (q < N && i <= b) ? F[size_t(q) * W + i] : TF(0);
     }
   };
   // forward: L y = r
-  for (int i = lane; i < W; i += 32) win[i] = (i < N) ? float(R[ref(i)]) : 0.f;
+  for (int i = lane; i < W; i += 32) win[i] = (i < N) ? TF(R[ref(i)]) : TF(0);
   __syncwarp();
-  float col[MAXI], nxt[MAXI];
+  TF col[MAXI], nxt[MAXI];
   load_col(0, col);
-  float dq = F[0];
+  TF dq = F[0];
   double rpre = 0.0;
   for (int q = 0; q < N; ++q) {
     if ((q & 31) == 0) {  // r values entering the window over the next 32 steps
@@ -235,9 +239,9 @@ __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, 
       rpre = (nq < N) ? R[ref(nq)] : 0.0;
     }
     load_col(q + 1, nxt);
-    const float dn = (q + 1 < N) ? F[size_t(q + 1) * W] : 1.f;
+    const TF dn = (q + 1 < N) ? F[size_t(q + 1) * W] : TF(1);
     const int p0 = q % W;
-    const float y = win[p0];
+    const TF y = win[p0];
 #pragma unroll
     for (int u = 0; u < MAXI; ++u) {
       const int i = lane + 1 + 32 * u;
@@ -247,7 +251,7 @@ __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, 
     __syncwarp();
     if (lane == 0) {
       Z[ref(q)] = double(y / dq);
-      win[p0] = (q + W < N) ? float(rin) : 0.f;
+      win[p0] = (q + W < N) ? TF(rin) : TF(0);
     }
     __syncwarp();
 #pragma unroll
@@ -256,7 +260,7 @@ __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, 
   }
   __threadfence_block();
   // backward: L^T x = z, x_q = z_q - sum_i l_{q+i,q} x_{q+i}
-  for (int i = lane; i < W; i += 32) win[i] = 0.f;
+  for (int i = lane; i < W; i += 32) win[i] = TF(0);
   __syncwarp();
   double acc = 0.0;
   load_col(N - 1, col);
@@ -269,7 +273,7 @@ __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, 
       rpre2 = (qq >= 0) ? R[ref(qq)] : 0.0;
     }
     load_col(q - 1 >= 0 ? q - 1 : N, nxt);
-    float s = 0.f;
+    TF s = TF(0);
 #pragma unroll
     for (int u = 0; u < MAXI; ++u) {
       const int i = lane + 1 + 32 * u;
@@ -279,7 +283,7 @@ __global__ void k_dc_precond(const DcGrid G, const float* fac, const double* r, 
     const double zq = __shfl_sync(0xffffffffu, zpre, k);
     const double rq = __shfl_sync(0xffffffffu, rpre2, k);
     if (lane == 0) {
-      const float x = float(zq) - s;
+      const TF x = TF(zq) - s;
       win[q % W] = x;
       Z[ref(q)] = double(x);
       acc += rq * double(x);
@@ -318,31 +322,38 @@ __global__ void k_dc_apply(const DcGrid G, const double* ox, const double* oz, c
   }
 }
 
-// CG update: alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = r.r
+// CG update: alpha = rz/pAp; x += alpha p; r -= alpha Ap; rr = r.r and
+// rzo = r_new . z_old (for the flexible Polak-Ribiere beta, since the FP32
+// preconditioner is only symmetric to rounding).
 __global__ void k_dc_cg_xr(int N, const double* rz, const double* pap, double* x, double* r, const double* p,
-                           const double* ap, double* rr, int nsys, const int* done) {
+                           const double* ap, const double* z, double* rr, double* rzo, int nsys, const int* done) {
   const int sys = blockIdx.y;
   if (sys >= nsys || (done && done[sys])) return;
   const double den = pap[sys];
   const double a = (den != 0.0) ? rz[sys] / den : 0.0;
   const size_t o = size_t(sys) * N;
-  double part = 0;
+  double part = 0, part2 = 0;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += blockDim.x * gridDim.x) {
     x[o + t] += a * p[o + t];
     const double v = r[o + t] - a * ap[o + t];
     r[o + t] = v;
     part += v * v;
+    part2 += v * z[o + t];
   }
-  for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
-  if ((threadIdx.x & 31) == 0) atomicAdd(rr + sys, part);
+  for (int off = 16; off > 0; off >>= 1) {
+    part += __shfl_down_sync(0xffffffffu, part, off);
+    part2 += __shfl_down_sync(0xffffffffu, part2, off);
+  }
+  if ((threadIdx.x & 31) == 0) { atomicAdd(rr + sys, part); atomicAdd(rzo + sys, part2); }
 }
 
-// p = z + beta p with beta = rz_new / rz_old (p = z when first).
-__global__ void k_dc_cg_p(int N, const double* rz_new, const double* rz_old, const double* z, double* p,
-                          int first, int nsys, const int* done) {
+// p = z + beta p, beta = (r.z_new - r.z_old) / rz_old (flexible CG); p = z when first.
+__global__ void k_dc_cg_p(int N, const double* rz_new, const double* rz_old, const double* rzo, const double* z,
+                          double* p, int first, int nsys, const int* done) {
   const int sys = blockIdx.y;
   if (sys >= nsys || (done && done[sys])) return;
-  const double beta = first ? 0.0 : (rz_old[sys] != 0.0 ? rz_new[sys] / rz_old[sys] : 0.0);
+  double beta = 0.0;
+  if (!first && rz_old[sys] != 0.0) beta = (rz_new[sys] - (rzo ? rzo[sys] : 0.0)) / rz_old[sys];
   const size_t o = size_t(sys) * N;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < N; t += blockDim.x * gridDim.x)
     p[o + t] = z[o + t] + beta * p[o + t];

@@ -79,6 +79,7 @@ struct DcPlan {
   std::vector<long> off;
 };
 
+template <class TF>
 static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B, double* X, double tol, int maxit,
                      int& iters, double& relmax, cudaStream_t st) {
   const DcGrid& G = P.G;
@@ -91,6 +92,7 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   double* d = P.dots.as<double>();
   double* rzA = d; double* rzB = d + nsys; double* pap = d + 2 * nsys; double* rr = d + 3 * nsys;
   double* bb = d + 4 * nsys;
+  double* rzo = d + 5 * nsys;
   int* done = P.done.as<int>();
   const double* ox = P.faces.as<double>();
   const double* oz = ox + N;
@@ -98,10 +100,10 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   const double* sg = P.sig.as<double>();
   const double* al = P.alpha.as<double>();
   const double* k2 = P.ky2.as<double>();
-  const float* F = P.fac.as<float>();
+  const TF* F = P.fac.as<TF>();
   const dim3 gv((N + 255) / 256 < 64 ? (N + 255) / 256 : 64, nsys);
   const int warps_per_block = 4;
-  const size_t shp = size_t(warps_per_block) * (G.b + 1) * sizeof(float);
+  const size_t shp = size_t(warps_per_block) * (G.b + 1) * sizeof(TF);
   const int pblocks = (nsys + warps_per_block - 1) / warps_per_block;
   GJ_CUDA(err, cudaMemsetAsync(X, 0, vn * sizeof(double), st));
   GJ_CUDA(err, cudaMemcpyAsync(R, B, vn * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -109,8 +111,8 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   GJ_CUDA(err, cudaMemsetAsync(bb, 0, nsys * sizeof(double), st));
   GJ_CUDA(err, cudaMemsetAsync(rr, 0, nsys * sizeof(double), st));
   k_dc_residual<<<gv, 256, 0, st>>>(N, B, X, R, rr, bb, nsys);  // r = b (x = 0)
-  k_dc_precond<<<pblocks, 32 * warps_per_block, shp, st>>>(G, F, R, Z, rzA, nsys, done);
-  k_dc_cg_p<<<gv, 256, 0, st>>>(N, rzA, rzA, Z, Pv, 1, nsys, done);
+  k_dc_precond<TF><<<pblocks, 32 * warps_per_block, shp, st>>>(G, F, R, Z, rzA, nsys, done);
+  k_dc_cg_p<<<gv, 256, 0, st>>>(N, rzA, rzA, nullptr, Z, Pv, 1, nsys, done);
   c.launches += 3;
   std::vector<double> hbb(nsys), hrr(nsys);
   std::vector<int> hdone(nsys, 0);
@@ -119,11 +121,12 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   for (int it = 0; it < maxit; ++it) {
     GJ_CUDA(err, cudaMemsetAsync(pap, 0, nsys * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(rr, 0, nsys * sizeof(double), st));
+    GJ_CUDA(err, cudaMemsetAsync(rzo, 0, nsys * sizeof(double), st));
     const bool tm = c.timer.begin(KK_DC, st, nsys);
     k_dc_apply<<<gv, 256, 0, st>>>(G, ox, oz, db, sg, al, k2, sys0, Pv, AP, pap, nsys, done);
-    k_dc_cg_xr<<<gv, 256, 0, st>>>(N, rzA, pap, X, R, Pv, AP, rr, nsys, done);
-    k_dc_precond<<<pblocks, 32 * warps_per_block, shp, st>>>(G, F, R, Z, rzB, nsys, done);
-    k_dc_cg_p<<<gv, 256, 0, st>>>(N, rzB, rzA, Z, Pv, 0, nsys, done);
+    k_dc_cg_xr<<<gv, 256, 0, st>>>(N, rzA, pap, X, R, Pv, AP, Z, rr, rzo, nsys, done);
+    k_dc_precond<TF><<<pblocks, 32 * warps_per_block, shp, st>>>(G, F, R, Z, rzB, nsys, done);
+    k_dc_cg_p<<<gv, 256, 0, st>>>(N, rzB, rzA, rzo, Z, Pv, 0, nsys, done);
     c.timer.end(tm, st);
     c.launches += 4;
     std::swap(rzA, rzB);
@@ -153,9 +156,10 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   return GJ_OK;
 }
 
-gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_src* srcs, int nsrc, bool grad,
-                 const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
-                 double* misfit_out, gj_dc_stats* stats) {
+template <class TF>
+static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_src* srcs, int nsrc,
+                          bool grad, const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
+                          double* misfit_out, gj_dc_stats* stats) {
   Err& err = c.err;
   if (!sigma || !srcs || nsrc < 1) return err.set(GJ_EINVAL, "null sigma/sources or nsrc < 1");
   if (gg.n < 3 || gg.m < 3 || gg.n_ky < 1 || gg.robin < 0 || 2 * gg.robin >= gg.n || gg.robin >= gg.m)
@@ -168,7 +172,8 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
   G.b = std::min(gg.n, gg.m);
   G.DX = gg.dx; G.DZ = gg.dz;
   G.nb = 2 * (gg.m - 2) + (gg.n - 2) + 4;
-  if (G.b > 200) return err.set(GJ_EUNSUPPORTED, "band width min(n, m) = %d above 200", G.b);
+  if (G.b > (sizeof(TF) == 8 ? 140 : 200))
+    return err.set(GJ_EUNSUPPORTED, "band width min(n, m) = %d above the shared-memory window limit", G.b);
   P.nky = gg.n_ky; P.nsrc = nsrc; P.robin = gg.robin;
   const int N = G.N, nky = P.nky, nsys_all = nsrc * nky;
   cudaStream_t st = 0;
@@ -231,20 +236,20 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
   size_t free_b = 0, total_b = 0;
   GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
   const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.7 * double(free_b));
-  const size_t per_sys = size_t(N) * (G.b + 1) * sizeof(float) + size_t(N) * 8 * sizeof(double) + 64;
+  const size_t per_sys = size_t(N) * (G.b + 1) * sizeof(TF) + size_t(N) * 8 * sizeof(double) + 64;
   int srcs_per_batch = int(std::min<size_t>(nsrc, std::max<size_t>(1, budget / (per_sys * nky))));
   if (o.sources_per_batch > 0) srcs_per_batch = std::min(srcs_per_batch, o.sources_per_batch);
   const int nsys_b = srcs_per_batch * nky;
-  GJ_TRY(P.fac.alloc(err, size_t(nsys_b) * N * (G.b + 1) * sizeof(float)));
+  GJ_TRY(P.fac.alloc(err, size_t(nsys_b) * N * (G.b + 1) * sizeof(TF)));
   GJ_TRY(P.vec.alloc(err, size_t(nsys_b) * N * 7 * sizeof(double)));  // B, X, R, Z, P, AP, U
-  GJ_TRY(P.dots.alloc(err, 5 * size_t(nsys_b) * sizeof(double)));
+  GJ_TRY(P.dots.alloc(err, 6 * size_t(nsys_b) * sizeof(double)));
   GJ_TRY(P.done.alloc(err, nsys_b * sizeof(int)));
   const double tol = o.tol > 0 ? o.tol : 1e-10;
   const int maxit = o.max_iter > 0 ? o.max_iter : 50;
   int it_max = 0;
   double rel_max = 0;
-  const size_t smem_f = size_t(G.b + 1) * (G.b + 2) * sizeof(float);
-  GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
+  const size_t smem_f = size_t(G.b + 1) * (G.b + 2) * sizeof(TF);
+  GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
   double* V = P.vec.as<double>();
   for (int s0 = 0; s0 < nsrc; s0 += srcs_per_batch) {
     const int nsb = std::min(srcs_per_batch, nsrc - s0);
@@ -256,8 +261,8 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
     // factor
     {
       const bool tm = c.timer.begin(KK_DC, st, nsys);
-      k_dc_factor<<<nsys, 128, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(), P.alpha.as<double>(),
-                                             P.ky2.as<double>(), sys0, P.fac.as<float>(), P.status.as<int>());
+      k_dc_factor<TF><<<nsys, 128, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(), P.alpha.as<double>(),
+                                                 P.ky2.as<double>(), sys0, P.fac.as<TF>(), P.status.as<int>());
       c.timer.end(tm, st);
       ++c.launches;
     }
@@ -266,7 +271,7 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
     k_dc_rhs_src<<<(nsys + 127) / 128, 128, 0, st>>>(N, P.ab.as<long>(), P.cur.as<double>(), nky, sys0, nsys, B);
     ++c.launches;
     int iters = 0; double rel = 0;
-    GJ_TRY(pcg(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
+    GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
     it_max = std::max(it_max, iters); rel_max = std::max(rel_max, rel);
     GJ_CUDA(err, cudaMemcpyAsync(U, X, vn * sizeof(double), cudaMemcpyDeviceToDevice, st));
     k_dc_data<<<dim3(4, nsb), 256, 0, st>>>(N, nky, s0, nsb, P.mnoff.as<long>(), P.mnbuf.as<long>(), P.wts.as<double>(),
@@ -293,7 +298,7 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
       k_dc_rhs_adj<<<dim3(1, nsb), 256, 0, st>>>(N, nky, s0, nsb, P.mnoff.as<long>(), P.mnbuf.as<long>(),
                                                  P.ebuf.as<double>(), B);
       ++c.launches;
-      GJ_TRY(pcg(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
+      GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
       it_max = std::max(it_max, iters); rel_max = std::max(rel_max, rel);
       k_dc_sens<<<dim3(64, nsys), 256, 0, st>>>(G, P.sig.as<double>(), P.alpha.as<double>(), P.ky2.as<double>(),
                                                 P.wts.as<double>(), sys0, nky, U, X, P.gbuf.as<double>(), nsys);
@@ -338,6 +343,14 @@ gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_
     }
   }
   return GJ_OK;
+}
+
+gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_src* srcs, int nsrc, bool grad,
+                 const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
+                 double* misfit_out, gj_dc_stats* stats) {
+  if (o.factor_fp32)
+    return dc_run_t<float>(c, gg, sigma, srcs, nsrc, grad, o, d_out, e_out, u_out, g_out, misfit_out, stats);
+  return dc_run_t<double>(c, gg, sigma, srcs, nsrc, grad, o, d_out, e_out, u_out, g_out, misfit_out, stats);
 }
 
 }  // namespace gj

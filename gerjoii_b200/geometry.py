@@ -128,11 +128,18 @@ def w_wavelet(t: np.ndarray, ampli: float, tau: float) -> np.ndarray:
 
 def surface_acquisition(grid: WGrid, nsrc: int, nrec: int, wavelet: np.ndarray,
                         row: int = 0, margin: int = 2) -> list[Shot]:
-    """Sources and receivers evenly spaced on model row ``row`` (0-based)."""
+    """Sources and receivers evenly spaced on model row ``row`` (0-based); a
+    single source sits at the centre, and no source shares a receiver's node."""
     i = grid.dom_i0 + row
-    js = np.linspace(margin, grid.n - 1 - margin, nsrc).round().astype(int) + grid.dom_j0
     jr = np.linspace(margin, grid.n - 1 - margin, nrec).round().astype(int) + grid.dom_j0
     # keep receivers off the model's first column (it lies in the PML band)
     jr = np.clip(jr, grid.dom_j0 + 1, grid.dom_j0 + grid.n - 1)
+    if nsrc == 1:
+        js = np.array([grid.dom_j0 + grid.n // 2])
+    else:
+        js = np.linspace(margin, grid.n - 1 - margin, nsrc).round().astype(int) + grid.dom_j0
+    # no source on a receiver node: move it to the next free column
+    taken = set(int(j) for j in jr)
+    js = np.array([j + 1 if int(j) in taken and int(j) + 1 < grid.dom_j0 + grid.n else j for j in js])
     rec = np.array([grid.node(i, j) for j in jr], dtype=np.int64)
     return [Shot(int(i), int(j), np.asarray(wavelet, np.float64), rec) for j in js]

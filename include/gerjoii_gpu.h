@@ -180,6 +180,8 @@ typedef struct gj_dc_opts {
   int per_source;          /* 1 = one gradient per source, else their sum */
   int sources_per_batch;   /* 0 = as many as fit mem_budget_bytes */
   size_t mem_budget_bytes; /* 0 = 70% of free device memory */
+  int factor_fp32;         /* 1 = FP32 band factor as the preconditioner (half the memory;
+                              converges slowly for the smallest ky), else FP64 */
 } gj_dc_opts;
 
 typedef struct gj_dc_stats {

@@ -70,3 +70,44 @@ def test_dc_halfspace_matches_analytic_potential(gpu_ctx):
     mask[abs(np.arange(n) - lb)[:, None].repeat(m, 1) < 4] = False
     err = np.abs(u[mask] - ua[mask]) / np.abs(ua[mask]).max()
     assert err.max() < 0.10 and np.median(err) < 0.02, (err.max(), np.median(err))
+
+
+def test_dc_full_survey_converges_in_few_iterations(gpu_ctx):
+    """400 x 100 cells, 200 dipole-dipole sources x 20 wavenumbers: the FP64 band
+    factor makes the preconditioner (numerically) exact, so CG reaches 1e-10 in a
+    handful of iterations for every wavenumber, down to ky dx = 2.5e-4 where the
+    operator is nearly singular; the adjoint solves of noisy data converge too,
+    and the gradient of two sources matches the direct-solve oracle."""
+    import np_dc_oracle as dco
+    from gerjoii_b200 import synth
+    c = synth.cfg5()
+    fw = gpu_ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], c["srcs"])
+    assert fw["rel_residual"] <= 1e-10 and fw["iters"] <= 6, (fw["iters"], fw["rel_residual"])
+    rng = np.random.default_rng(5)
+    for q, d in zip(c["srcs"], fw["d"]):
+        q.d_obs = d * (1 + 0.02 * rng.standard_normal(d.shape))
+    gr = gpu_ctx.dc_gradient(c["SIG"], c["DX"], c["DZ"], c["robin"], c["srcs"])
+    assert gr["rel_residual"] <= 1e-10 and gr["iters"] <= 8, (gr["iters"], gr["rel_residual"])
+    case = dict(c, srcs=c["srcs"][:2])
+    n, m, robin = c["n"], c["m"], c["robin"]
+    g = np.zeros((n - 2 * robin, m - robin))
+    for q, r in zip(case["srcs"], oracle_forward(dco, case)):
+        g += dco.dc_gradient2_5d(c["SIG"], c["DX"], c["DZ"], oracle_alphas(dco, case, q), q.ky_w,
+                                 dco.measuring_operator(n, m, q.mn), r[1], r[3], robin)
+    g2 = gpu_ctx.dc_gradient(c["SIG"], c["DX"], c["DZ"], robin, case["srcs"])["g"]
+    assert rel_l2(g2, g) < 1e-8
+
+
+def test_dc_fp32_factor_option(gpu_ctx):
+    """factor_fp32 = 1 keeps an FP32 band factor as the preconditioner (half
+    the memory); the FP64 iterations still meet the same tolerance."""
+    case = small_dc(seed=2)
+    o = N.DcOptsC()
+    o.factor_fp32 = 1
+    o.max_iter = 200
+    a = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], opts=o)
+    b = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
+    assert a["rel_residual"] <= 1e-10 and b["rel_residual"] <= 1e-10
+    assert b["iters"] <= a["iters"]
+    for x, y in zip(a["d"], b["d"]):
+        assert rel_l2(x, y) < 1e-9
