@@ -144,7 +144,7 @@ struct KernelTimer {
 };
 
 // Kernel kinds reported by gj_kernel_time().
-enum KernelKind { KK_FWD_STEP = 0, KK_REF_STEP = 1, KK_ADJ_STEP = 2, KK_IO = 3, KK_PLAIN = 4, KK_DC = 5 };
+enum KernelKind { KK_FWD_STEP = 0, KK_REF_STEP = 1, KK_ADJ_STEP = 2, KK_IO = 3, KK_PLAIN = 4, KK_DC = 5, KK_IMAGE = 6 };
 
 struct Ctx {
   int device = 0;

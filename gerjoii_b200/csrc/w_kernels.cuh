@@ -526,6 +526,9 @@ __global__ void k_build_coefs(const CoefBuild c, const TM* eps, const TM* sig, T
       vay = 1.0; vby = -dt / (dy * e0 * e);
     }
   }
+  // Free top: the Ez = 0 row keeps Ez (Ceze = 1, Cezhy = 0) in the interior
+  // columns, so a kernel may apply the interior update there without a branch.
+  if (c.Pt == 0 && I == 0 && J >= c.P + 1 && J <= c.NY - c.P - 1) { vce = 1.0; vch = 0.0; }
   ce[k] = T(vce); chy[k] = T(vch);
   ce_r[k] = T(rce); chy_r[k] = T(rch);
   ax[k] = T(vax); bx[k] = T(vbx); ay[k] = T(vay); by[k] = T(vby);

@@ -12,6 +12,7 @@
 #include "gj_internal.h"
 #include "w_kernels.cuh"
 #include "w_kernels_vec.cuh"
+#include "w_kernels_ring.cuh"
 #include "w_misfit.cuh"
 
 namespace gj {
@@ -103,6 +104,12 @@ class WSolver : public WSolverBase {
   int K = 0;
   // launch shape
   int bx = 128, tj = 16;
+  // warp-task ring kernels (w_kernels_ring.cuh): threads per CTA (0 = not
+  // available for T), ring stages, resident CTAs per SM, SMs; ring_on per call
+  int ring_nth = 0, ring_S = 0, ring_nb = 0, nsm = 148;
+  bool ring_on = false;
+  int Kd = 16;   // adjoint steps per imaging pass (slots of the l ring)
+  DevBuf lring;
 
 
   static std::string key(const gj_w_grid& g, const gj_w_shot* shots, int nshots) {
@@ -244,7 +251,124 @@ class WSolver : public WSolverBase {
     const long blocks_per_col = (ld + bx - 1) / bx;
     tj = 64;
     while (tj > 4 && blocks_per_col * ((NY + tj) / tj) * ns < 148L * 16) tj /= 2;
+    GJ_TRY(ring_setup(err));
+    ring_on = ring_nth > 0;
     return GJ_OK;
+  }
+
+  // Launch shape of the warp-task ring kernels (w_kernels_ring.cuh): CTAs of
+  // RW warps, S ring stages (GJ_RING_STAGES, default 2), one task per warp.
+  static constexpr int RW = 4;
+  template <int S>
+  gj_status ring_attr(Err& err, size_t sm) {
+    GJ_CUDA(err, cudaFuncSetAttribute(k_fwdw<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    GJ_CUDA(err, cudaFuncSetAttribute(k_adjw<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    int nb = 0;
+    GJ_CUDA(err, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_adjw<T, S>, 32 * RW, sm));
+    ring_nb = std::max(nb, 1);
+    return GJ_OK;
+  }
+  gj_status ring_setup(Err& err) {
+    ring_nth = 0;
+    tasks.clear();
+    if constexpr (VT<T>::V * sizeof(T) == 16) {
+      int dev = 0, maxsm = 0;
+      GJ_CUDA(err, cudaGetDevice(&dev));
+      GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+      GJ_CUDA(err, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+      int S = 2;
+      if (const char* e = getenv("GJ_RING_STAGES")) S = std::min(std::max(atoi(e), 2), 4);
+      while (S > 2 && ring_smem(RW, S) > size_t(maxsm)) --S;
+      const size_t sm = ring_smem(RW, S);
+      if (sm > size_t(maxsm)) return GJ_OK;
+      ring_nth = 32 * RW;
+      ring_S = S;
+      if (S == 2) GJ_TRY(ring_attr<2>(err, sm));
+      else if (S == 3) GJ_TRY(ring_attr<3>(err, sm));
+      else GJ_TRY(ring_attr<4>(err, sm));
+      if (const char* e = getenv("GJ_IMAGE_WINDOW")) Kd = std::min(std::max(atoi(e), 1), 256);
+    }
+    return GJ_OK;
+  }
+  // Fast rows of the ring kernels: interior Ez rows (plus the free-top Ez = 0
+  // row, whose Ceze/Cezhy are 1/0) that are also Hy interior rows.
+  bool fast_row(int I) const {
+    const bool e = (I >= w.ei0 && I <= w.ei1) || (I == 0 && g.pml_top == 0);
+    return e && I >= w.hyi0 && I <= w.hyi1;
+  }
+  bool interior_row(int I) const { return I >= w.ei0 && I <= w.ei1 && I >= w.hyi0 && I <= w.hyi1; }
+  // Task table for launches of gn shots (built outside graph capture).
+  struct TaskTable { DevBuf buf; int n = 0; };
+  std::map<int, std::unique_ptr<TaskTable>> tasks;
+  gj_status prepare_tasks(Err& err, int gn) {
+    if (ring_nth == 0 || tasks.count(gn)) return GJ_OK;
+    constexpr int V = VT<T>::V;
+    const int rows = 32 * V, nrb = (NX + 1 + rows - 1) / rows;
+    std::vector<int> fast(nrb, 0);
+    int nF = 0;
+    for (int rb = 0; rb < nrb; ++rb) {
+      const int r0 = rb * rows;
+      bool f = (r0 == 0 || interior_row(r0 - 1)) && interior_row(r0 + rows);
+      for (int I = r0; f && I < r0 + rows; ++I) f = fast_row(I);
+      fast[rb] = f ? 1 : 0;
+      nF += fast[rb];
+    }
+    const int nS = nrb - nF;
+    // column chunks: a general-path block costs about 4x a fast block per
+    // column; chunks sized for GJ_RING_WAVES (default 1.5) waves of resident warps
+    double waves = 1.5;
+    if (const char* e = getenv("GJ_RING_WAVES")) waves = std::max(0.25, atof(e));
+    const double nbw = double(ring_nb) * RW * nsm;
+    int tjF = int(std::ceil(double(NY + 1) * (nF + 4.0 * nS) * gn / (waves * nbw)));
+    tjF = std::min(std::max(tjF, 16), NY + 1);
+    const int tjS = std::max(4, tjF / 4);
+    std::vector<int4> h;
+    for (int pass = 0; pass < 2; ++pass)  // general-path tasks first
+      for (int z = 0; z < gn; ++z)
+        for (int rb = 0; rb < nrb; ++rb) {
+          if (fast[rb] != pass) continue;
+          const int tjr = fast[rb] ? tjF : tjS;
+          for (int j0 = 0; j0 <= NY; j0 += tjr)
+            h.push_back(make_int4(rb * rows, j0, std::min(j0 + tjr - 1, NY), (z << 1) | fast[rb]));
+        }
+    auto tt = std::make_unique<TaskTable>();
+    GJ_TRY(tt->buf.alloc(err, h.size() * sizeof(int4)));
+    GJ_CUDA(err, cudaMemcpy(tt->buf.p, h.data(), h.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    tt->n = int(h.size());
+    tasks.emplace(gn, std::move(tt));
+    return GJ_OK;
+  }
+
+  // One forward step of gn shots (A -> B).
+  void launch_fwd(StepArgs<T> a, int gn, cudaStream_t st) {
+    if constexpr (VT<T>::V * sizeof(T) == 16) {
+      if (ring_on) {
+        const TaskTable& tt = *tasks.at(gn);
+        const dim3 grd((tt.n + RW - 1) / RW);
+        const size_t sm = ring_smem(RW, ring_S);
+        const int4* tk = static_cast<const int4*>(tt.buf.p);
+        if (ring_S == 2) k_fwdw<T, 2><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+        else if (ring_S == 3) k_fwdw<T, 3><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+        else k_fwdw<T, 4><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+        return;
+      }
+    }
+    constexpr int V = VT<T>::V;
+    a.tj = tj_for(gn);
+    const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + a.tj - 1) / a.tj, gn);
+    k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+  }
+  // One exact adjoint step of gn shots with the l ring (ring kernels only).
+  void launch_adjr(AdjRingArgs<T> a, int gn, cudaStream_t st) {
+    if constexpr (VT<T>::V * sizeof(T) == 16) {
+      const TaskTable& tt = *tasks.at(gn);
+      const dim3 grd((tt.n + RW - 1) / RW);
+      const size_t sm = ring_smem(RW, ring_S);
+      const int4* tk = static_cast<const int4*>(tt.buf.p);
+      if (ring_S == 2) k_adjw<T, 2><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+      else if (ring_S == 3) k_adjw<T, 3><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+      else k_adjw<T, 4><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+    }
   }
 
   // Coefficients from the model (host doubles or device T / double).
@@ -299,14 +423,12 @@ class WSolver : public WSolverBase {
     DevBuf jzb, ub;
     if (jz_out) GJ_TRY(jzb.alloc(err, size_t(nshots) * g.nt * sizeof(T)));
     if (u_out) GJ_TRY(ub.alloc(err, size_t(nshots) * dn * (g.nt + 1) * sizeof(T)));
-    constexpr int V = VT<T>::V;
-    const int tjf = tj_for(nshots);
-    const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + tjf - 1) / tjf, nshots);
+    ring_on = ring_nth > 0;
+    GJ_TRY(prepare_tasks(err, nshots));
     for (int it = 0; it < g.nt; ++it) {
       StepArgs<T> a = step_args(A, B, it);
-      a.tj = tjf;
       if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * dn; a.hstride = dn; }
-      k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+      launch_fwd(a, nshots, st);
       k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
                                                    g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
                                                    nshots);
@@ -349,10 +471,11 @@ class WSolver : public WSolverBase {
     const size_t per_slot = size_t(nshots) * dn * sizeof(T);
     const size_t per_ck = size_t(nshots) * sstride * sizeof(T);
     if (o.ckpt_every > 0) { K = std::min(std::max(o.ckpt_every, 2), g.nt); return; }
-    if (size_t(g.nt + 1) * per_slot <= budget) { K = g.nt; return; }
+    const size_t extra = ring_on ? size_t(Kd) * per_slot : 0;  // the l ring
+    if (size_t(g.nt + 1) * per_slot + extra <= budget) { K = g.nt; return; }
     double k = std::sqrt(double(g.nt) * double(per_ck) / double(per_slot));
     K = std::min(std::max(int(k), 2), g.nt);
-    while (K > 2 && (size_t(g.nt / K + 2) * per_ck + size_t(K + 3) * per_slot) > budget) K = K * 3 / 4;
+    while (K > 2 && (size_t(g.nt / K + 2) * per_ck + size_t(K + 3) * per_slot + extra) > budget) K = K * 3 / 4;
   }
 
   // Inputs of a gradient call on the device: coefficients built from the model,
@@ -543,7 +666,7 @@ class WSolver : public WSolverBase {
     }
     if (o.ckpt_every > 0) return nshots;
     const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.8 * double(free_bytes));
-    const size_t per_shot = (size_t(g.nt + 1) * dn + 4 * sstride) * sizeof(T);
+    const size_t per_shot = (size_t(g.nt + 1 + (ring_on ? Kd : 0)) * dn + 4 * sstride) * sizeof(T);
     const int fit = int(std::min<size_t>(budget / std::max<size_t>(per_shot, 1), size_t(nshots)));
     if (fit >= nshots) return nshots;
     if (fit >= std::min(8, nshots)) {
@@ -595,10 +718,10 @@ class WSolver : public WSolverBase {
         ++segi;
       }
       StepArgs<T> a = step_args(A, B, it);
-      a.shot0 = g0; a.tj = tjg;
+      a.shot0 = g0;
       if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
       const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
-      k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+      launch_fwd(a, gn, st);
       c.timer.end(tm, st);
       k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, rec, nrr, nrs_d, it, nt, dgrp, d_src + g0,
                                                static_cast<T*>(nullptr), gn);
@@ -630,15 +753,16 @@ class WSolver : public WSolverBase {
         const int iend = std::min(s1 + 1, nt);
         for (int it = s0; it < iend; ++it) {
           StepArgs<T> a = step_args(A, B, it);
-          a.shot0 = g0; a.tj = tjg;
+          a.shot0 = g0;
           a.hist = slot_ptr(it + 1, base); a.hstride = hs;
           const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
-          k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+          launch_fwd(a, gn, st);
           c.timer.end(tm, st);
           ++nl;
           std::swap(A, B);
         }
       }
+      int win = 0;  // adjoint steps in the l ring not yet imaged
       for (int k = s1; k >= s0 + 1; --k) {  // k = history slot of forward step k-1
         const int itf = k - 1;
         if (mode == GJ_ADJ_REFERENCE) {
@@ -656,6 +780,28 @@ class WSolver : public WSolverBase {
           const bool tm = c.timer.begin(KK_REF_STEP, st, gn);
           k_stepv<T, 1><<<grd, 128, 0, st>>>(wr, a);
           c.timer.end(tm, st);
+        } else if (ring_on) {
+          if (nr > 0)
+            k_inject_add<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, nrr, nrs_d, egrp, itf, nt, gn);
+          AdjRingArgs<T> a{};
+          a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = g0;
+          a.lout = lring.as<T>() + size_t(win) * gn * hs; a.hstride = hs;
+          const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
+          launch_adjr(a, gn, st);
+          c.timer.end(tm, st);
+          ++win;
+          if (win == Kd || k == s0 + 1) {
+            // imaging over the steps k + win - 1 .. k
+            const bool ti = c.timer.begin(KK_IMAGE, st, gn);
+            const int ng = (w.di0 + g.m - 1) / V - w.di0 / V + 1;
+            const int nblk = int(std::min<long>((long(ng) * g.n + 255) / 256, 4L * nsm));
+            k_image<T><<<dim3(nblk, gn), 256, 0, st>>>(w, lring.as<T>(), size_t(gn) * hs,
+                                                       slot_ptr(k + win - 1, base), size_t(gn) * hs, win, hs,
+                                                       acc.as<T>(), 4 * dn, g0, kahan);
+            c.timer.end(ti, st);
+            win = 0;
+            ++nl;
+          }
         } else {
           if (nr > 0)
             k_inject_add<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, nrr, nrs_d, egrp, itf, nt, gn);
@@ -684,6 +830,7 @@ class WSolver : public WSolverBase {
       return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
     }
     const bool env = (mk == GJ_MISFIT_ENV_L2);
+    ring_on = ring_nth > 0 && !o.no_ring;
     // memory plan for one group
     size_t free_b = 0, total_b = 0;
     GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
@@ -711,10 +858,23 @@ class WSolver : public WSolverBase {
     GJ_TRY(adjA.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(adjB.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
+    if (ring_on && mode == GJ_ADJ_EXACT) {
+      const void* lold = lring.p;
+      GJ_TRY(lring.alloc(err, size_t(Kd) * G * dn * sizeof(T)));
+      if (lring.p != lold) {
+        drop_graphs();
+        // rows that no lane writes stay zero
+        GJ_CUDA(err, cudaMemsetAsync(lring.p, 0, size_t(Kd) * G * dn * sizeof(T), st));
+      }
+    }
     void* nw[5] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p};
     for (int q = 0; q < 5; ++q)
       if (old[q] != nw[q]) { drop_graphs(); break; }
     const int kahan = o.no_kahan ? 0 : 1;
+    if (ring_on) {
+      GJ_TRY(prepare_tasks(err, G));
+      if (nshots % G) GJ_TRY(prepare_tasks(err, nshots % G));
+    }
     GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
     long nl = 0;
@@ -744,7 +904,8 @@ class WSolver : public WSolverBase {
         continue;
       }
       char kb[96];
-      snprintf(kb, sizeof kb, "%d/%d/%d/%d/%d/%d/%d", g0, gn, int(mode), kahan, K, G, c.timer.on ? 1 : 0);
+      snprintf(kb, sizeof kb, "%d/%d/%d/%d/%d/%d/%d/%d/%d", g0, gn, int(mode), kahan, K, G, c.timer.on ? 1 : 0,
+               ring_on ? 1 : 0, Kd);
       auto itg = graphs.find(kb);
       if (itg == graphs.end()) {
         auto rec = std::make_unique<GraphRec>();

@@ -83,6 +83,8 @@ typedef struct gj_w_opts {
   int no_graph;          /* 1 = launch the time loop without CUDA graphs */
   int per_shot;          /* 1 = g_eps/g_sig hold nshots gradients (m*n each), else their sum */
   int plain;             /* 1 = the plain form: one half-step per launch, one shot at a time */
+  int no_ring;           /* 1 = register-marching step kernels instead of the warp-task ring
+                            kernels (the default for 16-byte vectors: FP32 and FP64) */
 } gj_w_opts;
 
 /* ---------------------------------------------------------------- context */
