@@ -285,6 +285,10 @@ def main():
             dist.all_reduce(ge_t)
             dist.all_reduce(gs_t)
 
+    # kernel timing is on during the warm-up as well: the CUDA graphs captured
+    # there (one per shot group, with the sampled timing events) are the ones
+    # the timed steps replay; switching it on again only clears the counters
+    ctx.set_kernel_timing(True)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -307,7 +311,7 @@ def main():
         dist.barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
-    ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step")}
+    ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step", "image")}
     ktimes = {k: v for k, v in ktimes.items() if v["launches"] > 0}
     ctx.set_kernel_timing(False)
     if world > 1:
@@ -319,35 +323,52 @@ def main():
     cells = g.NX * g.NY
     mn = g.m * g.n
     # cell-updates in the timed region: every forward, recompute and adjoint launch
-    upd = sum(k["shot_launches"] for k in ktimes.values()) * cells * world
+    upd = sum(ktimes[k]["shot_launches"] for k in ktimes if k != "image") * cells * world
     gcell = upd / (ms / 1e3) / 1e9
-    # algorithmic bytes per shot for each kernel kind
-    per_shot_bytes = {
-        "fwd_step": cells * 32.0,             # read Ez,Hx,Hy,Ceze,Cezhy; write Ez,Hx,Hy
-        "adj_step": cells * 32.0 + mn * 40.0,  # + 2 history reads + 4 Kahan sums r/w
-        "ref_step": cells * 32.0 + mn * 48.0,  # + 4 history reads + 4 Kahan sums r/w
+    # Algorithmic DRAM bytes of each kernel kind over the timed region.
+    #  fwd_step (k_fwdw): read Ez, Hx, Hy, Ceze, Cezhy + write Ez, Hx, Hy = 32 B per
+    #    padded cell, + 4 B per model node for the history write.
+    #  adj_step (k_adjw): the transposed stencil, 32 B per padded cell, + 4 B per
+    #    model node for the adjoint-field ring write.
+    #  image (k_image): per imaged step 8 B per model node (adjoint field + E
+    #    history), per launch 36 B per model node (one more E slot, the four
+    #    compensated accumulators read and written).
+    #  ref_step (k_stepv<float,1>): 32 B per cell + 48 B per model node (4 history
+    #    reads, 4 accumulators read and written).
+    adj_sl = ktimes.get("adj_step", {}).get("shot_launches", 0)
+    alg = {
+        "fwd_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0),
+        "adj_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0),
+        "image": lambda k: adj_sl * mn * 8.0 + k["shot_launches"] * mn * 36.0,
+        "ref_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 48.0),
     }
-    hist_launch_bytes = mn * 4.0               # history write of a forward launch that stores u
+    kname = {"fwd_step": "k_fwdw<float,2>", "adj_step": "k_adjw<float,2>", "image": "k_image<float>",
+             "ref_step": "k_stepv<float,1>"}
     pk, pk_src = peaks()
+    kern = {}
+    for kk, kt in ktimes.items():
+        tot_s = kt["avg_us"] * kt["launches"] / 1e6
+        b = alg[kk](kt)
+        kern[kk] = {"kernel": kname[kk], "launches": kt["launches"], "timed_launches": kt["sampled"],
+                    "avg_launch_us": kt["avg_us"], "ms_per_step": tot_s * 1e3 / args.steps,
+                    "algorithmic_bytes_per_launch": b / max(kt["launches"], 1),
+                    "achieved_gbs": b / tot_s / 1e9 if tot_s > 0 else 0.0,
+                    "frac_of_measured_hbm": (b / tot_s / 1e9) / pk["hbm_gbs"] if tot_s > 0 else 0.0}
     dom = max(ktimes, key=lambda k: ktimes[k]["avg_us"] * ktimes[k]["launches"])
     kt = ktimes[dom]
     shots_per_launch = kt["shot_launches"] / max(kt["launches"], 1)
-    bytes_per_launch = shots_per_launch * per_shot_bytes[dom]
-    if dom == "fwd_step":
-        bytes_per_launch += shots_per_launch * hist_launch_bytes
-    avg_s = kt["avg_us"] / 1e6
-    achieved = bytes_per_launch / avg_s / 1e9 if avg_s > 0 else 0.0
-    kname = {"fwd_step": "k_stepv<float,0>", "adj_step": "k_adj_stepv<float>", "ref_step": "k_stepv<float,1>"}[dom]
-    tpu = traffic_per_unit(kname)
-    roof = {"kernel": kname, "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+    achieved = kern[dom]["achieved_gbs"]
+    tpu = traffic_per_unit(kname[dom])
+    roof = {"kernel": kname[dom], "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "peak_source": pk_src,
             "traffic": (tpu * shots_per_launch * cells if tpu is not None else None),
-            "algorithmic_bytes_per_launch": bytes_per_launch, "shots_per_launch": shots_per_launch,
+            "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes_per_launch"],
+            "shots_per_launch": shots_per_launch,
             "launches": kt["launches"], "timed_launches": kt["sampled"], "avg_launch_us": kt["avg_us"],
-            "units": ("per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n history write" if dom == "fwd_step" else
-                      "per shot: 32 B x NX*NY cells (stencil) + 40 B x m*n (2 history reads, 4 Kahan sums r/w)"
-                      if dom == "adj_step" else
-                      "per shot: 32 B x NX*NY cells (stencil) + 48 B x m*n (4 history reads, 4 Kahan sums r/w)"),
+            "units": {"fwd_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n history write",
+                      "adj_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n adjoint-field ring write",
+                      "image": "per imaged shot-step 8 B x m*n, per shot-launch 36 B x m*n",
+                      "ref_step": "per shot: 32 B x NX*NY cells + 48 B x m*n (4 history reads, 4 sums r/w)"}[dom],
             "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / ms}
     line = {"metric": METRIC, "value": value, "unit": "shot-gradients/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -355,7 +376,8 @@ def main():
             "data": "synthetic (seeded layered model, observed traces modelled on the device)",
             "config": cfg, "gcell_updates_per_s": gcell, "gpu_launches": launches,
             "clocks": clk, "roofline": roof,
-            "kernel_ms_per_step": {k: v["avg_us"] * v["launches"] / 1e3 / args.steps for k, v in ktimes.items()}}
+            "kernel_ms_per_step": {k: v["avg_us"] * v["launches"] / 1e3 / args.steps for k, v in ktimes.items()},
+            "kernels": kern}
 
     if rank == 0 and not args.no_extras:
         # e2e: the public C ABI with host (pinned) buffers, copies inside the timed region

@@ -53,6 +53,13 @@ template <class T> __device__ __forceinline__ T slast(const uint4* p) {
 constexpr int RING_SLOTS = 15;  // 16-byte entries per lane per column
 constexpr int RING_HALO = 16;   // 16-byte halo entries per warp per column
 constexpr int RING_STAGE = RING_SLOTS * 32 + RING_HALO;  // uint4 per warp per stage
+// The fast-only variants keep 5 entries per lane and 5 halo entries.
+constexpr int RING_SLOTS_FAST = 5;
+constexpr int RING_STAGE_FAST = RING_SLOTS_FAST * 32 + 5;
+template <bool FAST> struct RingShape {
+  static constexpr int slots = FAST ? RING_SLOTS_FAST : RING_SLOTS;
+  static constexpr int stage = FAST ? RING_STAGE_FAST : RING_STAGE;
+};
 
 // Forward slots for column J.
 enum { RF_EZN = 0, RF_HX, RF_HY, RF_CE, RF_CH, RF_HXA, RF_HXB, RF_HYA, RF_HYB, RF_AX, RF_BX, RF_AY, RF_BY,
@@ -66,22 +73,27 @@ enum { RA_LN = 0, RA_CE, RA_CH, RA_AX, RA_BX, RA_AY, RA_BY, RA_SX, RA_SY, RA_LX,
 enum { HA_LDN = 0, HA_SXDN, HA_CHDN, HA_BXDN, HA_LUP, HA_SXUP, HA_CHUP, HA_BXUP, HA_LYUP, HA_HYBUP };
 
 // Shared memory of a launch with `warps` warps per CTA and S stages.
-inline size_t ring_smem(int warps, int S) { return size_t(warps) * S * RING_STAGE * 16; }
+inline size_t ring_smem(int warps, int S, bool fast) {
+  return size_t(warps) * S * (fast ? RING_STAGE_FAST : RING_STAGE) * 16;
+}
 
 // Task of one warp (int4): x = first row r0, y, z = first and last column,
 // w = (shot within the launch << 1) | fast, fast = 1 when every row of
 // [r0, r0+32V-1] is an interior Ez row (or the free-top Ez = 0 row) and a Hy
 // interior row, and the halo rows r0-1 (when r0 > 0) and r0+32V are
-// interior Ez and Hy rows.
+// interior Ez and Hy rows.  FAST kernels run only tasks of fast blocks
+// restricted to interior columns (forward [ej0, ej1], adjoint [ej0, ej1-1])
+// and keep only the fast path.
 
 // --------------------------------------------------------------------------
 // Forward Yee step (w_solve.m:85-105): new_H, new_H_pml, new_Ez, source,
 // new_Ez_pml; history of the domain Ez (domain-node layout) when a.hist.
 // Grid: x = tasks / warps per CTA.
 // --------------------------------------------------------------------------
-template <class T, int S>
+template <class T, int S, bool FAST>
 __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T> a, const int4* __restrict__ tasks,
                                               int ntask) {
+  constexpr int SLOTS = RingShape<FAST>::slots, STAGE = RingShape<FAST>::stage;
   constexpr int V = VT<T>::V;
   static_assert(V * sizeof(T) == 16, "ring kernels move 16 bytes per lane");
   extern __shared__ __align__(16) uint4 smem[];
@@ -107,7 +119,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
   T* HyB = EzB + 2 * fs;
   T* ExB = EzB + 3 * fs;
   T* EyB = EzB + 4 * fs;
-  uint4* ring = smem + size_t(wib) * S * RING_STAGE;
+  uint4* ring = smem + size_t(wib) * S * STAGE;
   const long src = a.src[s];
   T sval = T(0);
   if (src >= 0) sval = a.cezj[s] * a.wav[size_t(s) * a.nt + a.it];
@@ -129,8 +141,23 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
   auto needInt = [&](int J) { return colInt(J) && rowIntAny; };
   auto needBand = [&](int J) { return colE(J) && (rowBandAny || (!colInt(J) && rowIntAny)); };
   auto issue = [&](int J, int stg) {
-    uint4* R = ring + size_t(stg) * RING_STAGE;
-    if (live) {
+    uint4* R = ring + size_t(stg) * STAGE;
+    if (FAST) {
+      uint4* L = R + lane;
+      const size_t k = nidx(I0, J, ld);
+      cp16(L + RF_EZN * 32, EzA + k + ld);
+      cp16(L + RF_HX * 32, HxA + k);
+      cp16(L + RF_HY * 32, HyA + k);
+      cp16(L + RF_CE * 32, w.ce + k);
+      cp16(L + RF_CH * 32, w.chy + k);
+      uint4* H = R + SLOTS * 32;
+      if (lane == 31) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
+      if (lane == 0 && I0 >= 1) {
+        const size_t ku = nidx(I0 - V, J, ld);
+        cp16(H + HF_EZUP, EzA + ku);
+        cp16(H + HF_HYUP, HyA + ku);
+      }
+    } else if (live) {
       uint4* L = R + lane;
       const size_t k = nidx(I0, J, ld);
       cp16(L + RF_EZN * 32, EzA + k + ld);
@@ -144,7 +171,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
         cp16(L + RF_AY * 32, w.ay + k); cp16(L + RF_BY * 32, w.by + k);
         cp16(L + RF_EX * 32, ExA + k); cp16(L + RF_EY * 32, EyA + k);
       }
-      uint4* H = R + RING_SLOTS * 32;
+      uint4* H = R + SLOTS * 32;
       if (lane == 31 && I0 + V <= NX) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
       if (lane == 0 && I0 >= 1) {
         const size_t ku = nidx(I0 - V, J, ld);
@@ -182,12 +209,12 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
     if (J + S - 1 <= j1) issue(J + S - 1, (it + S - 1) % S);
     else cp_commit();
     cp_wait<S - 1>();
-    const uint4* R = ring + size_t(it % S) * RING_STAGE;
+    const uint4* R = ring + size_t(it % S) * STAGE;
     const uint4* L = R + lane;
-    const uint4* H = R + RING_SLOTS * 32;
+    const uint4* H = R + SLOTS * 32;
     const size_t k = nidx(I0, J, ld);
     T ez_n[V], hxo[V], hyo[V], hx_new[V], hy_new[V], e_new[V];
-    if (fastRows && J >= w.ej0 && J <= w.ej1) {
+    if (FAST || (fastRows && J >= w.ej0 && J <= w.ej1)) {
       // ---- interior block, interior column: no PML, no edges
       T ce_[V], ch_[V];
       sld(L + RF_EZN * 32, ez_n); sld(L + RF_HX * 32, hxo); sld(L + RF_HY * 32, hyo);
@@ -218,7 +245,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
           if (srcI == I0 + v) e_new[v] += sval;
       }
       vst(EzB + k, e_new);
-    } else {
+    } else if constexpr (!FAST) {
       // ---- general path (w_solve.m:136-268 with every row class)
       vzero<T, V>(ez_n); vzero<T, V>(hxo); vzero<T, V>(hyo);
       if (live) { sld(L + RF_EZN * 32, ez_n); sld(L + RF_HX * 32, hxo); sld(L + RF_HY * 32, hyo); }
@@ -357,9 +384,10 @@ struct AdjRingArgs {
   T* lout; size_t hstride;
 };
 
-template <class T, int S>
+template <class T, int S, bool FAST>
 __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs<T> a, const int4* __restrict__ tasks,
                                               int ntask) {
+  constexpr int SLOTS = RingShape<FAST>::slots, STAGE = RingShape<FAST>::stage;
   constexpr int V = VT<T>::V;
   static_assert(V * sizeof(T) == 16, "ring kernels move 16 bytes per lane");
   extern __shared__ __align__(16) uint4 smem[];
@@ -384,7 +412,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
   T* LyB = LB + 2 * fs;
   T* SxB = LB + 3 * fs;
   T* SyB = LB + 4 * fs;
-  uint4* ring = smem + size_t(wib) * S * RING_STAGE;
+  uint4* ring = smem + size_t(wib) * S * STAGE;
   bool hyStrip = false;
   AdjRows rr{false, false, false};
   unsigned dmask = 0;  // model rows of this lane
@@ -408,8 +436,28 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
     anyBand = colE && (colInt ? rr.outAny : rr.eAny);
   };
   auto issue = [&](int J, int stg) {
-    uint4* R = ring + size_t(stg) * RING_STAGE;
-    if (live) {
+    uint4* R = ring + size_t(stg) * STAGE;
+    if (FAST) {
+      uint4* L = R + lane;
+      const size_t k = nidx(I0, J, ld), kn = k + ld;
+      cp16(L + RF_EZN * 32, LA + kn);       // slot 0: l(J+1)
+      cp16(L + RF_HX * 32, LxA + k);        // slot 1: lx(J)
+      cp16(L + RF_HY * 32, LyA + k);        // slot 2: ly(J)
+      cp16(L + RF_CE * 32, w.ce + kn);      // slot 3: Ceze(J+1)
+      cp16(L + RF_CH * 32, w.chy + kn);     // slot 4: Cezhy(J+1)
+      uint4* H = R + SLOTS * 32;
+      if (lane == 31) {
+        const size_t kd = nidx(Idn, J, ld);
+        cp16(H + 0, LA + kd);
+        cp16(H + 1, w.chy + kd);
+      }
+      if (lane == 0 && I0 >= 1) {
+        const size_t ku = nidx(I0 - V, J, ld);
+        cp16(H + 2, LA + ku);
+        cp16(H + 3, w.chy + ku);
+        cp16(H + 4, LyA + ku);
+      }
+    } else if (live) {
       uint4* L = R + lane;
       const size_t k = nidx(I0, J, ld), kn = k + ld;
       cp16(L + RA_LN * 32, LA + kn);
@@ -425,7 +473,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       cp16(L + RA_LY * 32, LyA + k);
       if (!(J >= w.hxj0 && J <= w.hxj1)) { cp16(L + RA_HXA * 32, w.hxa + k); cp16(L + RA_HXB * 32, w.hxb + k); }
       if (hyStrip) { cp16(L + RA_HYA * 32, w.hya + k); cp16(L + RA_HYB * 32, w.hyb + k); }
-      uint4* H = R + RING_SLOTS * 32;
+      uint4* H = R + SLOTS * 32;
       if (lane == 31 && Idn <= NX) {
         const size_t kd = nidx(Idn, J, ld);
         const int cls = adj_class(w, Idn, J);
@@ -480,17 +528,27 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
     if (J + S - 1 <= j1) issue(J + S - 1, (it + S - 1) % S);
     else cp_commit();
     cp_wait<S - 1>();
-    const uint4* R = ring + size_t(it % S) * RING_STAGE;
+    const uint4* R = ring + size_t(it % S) * STAGE;
     const uint4* L = R + lane;
-    const uint4* H = R + RING_SLOTS * 32;
+    const uint4* H = R + SLOTS * 32;
     const size_t k = nidx(I0, J, ld);
     T l_n[V], px_n[V], py_n[V], lm_n[V], lx_n[V], ly_n[V], ax_n[V], ay_n[V], lxo[V], lyo[V];
     T lxn[V], lyn[V], qx[V], le[V], img[V];
-    if (fastRows && J >= w.ej0 && J + 1 <= w.ej1) {
+    if (FAST || (fastRows && J >= w.ej0 && J + 1 <= w.ej1)) {
       // ---- interior block, interior columns J and J+1
       T ce_[V], ch_[V];
-      sld(L + RA_LN * 32, l_n); sld(L + RA_LX * 32, lxo); sld(L + RA_LY * 32, lyo);
-      sld(L + RA_CE * 32, ce_); sld(L + RA_CH * 32, ch_);
+      T ldn, chdn, lup = T(0), chup = T(0), lyup = T(0);
+      if (FAST) {
+        sld(L + RF_EZN * 32, l_n); sld(L + RF_HX * 32, lxo); sld(L + RF_HY * 32, lyo);
+        sld(L + RF_CE * 32, ce_); sld(L + RF_CH * 32, ch_);
+        ldn = sfirst<T>(H + 0); chdn = sfirst<T>(H + 1);
+        if (I0 >= 1) { lup = slast<T>(H + 2); chup = slast<T>(H + 3); lyup = slast<T>(H + 4); }
+      } else {
+        sld(L + RA_LN * 32, l_n); sld(L + RA_LX * 32, lxo); sld(L + RA_LY * 32, lyo);
+        sld(L + RA_CE * 32, ce_); sld(L + RA_CH * 32, ch_);
+        ldn = sfirst<T>(H + HA_LDN); chdn = sfirst<T>(H + HA_CHDN);
+        if (I0 >= 1) { lup = slast<T>(H + HA_LUP); chup = slast<T>(H + HA_CHUP); lyup = slast<T>(H + HA_LYUP); }
+      }
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         px_n[v] = ch_[v] * l_n[v]; py_n[v] = (w.rxy * ch_[v]) * l_n[v]; lm_n[v] = ce_[v] * l_n[v];
@@ -498,8 +556,8 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       }
       T px_dn = __shfl_down_sync(0xffffffffu, px_c[0], 1);
       T px_up = __shfl_up_sync(0xffffffffu, px_c[V - 1], 1);
-      if (lane == 31) px_dn = sfirst<T>(H + HA_CHDN) * sfirst<T>(H + HA_LDN);
-      if (lane == 0) px_up = (I0 >= 1) ? slast<T>(H + HA_CHUP) * slast<T>(H + HA_LUP) : T(0);
+      if (lane == 31) px_dn = chdn * ldn;
+      if (lane == 0) px_up = (I0 >= 1) ? chup * lup : T(0);
       T qy[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
@@ -513,7 +571,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       }
       vst(LxB + k, lxn); vst(LyB + k, lyn);
       T qy_up = __shfl_up_sync(0xffffffffu, qy[V - 1], 1);
-      if (lane == 0) qy_up = (I0 >= 1) ? w.chyez * (slast<T>(H + HA_LYUP) + px_up - px_c[0]) : T(0);
+      if (lane == 0) qy_up = (I0 >= 1) ? w.chyez * (lyup + px_up - px_c[0]) : T(0);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const T qym = (v > 0) ? qy[v > 0 ? v - 1 : 0] : qy_up;
@@ -522,7 +580,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       }
       if (I0 == 0) le[0] = T(0);  // the Ez = 0 row of a free top is not a state
       vst(LB + k, le);
-    } else {
+    } else if constexpr (!FAST) {
       // ---- general path
       vzero<T, V>(l_n); vzero<T, V>(lxo); vzero<T, V>(lyo); vzero<T, V>(ax_n); vzero<T, V>(ay_n);
       if (live) { sld(L + RA_LN * 32, l_n); sld(L + RA_LX * 32, lxo); sld(L + RA_LY * 32, lyo); }

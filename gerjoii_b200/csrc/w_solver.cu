@@ -108,7 +108,7 @@ class WSolver : public WSolverBase {
   // available for T), ring stages, resident CTAs per SM, SMs; ring_on per call
   int ring_nth = 0, ring_S = 0, ring_nb = 0, nsm = 148;
   bool ring_on = false;
-  int Kd = 16;   // adjoint steps per imaging pass (slots of the l ring)
+  int Kd = 32;   // adjoint steps per imaging pass (slots of the l ring)
   DevBuf lring;
 
 
@@ -257,16 +257,31 @@ class WSolver : public WSolverBase {
   }
 
   // Launch shape of the warp-task ring kernels (w_kernels_ring.cuh): CTAs of
-  // RW warps, S ring stages (GJ_RING_STAGES, default 2), one task per warp.
+  // RW warps, one task per warp.  Each step launches the fast-only kernel
+  // (interior blocks x interior columns, ring_SF stages) on the calling stream
+  // and the general kernel (the rest, ring_S stages) on a forked side stream.
   static constexpr int RW = 4;
-  template <int S>
-  gj_status ring_attr(Err& err, size_t sm) {
-    GJ_CUDA(err, cudaFuncSetAttribute(k_fwdw<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    GJ_CUDA(err, cudaFuncSetAttribute(k_adjw<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    int nb = 0;
-    GJ_CUDA(err, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_adjw<T, S>, 32 * RW, sm));
-    ring_nb = std::max(nb, 1);
+  int RWG = 4;  // warps per CTA of the general kernel (GJ_RING_CTA_WARPS)
+  int ring_SF = 3, nb_fast = 1;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  template <int S, bool F>
+  gj_status ring_attr(Err& err, int& nb) {
+    const int rw = F ? RW : RWG;
+    const size_t sm = ring_smem(rw, S, F);
+    GJ_CUDA(err, cudaFuncSetAttribute(k_fwdw<T, S, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    GJ_CUDA(err, cudaFuncSetAttribute(k_adjw<T, S, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
+    int n1 = 0, n2 = 0;
+    GJ_CUDA(err, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_fwdw<T, S, F>, 32 * rw, sm));
+    GJ_CUDA(err, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, k_adjw<T, S, F>, 32 * rw, sm));
+    nb = std::max(1, std::min(n1, n2));
     return GJ_OK;
+  }
+  template <bool F>
+  gj_status ring_attr_s(Err& err, int S, int& nb) {
+    if (S == 2) return ring_attr<2, F>(err, nb);
+    if (S == 3) return ring_attr<3, F>(err, nb);
+    return ring_attr<4, F>(err, nb);
   }
   gj_status ring_setup(Err& err) {
     ring_nth = 0;
@@ -276,16 +291,20 @@ class WSolver : public WSolverBase {
       GJ_CUDA(err, cudaGetDevice(&dev));
       GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
       GJ_CUDA(err, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-      int S = 2;
+      int S = 2, SF = 2;
+      if (const char* e = getenv("GJ_RING_CTA_WARPS")) RWG = std::min(std::max(atoi(e), 1), 4);
       if (const char* e = getenv("GJ_RING_STAGES")) S = std::min(std::max(atoi(e), 2), 4);
-      while (S > 2 && ring_smem(RW, S) > size_t(maxsm)) --S;
-      const size_t sm = ring_smem(RW, S);
-      if (sm > size_t(maxsm)) return GJ_OK;
-      ring_nth = 32 * RW;
+      if (const char* e = getenv("GJ_RING_STAGES_FAST")) SF = std::min(std::max(atoi(e), 2), 4);
+      while (S > 2 && ring_smem(RWG, S, false) > size_t(maxsm)) --S;
+      if (ring_smem(RWG, S, false) > size_t(maxsm)) return GJ_OK;
       ring_S = S;
-      if (S == 2) GJ_TRY(ring_attr<2>(err, sm));
-      else if (S == 3) GJ_TRY(ring_attr<3>(err, sm));
-      else GJ_TRY(ring_attr<4>(err, sm));
+      ring_SF = SF;
+      GJ_TRY(ring_attr_s<false>(err, S, ring_nb));
+      GJ_TRY(ring_attr_s<true>(err, SF, nb_fast));
+      if (!side) GJ_CUDA(err, cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      if (!ev_fork) GJ_CUDA(err, cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+      if (!ev_join) GJ_CUDA(err, cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+      ring_nth = 32 * RW;
       if (const char* e = getenv("GJ_IMAGE_WINDOW")) Kd = std::min(std::max(atoi(e), 1), 256);
     }
     return GJ_OK;
@@ -297,8 +316,9 @@ class WSolver : public WSolverBase {
     return e && I >= w.hyi0 && I <= w.hyi1;
   }
   bool interior_row(int I) const { return I >= w.ei0 && I <= w.ei1 && I >= w.hyi0 && I <= w.hyi1; }
-  // Task table for launches of gn shots (built outside graph capture).
-  struct TaskTable { DevBuf buf; int n = 0; };
+  // Task tables for launches of gn shots (built outside graph capture):
+  // [0] forward fast, [1] forward general, [2] adjoint fast, [3] adjoint general.
+  struct TaskTable { DevBuf buf[4]; int n[4] = {0, 0, 0, 0}; };
   std::map<int, std::unique_ptr<TaskTable>> tasks;
   gj_status prepare_tasks(Err& err, int gn) {
     if (ring_nth == 0 || tasks.count(gn)) return GJ_OK;
@@ -313,62 +333,122 @@ class WSolver : public WSolverBase {
       fast[rb] = f ? 1 : 0;
       nF += fast[rb];
     }
-    const int nS = nrb - nF;
-    // column chunks: a general-path block costs about 4x a fast block per
-    // column; chunks sized for GJ_RING_WAVES (default 1.5) waves of resident warps
-    double waves = 1.5;
-    if (const char* e = getenv("GJ_RING_WAVES")) waves = std::max(0.25, atof(e));
-    const double nbw = double(ring_nb) * RW * nsm;
-    int tjF = int(std::ceil(double(NY + 1) * (nF + 4.0 * nS) * gn / (waves * nbw)));
-    tjF = std::min(std::max(tjF, 16), NY + 1);
-    const int tjS = std::max(4, tjF / 4);
-    std::vector<int4> h;
-    for (int pass = 0; pass < 2; ++pass)  // general-path tasks first
+    // Column chunks: 32 columns per fast task and 16 per general task, the
+    // measured best for 10-shot launches of the 431 x 1060 grid (shorter chunks
+    // add per-task start-up and let the two kernels crowd each other);
+    // GJ_RING_TJF and GJ_RING_TJS override.
+    int tjS = 16;
+    if (const char* e = getenv("GJ_RING_TJS")) tjS = std::max(2, atoi(e));
+    auto tt = std::make_unique<TaskTable>();
+    for (int dir = 0; dir < 2; ++dir) {
+      const int c0 = w.ej0, c1 = dir == 0 ? w.ej1 : w.ej1 - 1;  // fast columns
+      const int ncol = std::max(c1 - c0 + 1, 0);
+      int tjF = 32;
+      if (const char* e = getenv("GJ_RING_TJF")) tjF = std::max(2, atoi(e));
+      tjF = std::min(tjF, std::max(ncol, 1));
+      std::vector<int4> hf, hg;
+      auto chunks = [&](std::vector<int4>& h, int z, int r0, int a0, int a1, int tj) {
+        for (int j0 = a0; j0 <= a1; j0 += tj) h.push_back(make_int4(r0, j0, std::min(j0 + tj - 1, a1), z << 1));
+      };
       for (int z = 0; z < gn; ++z)
         for (int rb = 0; rb < nrb; ++rb) {
-          if (fast[rb] != pass) continue;
-          const int tjr = fast[rb] ? tjF : tjS;
-          for (int j0 = 0; j0 <= NY; j0 += tjr)
-            h.push_back(make_int4(rb * rows, j0, std::min(j0 + tjr - 1, NY), (z << 1) | fast[rb]));
+          const int r0 = rb * rows;
+          if (fast[rb] && ncol > 0) {
+            chunks(hf, z, r0, c0, c1, tjF);
+            if (c0 > 0) chunks(hg, z, r0, 0, c0 - 1, tjS);
+            if (c1 < NY) chunks(hg, z, r0, c1 + 1, NY, tjS);
+          } else {
+            chunks(hg, z, r0, 0, NY, tjS);
+          }
         }
-    auto tt = std::make_unique<TaskTable>();
-    GJ_TRY(tt->buf.alloc(err, h.size() * sizeof(int4)));
-    GJ_CUDA(err, cudaMemcpy(tt->buf.p, h.data(), h.size() * sizeof(int4), cudaMemcpyHostToDevice));
-    tt->n = int(h.size());
+      for (auto& q : hf) q.w |= 1;
+      std::vector<int4>* hh[2] = {&hf, &hg};
+      for (int k = 0; k < 2; ++k) {
+        const int slot = 2 * dir + k;
+        tt->n[slot] = int(hh[k]->size());
+        if (tt->n[slot] == 0) continue;
+        GJ_TRY(tt->buf[slot].alloc(err, hh[k]->size() * sizeof(int4)));
+        GJ_CUDA(err, cudaMemcpy(tt->buf[slot].p, hh[k]->data(), hh[k]->size() * sizeof(int4),
+                                cudaMemcpyHostToDevice));
+      }
+    }
     tasks.emplace(gn, std::move(tt));
     return GJ_OK;
   }
 
+  // Launches the fast-only kernel on st and the general kernel on the side
+  // stream, joined back into st.
+  template <class Args, class LF, class LG>
+  gj_status fork_join(Err& err, const TaskTable& tt, int dir, cudaStream_t st, LF launch_fast, LG launch_gen) {
+    const int nf = tt.n[2 * dir], ng = tt.n[2 * dir + 1];
+    const int4* tf = static_cast<const int4*>(tt.buf[2 * dir].p);
+    const int4* tg = static_cast<const int4*>(tt.buf[2 * dir + 1].p);
+    if (ng > 0) {
+      GJ_CUDA(err, cudaEventRecord(ev_fork, st));
+      GJ_CUDA(err, cudaStreamWaitEvent(side, ev_fork, 0));
+      launch_gen(tg, ng, side);
+      GJ_CUDA(err, cudaEventRecord(ev_join, side));
+    }
+    if (nf > 0) launch_fast(tf, nf, st);
+    if (ng > 0) GJ_CUDA(err, cudaStreamWaitEvent(st, ev_join, 0));
+    return GJ_OK;
+  }
+
   // One forward step of gn shots (A -> B).
-  void launch_fwd(StepArgs<T> a, int gn, cudaStream_t st) {
+  gj_status launch_fwd(Err& err, StepArgs<T> a, int gn, cudaStream_t st) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       if (ring_on) {
         const TaskTable& tt = *tasks.at(gn);
-        const dim3 grd((tt.n + RW - 1) / RW);
-        const size_t sm = ring_smem(RW, ring_S);
-        const int4* tk = static_cast<const int4*>(tt.buf.p);
-        if (ring_S == 2) k_fwdw<T, 2><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
-        else if (ring_S == 3) k_fwdw<T, 3><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
-        else k_fwdw<T, 4><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
-        return;
+        const WDev<T> wd = w;
+        const int S = ring_S, SF = ring_SF;
+        auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
+          const dim3 grd((n + RW - 1) / RW);
+          const size_t sm = ring_smem(RW, SF, true);
+          if (SF == 2) k_fwdw<T, 2, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+          else if (SF == 3) k_fwdw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+          else k_fwdw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+        };
+        const int rw = RWG;
+        auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
+          const dim3 grd((n + rw - 1) / rw);
+          const size_t sm = ring_smem(rw, S, false);
+          if (S == 2) k_fwdw<T, 2, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+          else if (S == 3) k_fwdw<T, 3, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+          else k_fwdw<T, 4, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+        };
+        return fork_join<StepArgs<T>>(err, tt, 0, st, lf, lg);
       }
     }
     constexpr int V = VT<T>::V;
     a.tj = tj_for(gn);
     const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + a.tj - 1) / a.tj, gn);
     k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+    return GJ_OK;
   }
   // One exact adjoint step of gn shots with the l ring (ring kernels only).
-  void launch_adjr(AdjRingArgs<T> a, int gn, cudaStream_t st) {
+  gj_status launch_adjr(Err& err, AdjRingArgs<T> a, int gn, cudaStream_t st) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       const TaskTable& tt = *tasks.at(gn);
-      const dim3 grd((tt.n + RW - 1) / RW);
-      const size_t sm = ring_smem(RW, ring_S);
-      const int4* tk = static_cast<const int4*>(tt.buf.p);
-      if (ring_S == 2) k_adjw<T, 2><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
-      else if (ring_S == 3) k_adjw<T, 3><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
-      else k_adjw<T, 4><<<grd, 32 * RW, sm, st>>>(w, a, tk, tt.n);
+      const WDev<T> wd = w;
+      const int S = ring_S, SF = ring_SF;
+      auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
+        const dim3 grd((n + RW - 1) / RW);
+        const size_t sm = ring_smem(RW, SF, true);
+        if (SF == 2) k_adjw<T, 2, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+        else if (SF == 3) k_adjw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+        else k_adjw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+      };
+      const int rw = RWG;
+      auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
+        const dim3 grd((n + rw - 1) / rw);
+        const size_t sm = ring_smem(rw, S, false);
+        if (S == 2) k_adjw<T, 2, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+        else if (S == 3) k_adjw<T, 3, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+        else k_adjw<T, 4, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+      };
+      return fork_join<AdjRingArgs<T>>(err, tt, 1, st, lf, lg);
     }
+    return GJ_OK;
   }
 
   // Coefficients from the model (host doubles or device T / double).
@@ -428,7 +508,7 @@ class WSolver : public WSolverBase {
     for (int it = 0; it < g.nt; ++it) {
       StepArgs<T> a = step_args(A, B, it);
       if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * dn; a.hstride = dn; }
-      launch_fwd(a, nshots, st);
+      GJ_TRY(launch_fwd(err, a, nshots, st));
       k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
                                                    g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
                                                    nshots);
@@ -587,6 +667,9 @@ class WSolver : public WSolverBase {
   int fft_batch = 0;
   ~WSolver() override {
     if (fftplan) cufftDestroy(fftplan);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 
   gj_status analytic(Err& err, typename CplxT<T>::type* X, cudaStream_t st) {
@@ -721,7 +804,7 @@ class WSolver : public WSolverBase {
       a.shot0 = g0;
       if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
       const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
-      launch_fwd(a, gn, st);
+      GJ_TRY(launch_fwd(err, a, gn, st));
       c.timer.end(tm, st);
       k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, rec, nrr, nrs_d, it, nt, dgrp, d_src + g0,
                                                static_cast<T*>(nullptr), gn);
@@ -756,7 +839,7 @@ class WSolver : public WSolverBase {
           a.shot0 = g0;
           a.hist = slot_ptr(it + 1, base); a.hstride = hs;
           const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
-          launch_fwd(a, gn, st);
+          GJ_TRY(launch_fwd(err, a, gn, st));
           c.timer.end(tm, st);
           ++nl;
           std::swap(A, B);
@@ -787,7 +870,7 @@ class WSolver : public WSolverBase {
           a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = g0;
           a.lout = lring.as<T>() + size_t(win) * gn * hs; a.hstride = hs;
           const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
-          launch_adjr(a, gn, st);
+          GJ_TRY(launch_adjr(err, a, gn, st));
           c.timer.end(tm, st);
           ++win;
           if (win == Kd || k == s0 + 1) {
