@@ -342,6 +342,8 @@ def main():
         "image": lambda k: adj_sl * mn * 8.0 + k["shot_launches"] * mn * 36.0,
         "ref_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 48.0),
     }
+    # (a forward or adjoint "launch" is one step: the fast-only and the general
+    # ring kernel of that step together)
     kname = {"fwd_step": "k_fwdw<float,2>", "adj_step": "k_adjw<float,2>", "image": "k_image<float>",
              "ref_step": "k_stepv<float,1>"}
     pk, pk_src = peaks()
