@@ -12,8 +12,9 @@ segment-by-segment recompute and the exact adjoint with the imaging condition
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Under torchrun (N > 1) every rank runs the same workload on its own GPU (weak
-scaling) and the gradients are summed with one NCCL all-reduce per step.
+Under torchrun (N > 1) the acquisition has 30 x N sources; every rank takes a
+round-robin share of 30 shots (gerjoii_b200/shard.py, weak scaling) and the
+gradients are summed with one NCCL all-reduce per step.
 The reference arm (--impl reference) times the CPU restatement of the
 reference (oracle/) on the host cores; rank 0 alone runs it.
 """
@@ -50,9 +51,9 @@ def parse():
     return ap.parse_args()
 
 
-def workload(args):
+def workload(args, world=1):
     from gerjoii_b200 import synth
-    p = synth.cfg2(nshots=args.nshots, nt=args.nt)
+    p = synth.cfg2(nshots=args.nshots * world, nt=args.nt)
     g = p.grid
     cfg = {"workload": f"radar FWI gradient, {g.n}x{g.m} model (padded {g.NX}x{g.NY} Yee grid), "
                        f"{args.nshots} shots x {len(p.shots[0].rec)} receivers, {g.nt} steps, FP32, "
@@ -63,10 +64,10 @@ def workload(args):
     return p, cfg
 
 
-def synth_dobs(p):
+def synth_dobs(p, device=0):
     """Observed traces: the true model's forward response, from the library itself."""
     from gerjoii_b200 import _native as N
-    ctx = N.Context(0)
+    ctx = N.Context(device)
     out = ctx.w_forward(p.grid, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F32)
     ctx.close()
     return out["d"]
@@ -265,11 +266,17 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
-    p, cfg = workload(args)
+    from gerjoii_b200 import shard
+    p, cfg = workload(args, world)
     g = p.grid
-    cfg["parallelism"] = f"shots replicated per GPU x{world} (weak), gradient all-reduce" if world > 1 else "1 GPU"
+    if world > 1:
+        p.shots = shard.select(p.shots, shard.shard(len(p.shots), rank, world))
+        cfg["parallelism"] = (f"dp{world}: shots sharded round-robin, {args.nshots} per GPU (weak), "
+                              "one gradient all-reduce per step")
+    else:
+        cfg["parallelism"] = "1 GPU"
     mode = N.GJ_ADJ_EXACT if args.mode == "exact" else N.GJ_ADJ_REFERENCE
-    dobs = synth_dobs(p)
+    dobs = synth_dobs(p, local)
     nr = len(p.shots[0].rec)
     dobs_t = torch.tensor(np.stack([d.T for d in dobs]), dtype=torch.float32, device=dev).contiguous()
     eps_t = torch.tensor(np.asfortranarray(p.eps0).ravel(order="F"), dtype=torch.float32, device=dev)
@@ -282,8 +289,7 @@ def main():
     def step():
         ctx.w_gradient_dev(g, eps_t, sig_t, p.shots, dobs_t, ge_t, gs_t, mode=mode, stream=stream.cuda_stream)
         if world > 1:
-            dist.all_reduce(ge_t)
-            dist.all_reduce(gs_t)
+            shard.allreduce_sum([ge_t, gs_t])
 
     # kernel timing is on during the warm-up as well: the CUDA graphs captured
     # there (one per shot group, with the sampled timing events) are the ones

@@ -117,7 +117,9 @@ def cfg1(seed=1001):
 
 
 def cfg2(seed=1002, nshots=30, nt=6000):
-    p = _problem("cfg2", 400, 1000, 0.02, 30, nt, 250e6, 30, 200, "layer", seed)
+    """1000 x 400 at 0.02 m, 30 PML cells, free top; 30 surface sources (more when
+    nshots asks for more), 200 receivers, 250 MHz, five layers + blobs."""
+    p = _problem("cfg2", 400, 1000, 0.02, 30, nt, 250e6, max(30, nshots), 200, "layer", seed)
     p.shots = p.shots[:nshots]
     return p
 
