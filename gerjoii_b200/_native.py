@@ -61,7 +61,8 @@ class DcStatsC(C.Structure):
 class OptsC(C.Structure):
     _fields_ = [("ckpt_every", C.c_int), ("mem_budget_bytes", C.c_size_t),
                 ("shots_per_launch", C.c_int), ("no_kahan", C.c_int), ("no_graph", C.c_int),
-                ("per_shot", C.c_int), ("plain", C.c_int), ("no_ring", C.c_int)]
+                ("per_shot", C.c_int), ("plain", C.c_int), ("no_ring", C.c_int),
+                ("filt_low", C.c_double), ("filt_high", C.c_double), ("filt_steep", C.c_int)]
 
 
 # Every symbol the header declares, with its signature.

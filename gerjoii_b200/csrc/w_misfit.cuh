@@ -85,4 +85,41 @@ __global__ void k_env_final(const T* d, const T* F, const C* HG, T* e, size_t n)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Gaussian band filter of residual traces (filt_gauss.m:16-47, applied to
+// e_2d in w_update_e.m:69-70): Tukey(0.1) taper, zero padding to ntp = 2^k,
+// FFT, product with the fftshift-ed Gaussian, inverse FFT, real part, trim.
+// The taper (nt) and the filter (ntp, with the 1/ntp of the inverse FFT folded
+// in) are computed on the host in double.
+
+// traces [trace][t] (nt) -> tapered, zero-padded complex [trace][k] (ntp)
+template <class T, class C>
+__global__ void k_filt_pre(const T* e, const T* win, C* X, int nt, int ntp, size_t ntr) {
+  const size_t n = size_t(ntp) * ntr;
+  for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < n; i += size_t(blockDim.x) * gridDim.x) {
+    const int k = int(i % ntp);
+    const size_t tr = i / ntp;
+    cset(X[i], k < nt ? e[tr * nt + k] * win[k] : T(0), T(0));
+  }
+}
+
+template <class T, class C>
+__global__ void k_filt_mul(C* X, const T* G, int ntp, size_t ntr) {
+  const size_t n = size_t(ntp) * ntr;
+  for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < n; i += size_t(blockDim.x) * gridDim.x) {
+    const T gk = G[i % ntp];
+    cset(X[i], cre(X[i]) * gk, cim(X[i]) * gk);
+  }
+}
+
+template <class T, class C>
+__global__ void k_filt_post(const C* X, T* e, int nt, int ntp, size_t ntr) {
+  const size_t n = size_t(nt) * ntr;
+  for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < n; i += size_t(blockDim.x) * gridDim.x) {
+    const size_t tr = i / nt;
+    const int t = int(i % nt);
+    e[i] = cre(X[tr * ntp + t]);
+  }
+}
+
 }  // namespace gj

@@ -667,6 +667,7 @@ class WSolver : public WSolverBase {
   int fft_batch = 0;
   ~WSolver() override {
     if (fftplan) cufftDestroy(fftplan);
+    if (filtplan) cufftDestroy(filtplan);
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
@@ -715,6 +716,73 @@ class WSolver : public WSolverBase {
     GJ_TRY(analytic(err, envG.as<C>(), st));
     k_env_final<T, C><<<512, 256, 0, st>>>(d, envF.as<T>(), envG.as<C>(), ebuf.as<T>() + size_t(g0) * tr, n);
     c.launches += 10;
+    GJ_CUDA(err, cudaGetLastError());
+    return GJ_OK;
+  }
+
+  // Gaussian band filter of the residual traces of shots [g0, g0+gn)
+  // (filt_gauss.m:16-47 on e_2d, w_update_e.m:69-70), in place in ebuf.
+  DevBuf filtX, filtW, filtG;
+  cufftHandle filtplan = 0;
+  int filt_batch = 0, filt_ntp = 0;
+  double filt_key[4] = {0, 0, 0, 0};
+  gj_status filt_residual(Err& err, Ctx& c, const gj_w_opts& o, int g0, int gn, cudaStream_t st) {
+    using C = typename CplxT<T>::type;
+    const int nrr = std::max(nr, 1), nt = g.nt;
+    int ntp = 1;
+    while (ntp < nt) ntp <<= 1;  // 2^nextpow2(nt)
+    const int batch = gn * nrr;
+    if (filtplan && (filt_batch != batch || filt_ntp != ntp)) { cufftDestroy(filtplan); filtplan = 0; }
+    if (!filtplan) {
+      int dims[1] = {ntp};
+      if (cufftPlanMany(&filtplan, 1, dims, nullptr, 1, ntp, nullptr, 1, ntp, sizeof(T) == 8 ? CUFFT_Z2Z : CUFFT_C2C,
+                        batch) != CUFFT_SUCCESS)
+        return err.set(GJ_ENOMEM, "cufftPlanMany(n=%d, batch=%d) failed", ntp, batch);
+      filt_batch = batch;
+      filt_ntp = ntp;
+    }
+    const int steep = o.filt_steep > 0 ? o.filt_steep : 8;
+    const double key[4] = {g.dt, o.filt_low, o.filt_high, double(steep)};
+    if (!filtW.p || !filtG.p || std::memcmp(key, filt_key, sizeof key) != 0 || filtG.bytes < ntp * sizeof(T)) {
+      // MATLAB tukeywin(nt, 0.1) and the fftshift-ed Gaussian of filt_gauss.m:26-33
+      std::vector<T> win(nt), gk(ntp);
+      const double r = 0.1, per = r / 2;
+      const int tl = int(std::floor(per * (nt - 1))) + 1, th = nt - tl + 1;
+      for (int t = 0; t < nt; ++t) {
+        const double x = nt > 1 ? double(t) / (nt - 1) : 0.0;
+        double v = 1.0;
+        if (t < tl) v = 0.5 * (1 + std::cos(M_PI / per * (x - per)));
+        else if (t >= th - 1) v = 0.5 * (1 + std::cos(M_PI / per * (x - 1 + per)));
+        win[t] = T(v);
+      }
+      const double df = 1.0 / g.dt / ntp, width = o.filt_high - o.filt_low, middle = o.filt_low + 0.5 * width;
+      for (int q = 0; q < ntp; ++q) {
+        const double f = double(q - ntp / 2) * df;  // f = (-ntp/2 : ntp/2-1) df
+        const double gq = std::exp(-std::pow(f - middle, steep) / ((df * 0.5) * std::pow(width, steep - 1)));
+        gk[(q + ntp / 2) % ntp] = T(gq / ntp);      // fftshift, with the inverse FFT's 1/ntp
+      }
+      GJ_TRY(filtW.alloc(err, nt * sizeof(T)));
+      GJ_TRY(filtG.alloc(err, ntp * sizeof(T)));
+      GJ_CUDA(err, cudaMemcpyAsync(filtW.p, win.data(), nt * sizeof(T), cudaMemcpyHostToDevice, st));
+      GJ_CUDA(err, cudaMemcpyAsync(filtG.p, gk.data(), ntp * sizeof(T), cudaMemcpyHostToDevice, st));
+      GJ_CUDA(err, cudaStreamSynchronize(st));  // host vectors go out of scope
+      std::memcpy(filt_key, key, sizeof key);
+    }
+    GJ_TRY(filtX.alloc(err, size_t(batch) * ntp * sizeof(C)));
+    T* e = ebuf.as<T>() + size_t(g0) * nrr * nt;
+    C* X = filtX.as<C>();
+    k_filt_pre<T, C><<<512, 256, 0, st>>>(e, filtW.as<T>(), X, nt, ntp, size_t(batch));
+    cufftSetStream(filtplan, st);
+    cufftResult rr;
+    if (sizeof(T) == 8) rr = cufftExecZ2Z(filtplan, (cufftDoubleComplex*)X, (cufftDoubleComplex*)X, CUFFT_FORWARD);
+    else rr = cufftExecC2C(filtplan, (cufftComplex*)X, (cufftComplex*)X, CUFFT_FORWARD);
+    if (rr != CUFFT_SUCCESS) return err.set(GJ_ECUDA, "cufft forward failed (%d)", int(rr));
+    k_filt_mul<T, C><<<512, 256, 0, st>>>(X, filtG.as<T>(), ntp, size_t(batch));
+    if (sizeof(T) == 8) rr = cufftExecZ2Z(filtplan, (cufftDoubleComplex*)X, (cufftDoubleComplex*)X, CUFFT_INVERSE);
+    else rr = cufftExecC2C(filtplan, (cufftComplex*)X, (cufftComplex*)X, CUFFT_INVERSE);
+    if (rr != CUFFT_SUCCESS) return err.set(GJ_ECUDA, "cufft inverse failed (%d)", int(rr));
+    k_filt_post<T, C><<<512, 256, 0, st>>>(X, e, nt, ntp, size_t(batch));
+    c.launches += 5;
     GJ_CUDA(err, cudaGetLastError());
     return GJ_OK;
   }
@@ -910,9 +978,11 @@ class WSolver : public WSolverBase {
     GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
     if (o.plain) {
       if (mk != GJ_MISFIT_L2) return err.set(GJ_EUNSUPPORTED, "the plain form supports the L2 misfit only");
+      if (o.filt_high > o.filt_low) return err.set(GJ_EUNSUPPORTED, "the plain form has no residual filter");
       return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
     }
     const bool env = (mk == GJ_MISFIT_ENV_L2);
+    const bool filt = o.filt_high > o.filt_low;
     ring_on = ring_nth > 0 && !o.no_ring;
     // memory plan for one group
     size_t free_b = 0, total_b = 0;
@@ -963,12 +1033,14 @@ class WSolver : public WSolverBase {
     long nl = 0;
     for (int g0 = 0; g0 < nshots; g0 += G) {
       const int gn = std::min(G, nshots - g0);
-      if (env) {
-        // forward, envelope residual (cuFFT), adjoint: launched directly
+      if (env || filt) {
+        // forward, residual (envelope: cuFFT), band filter (cuFFT), adjoint:
+        // launched directly
         Marks m;
         c.timer.cur = &m;
-        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 1, false);
-        if (rs == GJ_OK) rs = env_residual(err, c, g0, gn, st);
+        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 1, !env);
+        if (rs == GJ_OK && env) rs = env_residual(err, c, g0, gn, st);
+        if (rs == GJ_OK && filt) rs = filt_residual(err, c, o, g0, gn, st);
         if (rs == GJ_OK) rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 2, false);
         c.timer.cur = nullptr;
         GJ_TRY(rs);

@@ -85,6 +85,12 @@ typedef struct gj_w_opts {
   int plain;             /* 1 = the plain form: one half-step per launch, one shot at a time */
   int no_ring;           /* 1 = register-marching step kernels instead of the warp-task ring
                             kernels (the default for 16-byte vectors: FP32 and FP64) */
+  double filt_low;       /* Gaussian band filter of the residual before the adjoint
+                            (filt_gauss.m, as w_update_e.m:69-70 applies it to e_2d): band
+                            [filt_low, filt_high] in Hz, on when filt_high > filt_low; the
+                            misfit stays that of the unfiltered residual */
+  double filt_high;
+  int filt_steep;        /* exponent of the filter; 0 = 8 (w_update_e.m:70) */
 } gj_w_opts;
 
 /* ---------------------------------------------------------------- context */

@@ -172,3 +172,35 @@ def test_envelope_residual_and_exact_gradient_match_oracle(gpu_ctx, oracle, smal
     sl = (slice(0, g.m - 1), slice(1, g.n - 1))
     assert rel_l2(res["g_eps"][sl], ge[sl]) < 10 * tol
     assert rel_l2(res["g_sig"][sl], gs[sl]) < 10 * tol
+
+
+@pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-10), (N.GJ_F32, 2e-4)])
+@pytest.mark.parametrize("band", [(-350e6, 350e6), (80e6, 500e6)])
+def test_band_filtered_residual_and_gradient_match_oracle(gpu_ctx, oracle, small_ft, prec, tol, band):
+    """filt_gauss.m on the residual (w_update_e.m:69-70): the filtered residual
+    against the numpy twin of filt_gauss, the misfit of the unfiltered residual,
+    and the exact gradient against the oracle's exact adjoint driven by the
+    filtered residual (interior cells)."""
+    import np_oracle as npo
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    o = N.OptsC()
+    o.filt_low, o.filt_high = band
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=prec, opts=o,
+                             want_traces=True)
+    ge = np.zeros((g.m, g.n))
+    gs = np.zeros((g.m, g.n))
+    for k, sh in enumerate(p.shots):
+        d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+        e = d - dobs[k]
+        ef = npo.filt_gauss(e, g.dt, band[0], band[1], 8)
+        assert rel_l2(res["e"][k], ef) < tol
+        mis = 0.5 * np.sum(e * e) / np.sum(dobs[k] * dobs[k])  # w_update_e.m:75-76, unfiltered
+        assert abs(res["misfit"][k] - mis) <= 10 * tol * mis
+        a, b = oracle.grad_exact(g, p.eps0, p.sig0, sh, ef)
+        ge += a
+        gs += b
+    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
+    assert rel_l2(res["g_eps"][sl], ge[sl]) < 10 * tol
+    assert rel_l2(res["g_sig"][sl], gs[sl]) < 10 * tol
