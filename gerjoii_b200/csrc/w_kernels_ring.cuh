@@ -135,6 +135,19 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
   }
   const int Iup = I0 - 1;  // lane 0's halo row
   const bool upStrip = Iup >= 0 && Iup <= NX - 1 && !(Iup >= w.hyi0 && Iup <= w.hyi1);
+  // row classes of this lane's V rows as bit masks (the general path selects
+  // per row instead of branching): Hx row, Hy row, Hy interior row, updated
+  // Ez row, interior Ez row
+  unsigned mHx = 0, mHy = 0, mHyInt = 0, mE = 0, mEint = 0;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const int I = I0 + v;
+    if (I <= NX) mHx |= 1u << v;
+    if (I <= NX - 1) mHy |= 1u << v;
+    if (I >= w.hyi0 && I <= w.hyi1) mHyInt |= 1u << v;
+    if (I >= 1 && I <= NX - 1) mE |= 1u << v;
+    if (I >= w.ei0 && I <= w.ei1) mEint |= 1u << v;
+  }
   auto colInt = [&](int J) { return J >= w.ej0 && J <= w.ej1; };
   auto colE = [&](int J) { return J >= 1 && J <= NY - 1; };
   auto hxStrip = [&](int J) { return !(J >= w.hxj0 && J <= w.hxj1); };
@@ -260,18 +273,16 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       if (live && hyStrip) { sld(L + RF_HYA * 32, hya_); sld(L + RF_HYB * 32, hyb_); }
       T nxt = __shfl_down_sync(0xffffffffu, ez_c[0], 1);
       if (lane == 31) nxt = (I0 + V <= NX) ? sfirst<T>(H + HF_EZDN) : T(0);
+      const bool hxCol = J <= NY - 1;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const int I = I0 + v;
-        hx_new[v] = T(0);
-        if (I <= NX && J <= NY - 1) hx_new[v] = hxa_[v] * hxo[v] + hxb_[v] * (ez_n[v] - ez_c[v]);
+        const T hxv = hxa_[v] * hxo[v] + hxb_[v] * (ez_n[v] - ez_c[v]);
+        hx_new[v] = (hxCol && ((mHx >> v) & 1u)) ? hxv : T(0);
         const T edn = (v < V - 1) ? ez_c[v < V - 1 ? v + 1 : v] : nxt;
-        hy_new[v] = T(0);
-        if (I <= NX - 1) {
-          T ha = T(1), hb = w.chyez;
-          if (!(I >= w.hyi0 && I <= w.hyi1)) { ha = hya_[v]; hb = hyb_[v]; }
-          hy_new[v] = ha * hyo[v] + hb * (edn - ez_c[v]);
-        }
+        const bool hin = (mHyInt >> v) & 1u;
+        const T ha = hin ? T(1) : hya_[v], hb = hin ? w.chyez : hyb_[v];
+        const T hyv = ha * hyo[v] + hb * (edn - ez_c[v]);
+        hy_new[v] = ((mHy >> v) & 1u) ? hyv : T(0);
       }
       if (live) { vst(HxB + k, hx_new); vst(HyB + k, hy_new); }
       T hy_up = __shfl_up_sync(0xffffffffu, hy_new[V - 1], 1);
@@ -289,26 +300,28 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       const bool anyBand = needBand(J);
       T ce_[V], ch_[V], ax_[V], bx_[V], ay_[V], by_[V], exo[V], eyo[V];
       if (live && anyInt) { sld(L + RF_CE * 32, ce_); sld(L + RF_CH * 32, ch_); }
+      else { vzero<T, V>(ce_); vzero<T, V>(ch_); }
       if (live && anyBand) {
         sld(L + RF_AX * 32, ax_); sld(L + RF_BX * 32, bx_); sld(L + RF_AY * 32, ay_); sld(L + RF_BY * 32, by_);
         sld(L + RF_EX * 32, exo); sld(L + RF_EY * 32, eyo);
+      } else {
+        vzero<T, V>(ax_); vzero<T, V>(bx_); vzero<T, V>(ay_); vzero<T, V>(by_); vzero<T, V>(exo); vzero<T, V>(eyo);
       }
+      const bool srcCol = J == srcJ;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const int I = I0 + v;
-        e_new[v] = ez_c[v];
-        if (cE && I >= 1 && I <= NX - 1) {
-          const T dhy = hy_new[v] - (v > 0 ? hy_new[v > 0 ? v - 1 : 0] : hy_up);
-          const T dhx = hx_new[v] - hx_prev[v];
-          if (cInt && I >= w.ei0 && I <= w.ei1) {
-            e_new[v] = ce_[v] * ez_c[v] + ch_[v] * dhy + (w.rxy * ch_[v]) * dhx;
-            if (long(k) + v == src) e_new[v] += sval;
-          } else {
-            exo[v] = ax_[v] * exo[v] + bx_[v] * dhy;
-            eyo[v] = ay_[v] * eyo[v] + by_[v] * dhx;
-            e_new[v] = exo[v] + eyo[v];
-          }
-        }
+        const bool rE = cE && ((mE >> v) & 1u);
+        const bool rI = rE && cInt && ((mEint >> v) & 1u);
+        const bool rB = rE && !rI;
+        const T dhy = hy_new[v] - (v > 0 ? hy_new[v > 0 ? v - 1 : 0] : hy_up);
+        const T dhx = hx_new[v] - hx_prev[v];
+        T ei = ce_[v] * ez_c[v] + ch_[v] * dhy + (w.rxy * ch_[v]) * dhx;
+        if (srcCol && I0 + v == srcI) ei += sval;
+        const T exn = ax_[v] * exo[v] + bx_[v] * dhy;
+        const T eyn = ay_[v] * eyo[v] + by_[v] * dhx;
+        e_new[v] = rI ? ei : (rB ? exn + eyn : ez_c[v]);
+        exo[v] = rB ? exn : exo[v];
+        eyo[v] = rB ? eyn : eyo[v];
       }
       if (live) {
         vst(EzB + k, e_new);
@@ -328,32 +341,37 @@ struct AdjRows {
   bool eAny, inAny, outAny;  // some row in [1, NX-1]; of those, some interior / some band
 };
 
-// p-values of V nodes of column J from ring data (same arithmetic as adj_pv).
+// p-values of V nodes of column J from ring data (same arithmetic as adj_pv),
+// selecting per row by the lane's row masks.
 template <class T, int V>
-__device__ __forceinline__ void adj_pv_ring(const WDev<T>& w, int I0, int J, bool live, const AdjRows& rr,
-                                            const uint4* L, const T (&l)[V], T (&px)[V], T (&py)[V],
-                                            T (&lm)[V], T (&lx)[V], T (&ly)[V], T (&axn)[V], T (&ayn)[V]) {
+__device__ __forceinline__ void adj_pv_ring(const WDev<T>& w, int J, bool live, const AdjRows& rr, unsigned mE,
+                                            unsigned mEint, const uint4* L, const T (&l)[V], T (&px)[V],
+                                            T (&py)[V], T (&lm)[V], T (&lx)[V], T (&ly)[V], T (&axn)[V],
+                                            T (&ayn)[V]) {
   const bool colE = J >= 1 && J <= w.NY - 1;
   const bool colInt = J >= w.ej0 && J <= w.ej1;
   const bool anyInt = colE && colInt && rr.inAny;
   const bool anyBand = colE && (colInt ? rr.outAny : rr.eAny);
   T ce_[V], ch_[V], bx_[V], by_[V], sx[V], sy[V];
   if (live && anyInt) { sld(L + RA_CE * 32, ce_); sld(L + RA_CH * 32, ch_); }
+  else { vzero<T, V>(ce_); vzero<T, V>(ch_); }
   if (live && anyBand) {
     sld(L + RA_AX * 32, axn); sld(L + RA_BX * 32, bx_); sld(L + RA_AY * 32, ayn); sld(L + RA_BY * 32, by_);
     sld(L + RA_SX * 32, sx); sld(L + RA_SY * 32, sy);
+  } else {
+    vzero<T, V>(bx_); vzero<T, V>(by_); vzero<T, V>(sx); vzero<T, V>(sy);
   }
 #pragma unroll
   for (int v = 0; v < V; ++v) {
-    const int I = I0 + v;
-    px[v] = py[v] = lm[v] = lx[v] = ly[v] = T(0);
-    if (!(colE && I >= 1 && I <= w.NX - 1)) continue;
-    if (colInt && I >= w.ei0 && I <= w.ei1) {
-      px[v] = ch_[v] * l[v]; py[v] = (w.rxy * ch_[v]) * l[v]; lm[v] = ce_[v] * l[v];
-    } else {
-      lx[v] = sx[v] + l[v]; ly[v] = sy[v] + l[v];
-      px[v] = bx_[v] * lx[v]; py[v] = by_[v] * ly[v];
-    }
+    const bool rE = colE && ((mE >> v) & 1u);
+    const bool rI = rE && colInt && ((mEint >> v) & 1u);
+    const bool rB = rE && !rI;
+    const T lxv = sx[v] + l[v], lyv = sy[v] + l[v];
+    px[v] = rI ? ch_[v] * l[v] : (rB ? bx_[v] * lxv : T(0));
+    py[v] = rI ? (w.rxy * ch_[v]) * l[v] : (rB ? by_[v] * lyv : T(0));
+    lm[v] = rI ? ce_[v] * l[v] : T(0);
+    lx[v] = rB ? lxv : T(0);
+    ly[v] = rB ? lyv : T(0);
   }
 }
 
@@ -429,6 +447,17 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
   }
   const int Idn = I0 + V, Iup = I0 - 1;  // halo rows of lanes 31 and 0
   const bool upStrip = Iup >= 0 && Iup <= NX - 1 && !(Iup >= w.hyi0 && Iup <= w.hyi1);
+  // row classes as bit masks (see k_fwdw)
+  unsigned mHx = 0, mHy = 0, mHyInt = 0, mE = 0, mEint = 0;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    const int I = I0 + v;
+    if (I <= NX) mHx |= 1u << v;
+    if (I <= NX - 1) mHy |= 1u << v;
+    if (I >= w.hyi0 && I <= w.hyi1) mHyInt |= 1u << v;
+    if (I >= 1 && I <= NX - 1) mE |= 1u << v;
+    if (I >= w.ei0 && I <= w.ei1) mEint |= 1u << v;
+  }
   auto pvNeed = [&](int J, bool& anyInt, bool& anyBand) {
     const bool colE = J >= 1 && J <= NY - 1;
     const bool colInt = J >= w.ej0 && J <= w.ej1;
@@ -584,7 +613,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       // ---- general path
       vzero<T, V>(l_n); vzero<T, V>(lxo); vzero<T, V>(lyo); vzero<T, V>(ax_n); vzero<T, V>(ay_n);
       if (live) { sld(L + RA_LN * 32, l_n); sld(L + RA_LX * 32, lxo); sld(L + RA_LY * 32, lyo); }
-      adj_pv_ring<T, V>(w, I0, J + 1, live, rr, L, l_n, px_n, py_n, lm_n, lx_n, ly_n, ax_n, ay_n);
+      adj_pv_ring<T, V>(w, J + 1, live, rr, mE, mEint, L, l_n, px_n, py_n, lm_n, lx_n, ly_n, ax_n, ay_n);
       const bool hxs = !(J >= w.hxj0 && J <= w.hxj1);
       T hxa_[V], hxb_[V], hya_[V], hyb_[V];
       if (live && hxs) { sld(L + RA_HXA * 32, hxa_); sld(L + RA_HXB * 32, hxb_); }
@@ -613,23 +642,19 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
         }
       }
       T qy[V];
+      const bool hxCol = J <= NY - 1;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const int I = I0 + v;
-        qx[v] = qy[v] = lxn[v] = lyn[v] = T(0);
-        if (I <= NX && J <= NY - 1) {
-          const T lt = lxo[v] + py_c[v] - py_n[v];
-          lxn[v] = hxa_[v] * lt;
-          qx[v] = hxb_[v] * lt;
-        }
-        if (I <= NX - 1) {
-          T ha = T(1), hb = w.chyez;
-          if (!(I >= w.hyi0 && I <= w.hyi1)) { ha = hya_[v]; hb = hyb_[v]; }
-          const T pdn = (v < V - 1) ? px_c[v < V - 1 ? v + 1 : v] : px_dn;
-          const T lt = lyo[v] + px_c[v] - pdn;
-          lyn[v] = ha * lt;
-          qy[v] = hb * lt;
-        }
+        const bool rx = hxCol && ((mHx >> v) & 1u);
+        const T lt = lxo[v] + py_c[v] - py_n[v];
+        lxn[v] = rx ? hxa_[v] * lt : T(0);
+        qx[v] = rx ? hxb_[v] * lt : T(0);
+        const bool ry = (mHy >> v) & 1u, hin = (mHyInt >> v) & 1u;
+        const T ha = hin ? T(1) : hya_[v], hb = hin ? w.chyez : hyb_[v];
+        const T pdn = (v < V - 1) ? px_c[v < V - 1 ? v + 1 : v] : px_dn;
+        const T lt2 = lyo[v] + px_c[v] - pdn;
+        lyn[v] = ry ? ha * lt2 : T(0);
+        qy[v] = ry ? hb * lt2 : T(0);
       }
       if (live) { vst(LxB + k, lxn); vst(LyB + k, lyn); }
       T qy_up = __shfl_up_sync(0xffffffffu, qy[V - 1], 1);
@@ -647,17 +672,15 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       T sxn[V], syn[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
-        const int I = I0 + v;
-        le[v] = T(0); sxn[v] = T(0); syn[v] = T(0); img[v] = T(0);
-        if (!(colE && I >= 1 && I <= NX - 1)) continue;
+        const bool rE = colE && ((mE >> v) & 1u);
+        const bool rI = rE && colInt && ((mEint >> v) & 1u);
+        const bool rB = rE && !rI;
         const T qym = (v > 0) ? qy[v > 0 ? v - 1 : 0] : qy_up;
-        le[v] = lm_c[v] + qx_prev[v] - qx[v] + qym - qy[v];
-        if (!(colInt && I >= w.ei0 && I <= w.ei1)) {
-          sxn[v] = ax_c[v] * lx_c[v];
-          syn[v] = ay_c[v] * ly_c[v];
-        } else if ((dmask >> v) & 1u) {
-          img[v] = l_c[v];
-        }
+        const T lev = lm_c[v] + qx_prev[v] - qx[v] + qym - qy[v];
+        le[v] = rE ? lev : T(0);
+        sxn[v] = rB ? ax_c[v] * lx_c[v] : T(0);
+        syn[v] = rB ? ay_c[v] * ly_c[v] : T(0);
+        img[v] = (rI && ((dmask >> v) & 1u)) ? l_c[v] : T(0);
       }
       if (live) {
         vst(LB + k, le);

@@ -263,6 +263,7 @@ class WSolver : public WSolverBase {
   static constexpr int RW = 4;
   int RWG = 4;  // warps per CTA of the general kernel (GJ_RING_CTA_WARPS)
   int ring_SF = 3, nb_fast = 1;
+  const bool ring_serial = getenv("GJ_RING_SERIAL") != nullptr;
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   template <int S, bool F>
@@ -383,6 +384,11 @@ class WSolver : public WSolverBase {
     const int nf = tt.n[2 * dir], ng = tt.n[2 * dir + 1];
     const int4* tf = static_cast<const int4*>(tt.buf[2 * dir].p);
     const int4* tg = static_cast<const int4*>(tt.buf[2 * dir + 1].p);
+    if (ring_serial) {  // both kernels on st, one after the other (for timing each)
+      if (ng > 0) launch_gen(tg, ng, st);
+      if (nf > 0) launch_fast(tf, nf, st);
+      return GJ_OK;
+    }
     if (ng > 0) {
       GJ_CUDA(err, cudaEventRecord(ev_fork, st));
       GJ_CUDA(err, cudaStreamWaitEvent(side, ev_fork, 0));
