@@ -62,7 +62,8 @@ class OptsC(C.Structure):
     _fields_ = [("ckpt_every", C.c_int), ("mem_budget_bytes", C.c_size_t),
                 ("shots_per_launch", C.c_int), ("no_kahan", C.c_int), ("no_graph", C.c_int),
                 ("per_shot", C.c_int), ("plain", C.c_int), ("no_ring", C.c_int),
-                ("filt_low", C.c_double), ("filt_high", C.c_double), ("filt_steep", C.c_int)]
+                ("filt_low", C.c_double), ("filt_high", C.c_double), ("filt_steep", C.c_int),
+                ("condition", C.c_int), ("cond_fo", C.c_double), ("cond_ax", C.c_double), ("cond_az", C.c_double)]
 
 
 # Every symbol the header declares, with its signature.
@@ -78,6 +79,7 @@ SIGNATURES = {
     "gj_w_forward": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _DP, _DP]),
     "gj_w_gradient": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _I,
                            C.POINTER(OptsC), _DP, _DP, _DP, _DP, _DP]),
+    "gj_w_misfit": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _DP]),
     "gj_w_grad": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _DP, _DP, _DP, _DP]),
     "gj_w_gradient_dev": (_I, [_VP, C.POINTER(GridC), _I, _VP, _VP, C.POINTER(ShotC), _I, _VP, _I, _I,
                                C.POINTER(OptsC), _VP, _VP, _DP, _VP]),
@@ -325,6 +327,18 @@ class Context:
         gg = gout.reshape((per, m0, n0)).transpose(0, 2, 1)
         return {"g": gg[0] if per == 1 else gg, "d": d[:nd], "e": e[:nd], "misfit": mis,
                 "iters": st.max_iterations, "rel_residual": st.max_rel_residual}
+
+    def w_misfit(self, g, eps, sig, shots, dobs, misfit=GJ_MISFIT_L2, precision=GJ_F32):
+        """Per-shot misfits of forward runs only (the step-length search's
+        objective evaluations); dobs: list of nt x nr arrays."""
+        sp = _ShotPack(shots, g.nt)
+        gc = grid_c(g)
+        ob = np.concatenate([_f(d).ravel(order="F") for d in dobs])
+        out = np.zeros(len(shots))
+        e, s_ = _f(eps), _f(sig)
+        self._check(self.lib.gj_w_misfit(self.h, C.byref(gc), precision, _dp(e), _dp(s_), sp.arr, sp.n, _dp(ob),
+                                          int(misfit), _dp(out)))
+        return out
 
     def w_gradient_dev(self, g, eps_t, sig_t, shots, dobs_t, ge_t, gs_t, mode=GJ_ADJ_REFERENCE,
                        misfit=GJ_MISFIT_L2, opts=None, stream=0):

@@ -90,6 +90,14 @@ gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precisi
                         o, g_eps, g_sig, false, misfit_out, d_out, e_out, 0);
 }
 
+gj_status gj_w_misfit(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const double* eps_r,
+                      const double* sigma, const gj_w_shot* shots, int nshots, const double* d_obs,
+                      gj_misfit_kind misfit, double* misfit_out) {
+  GJ_TRY(guard_ctx(ctx));
+  if (!grid) return ctx->c.err.set(GJ_EINVAL, "null grid");
+  return gj::w_misfit(ctx->c, *grid, precision, eps_r, sigma, shots, nshots, d_obs, misfit, misfit_out);
+}
+
 gj_status gj_w_gradient_dev(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const void* eps_r_dev,
                             const void* sigma_dev, const gj_w_shot* shots, int nshots, const void* d_obs_dev,
                             gj_adj_mode mode, gj_misfit_kind misfit, const gj_w_opts* opts, void* g_eps_dev,

@@ -164,6 +164,8 @@ gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* 
                      const void* d_obs, bool dev_dobs, gj_adj_mode mode, gj_misfit_kind mk,
                      const gj_w_opts& o, void* g_eps, void* g_sig, bool dev_out,
                      double* misfit_out, double* d_out, double* e_out, cudaStream_t stream);
+gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
+                   const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out);
 gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps,
                       const double* sig, const gj_w_shot& shot, const double* e, const double* u,
                       double* gout, double* amax);

@@ -14,6 +14,7 @@
 #include "w_kernels_vec.cuh"
 #include "w_kernels_ring.cuh"
 #include "w_misfit.cuh"
+#include "w_condition.cuh"
 
 namespace gj {
 
@@ -96,6 +97,7 @@ class WSolver : public WSolverBase {
   DevBuf coef, model_d, prof, shotbuf, recbuf, selbuf, nrsbuf, nselbuf, sibuf, sjbuf;
   DevBuf fwdA, fwdB, adjA, adjB, hist, ckpt, acc, dbuf, ebuf, dobsbuf, sums, scratch, stage, stage2, gout;
   std::vector<ShotHost> sh;
+  std::vector<int> sh_src_i, sh_src_j;  // source nodes as given (Ez row, column)
   std::vector<int> nrs, nsel;
   // layout of shotbuf: src (long) | cezj (T) | wav (T, nshots*nt)
   long* d_src = nullptr; T* d_cezj = nullptr; T* d_wav = nullptr;
@@ -145,6 +147,8 @@ class WSolver : public WSolverBase {
     nshots = ns;
     nr = 0;
     sh.assign(ns, ShotHost{});
+    sh_src_i.assign(ns, 0);
+    sh_src_j.assign(ns, 0);
     nrs.assign(ns, 0);
     nsel.assign(ns, 0);
     for (int s = 0; s < ns; ++s) {
@@ -216,6 +220,7 @@ class WSolver : public WSolverBase {
     for (int s = 0; s < ns; ++s) {
       hsrc[s] = sh[s].src;
       hsi[s] = shots[s].src_i; hsj[s] = shots[s].src_j;
+      sh_src_i[s] = shots[s].src_i; sh_src_j[s] = shots[s].src_j;
       for (int t = 0; t < g.nt; ++t) hwav[size_t(s) * g.nt + t] = T(sh[s].wav[t]);
     }
     GJ_CUDA(err, cudaMemcpy(d_src, hsrc.data(), ns * sizeof(long), cudaMemcpyHostToDevice));
@@ -550,6 +555,113 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
+  // Conditioning of nshots per-shot gradients g (double, m x n each) in place:
+  // source taper, k-space low-pass with widths (ka, kb), normali, NaN guard.
+  DevBuf cbuf, condX, condF, condP;
+  cufftHandle condplan = 0;
+  int cond_batch = 0;
+  gj_status condition(Err& err, Ctx& c, const gj_w_opts& o, double* gdev, double ka, double kb, cudaStream_t st) {
+    const int m = g.m, n = g.n;
+    int m_ = 1, n_ = 1;
+    while (m_ < m) m_ <<= 1;  // 2^nextpow2
+    while (n_ < n) n_ <<= 1;
+    if (!(o.cond_fo > 0)) return err.set(GJ_EINVAL, "condition needs cond_fo > 0");
+    if (!(ka > 0 && kb > 0)) return err.set(GJ_EINVAL, "condition needs cond_ax, cond_az > 0");
+    // taper parameters per shot: source cell (clamped to the model), L = 4 lo
+    std::vector<double> em(mn);
+    GJ_CUDA(err, cudaMemcpyAsync(em.data(), eps_m, mn * sizeof(double), cudaMemcpyDeviceToHost, st));
+    GJ_CUDA(err, cudaStreamSynchronize(st));
+    const double cl = 1.0 / std::sqrt(g.mu0 * g.eps0);
+    std::vector<double> par(4 * size_t(nshots));
+    for (int s = 0; s < nshots; ++s) {
+      const int as = std::min(std::max(sh_src_i[s] - w.di0, 0), m - 1);
+      const int bs = std::min(std::max(sh_src_j[s] - w.dj0, 0), n - 1);
+      const double lo = cl / std::sqrt(em[size_t(as) + size_t(bs) * m]) / o.cond_fo;
+      const double L = 2.0 * (2.0 * lo);
+      double mx = 0.0;  // normali of the taper: its largest value is at a corner
+      for (int a : {0, m - 1})
+        for (int b : {0, n - 1}) {
+          const double xa = (b - bs) * g.dx / L, za = (a - as) * g.dy / L;
+          mx = std::max(mx, std::fabs(1.0 - std::exp(-(xa * xa + za * za))));
+        }
+      par[4 * s] = as; par[4 * s + 1] = bs; par[4 * s + 2] = L; par[4 * s + 3] = 1.0 / (mx == 0.0 ? 1.0 : mx);
+    }
+    // low-pass filter in k (image_gaussian.m:37-52), fftshift-ed, with 1/(m_ n_)
+    std::vector<double> F(size_t(m_) * n_);
+    const double A = n_ * (ka / 2) * std::sqrt(2.0), B = m_ * (kb / 2) * std::sqrt(2.0);
+    for (int j = 0; j < n_; ++j)
+      for (int i = 0; i < m_; ++i) {
+        const int X = (j + n_ / 2) % n_, Y = (i + m_ / 2) % m_;
+        const double kx = (X - n_ / 2) / A, ky = (Y - m_ / 2) / B;
+        F[size_t(i) + size_t(j) * m_] = std::exp(-(kx * kx + ky * ky)) / (double(m_) * n_);
+      }
+    GJ_TRY(condP.alloc(err, par.size() * sizeof(double)));
+    GJ_TRY(condF.alloc(err, F.size() * sizeof(double)));
+    GJ_TRY(condX.alloc(err, size_t(nshots) * m_ * n_ * sizeof(cuDoubleComplex)));
+    GJ_CUDA(err, cudaMemcpyAsync(condP.p, par.data(), par.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    GJ_CUDA(err, cudaMemcpyAsync(condF.p, F.data(), F.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (condplan && cond_batch != nshots) { cufftDestroy(condplan); condplan = 0; }
+    if (!condplan) {
+      int dims[2] = {n_, m_};  // column-major m_ x n_: the slow dimension is n_
+      if (cufftPlanMany(&condplan, 2, dims, nullptr, 1, m_ * n_, nullptr, 1, m_ * n_, CUFFT_Z2Z, nshots) !=
+          CUFFT_SUCCESS)
+        return err.set(GJ_ENOMEM, "cufftPlanMany(%d x %d, batch=%d) failed", m_, n_, nshots);
+      cond_batch = nshots;
+    }
+    cuDoubleComplex* X = condX.as<cuDoubleComplex>();
+    k_cond_taper<<<512, 256, 0, st>>>(gdev, nshots, m, n, g.dx, g.dy, condP.as<double>());
+    k_cond_pad<<<512, 256, 0, st>>>(gdev, X, nshots, m, n, m_, n_);
+    cufftSetStream(condplan, st);
+    if (cufftExecZ2Z(condplan, X, X, CUFFT_FORWARD) != CUFFT_SUCCESS) return err.set(GJ_ECUDA, "cufft 2-D failed");
+    k_cond_mul<<<512, 256, 0, st>>>(X, condF.as<double>(), size_t(m_) * n_, nshots);
+    if (cufftExecZ2Z(condplan, X, X, CUFFT_INVERSE) != CUFFT_SUCCESS) return err.set(GJ_ECUDA, "cufft 2-D failed");
+    k_cond_trim<<<512, 256, 0, st>>>(X, gdev, nshots, m, n, m_, n_);
+    k_cond_norm<<<nshots, 1024, 0, st>>>(gdev, mn);
+    c.launches += 7;
+    GJ_CUDA(err, cudaStreamSynchronize(st));  // F and par go out of scope
+    return GJ_OK;
+  }
+
+  // ------------------------------------------------------------ misfit only
+  // Forward runs and misfits of all shots, no history and no adjoint: the
+  // objective evaluations of a step-length search (w_objs_e.m:24-65, called
+  // by w_stepparabola_e.m:20-41 for each trial model).
+  gj_status misfit(Err& err, Ctx& c, const double* eps, const double* sig, const double* dobs, gj_misfit_kind mk,
+                   double* misfit_out, cudaStream_t st) {
+    GJ_TRY(stage_inputs(err, c, eps, sig, false, dobs, false, st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+    ring_on = ring_nth > 0;
+    GJ_TRY(prepare_tasks(err, nshots));
+    T* A = fwdA.as<T>() + ld;
+    T* B = fwdB.as<T>() + ld;
+    const int nrr = std::max(nr, 1);
+    const size_t tr = size_t(nrr) * g.nt;
+    for (int it = 0; it < g.nt; ++it) {
+      StepArgs<T> a = step_args(A, B, it);
+      GJ_TRY(launch_fwd(err, a, nshots, st));
+      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it, g.nt,
+                                                   dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
+      c.launches += 2;
+      std::swap(A, B);
+    }
+    if (mk == GJ_MISFIT_ENV_L2) {
+      GJ_TRY(env_residual(err, c, 0, nshots, st));
+    } else {
+      k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr,
+                                                      sums.as<double>());
+      ++c.launches;
+    }
+    GJ_CUDA(err, cudaGetLastError());
+    std::vector<double> hs(2 * nshots);
+    GJ_CUDA(err, cudaMemcpyAsync(hs.data(), sums.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    GJ_CUDA(err, cudaStreamSynchronize(st));
+    for (int q = 0; q < nshots; ++q)
+      misfit_out[q] = hs[2 * q + 1] > 0 ? 0.5 * hs[2 * q] / hs[2 * q + 1] : 0.5 * hs[2 * q];
+    return GJ_OK;
+  }
+
   // ------------------------------------------------------------ gradient
   // Chooses K: the whole history when it fits, else checkpoints every K steps.
   void choose_k(const gj_w_opts& o, size_t free_bytes) {
@@ -636,9 +748,29 @@ class WSolver : public WSolverBase {
       GJ_TRY(gout.alloc(err, 2 * gsz * sizeof(double)));
       ge_d = gout.as<double>(); gs_d = ge_d + gsz;
     }
-    k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, nshots, o.per_shot, mode == GJ_ADJ_EXACT ? 1 : 0,
-                                     g.dt, g.eps0, eps_m, sig_m, ge_d, gs_d);
-    ++c.launches;
+    if (o.condition) {
+      // per-shot gradients, conditioned, then averaged (or returned per shot)
+      GJ_TRY(cbuf.alloc(err, 2 * size_t(nshots) * mn * sizeof(double)));
+      double* ce_ = cbuf.as<double>();
+      double* cs_ = ce_ + size_t(nshots) * mn;
+      k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, nshots, 1, mode == GJ_ADJ_EXACT ? 1 : 0, g.dt,
+                                       g.eps0, eps_m, sig_m, ce_, cs_);
+      ++c.launches;
+      GJ_TRY(condition(err, c, o, ce_, o.cond_ax, o.cond_az, st));
+      GJ_TRY(condition(err, c, o, cs_, 2 * o.cond_ax, 2 * o.cond_az, st));
+      if (o.per_shot) {
+        GJ_CUDA(err, cudaMemcpyAsync(ge_d, ce_, gsz * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        GJ_CUDA(err, cudaMemcpyAsync(gs_d, cs_, gsz * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      } else {
+        k_shot_mean<<<256, 256, 0, st>>>(ce_, nshots, mn, ge_d);
+        k_shot_mean<<<256, 256, 0, st>>>(cs_, nshots, mn, gs_d);
+        c.launches += 2;
+      }
+    } else {
+      k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, nshots, o.per_shot, mode == GJ_ADJ_EXACT ? 1 : 0,
+                                       g.dt, g.eps0, eps_m, sig_m, ge_d, gs_d);
+      ++c.launches;
+    }
     if (dev_out && sizeof(T) == 4) {
       k_convert<double, float><<<256, 256, 0, st>>>(ge_d, static_cast<float*>(geps), gsz);
       k_convert<double, float><<<256, 256, 0, st>>>(gs_d, static_cast<float*>(gsig), gsz);
@@ -674,6 +806,7 @@ class WSolver : public WSolverBase {
   ~WSolver() override {
     if (fftplan) cufftDestroy(fftplan);
     if (filtplan) cufftDestroy(filtplan);
+    if (condplan) cufftDestroy(condplan);
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
@@ -1330,6 +1463,18 @@ gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* 
   WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
   return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, mk, o, geps, gsig, dev_out, misfit_out,
                      d_out, e_out, st);
+}
+
+gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
+                   const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out) {
+  if (!eps || !sig || !dobs || !misfit_out) return c.err.set(GJ_EINVAL, "null input or output pointer");
+  if (mk != GJ_MISFIT_L2 && mk != GJ_MISFIT_ENV_L2) return c.err.set(GJ_EINVAL, "unknown misfit kind");
+  if (prec == GJ_F64) {
+    WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+    return s->misfit(c.err, c, eps, sig, dobs, mk, misfit_out, 0);
+  }
+  WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+  return s->misfit(c.err, c, eps, sig, dobs, mk, misfit_out, 0);
 }
 
 gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,

@@ -91,6 +91,14 @@ typedef struct gj_w_opts {
                             misfit stays that of the unfiltered residual */
   double filt_high;
   int filt_steep;        /* exponent of the filter; 0 = 8 (w_update_e.m:70) */
+  int condition;         /* 1 = condition every shot's gradients as w_update_e.m:99-137 and
+                            w_update_s.m:96-137 do (source taper gaussi.m of width
+                            4 c/sqrt(eps_r(source))/cond_fo, k-space low-pass image_gaussian.m,
+                            normali.m, zero on NaN), then return their mean over shots
+                            (w_update_e_.m:38), or each of them with per_shot */
+  double cond_fo;        /* source frequency of the taper width, Hz (regu.fo) */
+  double cond_ax, cond_az; /* image_gaussian widths for eps (regu.ax, regu.az); sigma uses twice
+                              these (w_update_s.m:105-106) */
 } gj_w_opts;
 
 /* ---------------------------------------------------------------- context */
@@ -127,6 +135,14 @@ gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precisi
                         int nshots, const double* d_obs, gj_adj_mode mode,
                         gj_misfit_kind misfit, const gj_w_opts* opts, double* g_eps,
                         double* g_sig, double* misfit_out, double* d_out, double* e_out);
+
+/* Forward runs and misfits only (no history, no adjoint): replaces the
+ * objective evaluations of the step-length search, w_objs_e.m:24-65 as called
+ * by w_stepparabola_e.m:20-41 for each trial model.  misfit_out: nshots
+ * misfits normalised as in w_update_e.m:75-76 (L2) or of the envelopes (env_L2). */
+gj_status gj_w_misfit(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision,
+                      const double* eps_r, const double* sigma, const gj_w_shot* shots,
+                      int nshots, const double* d_obs, gj_misfit_kind misfit, double* misfit_out);
 
 /* The adjoint half on its own: replaces [g, a_max] = w_grad(u, ...) (w_grad.m:1-115)
  * for one shot.  u is the m x n x nt history (or its time derivative), e the

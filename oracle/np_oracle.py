@@ -371,3 +371,55 @@ def tukeywin(n, r=0.5):
     w[:tl] = (1 + np.cos(np.pi / per * (t[:tl] - per))) / 2
     w[th - 1:] = (1 + np.cos(np.pi / per * (t[th - 1:] - 1 + per))) / 2
     return w
+
+
+# ---------------------------------------------------------------------------
+# Gradient conditioning of w_update_e.m:99-137 / w_update_s.m:96-137.
+
+def normali(a):
+    """normali.m: a / max|a| (1 when that is 0)."""
+    a = np.asarray(a, np.float64)
+    mx = np.nanmax(np.abs(a)) if a.size else 0.0
+    return a / (mx if mx != 0 else 1.0)
+
+
+def gaussi(x, z, s, lo):
+    """gaussi.m with s = (iz, ix) 0-based: normali(1 - exp(-r^2)), r measured in
+    units of 2*lo (the caller passes 2*lo, gaussi doubles it again)."""
+    X, Z = np.meshgrid(np.asarray(x, np.float64), np.asarray(z, np.float64))
+    lo = 2 * lo
+    g = ((X - x[s[1]]) / lo) ** 2 + ((Z - z[s[0]]) / lo) ** 2
+    return normali(1 - np.exp(-g))
+
+
+def image_gaussian_low(img, a, b):
+    """image_gaussian.m with filt_TYPE 'LOW_PASS'."""
+    img = np.asarray(img, np.float64)
+    m, n = img.shape
+    m_ = 1 << int(np.ceil(np.log2(m)))
+    n_ = 1 << int(np.ceil(np.log2(n)))
+    pad = np.zeros((m_, n_))
+    pad[:m, :n] = img
+    K = np.fft.fft2(pad)
+    A = n_ * (a / 2) * np.sqrt(2)
+    B = m_ * (b / 2) * np.sqrt(2)
+    XY, YX = np.meshgrid(np.arange(n_), np.arange(m_))
+    kk = np.exp(-(((XY - n_ / 2) / A) ** 2 + ((YX - m_ / 2) / B) ** 2))
+    kk = kk / np.max(np.abs(kk))
+    out = np.real(np.fft.ifft2(np.fft.fftshift(kk) * K))
+    return out[:m, :n]
+
+
+def condition_shot(g, dx, dz, src_model, eps_model, fo, ax, az, c=299792458.0):
+    """One shot's gradient through the taper, the k-space low-pass, normali and
+    the NaN guard (w_update_e.m:110-135).  src_model = (row, column) of the
+    source in the model, 0-based."""
+    m, n = g.shape
+    x = np.arange(n) * dx
+    z = np.arange(m) * dz
+    lo = c / np.sqrt(eps_model[src_model[0], src_model[1]]) / fo
+    g = gaussi(x, z, src_model, 2 * lo) * g
+    g = normali(image_gaussian_low(g, ax, az))
+    if np.isnan(g).any():
+        g = np.zeros_like(g)
+    return g

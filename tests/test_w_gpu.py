@@ -204,3 +204,57 @@ def test_band_filtered_residual_and_gradient_match_oracle(gpu_ctx, oracle, small
     sl = (slice(0, g.m - 1), slice(1, g.n - 1))
     assert rel_l2(res["g_eps"][sl], ge[sl]) < 10 * tol
     assert rel_l2(res["g_sig"][sl], gs[sl]) < 10 * tol
+
+
+@pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-12), (N.GJ_F32, 1e-5)])
+def test_forward_only_misfit_matches_oracle_and_gradient(gpu_ctx, oracle, small_ft, prec, tol):
+    """gj_w_misfit (w_objs_e.m, the step-length search's objective): the same
+    misfits as the oracle and as the full gradient call, for L2 and env_L2,
+    on two trial models in a row."""
+    import np_oracle as npo
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    for scale in (1.0, 1.05):
+        eps = p.eps0 * scale
+        m = gpu_ctx.w_misfit(g, eps, p.sig0, p.shots, dobs, precision=prec)
+        _, _, mis = oracle.gradient_batch(g, eps, p.sig0, p.shots, np.stack([d.T for d in dobs]), mode="exact")
+        assert np.allclose(m, mis, rtol=tol)
+        r = gpu_ctx.w_gradient(g, eps, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=prec)
+        assert np.allclose(m, r["misfit"], rtol=tol)
+    me = gpu_ctx.w_misfit(g, p.eps0, p.sig0, p.shots, dobs, misfit=N.GJ_MISFIT_ENV_L2, precision=prec)
+    for k, sh in enumerate(p.shots):
+        d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+        _, de, doe = npo.w_bozdag(dobs[k], d, "env_L2")
+        assert abs(me[k] - npo.w_E(doe, de)) <= max(tol, 2e-4) * npo.w_E(doe, de)
+
+
+def test_gradient_conditioning_matches_numpy_twin(gpu_ctx, oracle, small_ft):
+    """Per-shot conditioning (source taper, k-space low-pass, normali, NaN
+    guard; w_update_e.m:110-135, w_update_s.m:96-137) and the shot mean
+    (w_update_e_.m:38) against the numpy twin applied to the GPU's own
+    per-shot gradients."""
+    import np_oracle as npo
+    from gerjoii_b200.geometry import C_0
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    o = N.OptsC()
+    o.per_shot = 1
+    raw = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=o)
+    fo, ax, az = 300e6, 0.2, 0.3
+    oc = N.OptsC()
+    oc.condition, oc.cond_fo, oc.cond_ax, oc.cond_az = 1, fo, ax, az
+    cond = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=oc)
+    oc.per_shot = 1
+    cps = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=oc)
+    te, ts = [], []
+    for k, sh in enumerate(p.shots):
+        sm = (sh.src_i - g.dom_i0, sh.src_j - g.dom_j0)
+        te.append(npo.condition_shot(raw["g_eps"][k], g.dx, g.dy, sm, p.eps0, fo, ax, az, c=C_0))
+        ts.append(npo.condition_shot(raw["g_sig"][k], g.dx, g.dy, sm, p.eps0, fo, 2 * ax, 2 * az, c=C_0))
+        assert rel_l2(cps["g_eps"][k], te[-1]) < 1e-10
+        assert rel_l2(cps["g_sig"][k], ts[-1]) < 1e-10
+    assert rel_l2(cond["g_eps"], np.mean(te, axis=0)) < 1e-10
+    assert rel_l2(cond["g_sig"], np.mean(ts, axis=0)) < 1e-10
+    assert np.abs(cps["g_eps"]).max() == pytest.approx(1.0)
