@@ -72,6 +72,29 @@ enum { RA_LN = 0, RA_CE, RA_CH, RA_AX, RA_BX, RA_AY, RA_BY, RA_SX, RA_SY, RA_LX,
 // Adjoint halo, column J: p-value inputs below (lane 31) and above (lane 0).
 enum { HA_LDN = 0, HA_SXDN, HA_CHDN, HA_BXDN, HA_LUP, HA_SXUP, HA_CHUP, HA_BXUP, HA_LYUP, HA_HYBUP };
 
+// Receivers of the launch's shots for the fused record (forward) and
+// injection (exact adjoint): per shot nrr entries {column J, row I, receiver r}
+// sorted by column, `nrs` valid.  Traces are [shot in launch][r][t].
+template <class T>
+struct RecArgs {
+  const int* rs;   // first shot of the launch
+  const int* nrs;  // first shot of the launch
+  int nrr, nt;
+  T* d; int it;          // forward: d(r, it) = Ez after the step (k_record), when d
+  const T* e; int kinj;  // adjoint: output += e(r, kinj) (k_inject_add of the next step), when kinj >= 0
+};
+
+// First receiver of a shot's column-sorted list at column >= j0.
+__device__ __forceinline__ int rec_first(const int* rs, int n, int j0) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (rs[3 * mid] < j0) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // Shared memory of a launch with `warps` warps per CTA and S stages.
 inline size_t ring_smem(int warps, int S, bool fast) {
   return size_t(warps) * S * (fast ? RING_STAGE_FAST : RING_STAGE) * 16;
@@ -92,7 +115,7 @@ inline size_t ring_smem(int warps, int S, bool fast) {
 // --------------------------------------------------------------------------
 template <class T, int S, bool FAST>
 __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T> a, const int4* __restrict__ tasks,
-                                              int ntask) {
+                                              int ntask, const RecArgs<T> ra) {
   constexpr int SLOTS = RingShape<FAST>::slots, STAGE = RingShape<FAST>::stage;
   constexpr int V = VT<T>::V;
   static_assert(V * sizeof(T) == 16, "ring kernels move 16 bytes per lane");
@@ -217,6 +240,20 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       }
     }
   }
+  // receiver window (fused k_record): lane q holds receiver rp + q of this
+  // shot's column-sorted list, from the first one at column >= j0
+  const int* rsl = ra.rs + size_t(zl) * 3 * ra.nrr;
+  const int rn = ra.d ? ra.nrs[zl] : 0;
+  int rp = rn ? rec_first(rsl, rn, j0) : 0;
+  int wJ = 0x7fffffff, wI = 0, wR = 0, widx = 0;
+  auto rec_window = [&]() {
+    const int q = rp + lane;
+    wJ = 0x7fffffff;
+    if (q < rn) { wJ = rsl[3 * q]; wI = rsl[3 * q + 1]; wR = rsl[3 * q + 2]; }
+    widx = 0;
+  };
+  if (rn) rec_window();
+  int rJ = __shfl_sync(0xffffffffu, wJ, 0);
   for (int J = j0; J <= j1; ++J) {
     const int it = J - j0;
     if (J + S - 1 <= j1) issue(J + S - 1, (it + S - 1) % S);
@@ -330,6 +367,18 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
     }
     if (live && a.hist && J >= w.dj0 && J < w.dj0 + w.n)
       vst(a.hist + size_t(zl) * a.hstride + dnode(I0, J, ld, w.dj0), e_new);
+    while (rJ == J) {  // d(it, r) = Ez(receiver) after the step (w_solve.m:100)
+      const int I = __shfl_sync(0xffffffffu, wI, widx), r = __shfl_sync(0xffffffffu, wR, widx);
+      if (I >= I0 && I < I0 + V) {
+        T val = T(0);
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if (I == I0 + v) val = e_new[v];
+        ra.d[(size_t(zl) * ra.nrr + r) * ra.nt + ra.it] = val;
+      }
+      if (++widx == 32) { rp += 32; rec_window(); }
+      rJ = __shfl_sync(0xffffffffu, wJ, widx);
+    }
 #pragma unroll
     for (int v = 0; v < V; ++v) { hx_prev[v] = hx_new[v]; ez_c[v] = ez_n[v]; }
   }
@@ -404,7 +453,7 @@ struct AdjRingArgs {
 
 template <class T, int S, bool FAST>
 __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs<T> a, const int4* __restrict__ tasks,
-                                              int ntask) {
+                                              int ntask, const RecArgs<T> ra) {
   constexpr int SLOTS = RingShape<FAST>::slots, STAGE = RingShape<FAST>::stage;
   constexpr int V = VT<T>::V;
   static_assert(V * sizeof(T) == 16, "ring kernels move 16 bytes per lane");
@@ -552,6 +601,38 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
         qx_prev[v] = hb * (lxo[v] + py_m[v] - py_c[v]);
       }
   }
+  // receiver window (fused injection of the next step's adjoint source):
+  // lane q holds receiver rp + q of this shot's column-sorted list and its e
+  const int* rsl = ra.rs + size_t(zl) * 3 * ra.nrr;
+  const int rn = ra.kinj >= 0 ? ra.nrs[zl] : 0;
+  int rp = rn ? rec_first(rsl, rn, j0) : 0;
+  int wJ = 0x7fffffff, wI = 0, widx = 0;
+  T wE = T(0);
+  auto rec_window = [&]() {
+    const int q = rp + lane;
+    wJ = 0x7fffffff;
+    if (q < rn) {
+      wJ = rsl[3 * q]; wI = rsl[3 * q + 1];
+      wE = ra.e[(size_t(zl) * ra.nrr + rsl[3 * q + 2]) * ra.nt + ra.kinj];
+    }
+    widx = 0;
+  };
+  if (rn) rec_window();
+  int rJ = __shfl_sync(0xffffffffu, wJ, 0);
+  // output += e(receiver, kinj) at the receivers of column J (k_inject_add)
+  auto inject = [&](int J, T (&le)[V]) {
+    while (rJ == J) {
+      const int I = __shfl_sync(0xffffffffu, wI, widx);
+      const T ev = __shfl_sync(0xffffffffu, wE, widx);
+      if (I >= I0 && I < I0 + V) {
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+          if (I == I0 + v) le[v] += ev;
+      }
+      if (++widx == 32) { rp += 32; rec_window(); }
+      rJ = __shfl_sync(0xffffffffu, wJ, widx);
+    }
+  };
   for (int J = j0; J <= j1; ++J) {
     const int it = J - j0;
     if (J + S - 1 <= j1) issue(J + S - 1, (it + S - 1) % S);
@@ -608,6 +689,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
         img[v] = ((dmask >> v) & 1u) ? l_c[v] : T(0);
       }
       if (I0 == 0) le[0] = T(0);  // the Ez = 0 row of a free top is not a state
+      inject(J, le);
       vst(LB + k, le);
     } else if constexpr (!FAST) {
       // ---- general path
@@ -682,6 +764,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
         syn[v] = rB ? ay_c[v] * ly_c[v] : T(0);
         img[v] = (rI && ((dmask >> v) & 1u)) ? l_c[v] : T(0);
       }
+      inject(J, le);
       if (live) {
         vst(LB + k, le);
         if (anyBand) { vst(SxB + k, sxn); vst(SyB + k, syn); }

@@ -5,6 +5,7 @@
 // the per-shot source/receiver tables, the A/B state buffers of the forward
 // and adjoint fields, the checkpoints and the u-history ring.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -95,6 +96,7 @@ class WSolver : public WSolverBase {
   WDev<T> w{};   // forward coefficients
   WDev<T> wr{};  // reference-adjoint coefficients (sigma -> -sigma in the interior)
   DevBuf coef, model_d, prof, shotbuf, recbuf, selbuf, nrsbuf, nselbuf, sibuf, sjbuf;
+  DevBuf rsbuf;  // per shot nrr x {column, row, receiver}, sorted by column (ring kernels)
   DevBuf fwdA, fwdB, adjA, adjB, hist, ckpt, acc, dbuf, ebuf, dobsbuf, sums, scratch, stage, stage2, gout;
   std::vector<ShotHost> sh;
   std::vector<int> sh_src_i, sh_src_j;  // source nodes as given (Ez row, column)
@@ -244,6 +246,21 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaMemcpy(selbuf.p, hsel.data(), hsel.size() * sizeof(int), cudaMemcpyHostToDevice));
     GJ_CUDA(err, cudaMemcpy(nrsbuf.p, nrs.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
     GJ_CUDA(err, cudaMemcpy(nselbuf.p, nsel.data(), ns * sizeof(int), cudaMemcpyHostToDevice));
+    {
+      std::vector<int> hrs(size_t(ns) * nrr * 3, 0);
+      for (int s = 0; s < ns; ++s) {
+        std::vector<std::array<int, 3>> v(nrs[s]);
+        for (int r = 0; r < nrs[s]; ++r) {
+          const long kk = sh[s].rec[r];
+          v[r] = {int(kk / ld), int(kk % ld), r};
+        }
+        std::sort(v.begin(), v.end());
+        for (int r = 0; r < nrs[s]; ++r)
+          for (int q = 0; q < 3; ++q) hrs[(size_t(s) * nrr + r) * 3 + q] = v[r][q];
+      }
+      GJ_TRY(rsbuf.alloc(err, hrs.size() * sizeof(int)));
+      GJ_CUDA(err, cudaMemcpy(rsbuf.p, hrs.data(), hrs.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // traces
     GJ_TRY(dbuf.alloc(err, size_t(ns) * nrr * g.nt * sizeof(T)));
     GJ_TRY(ebuf.alloc(err, size_t(ns) * nrr * g.nt * sizeof(T)));
@@ -269,6 +286,7 @@ class WSolver : public WSolverBase {
   int RWG = 4;  // warps per CTA of the general kernel (GJ_RING_CTA_WARPS)
   int ring_SF = 3, nb_fast = 1;
   const bool ring_serial = getenv("GJ_RING_SERIAL") != nullptr;
+  int last_kernels = 0;  // kernels launched by the last launch_fwd / launch_adjr
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   template <int S, bool F>
@@ -389,6 +407,7 @@ class WSolver : public WSolverBase {
     const int nf = tt.n[2 * dir], ng = tt.n[2 * dir + 1];
     const int4* tf = static_cast<const int4*>(tt.buf[2 * dir].p);
     const int4* tg = static_cast<const int4*>(tt.buf[2 * dir + 1].p);
+    last_kernels = (nf > 0) + (ng > 0);
     if (ring_serial) {  // both kernels on st, one after the other (for timing each)
       if (ng > 0) launch_gen(tg, ng, st);
       if (nf > 0) launch_fast(tf, nf, st);
@@ -406,7 +425,17 @@ class WSolver : public WSolverBase {
   }
 
   // One forward step of gn shots (A -> B).
-  gj_status launch_fwd(Err& err, StepArgs<T> a, int gn, cudaStream_t st) {
+  RecArgs<T> rec_args(int g0) const {
+    RecArgs<T> r{};
+    const int nrr = std::max(nr, 1);
+    r.rs = rsbuf.as<int>() + size_t(g0) * nrr * 3;
+    r.nrs = nrsbuf.as<int>() + g0;
+    r.nrr = nrr;
+    r.nt = g.nt;
+    r.d = nullptr; r.it = 0; r.e = nullptr; r.kinj = -1;
+    return r;
+  }
+  gj_status launch_fwd(Err& err, StepArgs<T> a, int gn, cudaStream_t st, RecArgs<T> ra = RecArgs<T>{}) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       if (ring_on) {
         const TaskTable& tt = *tasks.at(gn);
@@ -415,17 +444,17 @@ class WSolver : public WSolverBase {
         auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
           const dim3 grd((n + RW - 1) / RW);
           const size_t sm = ring_smem(RW, SF, true);
-          if (SF == 2) k_fwdw<T, 2, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
-          else if (SF == 3) k_fwdw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
-          else k_fwdw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+          if (SF == 2) k_fwdw<T, 2, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
+          else if (SF == 3) k_fwdw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
+          else k_fwdw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
         };
         const int rw = RWG;
         auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
           const dim3 grd((n + rw - 1) / rw);
           const size_t sm = ring_smem(rw, S, false);
-          if (S == 2) k_fwdw<T, 2, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
-          else if (S == 3) k_fwdw<T, 3, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
-          else k_fwdw<T, 4, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+          if (S == 2) k_fwdw<T, 2, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n, ra);
+          else if (S == 3) k_fwdw<T, 3, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n, ra);
+          else k_fwdw<T, 4, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n, ra);
         };
         return fork_join<StepArgs<T>>(err, tt, 0, st, lf, lg);
       }
@@ -434,10 +463,11 @@ class WSolver : public WSolverBase {
     a.tj = tj_for(gn);
     const dim3 grd((NX + 1 + 128 * V - 1) / (128 * V), (NY + 1 + a.tj - 1) / a.tj, gn);
     k_stepv<T, 0><<<grd, 128, 0, st>>>(w, a);
+    last_kernels = 1;
     return GJ_OK;
   }
   // One exact adjoint step of gn shots with the l ring (ring kernels only).
-  gj_status launch_adjr(Err& err, AdjRingArgs<T> a, int gn, cudaStream_t st) {
+  gj_status launch_adjr(Err& err, AdjRingArgs<T> a, int gn, cudaStream_t st, RecArgs<T> ra) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       const TaskTable& tt = *tasks.at(gn);
       const WDev<T> wd = w;
@@ -445,17 +475,17 @@ class WSolver : public WSolverBase {
       auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
         const dim3 grd((n + RW - 1) / RW);
         const size_t sm = ring_smem(RW, SF, true);
-        if (SF == 2) k_adjw<T, 2, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
-        else if (SF == 3) k_adjw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
-        else k_adjw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n);
+        if (SF == 2) k_adjw<T, 2, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
+        else if (SF == 3) k_adjw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
+        else k_adjw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
       };
       const int rw = RWG;
       auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
         const dim3 grd((n + rw - 1) / rw);
         const size_t sm = ring_smem(rw, S, false);
-        if (S == 2) k_adjw<T, 2, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
-        else if (S == 3) k_adjw<T, 3, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
-        else k_adjw<T, 4, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n);
+        if (S == 2) k_adjw<T, 2, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n, ra);
+        else if (S == 3) k_adjw<T, 3, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n, ra);
+        else k_adjw<T, 4, false><<<grd, 32 * rw, sm, s_>>>(wd, a, tk, n, ra);
       };
       return fork_join<AdjRingArgs<T>>(err, tt, 1, st, lf, lg);
     }
@@ -523,7 +553,7 @@ class WSolver : public WSolverBase {
       k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
                                                    g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
                                                    nshots);
-      c.launches += 2;
+      c.launches += 1 + last_kernels;
       std::swap(A, B);
     }
     GJ_CUDA(err, cudaGetLastError());
@@ -643,7 +673,7 @@ class WSolver : public WSolverBase {
       GJ_TRY(launch_fwd(err, a, nshots, st));
       k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it, g.nt,
                                                    dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
-      c.launches += 2;
+      c.launches += 1 + last_kernels;
       std::swap(A, B);
     }
     if (mk == GJ_MISFIT_ENV_L2) {
@@ -1011,11 +1041,16 @@ class WSolver : public WSolverBase {
       a.shot0 = g0;
       if (full) { a.hist = slot_ptr(it + 1, 0); a.hstride = hs; }
       const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
-      GJ_TRY(launch_fwd(err, a, gn, st));
+      RecArgs<T> ra = rec_args(g0);
+      if (ring_on && nr > 0) { ra.d = dgrp; ra.it = it; }  // receivers recorded inside the step
+      GJ_TRY(launch_fwd(err, a, gn, st, ra));
       c.timer.end(tm, st);
-      k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, rec, nrr, nrs_d, it, nt, dgrp, d_src + g0,
-                                               static_cast<T*>(nullptr), gn);
-      nl += 2;
+      nl += last_kernels;
+      if (!ring_on) {
+        k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, rec, nrr, nrs_d, it, nt, dgrp, d_src + g0,
+                                                 static_cast<T*>(nullptr), gn);
+        ++nl;
+      }
       std::swap(A, B);
     }
     if (l2) {
@@ -1048,7 +1083,7 @@ class WSolver : public WSolverBase {
           const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
           GJ_TRY(launch_fwd(err, a, gn, st));
           c.timer.end(tm, st);
-          ++nl;
+          nl += last_kernels;
           std::swap(A, B);
         }
       }
@@ -1070,15 +1105,23 @@ class WSolver : public WSolverBase {
           const bool tm = c.timer.begin(KK_REF_STEP, st, gn);
           k_stepv<T, 1><<<grd, 128, 0, st>>>(wr, a);
           c.timer.end(tm, st);
+          nl += 2;
         } else if (ring_on) {
-          if (nr > 0)
+          // the adjoint source of step k is added by step k+1's kernel; only the
+          // first adjoint step (k = nt) needs its own injection
+          if (nr > 0 && k == nt) {
             k_inject_add<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, nrr, nrs_d, egrp, itf, nt, gn);
+            ++nl;
+          }
+          RecArgs<T> ra = rec_args(g0);
+          if (nr > 0 && itf - 1 >= 0) { ra.e = egrp; ra.kinj = itf - 1; }
           AdjRingArgs<T> a{};
           a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = g0;
           a.lout = lring.as<T>() + size_t(win) * gn * hs; a.hstride = hs;
           const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
-          GJ_TRY(launch_adjr(err, a, gn, st));
+          GJ_TRY(launch_adjr(err, a, gn, st, ra));
           c.timer.end(tm, st);
+          nl += last_kernels;
           ++win;
           if (win == Kd || k == s0 + 1) {
             // imaging over the steps k + win - 1 .. k
@@ -1102,8 +1145,8 @@ class WSolver : public WSolverBase {
           const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
           k_adj_stepv<T><<<grd, 128, 0, st>>>(w, a);
           c.timer.end(tm, st);
+          nl += 2;
         }
-        nl += 2;
         std::swap(LA, LB);
       }
     }
