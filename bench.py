@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--mode", default="exact", choices=["exact", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, plain-FP64, DC and CPU legs")
     ap.add_argument("--no-dc", action="store_true", help="skip the DC leg")
+    ap.add_argument("--cfg4", action="store_true",
+                    help="the 48 uneven problems instead (one gradient call each, vs plain FP64 on a sample)")
     return ap.parse_args()
 
 
@@ -222,6 +224,64 @@ def dc_leg(ctx):
             "path": "gj_dc_forward / gj_dc_gradient, host buffers"}
 
 
+def cfg4_leg(args):
+    """48 uneven problems (grids 256..1536 x 128..512, dx 0.02..0.05 m, 1500..5000
+    steps, 4..24 shots; blob / layer models): every problem is one gradient call
+    (FP32, exact adjoint, Kahan sums, shot groups and graphs chosen per problem).
+    Timed: one whole pass over the 48 problems after a warm-up pass (the warm-up
+    builds each problem's plan and CUDA graphs).  Baseline: the plain per-shot
+    FP64 form on one shot of every 12th problem, compared per cell-update."""
+    import torch
+    from gerjoii_b200 import synth
+    from gerjoii_b200 import _native as N
+    probs = synth.cfg4_problems()
+    ctx = N.Context(0)
+    data = []
+    for p in probs:
+        d = ctx.w_forward(p.grid, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F32)["d"]
+        data.append(d)
+
+    def one_pass():
+        t0 = time.perf_counter()
+        for p, d in zip(probs, data):
+            ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, d, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    one_pass()
+    clocks = Clocks(0)
+    clocks.start()
+    t = one_pass()
+    clk = clocks.stop()
+    shots = sum(len(p.shots) for p in probs)
+    upd = sum(2 * len(p.shots) * p.grid.nt * p.grid.NX * p.grid.NY for p in probs)
+    # plain FP64 sample
+    o = N.OptsC()
+    o.plain = 1
+    s_upd, s_t = 0, 0.0
+    for p, d in list(zip(probs, data))[::12]:
+        ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots[:1], d[:1], mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64,
+                       opts=o)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots[:1], d[:1], mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64,
+                       opts=o)
+        torch.cuda.synchronize()
+        s_t += time.perf_counter() - t0
+        s_upd += 2 * p.grid.nt * p.grid.NX * p.grid.NY
+    line = {"metric": "cfg4: 48 uneven radar gradients, shot-gradients/s & Gcell-upd/s, 1 B200", "value": shots / t,
+            "unit": "shot-gradients/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded blob / layer models, observed traces modelled on the device)",
+            "config": {"workload": "48 uneven problems (cfg4), one gradient call each, exact adjoint, FP32",
+                       "problems": len(probs), "shots": shots, "cell_updates": upd},
+            "gcell_updates_per_s": upd / t / 1e9, "clocks": clk,
+            "plain_fp64_sample": {"gcell_updates_per_s": s_upd / s_t / 1e9,
+                                  "sample": "1 shot of problems 0, 12, 24, 36, plain per-shot FP64 form",
+                                  "speedup_fp32_over_plain_fp64": (upd / t) / (s_upd / s_t)}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -254,6 +314,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.cfg4:
+        return cfg4_leg(args)
     import torch
     import torch.distributed as dist
     from gerjoii_b200 import _native as N
