@@ -69,3 +69,41 @@ def test_ring_forward_api_matches_oracle(gpu_ctx, oracle, tall):
         d, _, u = oracle.forward(p.grid, p.eps0, p.sig0, sh, store_u=True)
         assert rel_l2(out["d"][k], d) < 1e-12
         assert rel_l2(out["u"][k], u) < 1e-12
+
+
+def test_ring_edge_receivers_and_sources_match_oracle(gpu_ctx, oracle):
+    """Receivers the fused record / injection must handle: the same node twice,
+    inside the left and bottom PML, on the Ez = 0 top row, on the last interior
+    row, on the boundary column and row; a source inside the PML (no effect,
+    w_solve.m:92-94); a shot without receivers.  FP64 traces and per-shot exact
+    gradients (interior cells) against the oracle."""
+    from gerjoii_b200.geometry import Shot
+    p = synth.small(m=150, n=44, pml=10, nt=220, nsrc=2, nrec=6, free_top=True, seed=33)
+    g = p.grid
+    NX, NY = g.NX, g.NY
+    node = g.node
+    w = p.shots[0].wavelet
+    recA = np.array([node(1, 30), node(1, 30), node(50, 3), node(NX - 3, 30), node(0, 20),
+                     node(NX - g.pml - 1, 40), node(70, 0), node(NX, 25), node(5, 12)], np.int64)
+    shots = [Shot(2, 30, w, recA),
+             Shot(100, 5, w, p.shots[1].rec),          # source in the left PML band
+             Shot(3, 22, w, np.zeros(0, np.int64))]    # no receivers
+    dobs = [oracle.forward(g, p.eps_true, p.sig_true, sh)[0] for sh in shots]
+    out = gpu_ctx.w_forward(g, p.eps0, p.sig0, shots, precision=N.GJ_F64)
+    o = N.OptsC()
+    o.per_shot = 1
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=o,
+                             want_traces=True)
+    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
+    for k, sh in enumerate(shots):
+        d, _, _ = oracle.forward(g, p.eps0, p.sig0, sh)
+        if sh.nr:
+            assert rel_l2(out["d"][k], d) < 1e-12
+            assert rel_l2(res["d"][k], d) < 1e-12
+        e = d - dobs[k]
+        ge, gs = oracle.grad_exact(g, p.eps0, p.sig0, sh, e)
+        if sh.nr == 0:
+            assert np.abs(res["g_eps"][k]).max() == 0 and np.abs(res["g_sig"][k]).max() == 0
+            continue
+        assert rel_l2(res["g_eps"][k][sl], ge[sl]) < 1e-9
+        assert rel_l2(res["g_sig"][k][sl], gs[sl]) < 1e-9
