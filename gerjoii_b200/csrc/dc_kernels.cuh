@@ -7,11 +7,10 @@
 // and the source- and ky-dependent Robin ghost terms.
 //
 // Unknowns are ordered with the shorter grid direction fastest, so the matrix
-// is banded with half-bandwidth b = min(n, m).  The preconditioner is the FP32
-// LDL^T factor of that band (incomplete Cholesky with fill allowed inside the
-// band, i.e. complete within it), computed by one CTA per system with a
-// rolling (b+1) x (b+1) window in shared memory.  CG runs in FP64 with that
-// preconditioner, which is the FP64 iterative refinement of the FP32 solve.
+// is banded with half-bandwidth b = min(n, m).  The preconditioner is the
+// LDL^T factor of that band (FP64 by default, FP32 on request; complete within
+// the band), computed by one CTA per system with a rolling window of b+1 band
+// columns in shared memory.  CG runs in FP64 with that preconditioner.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -113,89 +112,106 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
 // split into equal contiguous runs over all threads (row-major packed order),
 // and the next band row's entries are fetched from global memory while the
 // update runs.
+// Band LDL^T of every system (TF = double by default, float on request): one
+// CTA per system.  The trailing window holds the b+1 band columns c = q..q+b
+// as cw[slot][k] = A(c + k, c), k = 0..b, in slots c mod (b+1).  At pivot q:
+//   1. (every 64 pivots) stage the entries of the columns entering at the next
+//      64 pivots (diagonal, A(c+1, c), A(c+b, c)), double-buffered;
+//   2. column q+b enters the slot that pivot q-1 freed;
+//   3. d = A(q, q), l_i = A(q+i, q) / d, output F[q] = {d, l_1 .. l_b};
+//   4. rank-1 update A(q+j+k, q+j) -= (l_{j+k} d) l_j over the packed
+//      elements (j in 1..b, k in 0..b-j) of the host-built table `jk`,
+//      interleaved over the threads so neighbouring threads touch neighbouring
+//      entries of one column.
+// Two barriers per pivot.
+constexpr int DC_STAGE = 64;
+
 template <class TF>
-__global__ void k_dc_factor(const DcGrid G, const double* ox, const double* oz, const double* dbase,
-                            const double* sig, const double* alpha, const double* ky2, int sys0,
-                            TF* fac, int* status) {
+__host__ __device__ inline size_t dc_factor_smem(int b) {
+  const size_t W = size_t(b) + 1, T = size_t(b) * (b + 1) / 2;
+  return (W * W + 2 * W + 6 * DC_STAGE) * sizeof(TF) + T * sizeof(unsigned);
+}
+
+template <class TF>
+__global__ void __launch_bounds__(256) k_dc_factor(const DcGrid G, const double* ox, const double* oz,
+                                                   const double* dbase, const double* sig, const double* alpha,
+                                                   const double* ky2, const unsigned* jk, int sys0, TF* fac,
+                                                   int* status) {
   extern __shared__ __align__(16) unsigned char shraw[];
-  TF* sh = reinterpret_cast<TF*>(shraw);
-  const int W = G.b + 1;
-  TF* win = sh;
-  TF* lc = sh + W * W;
+  const int N = G.N, b = G.b, W = b + 1;
+  const int T = b * (b + 1) / 2;
+  TF* cw = reinterpret_cast<TF*>(shraw);
+  TF* lc = cw + W * W;        // l_i, i = 1..b
+  TF* lcd = lc + W;           // l_i d
+  TF* stg = lcd + W;          // [2][3][DC_STAGE]: diag | A(c+1, c) | A(c+b, c)
+  unsigned* tab = reinterpret_cast<unsigned*>(stg + 6 * DC_STAGE);
   const int sys = blockIdx.x;
   const double* al = alpha + size_t(sys0 + sys) * G.nb;
   const double k2 = ky2[sys0 + sys];
-  TF* F = fac + size_t(sys) * size_t(G.N) * W;
-  const int N = G.N, b = G.b;
-  // this thread's run of the packed lower triangle (rows i = 1..b, cols 1..i)
-  const int T = b * (b + 1) / 2;
-  const int chunk = (T + blockDim.x - 1) / blockDim.x;
-  const int e0 = min(int(threadIdx.x) * chunk, T), e1 = min(e0 + chunk, T);
-  int i0 = 1, j0 = 1;
-  {
-    int e = e0, i = 1;
-    while (e >= i) { e -= i; ++i; }
-    i0 = i; j0 = e + 1;
+  TF* F = fac + size_t(sys) * size_t(N) * W;
+  const int nth = blockDim.x, tid = threadIdx.x;
+  auto diag = [&](int c) {
+    int l, h;
+    dc_lh(G, c, l, h);
+    return TF(dc_diag(G, dbase, sig, al, k2, l, h));
+  };
+  for (int e = tid; e < T; e += nth) tab[e] = jk[e];
+  for (int e = tid; e < W * W; e += nth) {  // columns 0..b
+    const int c = e / W, k = e % W;
+    TF v = TF(0);
+    if (c < N && c + k < N) {
+      if (k == 0) v = diag(c);
+      else if (k == 1) v = TF(dc_sub(G, ox, oz, c + 1, 1));
+      else if (k == b) v = TF(dc_sub(G, ox, oz, c + b, b));
+    }
+    cw[e] = v;
   }
-  for (int e = threadIdx.x; e < W * W; e += blockDim.x) win[e] = TF(0);
-  __syncthreads();
-  for (int r = threadIdx.x; r < W && r < N; r += blockDim.x) {
-    int l, h; dc_lh(G, r, l, h);
-    win[r * W + r] = TF(dc_diag(G, dbase, sig, al, k2, l, h));
-    if (r >= 1) win[r * W + (r - 1)] = TF(dc_sub(G, ox, oz, r, 1));
-    if (r >= b) win[r * W + (r - b)] = TF(dc_sub(G, ox, oz, r, b));
-  }
-  __syncthreads();
-  const bool loader = threadIdx.x == blockDim.x - 1;
   for (int q = 0; q < N; ++q) {
     const int p0 = q % W;
-    // prefetch the entries of band row q+b+1 (enters the window after this step)
-    const int nr = q + b + 1;
-    TF nd = 0, n1 = 0, nb_ = 0;
-    if (loader && nr < N) {
-      int l, h; dc_lh(G, nr, l, h);
-      nd = TF(dc_diag(G, dbase, sig, al, k2, l, h));
-      n1 = TF(dc_sub(G, ox, oz, nr, 1));
-      nb_ = TF(dc_sub(G, ox, oz, nr, b));
+    if (q % DC_STAGE == 0) {  // 1. columns entering after pivots q .. q+63
+      TF* sb = stg + ((q / DC_STAGE) & 1) * 3 * DC_STAGE;
+      for (int t = tid; t < DC_STAGE; t += nth) {
+        const int c = q + W + t;
+        TF d = TF(0), s1 = TF(0), s2 = TF(0);
+        if (c < N) {
+          d = diag(c);
+          if (c + 1 < N) s1 = TF(dc_sub(G, ox, oz, c + 1, 1));
+          if (c + b < N) s2 = TF(dc_sub(G, ox, oz, c + b, b));
+        }
+        sb[t] = d; sb[DC_STAGE + t] = s1; sb[2 * DC_STAGE + t] = s2;
+      }
     }
-    const TF d = win[p0 * W + p0];
-    if (threadIdx.x == 0) {
+    if (q >= 1) {  // 2. column q-1+W into slot (q-1) mod W
+      const int qq = q - 1;
+      const TF* sb = stg + ((qq / DC_STAGE) & 1) * 3 * DC_STAGE;
+      const int t = qq % DC_STAGE;
+      TF* col = cw + (qq % W) * W;
+      for (int k = tid; k < W; k += nth)
+        col[k] = k == 0 ? sb[t] : (k == 1 ? sb[DC_STAGE + t] : (k == b ? sb[2 * DC_STAGE + t] : TF(0)));
+    }
+    __syncthreads();  // stage 1 of pivot q-64.. and 2 visible; previous update complete
+    // 3. pivot
+    const TF* pc = cw + p0 * W;
+    const TF d = pc[0];
+    if (tid == 0) {
       F[size_t(q) * W] = d;
       if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
     }
-    for (int i = threadIdx.x + 1; i <= b; i += blockDim.x) {
-      int pi = p0 + i; if (pi >= W) pi -= W;
-      const TF li = (q + i < N) ? win[pi * W + p0] / d : TF(0);
+    for (int i = tid + 1; i <= b; i += nth) {
+      const TF li = (q + i < N) ? pc[i] / d : TF(0);
       lc[i] = li;
+      lcd[i] = li * d;
       F[size_t(q) * W + i] = li;
     }
     __syncthreads();
-    // rank-1 update A(i, j) -= (l_i d) l_j for 1 <= j <= i <= b
-    {
-      int i = i0, j = j0;
-      int pi = p0 + i; if (pi >= W) pi -= W;
-      int pj = p0 + j; if (pj >= W) pj -= W;
-      TF ci = (i <= b) ? lc[i] * d : TF(0);
-      for (int e = e0; e < e1; ++e) {
-        win[pi * W + pj] -= ci * lc[j];
-        if (++j > i) {
-          ++i; j = 1;
-          if (++pi >= W) pi -= W;
-          pj = p0 + 1; if (pj >= W) pj -= W;
-          ci = (i <= b) ? lc[i] * d : TF(0);
-        } else if (++pj >= W) pj -= W;
-      }
+    // 4. rank-1 update of columns q+1 .. q+b
+    for (int e = tid; e < T; e += nth) {
+      const unsigned jkv = tab[e];
+      const int j = int(jkv >> 16), k = int(jkv & 0xffffu);
+      int slot = p0 + j;
+      if (slot >= W) slot -= W;
+      cw[slot * W + k] -= lcd[j + k] * lc[j];
     }
-    __syncthreads();
-    // slide: row/col q+b+1 enters at the slot of q
-    for (int c = threadIdx.x; c < W; c += blockDim.x) { win[p0 * W + c] = TF(0); win[c * W + p0] = TF(0); }
-    __syncthreads();
-    if (loader && nr < N) {
-      win[p0 * W + p0] = nd;
-      win[p0 * W + (nr - 1) % W] = n1;
-      win[p0 * W + (nr - b) % W] = nb_;
-    }
-    __syncthreads();
   }
 }
 

@@ -76,6 +76,7 @@ struct DcPlan {
   DcGrid G{};
   int nky = 0, nsrc = 0, robin = 0;
   DevBuf sig, faces, ky2, wts, alpha, ab, cur, mnoff, mnbuf, fac, vec, dots, done, status, gbuf, dbuf, ebuf, ubuf;
+  DevBuf jk;  // packed (j << 16 | k) elements of the factor's rank-1 update
   std::vector<long> off;
 };
 
@@ -172,8 +173,14 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   G.b = std::min(gg.n, gg.m);
   G.DX = gg.dx; G.DZ = gg.dz;
   G.nb = 2 * (gg.m - 2) + (gg.n - 2) + 4;
-  if (G.b > (sizeof(TF) == 8 ? 140 : 200))
-    return err.set(GJ_EUNSUPPORTED, "band width min(n, m) = %d above the shared-memory window limit", G.b);
+  {
+    int dev = 0, maxsm = 0;
+    GJ_CUDA(err, cudaGetDevice(&dev));
+    GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (G.b > 256 || dc_factor_smem<TF>(G.b) > size_t(maxsm))
+      return err.set(GJ_EUNSUPPORTED, "band width min(n, m) = %d: the factor window needs %zu bytes of shared memory "
+                                      "(limit %d)", G.b, dc_factor_smem<TF>(G.b), maxsm);
+  }
   P.nky = gg.n_ky; P.nsrc = nsrc; P.robin = gg.robin;
   const int N = G.N, nky = P.nky, nsys_all = nsrc * nky;
   cudaStream_t st = 0;
@@ -248,8 +255,16 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   const int maxit = o.max_iter > 0 ? o.max_iter : 50;
   int it_max = 0;
   double rel_max = 0;
-  const size_t smem_f = size_t(G.b + 1) * (G.b + 2) * sizeof(TF);
+  const size_t smem_f = dc_factor_smem<TF>(G.b);
   GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
+  {
+    std::vector<unsigned> hjk;
+    hjk.reserve(size_t(G.b) * (G.b + 1) / 2);
+    for (int j = 1; j <= G.b; ++j)
+      for (int k = 0; k <= G.b - j; ++k) hjk.push_back((unsigned(j) << 16) | unsigned(k));
+    GJ_TRY(P.jk.alloc(err, hjk.size() * sizeof(unsigned)));
+    GJ_CUDA(err, cudaMemcpy(P.jk.p, hjk.data(), hjk.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  }
   double* V = P.vec.as<double>();
   for (int s0 = 0; s0 < nsrc; s0 += srcs_per_batch) {
     const int nsb = std::min(srcs_per_batch, nsrc - s0);
@@ -261,8 +276,9 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     // factor
     {
       const bool tm = c.timer.begin(KK_DC, st, nsys);
-      k_dc_factor<TF><<<nsys, 128, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(), P.alpha.as<double>(),
-                                                 P.ky2.as<double>(), sys0, P.fac.as<TF>(), P.status.as<int>());
+      k_dc_factor<TF><<<nsys, 256, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(), P.alpha.as<double>(),
+                                                 P.ky2.as<double>(), P.jk.as<unsigned>(), sys0, P.fac.as<TF>(),
+                                                 P.status.as<int>());
       c.timer.end(tm, st);
       ++c.launches;
     }
