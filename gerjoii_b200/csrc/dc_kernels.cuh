@@ -217,8 +217,33 @@ __global__ void __launch_bounds__(256) k_dc_factor(const DcGrid G, const double*
 
 // z = (L D L^T)^{-1} r for every system, one warp per system, and rz = r.z.
 // r, z are FP64 vectors in the reference layout [sys][l + h*n].  The rolling
-// windows (b+1 values) live in shared memory per warp; factor columns are
-// loaded one step ahead, and r / z values 32 steps at a time (one per lane).
+// window (b+1 values) lives in shared memory per warp; factor columns stream
+// through a per-warp ring of DC_RING columns with cp.async (issued DC_RING - 1
+// pivots ahead), r / z values 32 steps at a time (one per lane).
+constexpr int DC_RING = 16;
+
+template <class TF>
+__host__ __device__ inline size_t dc_precond_smem(int b, int warps) {
+  return size_t(warps) * (size_t(b) + 1) * (DC_RING + 1) * sizeof(TF);
+}
+
+__device__ __forceinline__ unsigned dc_smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Copies factor column q (b+1 entries) into a ring slot, one commit group.
+template <class TF>
+__device__ __forceinline__ void dc_col_async(TF* dst, const TF* F, int q, int N, int W, int lane) {
+  if (q >= 0 && q < N) {
+    const TF* src = F + size_t(q) * W;
+    for (int i = lane; i < W; i += 32)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dc_smem_addr(dst + i)), "l"(src + i),
+                   "n"(int(sizeof(TF)))
+                   : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
 template <class TF>
 __global__ void k_dc_precond(const DcGrid G, const TF* fac, const double* r, double* z, double* rz,
                              int nsys, const int* done) {
@@ -228,40 +253,35 @@ __global__ void k_dc_precond(const DcGrid G, const TF* fac, const double* r, dou
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sys = blockIdx.x * (blockDim.x >> 5) + warp;
   if (sys >= nsys || (done && done[sys])) return;
-  TF* win = shp + warp * W;
+  TF* win = shp + size_t(warp) * W * (DC_RING + 1);
+  TF* ring = win + W;  // DC_RING columns of W entries
   const TF* F = fac + size_t(sys) * size_t(G.N) * W;
   const double* R = r + size_t(sys) * G.N;
   double* Z = z + size_t(sys) * G.N;
   const int N = G.N, b = G.b;
-  constexpr int MAXI = 7;  // b <= 200 -> at most 7 entries of a column per lane
+  constexpr int MAXI = 8;  // b <= 256 -> at most 8 entries of a column per lane
   auto ref = [&](int q) { int l, h; dc_lh(G, q, l, h); return l + h * G.n; };
-  auto load_col = [&](int q, TF (&c)[MAXI]) {
-#pragma unroll
-    for (int u = 0; u < MAXI; ++u) {
-      const int i = lane + 1 + 32 * u;
-      c[u] = (q < N && i <= b) ? F[size_t(q) * W + i] : TF(0);
-    }
-  };
+  auto wait_ring = [&]() { asm volatile("cp.async.wait_group %0;\n" ::"n"(DC_RING - 1) : "memory"); __syncwarp(); };
   // forward: L y = r
   for (int i = lane; i < W; i += 32) win[i] = (i < N) ? TF(R[ref(i)]) : TF(0);
+  for (int p = 0; p < DC_RING - 1; ++p) dc_col_async(ring + (p % DC_RING) * W, F, p, N, W, lane);
   __syncwarp();
-  TF col[MAXI], nxt[MAXI];
-  load_col(0, col);
-  TF dq = F[0];
   double rpre = 0.0;
   for (int q = 0; q < N; ++q) {
     if ((q & 31) == 0) {  // r values entering the window over the next 32 steps
       const int nq = q + W + lane;
       rpre = (nq < N) ? R[ref(nq)] : 0.0;
     }
-    load_col(q + 1, nxt);
-    const TF dn = (q + 1 < N) ? F[size_t(q + 1) * W] : TF(1);
+    dc_col_async(ring + ((q + DC_RING - 1) % DC_RING) * W, F, q + DC_RING - 1, N, W, lane);
+    wait_ring();
+    const TF* col = ring + (q % DC_RING) * W;
+    const TF dq = col[0];
     const int p0 = q % W;
     const TF y = win[p0];
 #pragma unroll
     for (int u = 0; u < MAXI; ++u) {
       const int i = lane + 1 + 32 * u;
-      if (i <= b && q + i < N) { int pi = p0 + i; if (pi >= W) pi -= W; win[pi] -= col[u] * y; }
+      if (i <= b && q + i < N) { int pi = p0 + i; if (pi >= W) pi -= W; win[pi] -= col[i] * y; }
     }
     const double rin = __shfl_sync(0xffffffffu, rpre, q & 31);
     __syncwarp();
@@ -269,45 +289,45 @@ __global__ void k_dc_precond(const DcGrid G, const TF* fac, const double* r, dou
       Z[ref(q)] = double(y / dq);
       win[p0] = (q + W < N) ? TF(rin) : TF(0);
     }
-    __syncwarp();
-#pragma unroll
-    for (int u = 0; u < MAXI; ++u) col[u] = nxt[u];
-    dq = dn;
+    __syncwarp();  // the ring slot of column q is refilled at pivot q+1
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __threadfence_block();
   // backward: L^T x = z, x_q = z_q - sum_i l_{q+i,q} x_{q+i}
   for (int i = lane; i < W; i += 32) win[i] = TF(0);
   __syncwarp();
+  for (int p = 0; p < DC_RING - 1; ++p) dc_col_async(ring + (p % DC_RING) * W, F, N - 1 - p, N, W, lane);
   double acc = 0.0;
-  load_col(N - 1, col);
   double zpre = 0.0, rpre2 = 0.0;
   for (int q = N - 1; q >= 0; --q) {
-    const int k = (N - 1 - q) & 31;
+    const int s_ = N - 1 - q;  // step of the backward sweep
+    const int k = s_ & 31;
     if (k == 0) {  // z and r values of the next 32 steps (descending)
       const int qq = q - lane;
       zpre = (qq >= 0) ? Z[ref(qq)] : 0.0;
       rpre2 = (qq >= 0) ? R[ref(qq)] : 0.0;
     }
-    load_col(q - 1 >= 0 ? q - 1 : N, nxt);
-    TF s = TF(0);
+    dc_col_async(ring + ((s_ + DC_RING - 1) % DC_RING) * W, F, q - (DC_RING - 1), N, W, lane);
+    wait_ring();
+    const TF* col = ring + (s_ % DC_RING) * W;
+    TF sum = TF(0);
 #pragma unroll
     for (int u = 0; u < MAXI; ++u) {
       const int i = lane + 1 + 32 * u;
-      if (i <= b && q + i < N) { int pi = q % W + i; if (pi >= W) pi -= W; s += col[u] * win[pi]; }
+      if (i <= b && q + i < N) { int pi = q % W + i; if (pi >= W) pi -= W; sum += col[i] * win[pi]; }
     }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     const double zq = __shfl_sync(0xffffffffu, zpre, k);
     const double rq = __shfl_sync(0xffffffffu, rpre2, k);
     if (lane == 0) {
-      const TF x = TF(zq) - s;
+      const TF x = TF(zq) - sum;
       win[q % W] = x;
       Z[ref(q)] = double(x);
       acc += rq * double(x);
     }
     __syncwarp();
-#pragma unroll
-    for (int u = 0; u < MAXI; ++u) col[u] = nxt[u];
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   if (lane == 0) rz[sys] = acc;
 }
 

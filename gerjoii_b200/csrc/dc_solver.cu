@@ -104,7 +104,7 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   const TF* F = P.fac.as<TF>();
   const dim3 gv((N + 255) / 256 < 64 ? (N + 255) / 256 : 64, nsys);
   const int warps_per_block = 4;
-  const size_t shp = size_t(warps_per_block) * (G.b + 1) * sizeof(TF);
+  const size_t shp = dc_precond_smem<TF>(G.b, warps_per_block);
   const int pblocks = (nsys + warps_per_block - 1) / warps_per_block;
   GJ_CUDA(err, cudaMemsetAsync(X, 0, vn * sizeof(double), st));
   GJ_CUDA(err, cudaMemcpyAsync(R, B, vn * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -257,6 +257,8 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   double rel_max = 0;
   const size_t smem_f = dc_factor_smem<TF>(G.b);
   GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
+  GJ_CUDA(err, cudaFuncSetAttribute(k_dc_precond<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(dc_precond_smem<TF>(G.b, 4))));
   {
     std::vector<unsigned> hjk;
     hjk.reserve(size_t(G.b) * (G.b + 1) / 2);
