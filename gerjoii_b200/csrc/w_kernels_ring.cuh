@@ -837,4 +837,67 @@ __global__ void __launch_bounds__(256) k_image(const WDev<T> w, const T* lring, 
   }
 }
 
+// --------------------------------------------------------------------------
+// Reference imaging (w_grad.m:86-87 with differentiate_cube.m:33-51) over a
+// window of adjoint steps.  Slot r of the ring holds the adjoint Ez after the
+// step of history index k = kA - r (1..nt); history slot k sits at
+// H + (k - base) * hsl (slot k: E after forward step k-1).  Per step:
+//   S1 -= (c0 u[k0] + c1 u[k1] + c2 u[k2]) l,  S2 -= u[k] l
+// with differentiate_cube's stencil (one-sided at k = 1 and k = nt), summed in
+// T over the window and then added to the accumulators (compensated when kahan).
+// --------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_image_ref(const WDev<T> w, const T* lring, size_t lsl, const T* H,
+                                                   long base, size_t hsl, int kA, int cnt, int nt, T idt,
+                                                   size_t hstride, T* acc, size_t astride, int shot0, int kahan) {
+  constexpr int V = VT<T>::V;
+  const int zl = blockIdx.y;
+  const int s = shot0 + zl;
+  const int g0 = w.di0 / V, g1 = (w.di0 + w.m - 1) / V;
+  const int ng = g1 - g0 + 1;
+  const size_t total = size_t(ng) * w.n;
+  const size_t dn = size_t(w.ld) * size_t(w.n);
+  for (size_t t = threadIdx.x + size_t(blockIdx.x) * blockDim.x; t < total; t += size_t(blockDim.x) * gridDim.x) {
+    const int gi = int(t % ng), b = int(t / ng);
+    const size_t q = size_t(b) * w.ld + size_t(g0 + gi) * V;
+    const T* L = lring + size_t(zl) * hstride + q;
+    const T* U = H + size_t(zl) * hstride + q;
+    T s1[V], s2[V];
+    vzero<T, V>(s1); vzero<T, V>(s2);
+    for (int r = 0; r < cnt; ++r) {
+      const int k = kA - r;
+      int k0, k1, k2;
+      T c0, c1, c2;
+      if (k == 1) { k0 = 1; k1 = 2; k2 = 3; c0 = T(-1.5) * idt; c1 = T(2.0) * idt; c2 = T(-0.5) * idt; }
+      else if (k == nt) { k0 = nt - 2; k1 = nt - 1; k2 = nt; c0 = T(0.5) * idt; c1 = T(-2.0) * idt; c2 = T(1.5) * idt; }
+      else { k0 = k - 1; k1 = k; k2 = k + 1; c0 = T(-0.5) * idt; c1 = T(0); c2 = T(0.5) * idt; }
+      T l[V], u0[V], u1[V], u2[V], uk[V];
+      vldw(L + size_t(r) * lsl, l);
+      vldw(U + size_t(k0 - base) * hsl, u0);
+      vldw(U + size_t(k1 - base) * hsl, u1);
+      vldw(U + size_t(k2 - base) * hsl, u2);
+      vldw(U + size_t(k - base) * hsl, uk);
+#pragma unroll
+      for (int v = 0; v < V; ++v) {
+        const T du = c0 * u0[v] + c1 * u1[v] + c2 * u2[v];
+        s1[v] -= du * l[v];
+        s2[v] -= uk[v] * l[v];
+      }
+    }
+    T* A = acc + size_t(s) * astride + q;
+    T sE[V], cE[V], sS[V], cS[V];
+    vldw(A, sE); vldw(A + 2 * dn, sS);
+    if (kahan) {
+      vldw(A + dn, cE); vldw(A + 3 * dn, cS);
+#pragma unroll
+      for (int v = 0; v < V; ++v) { kahan_add(&sE[v], &cE[v], s1[v]); kahan_add(&sS[v], &cS[v], s2[v]); }
+      vst(A + dn, cE); vst(A + 3 * dn, cS);
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) { sE[v] += s1[v]; sS[v] += s2[v]; }
+    }
+    vst(A, sE); vst(A + 2 * dn, sS);
+  }
+}
+
 }  // namespace gj

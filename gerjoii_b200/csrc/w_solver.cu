@@ -97,6 +97,7 @@ class WSolver : public WSolverBase {
   WDev<T> wr{};  // reference-adjoint coefficients (sigma -> -sigma in the interior)
   DevBuf coef, model_d, prof, shotbuf, recbuf, selbuf, nrsbuf, nselbuf, sibuf, sjbuf;
   DevBuf rsbuf;  // per shot nrr x {column, row, receiver}, sorted by column (ring kernels)
+  DevBuf nosrc;  // per shot -1: steps without a source (the reference adjoint)
   DevBuf fwdA, fwdB, adjA, adjB, hist, ckpt, acc, dbuf, ebuf, dobsbuf, sums, scratch, stage, stage2, gout;
   std::vector<ShotHost> sh;
   std::vector<int> sh_src_i, sh_src_j;  // source nodes as given (Ez row, column)
@@ -260,6 +261,9 @@ class WSolver : public WSolverBase {
       }
       GJ_TRY(rsbuf.alloc(err, hrs.size() * sizeof(int)));
       GJ_CUDA(err, cudaMemcpy(rsbuf.p, hrs.data(), hrs.size() * sizeof(int), cudaMemcpyHostToDevice));
+      std::vector<long> hns(ns, -1);
+      GJ_TRY(nosrc.alloc(err, ns * sizeof(long)));
+      GJ_CUDA(err, cudaMemcpy(nosrc.p, hns.data(), ns * sizeof(long), cudaMemcpyHostToDevice));
     }
     // traces
     GJ_TRY(dbuf.alloc(err, size_t(ns) * nrr * g.nt * sizeof(T)));
@@ -435,11 +439,12 @@ class WSolver : public WSolverBase {
     r.d = nullptr; r.it = 0; r.e = nullptr; r.kinj = -1;
     return r;
   }
-  gj_status launch_fwd(Err& err, StepArgs<T> a, int gn, cudaStream_t st, RecArgs<T> ra = RecArgs<T>{}) {
+  gj_status launch_fwd(Err& err, StepArgs<T> a, int gn, cudaStream_t st, RecArgs<T> ra = RecArgs<T>{},
+                       const WDev<T>* wsel = nullptr) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       if (ring_on) {
         const TaskTable& tt = *tasks.at(gn);
-        const WDev<T> wd = w;
+        const WDev<T> wd = wsel ? *wsel : w;
         const int S = ring_S, SF = ring_SF;
         auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
           const dim3 grd((n + RW - 1) / RW);
@@ -1090,7 +1095,36 @@ class WSolver : public WSolverBase {
       int win = 0;  // adjoint steps in the l ring not yet imaged
       for (int k = s1; k >= s0 + 1; --k) {  // k = history slot of forward step k-1
         const int itf = k - 1;
-        if (mode == GJ_ADJ_REFERENCE) {
+        if (mode == GJ_ADJ_REFERENCE && ring_on) {
+          // w_grad.m:70-87: receivers hard-set, a sigma-flipped source-free step
+          // (the forward ring kernel with the flipped coefficients), its Ez at the
+          // model nodes into the ring; imaging every Kd steps (k_image_ref)
+          if (nr > 0) {
+            k_inject_set<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, sel, nrr, nsel_d, egrp, itf, nt, gn);
+            ++nl;
+          }
+          StepArgs<T> a = step_args(LA, LB, itf);
+          a.shot0 = g0;
+          a.src = nosrc.as<long>();
+          a.hist = lring.as<T>() + size_t(win) * gn * hs; a.hstride = hs;
+          const bool tm = c.timer.begin(KK_REF_STEP, st, gn);
+          GJ_TRY(launch_fwd(err, a, gn, st, RecArgs<T>{}, &wr));
+          c.timer.end(tm, st);
+          nl += last_kernels;
+          ++win;
+          if (win == Kd || k == s0 + 1) {
+            const bool ti = c.timer.begin(KK_IMAGE, st, gn);
+            const int ng = (w.di0 + g.m - 1) / V - w.di0 / V + 1;
+            const int nblk = int(std::min<long>((long(ng) * g.n + 255) / 256, 4L * nsm));
+            k_image_ref<T><<<dim3(nblk, gn), 256, 0, st>>>(w, lring.as<T>(), size_t(gn) * hs, H, base,
+                                                           size_t(gn) * hs,
+                                                           k + win - 1, win, nt, T(1.0 / g.dt), hs, acc.as<T>(),
+                                                           4 * dn, g0, kahan);
+            c.timer.end(ti, st);
+            win = 0;
+            ++nl;
+          }
+        } else if (mode == GJ_ADJ_REFERENCE) {
           if (nr > 0)
             k_inject_set<T><<<dim3(1, gn), 128, 0, st>>>(LA, sstride, rec, sel, nrr, nsel_d, egrp, itf, nt, gn);
           StepArgs<T> a = step_args(LA, LB, itf);
@@ -1193,7 +1227,7 @@ class WSolver : public WSolverBase {
     GJ_TRY(adjA.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(adjB.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
-    if (ring_on && mode == GJ_ADJ_EXACT) {
+    if (ring_on) {
       const void* lold = lring.p;
       GJ_TRY(lring.alloc(err, size_t(Kd) * G * dn * sizeof(T)));
       if (lring.p != lold) {

@@ -107,3 +107,23 @@ def test_ring_edge_receivers_and_sources_match_oracle(gpu_ctx, oracle):
             continue
         assert rel_l2(res["g_eps"][k][sl], ge[sl]) < 1e-9
         assert rel_l2(res["g_sig"][k][sl], gs[sl]) < 1e-9
+
+
+@pytest.mark.parametrize("ckpt", [0, 11])
+def test_ring_reference_adjoint_matches_marching_and_oracle(gpu_ctx, oracle, tall, ckpt):
+    """w_grad semantics (GJ_ADJ_REFERENCE) on the ring kernels with windowed
+    imaging: equal to the register-marching kernels with per-step imaging and
+    to the oracle, with and without checkpoints."""
+    p = tall
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    o = N.OptsC()
+    o.ckpt_every = ckpt
+    r = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_REFERENCE, precision=N.GJ_F64, opts=o)
+    o.no_ring = 1
+    m = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_REFERENCE, precision=N.GJ_F64, opts=o)
+    assert rel_l2(r["g_eps"], m["g_eps"]) < 1e-10
+    assert rel_l2(r["g_sig"], m["g_sig"]) < 1e-10
+    ge, gs, _ = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]), mode="reference")
+    assert rel_l2(r["g_eps"], ge) < 1e-9
+    assert rel_l2(r["g_sig"], gs) < 1e-9
