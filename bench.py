@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--mode", default="exact", choices=["exact", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, plain-FP64, DC and CPU legs")
     ap.add_argument("--no-dc", action="store_true", help="skip the DC leg")
+    ap.add_argument("--dc-only", action="store_true", help="only the DC leg (JSON line of its own)")
+    ap.add_argument("--dc-sources", type=int, default=200, help="DC sources (x 20 wavenumbers)")
     ap.add_argument("--cfg4", action="store_true",
                     help="the 48 uneven problems instead (one gradient call each, vs plain FP64 on a sample)")
     return ap.parse_args()
@@ -185,13 +187,13 @@ class CpuPool:
         self.pool.join()
 
 
-def dc_leg(ctx):
-    """Timed DC forward + sensitivity on the full survey; accuracy on one source."""
+def dc_leg(ctx, n_sources=200):
+    """Timed DC forward + sensitivity on the survey; accuracy on one source."""
     import torch
     from gerjoii_b200 import synth
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import np_dc_oracle as dco
-    c = synth.cfg5()
+    c = synth.cfg5(n_sources=n_sources)
     srcs = c["srcs"]
     fw = ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], srcs)  # warm-up and observed data
     rng = np.random.default_rng(5)
@@ -321,6 +323,11 @@ def main():
         return run_reference(args)
     if args.cfg4:
         return cfg4_leg(args)
+    if args.dc_only:
+        from gerjoii_b200 import _native as N
+        ctx = N.Context(0)
+        print(json.dumps({"metric": "2.5D DC solves/s, 1 B200", "dc": dc_leg(ctx, args.dc_sources)}), flush=True)
+        return
     import torch
     import torch.distributed as dist
     from gerjoii_b200 import _native as N
