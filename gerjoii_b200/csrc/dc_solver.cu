@@ -5,7 +5,8 @@
 // Lk a_k = M' e (dc_adjoint.m:10, Lk is symmetric), g_k = Sk(u_k) a_k and
 // g = (2/pi) sum_k w_k g_k trimmed of the Robin padding (dc_gradient2_5d.m).
 // All systems of a batch of sources are solved together by FP64 CG
-// preconditioned with the FP32 band LDL^T factor of each system.
+// preconditioned with the band LDL^T factor of each system (FP64 by default,
+// FP32 on request).
 #include <algorithm>
 #include <cmath>
 #include <vector>
