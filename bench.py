@@ -200,9 +200,12 @@ def dc_leg(ctx, n_sources=200):
     for q, d in zip(srcs, fw["d"]):
         q.d_obs = d * (1 + 0.02 * rng.standard_normal(d.shape))
     torch.cuda.synchronize()
+    ctx.set_kernel_timing(True)
     t0 = time.perf_counter()
     fw = ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], srcs)
     t_f = time.perf_counter() - t0
+    kt = {k: ctx.kernel_time(k) for k in ("dc_factor", "dc_precond")}
+    ctx.set_kernel_timing(False)
     t0 = time.perf_counter()
     gr = ctx.dc_gradient(c["SIG"], c["DX"], c["DZ"], c["robin"], srcs)
     t_g = time.perf_counter() - t0
@@ -218,6 +221,29 @@ def dc_leg(ctx, n_sources=200):
                                     dco.measuring_operator(n, m, q.mn))
     t_cpu = time.perf_counter() - t0
     rel = float(np.linalg.norm(fw["d"][0] - d_ref) / np.linalg.norm(d_ref))
+    # per-kernel device time of the timed forward; algorithmic work per system:
+    # factor b(b+1)/2 FMA per unknown, substitution reads the FP64 factor twice
+    # (N rounded up to 32 columns of b+1 rounded up to even entries) and moves
+    # r (twice), z (write, read, write) in FP64
+    N_, b_ = n * m, min(n, m)
+    wp_, nq_ = (b_ + 2) // 2 * 2, (N_ + 31) // 32 * 32
+    pk, pk_src = peaks()
+    kern = {}
+    f, pc = kt["dc_factor"], kt["dc_precond"]
+    if f["sampled"]:
+        sys_per = f["shot_launches"] / f["launches"]
+        flops = 2.0 * N_ * b_ * (b_ + 1) / 2 * sys_per
+        kern["k_dc_factor"] = {"avg_ms": f["ms"] / f["sampled"], "launches": f["launches"], "systems_per_launch": sys_per,
+                               "achieved_fp64_tflops": flops / (f["ms"] / f["sampled"] * 1e-3) / 1e12,
+                               "bound": "fp64 issue / shared memory"}
+    if pc["sampled"]:
+        sys_per = pc["shot_launches"] / pc["launches"]
+        byts = (2.0 * nq_ * wp_ * 8 + 5.0 * 8 * N_) * sys_per
+        gbs = byts / (pc["ms"] / pc["sampled"] * 1e-3) / 1e9
+        kern["k_dc_precond"] = {"avg_ms": pc["ms"] / pc["sampled"], "launches": pc["launches"],
+                                "systems_per_launch": sys_per, "bytes_per_launch": byts, "achieved_gbs": gbs,
+                                "peak_gbs": pk["hbm_gbs"], "frac": gbs / pk["hbm_gbs"], "peak_source": pk_src,
+                                "bound": "hbm"}
     return {"workload": f"2.5D DC, {n - 2}x{m - 1} cells (+Robin), {len(srcs)} sources x {nky} ky, "
                         f"{sum(x.nd for x in srcs)} data",
             "forward_solves_per_s": len(srcs) * nky / t_f, "forward_s": t_f,
@@ -225,6 +251,7 @@ def dc_leg(ctx, n_sources=200):
             "cg_iterations_max": max(fw["iters"], gr["iters"]),
             "max_rel_residual": max(fw["rel_residual"], gr["rel_residual"]),
             "data_rel_err_vs_fp64_direct_solve": rel,
+            "kernels": kern,
             "cpu_baseline": {"forward_solves_per_s": nky / t_cpu, "cores": 1, "kind": "port",
                              "sample": f"1 source x {nky} ky, FP64 sparse direct solves (scipy SuperLU) of the "
                                        "restated operator, operator assembly included"},

@@ -9,7 +9,7 @@
 // Unknowns are ordered with the shorter grid direction fastest, so the matrix
 // is banded with half-bandwidth b = min(n, m).  The preconditioner is the
 // LDL^T factor of that band (FP64 by default, FP32 on request; complete within
-// the band), computed by one CTA per system with a rolling window of b+1 band
+// the band), computed by one CTA per system, blocked, with the active band
 // columns in shared memory.  CG runs in FP64 with that preconditioner.
 #pragma once
 #include <cuda_runtime.h>
@@ -25,6 +25,7 @@ struct DcGrid {
   int depth_fast;   // 1: band index q = h + l*m (b = m); 0: q = l + h*n (b = n)
   double DX, DZ;    // DELTAS(:,:,1), DELTAS(:,:,2) as the reference computes them
   int nb;           // compact Robin entries per system: 2(m-2) + (n-2) + 4
+  int wp, nq;       // factor layout: column stride (16-byte multiple), columns (N rounded up to 32)
 };
 
 __device__ __forceinline__ int dc_q(const DcGrid& G, int l, int h) {
@@ -105,229 +106,357 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
   else { l = q % G.n; h = q / G.n; }
 }
 
-// Band LDL^T of every system (TF = double by default, float on request): one CTA per system.  Output per system:
-// N columns of (b+1) floats: [d_q, l_{q+1,q}, ..., l_{q+b,q}].
-// Shared memory: (b+1)^2 floats (rolling window, circular in both indices)
-// + (b+1) floats (current column).  The b(b+1)/2 updates of each step are
-// split into equal contiguous runs over all threads (row-major packed order),
-// and the next band row's entries are fetched from global memory while the
-// update runs.
 // Band LDL^T of every system (TF = double by default, float on request): one
-// CTA per system.  The trailing window holds the b+1 band columns c = q..q+b
-// as cw[slot][k] = A(c + k, c), k = 0..b, in slots c mod (b+1).  At pivot q:
-//   1. (every 64 pivots) stage the entries of the columns entering at the next
-//      64 pivots (diagonal, A(c+1, c), A(c+b, c)), double-buffered;
-//   2. column q+b enters the slot that pivot q-1 freed;
-//   3. d = A(q, q), l_i = A(q+i, q) / d, output F[q] = {d, l_1 .. l_b};
-//   4. rank-1 update A(q+j+k, q+j) -= (l_{j+k} d) l_j over the packed
-//      elements (j in 1..b, k in 0..b-j) of the host-built table `jk`,
-//      interleaved over the threads so neighbouring threads touch neighbouring
-//      entries of one column.
-// Two barriers per pivot.
-constexpr int DC_STAGE = 64;
+// CTA of 256 threads per system, blocked right-looking with panels of DC_NB
+// columns.  The window holds the M = b + DC_NB band columns of the current
+// block as S[c mod M][r mod Mr] = A(r, c), r = c .. c+b, with Mr = b + 1
+// rounded up to 4 so that four rows starting at a multiple of 4 are contiguous.
+// Per block of pivots q .. q+DC_NB-1:
+//   panel: for each pivot c0 = q+p: d = A(c0, c0), l_i = A(c0+i, c0) / d (written
+//     out); the rows below the panel go to U[p][r'] = l and Ud[p][r'] = l d
+//     (r' = row - q - DC_NB, zero outside the band); then the later panel
+//     columns take the rank-1 update.  Two barriers per pivot.
+//   trailing: the b x b lower triangle of columns q+DC_NB .. takes the
+//     rank-DC_NB update A(r, c) -= sum_p Ud[p][r'] U[p][c'], one 4 x 4 register
+//     tile per thread and pass (host-built tile list, column-major, so the lanes
+//     of a warp share the U operand and read contiguous rows of one column);
+//   the DC_NB columns entering the window (original entries: diagonal,
+//     A(c+1, c), A(c+b, c), fetched during the panel by the last DC_NB threads)
+//     take the panel's slots.
+// Pivots past N belong to an identity padding up to a multiple of DC_NB.
+// Output per system: G.nq columns of G.wp entries, column q = [1 / d_q,
+// l_{q+1,q}, ..., l_{q+b,q}, padding] (l = 0 past N); the columns N .. nq-1
+// are zero.
+constexpr int DC_NB = 8;
+constexpr int DC_FACTOR_THREADS = 256;
+
+struct DcFactorShape {
+  int M, Mr, BP, ntiles;
+};
+
+__host__ __device__ inline DcFactorShape dc_factor_shape(int b) {
+  DcFactorShape f;
+  f.M = b + DC_NB;
+  f.Mr = (b + 1 + 3) / 4 * 4;
+  f.BP = (b + 3) / 4 * 4;
+  const int nt = f.BP / 4;
+  f.ntiles = nt * (nt + 1) / 2;
+  return f;
+}
 
 template <class TF>
 __host__ __device__ inline size_t dc_factor_smem(int b) {
-  const size_t W = size_t(b) + 1, T = size_t(b) * (b + 1) / 2;
-  return (W * W + 2 * W + 6 * DC_STAGE) * sizeof(TF) + T * sizeof(unsigned);
+  const DcFactorShape f = dc_factor_shape(b);
+  return (size_t(f.M) * f.Mr + 2 * size_t(DC_NB) * f.BP + 4 * DC_NB) * sizeof(TF) + size_t(f.ntiles) * sizeof(unsigned);
+}
+
+__device__ __forceinline__ void dc_ld4(const double* p, double v[4]) {
+  const double2 a = *reinterpret_cast<const double2*>(p), c = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+}
+__device__ __forceinline__ void dc_ld4(const float* p, float v[4]) {
+  const float4 a = *reinterpret_cast<const float4*>(p);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void dc_st4(double* p, const double v[4]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void dc_st4(float* p, const float v[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
 template <class TF>
-__global__ void __launch_bounds__(256) k_dc_factor(const DcGrid G, const double* ox, const double* oz,
-                                                   const double* dbase, const double* sig, const double* alpha,
-                                                   const double* ky2, const unsigned* jk, int sys0, TF* fac,
-                                                   int* status) {
+__global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G, const double* ox, const double* oz,
+                                                                 const double* dbase, const double* sig,
+                                                                 const double* alpha, const double* ky2,
+                                                                 const unsigned* tiles, int sys0, TF* fac,
+                                                                 int* status) {
   extern __shared__ __align__(16) unsigned char shraw[];
-  const int N = G.N, b = G.b, W = b + 1;
-  const int T = b * (b + 1) / 2;
-  TF* cw = reinterpret_cast<TF*>(shraw);
-  TF* lc = cw + W * W;        // l_i, i = 1..b
-  TF* lcd = lc + W;           // l_i d
-  TF* stg = lcd + W;          // [2][3][DC_STAGE]: diag | A(c+1, c) | A(c+b, c)
-  unsigned* tab = reinterpret_cast<unsigned*>(stg + 6 * DC_STAGE);
-  const int sys = blockIdx.x;
+  const int N = G.N, b = G.b, wp = G.wp;
+  const DcFactorShape fs = dc_factor_shape(b);
+  const int M = fs.M, Mr = fs.Mr, BP = fs.BP;
+  TF* S = reinterpret_cast<TF*>(shraw);
+  TF* U = S + size_t(M) * Mr;  // [DC_NB][BP]
+  TF* Ud = U + DC_NB * BP;     // [DC_NB][BP]
+  TF* lc = Ud + DC_NB * BP;    // l_j of the current pivot, j < DC_NB
+  TF* stg = lc + DC_NB;        // [3][DC_NB]: entering columns' diagonal, A(c+1, c), A(c+b, c)
+  unsigned* tab = reinterpret_cast<unsigned*>(stg + 3 * DC_NB);
+  const int sys = blockIdx.x, tid = threadIdx.x, nth = DC_FACTOR_THREADS;
   const double* al = alpha + size_t(sys0 + sys) * G.nb;
   const double k2 = ky2[sys0 + sys];
-  TF* F = fac + size_t(sys) * size_t(N) * W;
-  const int nth = blockDim.x, tid = threadIdx.x;
-  auto diag = [&](int c) {
-    int l, h;
-    dc_lh(G, c, l, h);
-    return TF(dc_diag(G, dbase, sig, al, k2, l, h));
+  TF* F = fac + size_t(sys) * size_t(G.nq) * wp;
+  // original band entries of column c (identity past N)
+  auto entering = [&](int c, TF& dg, TF& s1, TF& s2) {
+    dg = TF(1); s1 = TF(0); s2 = TF(0);
+    if (c < N) {
+      int l, h;
+      dc_lh(G, c, l, h);
+      dg = TF(dc_diag(G, dbase, sig, al, k2, l, h));
+      if (c + 1 < N) s1 = TF(dc_sub(G, ox, oz, c + 1, 1));
+      if (c + b < N) s2 = TF(dc_sub(G, ox, oz, c + b, b));
+    }
   };
-  for (int e = tid; e < T; e += nth) tab[e] = jk[e];
-  for (int e = tid; e < W * W; e += nth) {  // columns 0..b
-    const int c = e / W, k = e % W;
-    TF v = TF(0);
-    if (c < N && c + k < N) {
-      if (k == 0) v = diag(c);
-      else if (k == 1) v = TF(dc_sub(G, ox, oz, c + 1, 1));
-      else if (k == b) v = TF(dc_sub(G, ox, oz, c + b, b));
-    }
-    cw[e] = v;
+  auto column_value = [&](int c, int k, TF dg, TF s1, TF s2) {  // row slot k of column c
+    const int r0 = c % Mr;
+    int r1 = r0 + 1, rb = r0 + b;
+    if (r1 >= Mr) r1 -= Mr;
+    if (rb >= Mr) rb -= Mr;
+    return k == r0 ? dg : (k == r1 ? s1 : (k == rb ? s2 : TF(0)));
+  };
+  for (int e = tid; e < fs.ntiles; e += nth) tab[e] = tiles[e];
+  for (int e = tid; e < M * Mr; e += nth) {  // columns 0 .. M-1
+    const int c = e / Mr, k = e % Mr;
+    TF dg, s1, s2;
+    entering(c, dg, s1, s2);
+    S[e] = column_value(c, k, dg, s1, s2);
   }
-  for (int q = 0; q < N; ++q) {
-    const int p0 = q % W;
-    if (q % DC_STAGE == 0) {  // 1. columns entering after pivots q .. q+63
-      TF* sb = stg + ((q / DC_STAGE) & 1) * 3 * DC_STAGE;
-      for (int t = tid; t < DC_STAGE; t += nth) {
-        const int c = q + W + t;
-        TF d = TF(0), s1 = TF(0), s2 = TF(0);
-        if (c < N) {
-          d = diag(c);
-          if (c + 1 < N) s1 = TF(dc_sub(G, ox, oz, c + 1, 1));
-          if (c + b < N) s2 = TF(dc_sub(G, ox, oz, c + b, b));
-        }
-        sb[t] = d; sb[DC_STAGE + t] = s1; sb[2 * DC_STAGE + t] = s2;
+  const int Nn = (N + DC_NB - 1) / DC_NB * DC_NB;
+  const int i0 = tid + 1;  // this thread's row below the pivot (b < 256)
+  int sq = 0, rq = 0;      // q mod M, q mod Mr
+  __syncthreads();
+  for (int q = 0; q < Nn; q += DC_NB) {
+    if (tid >= nth - DC_NB) {  // entering columns of this block (these threads have no panel row: b < 248)
+      const int t = tid - (nth - DC_NB);
+      TF dg, s1, s2;
+      entering(q + M + t, dg, s1, s2);
+      stg[t] = dg; stg[DC_NB + t] = s1; stg[2 * DC_NB + t] = s2;
+    }
+    // ---- panel
+#pragma unroll 1
+    for (int p = 0; p < DC_NB; ++p) {
+      const int c0 = q + p;
+      int s0 = sq + p, rb0 = rq + p;
+      if (s0 >= M) s0 -= M;
+      while (rb0 >= Mr) rb0 -= Mr;  // Mr < DC_NB only for b < 7
+      const TF d = S[s0 * Mr + rb0];
+      const TF dinv = TF(1) / d;
+      int pos = rb0 + i0;
+      if (pos >= Mr) pos -= Mr;
+      TF ld = TF(0);
+      if (i0 <= b) {
+        const TF l = S[s0 * Mr + pos] * dinv;
+        ld = l * d;
+        if (c0 < N) F[size_t(c0) * wp + i0] = (c0 + i0 < N) ? l : TF(0);
+        if (i0 < DC_NB) lc[i0] = l;
+        if (i0 >= DC_NB - p) { U[p * BP + i0 - DC_NB + p] = l; Ud[p * BP + i0 - DC_NB + p] = ld; }
       }
-    }
-    if (q >= 1) {  // 2. column q-1+W into slot (q-1) mod W
-      const int qq = q - 1;
-      const TF* sb = stg + ((qq / DC_STAGE) & 1) * 3 * DC_STAGE;
-      const int t = qq % DC_STAGE;
-      TF* col = cw + (qq % W) * W;
-      for (int k = tid; k < W; k += nth)
-        col[k] = k == 0 ? sb[t] : (k == 1 ? sb[DC_STAGE + t] : (k == b ? sb[2 * DC_STAGE + t] : TF(0)));
-    }
-    __syncthreads();  // stage 1 of pivot q-64.. and 2 visible; previous update complete
-    // 3. pivot
-    const TF* pc = cw + p0 * W;
-    const TF d = pc[0];
-    if (tid == 0) {
-      F[size_t(q) * W] = d;
-      if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
-    }
-    for (int i = tid + 1; i <= b; i += nth) {
-      const TF li = (q + i < N) ? pc[i] / d : TF(0);
-      lc[i] = li;
-      lcd[i] = li * d;
-      F[size_t(q) * W + i] = li;
+      for (int i = (i0 > b ? i0 : i0 + nth); i < BP + DC_NB - p; i += nth) {  // rows past the band
+        const int r = i - DC_NB + p;
+        if (r >= 0) { U[p * BP + r] = TF(0); Ud[p * BP + r] = TF(0); }
+      }
+      if (tid == 0 && c0 < N) {
+        F[size_t(c0) * wp] = dinv;
+        if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
+      }
+      if (p + 1 == DC_NB) break;
+      __syncthreads();
+      if (i0 <= b) {
+        int sj = s0;
+        for (int j = 1; j < DC_NB - p; ++j) {
+          if (++sj >= M) sj -= M;
+          if (i0 >= j) S[sj * Mr + pos] -= ld * lc[j];
+        }
+      }
+      __syncthreads();
     }
     __syncthreads();
-    // 4. rank-1 update of columns q+1 .. q+b
-    for (int e = tid; e < T; e += nth) {
-      const unsigned jkv = tab[e];
-      const int j = int(jkv >> 16), k = int(jkv & 0xffffu);
-      int slot = p0 + j;
-      if (slot >= W) slot -= W;
-      cw[slot * W + k] -= lcd[j + k] * lc[j];
+    // ---- trailing rank-DC_NB update
+    int sqn = sq + DC_NB, rqn = (rq + DC_NB) % Mr;
+    if (sqn >= M) sqn -= M;
+    for (int e = tid; e < fs.ntiles; e += nth) {
+      const unsigned tv = tab[e];
+      const int rt = int(tv & 0xffffu), ct = int(tv >> 16);
+      int rbase = rqn + 4 * rt;
+      if (rbase >= Mr) rbase -= Mr;
+      TF acc[4][4];
+      int sc[4];
+#pragma unroll
+      for (int kc = 0; kc < 4; ++kc) {
+        int s_ = sqn + 4 * ct + kc;
+        if (s_ >= M) s_ -= M;
+        sc[kc] = s_;
+        dc_ld4(S + s_ * Mr + rbase, acc[kc]);
+      }
+#pragma unroll
+      for (int p = 0; p < DC_NB; ++p) {
+        TF av[4], bv[4];
+        dc_ld4(Ud + p * BP + 4 * rt, av);
+        dc_ld4(U + p * BP + 4 * ct, bv);
+#pragma unroll
+        for (int kc = 0; kc < 4; ++kc)
+#pragma unroll
+          for (int kr = 0; kr < 4; ++kr) acc[kc][kr] -= av[kr] * bv[kc];
+      }
+      if (rt > ct && 4 * rt + 3 < b) {
+#pragma unroll
+        for (int kc = 0; kc < 4; ++kc) dc_st4(S + sc[kc] * Mr + rbase, acc[kc]);
+      } else {
+#pragma unroll
+        for (int kc = 0; kc < 4; ++kc)
+#pragma unroll
+          for (int kr = 0; kr < 4; ++kr) {
+            const int rp = 4 * rt + kr, cp = 4 * ct + kc;
+            if (rp >= cp && rp < b) S[sc[kc] * Mr + rbase + kr] = acc[kc][kr];
+          }
+      }
     }
+    // ---- entering columns q+M .. q+M+DC_NB-1 into the panel's slots
+    for (int e = tid; e < DC_NB * Mr; e += nth) {
+      const int t = e / Mr, k = e % Mr;
+      int s_ = sq + t;
+      if (s_ >= M) s_ -= M;
+      S[s_ * Mr + k] = column_value(q + M + t, k, stg[t], stg[DC_NB + t], stg[2 * DC_NB + t]);
+    }
+    sq = sqn;
+    rq = rqn;
+    __syncthreads();
   }
+  for (size_t e = size_t(N) * wp + tid; e < size_t(G.nq) * wp; e += nth) F[e] = TF(0);
 }
 
-// z = (L D L^T)^{-1} r for every system, one warp per system, and rz = r.z.
-// r, z are FP64 vectors in the reference layout [sys][l + h*n].  The rolling
-// window (b+1 values) lives in shared memory per warp; factor columns stream
-// through a per-warp ring of DC_RING columns with cp.async (issued DC_RING - 1
-// pivots ahead), r / z values 32 steps at a time (one per lane).
-constexpr int DC_RING = 16;
+// z = (L D L^T)^{-1} r and rz = r.z for every system; one warp (one CTA) per
+// system.  r, z are FP64 vectors in the reference layout [sys][l + h*n].
+// Factor columns stream through a shared-memory ring of DC_NST chunks of DC_CH
+// columns (16-byte cp.async, DC_NST - 1 chunks ahead).  The substitution window
+// lives in registers: within the 32-step sub-block starting at band index qs,
+// slot u of lane t holds position qs + 32u + t (mod 32R), so slot 0 holds the
+// sub-block's own positions; the slots rotate by one between sub-blocks and
+// every register index is a compile-time constant.
+//   forward  L y = r, column form: y_q = w_q, then w_{q+i} -= l_{q+i,q} y_q for
+//            i = 1..b, and z_q = y_q / d_q (the factor stores 1 / d_q);
+//   backward L^T x = z, row form: x_q = z_q - sum_i l_{q+i,q} x_{q+i}.  Lanes
+//            sum the terms i >= DC_NEAR over their slots and the warp reduces
+//            them; the DC_NEAR - 1 nearest terms come from registers, so the
+//            reduction of step q waits only for x_{q+DC_NEAR}, which enters the
+//            window DC_NEAR steps after it is computed.
+constexpr int DC_CH = 16, DC_NST = 4, DC_NEAR = 4;
 
 template <class TF>
-__host__ __device__ inline size_t dc_precond_smem(int b, int warps) {
-  return size_t(warps) * (size_t(b) + 1) * (DC_RING + 1) * sizeof(TF);
+__host__ __device__ inline size_t dc_precond_smem(int wp) {
+  return size_t(DC_NST) * DC_CH * wp * sizeof(TF);
 }
 
 __device__ __forceinline__ unsigned dc_smem_addr(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
-// Copies factor column q (b+1 entries) into a ring slot, one commit group.
+// Copies factor chunk c (columns c*DC_CH ..) into ring slot c mod DC_NST as one
+// commit group (an empty group when c is outside [0, nch)).
 template <class TF>
-__device__ __forceinline__ void dc_col_async(TF* dst, const TF* F, int q, int N, int W, int lane) {
-  if (q >= 0 && q < N) {
-    const TF* src = F + size_t(q) * W;
-    for (int i = lane; i < W; i += 32)
-      asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dc_smem_addr(dst + i)), "l"(src + i),
-                   "n"(int(sizeof(TF)))
+__device__ __forceinline__ void dc_chunk_async(TF* ring, const TF* F, int c, int nch, int wp, int lane) {
+  if (c >= 0 && c < nch) {
+    const int pieces = DC_CH * wp * int(sizeof(TF)) / 16;
+    const char* src = reinterpret_cast<const char*>(F + size_t(c) * DC_CH * wp);
+    const unsigned dst = dc_smem_addr(ring + (c & (DC_NST - 1)) * DC_CH * wp);
+    for (int p = lane; p < pieces; p += 32)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * unsigned(p)),
+                   "l"(src + 16 * size_t(p))
                    : "memory");
   }
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-template <class TF>
-__global__ void k_dc_precond(const DcGrid G, const TF* fac, const double* r, double* z, double* rz,
-                             int nsys, const int* done) {
+template <class TF, int R>
+__global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac, const double* r, double* z,
+                                                   double* rz, int nsys, const int* done) {
   extern __shared__ __align__(16) unsigned char shpraw[];
-  TF* shp = reinterpret_cast<TF*>(shpraw);
-  const int W = G.b + 1;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int sys = blockIdx.x * (blockDim.x >> 5) + warp;
+  TF* ring = reinterpret_cast<TF*>(shpraw);
+  constexpr int WIN = 32 * R;
+  const int sys = blockIdx.x, lane = threadIdx.x & 31;
   if (sys >= nsys || (done && done[sys])) return;
-  TF* win = shp + size_t(warp) * W * (DC_RING + 1);
-  TF* ring = win + W;  // DC_RING columns of W entries
-  const TF* F = fac + size_t(sys) * size_t(G.N) * W;
-  const double* R = r + size_t(sys) * G.N;
-  double* Z = z + size_t(sys) * G.N;
-  const int N = G.N, b = G.b;
-  constexpr int MAXI = 8;  // b <= 256 -> at most 8 entries of a column per lane
+  const int N = G.N, b = G.b, wp = G.wp, nq = G.nq;
+  const int nch = nq / DC_CH;
+  const TF* F = fac + size_t(sys) * nq * wp;
+  const double* Rv = r + size_t(sys) * N;
+  double* Z = z + size_t(sys) * N;
   auto ref = [&](int q) { int l, h; dc_lh(G, q, l, h); return l + h * G.n; };
-  auto wait_ring = [&]() { asm volatile("cp.async.wait_group %0;\n" ::"n"(DC_RING - 1) : "memory"); __syncwarp(); };
-  // forward: L y = r
-  for (int i = lane; i < W; i += 32) win[i] = (i < N) ? TF(R[ref(i)]) : TF(0);
-  for (int p = 0; p < DC_RING - 1; ++p) dc_col_async(ring + (p % DC_RING) * W, F, p, N, W, lane);
-  __syncwarp();
-  double rpre = 0.0;
-  for (int q = 0; q < N; ++q) {
-    if ((q & 31) == 0) {  // r values entering the window over the next 32 steps
-      const int nq = q + W + lane;
-      rpre = (nq < N) ? R[ref(nq)] : 0.0;
-    }
-    dc_col_async(ring + ((q + DC_RING - 1) % DC_RING) * W, F, q + DC_RING - 1, N, W, lane);
-    wait_ring();
-    const TF* col = ring + (q % DC_RING) * W;
-    const TF dq = col[0];
-    const int p0 = q % W;
-    const TF y = win[p0];
-#pragma unroll
-    for (int u = 0; u < MAXI; ++u) {
-      const int i = lane + 1 + 32 * u;
-      if (i <= b && q + i < N) { int pi = p0 + i; if (pi >= W) pi -= W; win[pi] -= col[i] * y; }
-    }
-    const double rin = __shfl_sync(0xffffffffu, rpre, q & 31);
+  auto rld = [&](const double* v, int a) { return (a >= 0 && a < N) ? v[ref(a)] : 0.0; };
+  auto chunk_wait = [&](int c_issue) {
+    __syncwarp();  // every lane is done with the slot being refilled
+    dc_chunk_async(ring, F, c_issue, nch, wp, lane);
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(DC_NST - 1) : "memory");
     __syncwarp();
-    if (lane == 0) {
-      Z[ref(q)] = double(y / dq);
-      win[p0] = (q + W < N) ? TF(rin) : TF(0);
+  };
+  auto column = [&](int q) { return ring + (((q / DC_CH) & (DC_NST - 1)) * DC_CH + (q & (DC_CH - 1))) * wp; };
+  // ---- forward sweep
+  TF w[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) w[u] = TF(rld(Rv, 32 * u + lane));
+  double rn = rld(Rv, WIN + lane);  // refills of the sub-block's slot 0
+  for (int c = 0; c < DC_NST - 1; ++c) dc_chunk_async(ring, F, c, nch, wp, lane);
+  for (int qs = 0; qs < nq; qs += 32) {
+    const double rnn = rld(Rv, qs + 32 + WIN + lane);
+    TF zv = TF(0);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if ((j & (DC_CH - 1)) == 0) chunk_wait((qs + j) / DC_CH + DC_NST - 1);
+      const TF* col = column(qs + j);
+      const TF y = __shfl_sync(0xffffffffu, w[0], j);
+      if (lane == j) { zv = y * col[0]; w[0] = TF(rn); }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int i = (32 * u + lane - j + WIN) & (WIN - 1);
+        if (i >= 1 && i <= b) w[u] -= col[i] * y;
+      }
     }
-    __syncwarp();  // the ring slot of column q is refilled at pivot q+1
+    if (qs + lane < N) Z[ref(qs + lane)] = double(zv);
+    const TF w0 = w[0];
+#pragma unroll
+    for (int u = 0; u + 1 < R; ++u) w[u] = w[u + 1];
+    w[R - 1] = w0;
+    rn = rnn;
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  __threadfence_block();
-  // backward: L^T x = z, x_q = z_q - sum_i l_{q+i,q} x_{q+i}
-  for (int i = lane; i < W; i += 32) win[i] = TF(0);
   __syncwarp();
-  for (int p = 0; p < DC_RING - 1; ++p) dc_col_async(ring + (p % DC_RING) * W, F, N - 1 - p, N, W, lane);
+  // ---- backward sweep
+#pragma unroll
+  for (int u = 0; u < R; ++u) w[u] = TF(0);
+  TF nx[DC_NEAR];  // nx[k] = x_{q+1+k}
+#pragma unroll
+  for (int k = 0; k < DC_NEAR; ++k) nx[k] = TF(0);
+  for (int c = 0; c < DC_NST - 1; ++c) dc_chunk_async(ring, F, nch - 1 - c, nch, wp, lane);
+  double zc = rld(Z, nq - 32 + lane), rc = rld(Rv, nq - 32 + lane);
   double acc = 0.0;
-  double zpre = 0.0, rpre2 = 0.0;
-  for (int q = N - 1; q >= 0; --q) {
-    const int s_ = N - 1 - q;  // step of the backward sweep
-    const int k = s_ & 31;
-    if (k == 0) {  // z and r values of the next 32 steps (descending)
-      const int qq = q - lane;
-      zpre = (qq >= 0) ? Z[ref(qq)] : 0.0;
-      rpre2 = (qq >= 0) ? R[ref(qq)] : 0.0;
-    }
-    dc_col_async(ring + ((s_ + DC_RING - 1) % DC_RING) * W, F, q - (DC_RING - 1), N, W, lane);
-    wait_ring();
-    const TF* col = ring + (s_ % DC_RING) * W;
-    TF sum = TF(0);
+  for (int qs = nq - 32; qs >= 0; qs -= 32) {
+    const double zn = rld(Z, qs - 32 + lane), rnx = rld(Rv, qs - 32 + lane);
+    TF xv = TF(0);
 #pragma unroll
-    for (int u = 0; u < MAXI; ++u) {
-      const int i = lane + 1 + 32 * u;
-      if (i <= b && q + i < N) { int pi = q % W + i; if (pi >= W) pi -= W; sum += col[i] * win[pi]; }
+    for (int j = 31; j >= 0; --j) {
+      if ((j & (DC_CH - 1)) == DC_CH - 1) chunk_wait((qs + j) / DC_CH - (DC_NST - 1));
+      const TF* col = column(qs + j);
+      if (j + DC_NEAR < 32) { if (lane == j + DC_NEAR) w[0] = nx[DC_NEAR - 1]; }
+      else if (lane == j + DC_NEAR - 32) w[1] = nx[DC_NEAR - 1];
+      TF part = TF(0);
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        const int i = (32 * u + lane - j + WIN) & (WIN - 1);
+        if (i >= DC_NEAR && i <= b) part += col[i] * w[u];
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      TF x = TF(__shfl_sync(0xffffffffu, zc, j)) - part;
+#pragma unroll
+      for (int k = DC_NEAR - 2; k >= 0; --k) x -= col[k + 1] * nx[k];
+#pragma unroll
+      for (int k = DC_NEAR - 1; k > 0; --k) nx[k] = nx[k - 1];
+      nx[0] = x;
+      if (lane == j) xv = x;
     }
-    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    const double zq = __shfl_sync(0xffffffffu, zpre, k);
-    const double rq = __shfl_sync(0xffffffffu, rpre2, k);
-    if (lane == 0) {
-      const TF x = TF(zq) - sum;
-      win[q % W] = x;
-      Z[ref(q)] = double(x);
-      acc += rq * double(x);
+    if (qs + lane < N) {
+      Z[ref(qs + lane)] = double(xv);
+      acc += rc * double(xv);
     }
-    __syncwarp();
+    const TF wl = w[R - 1];
+#pragma unroll
+    for (int u = R - 1; u > 0; --u) w[u] = w[u - 1];
+    w[0] = wl;
+    zc = zn;
+    rc = rnx;
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (lane == 0) rz[sys] = acc;
 }
 

@@ -77,7 +77,7 @@ struct DcPlan {
   DcGrid G{};
   int nky = 0, nsrc = 0, robin = 0;
   DevBuf sig, faces, ky2, wts, alpha, ab, cur, mnoff, mnbuf, fac, vec, dots, done, status, gbuf, dbuf, ebuf, ubuf;
-  DevBuf jk;  // packed (j << 16 | k) elements of the factor's rank-1 update
+  DevBuf tiles;  // the factor's trailing-update tiles, (ct << 16) | rt, column-major
   std::vector<long> off;
 };
 
@@ -104,16 +104,20 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   const double* k2 = P.ky2.as<double>();
   const TF* F = P.fac.as<TF>();
   const dim3 gv((N + 255) / 256 < 64 ? (N + 255) / 256 : 64, nsys);
-  const int warps_per_block = 4;
-  const size_t shp = dc_precond_smem<TF>(G.b, warps_per_block);
-  const int pblocks = (nsys + warps_per_block - 1) / warps_per_block;
+  const size_t shp = dc_precond_smem<TF>(G.wp);
+  auto precond = [&](double* rzv) {  // one warp per system; window of 32R >= b + 1 positions
+    const bool tm = c.timer.begin(KK_DC_PRECOND, st, nsys);
+    if (G.b < 128) k_dc_precond<TF, 4><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
+    else k_dc_precond<TF, 8><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
+    c.timer.end(tm, st);
+  };
   GJ_CUDA(err, cudaMemsetAsync(X, 0, vn * sizeof(double), st));
   GJ_CUDA(err, cudaMemcpyAsync(R, B, vn * sizeof(double), cudaMemcpyDeviceToDevice, st));
   GJ_CUDA(err, cudaMemsetAsync(done, 0, nsys * sizeof(int), st));
   GJ_CUDA(err, cudaMemsetAsync(bb, 0, nsys * sizeof(double), st));
   GJ_CUDA(err, cudaMemsetAsync(rr, 0, nsys * sizeof(double), st));
   k_dc_residual<<<gv, 256, 0, st>>>(N, B, X, R, rr, bb, nsys);  // r = b (x = 0)
-  k_dc_precond<TF><<<pblocks, 32 * warps_per_block, shp, st>>>(G, F, R, Z, rzA, nsys, done);
+  precond(rzA);
   k_dc_cg_p<<<gv, 256, 0, st>>>(N, rzA, rzA, nullptr, Z, Pv, 1, nsys, done);
   c.launches += 3;
   std::vector<double> hbb(nsys), hrr(nsys);
@@ -124,12 +128,10 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
     GJ_CUDA(err, cudaMemsetAsync(pap, 0, nsys * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(rr, 0, nsys * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(rzo, 0, nsys * sizeof(double), st));
-    const bool tm = c.timer.begin(KK_DC, st, nsys);
     k_dc_apply<<<gv, 256, 0, st>>>(G, ox, oz, db, sg, al, k2, sys0, Pv, AP, pap, nsys, done);
     k_dc_cg_xr<<<gv, 256, 0, st>>>(N, rzA, pap, X, R, Pv, AP, Z, rr, rzo, nsys, done);
-    k_dc_precond<TF><<<pblocks, 32 * warps_per_block, shp, st>>>(G, F, R, Z, rzB, nsys, done);
+    precond(rzB);
     k_dc_cg_p<<<gv, 256, 0, st>>>(N, rzB, rzA, rzo, Z, Pv, 0, nsys, done);
-    c.timer.end(tm, st);
     c.launches += 4;
     std::swap(rzA, rzB);
     GJ_CUDA(err, cudaMemcpyAsync(hrr.data(), rr, nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -175,10 +177,16 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   G.DX = gg.dx; G.DZ = gg.dz;
   G.nb = 2 * (gg.m - 2) + (gg.n - 2) + 4;
   {
+    const int per16 = 16 / int(sizeof(TF));  // factor columns start on 16-byte boundaries
+    G.wp = (G.b + 1 + per16 - 1) / per16 * per16;
+    G.nq = (G.N + 31) / 32 * 32;
+  }
+  {
     int dev = 0, maxsm = 0;
     GJ_CUDA(err, cudaGetDevice(&dev));
     GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (G.b > 256 || dc_factor_smem<TF>(G.b) > size_t(maxsm))
+    if (G.b > DC_FACTOR_THREADS - DC_NB - 1 || dc_factor_smem<TF>(G.b) > size_t(maxsm) ||
+        dc_precond_smem<TF>(G.wp) > size_t(maxsm))
       return err.set(GJ_EUNSUPPORTED, "band width min(n, m) = %d: the factor window needs %zu bytes of shared memory "
                                       "(limit %d)", G.b, dc_factor_smem<TF>(G.b), maxsm);
   }
@@ -244,11 +252,11 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   size_t free_b = 0, total_b = 0;
   GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
   const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.7 * double(free_b));
-  const size_t per_sys = size_t(N) * (G.b + 1) * sizeof(TF) + size_t(N) * 8 * sizeof(double) + 64;
+  const size_t per_sys = size_t(G.nq) * G.wp * sizeof(TF) + size_t(N) * 8 * sizeof(double) + 64;
   int srcs_per_batch = int(std::min<size_t>(nsrc, std::max<size_t>(1, budget / (per_sys * nky))));
   if (o.sources_per_batch > 0) srcs_per_batch = std::min(srcs_per_batch, o.sources_per_batch);
   const int nsys_b = srcs_per_batch * nky;
-  GJ_TRY(P.fac.alloc(err, size_t(nsys_b) * N * (G.b + 1) * sizeof(TF)));
+  GJ_TRY(P.fac.alloc(err, size_t(nsys_b) * G.nq * G.wp * sizeof(TF)));
   GJ_TRY(P.vec.alloc(err, size_t(nsys_b) * N * 7 * sizeof(double)));  // B, X, R, Z, P, AP, U
   GJ_TRY(P.dots.alloc(err, 6 * size_t(nsys_b) * sizeof(double)));
   GJ_TRY(P.done.alloc(err, nsys_b * sizeof(int)));
@@ -258,15 +266,15 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   double rel_max = 0;
   const size_t smem_f = dc_factor_smem<TF>(G.b);
   GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
-  GJ_CUDA(err, cudaFuncSetAttribute(k_dc_precond<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(dc_precond_smem<TF>(G.b, 4))));
+  GJ_CUDA(err, cudaFuncSetAttribute(G.b < 128 ? k_dc_precond<TF, 4> : k_dc_precond<TF, 8>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(dc_precond_smem<TF>(G.wp))));
   {
-    std::vector<unsigned> hjk;
-    hjk.reserve(size_t(G.b) * (G.b + 1) / 2);
-    for (int j = 1; j <= G.b; ++j)
-      for (int k = 0; k <= G.b - j; ++k) hjk.push_back((unsigned(j) << 16) | unsigned(k));
-    GJ_TRY(P.jk.alloc(err, hjk.size() * sizeof(unsigned)));
-    GJ_CUDA(err, cudaMemcpy(P.jk.p, hjk.data(), hjk.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+    const int nt = dc_factor_shape(G.b).BP / 4;
+    std::vector<unsigned> ht;
+    for (int ct = 0; ct < nt; ++ct)
+      for (int rt = ct; rt < nt; ++rt) ht.push_back((unsigned(ct) << 16) | unsigned(rt));
+    GJ_TRY(P.tiles.alloc(err, ht.size() * sizeof(unsigned)));
+    GJ_CUDA(err, cudaMemcpy(P.tiles.p, ht.data(), ht.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
   }
   double* V = P.vec.as<double>();
   for (int s0 = 0; s0 < nsrc; s0 += srcs_per_batch) {
@@ -278,10 +286,11 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     double* U = X + 5 * vn;
     // factor
     {
-      const bool tm = c.timer.begin(KK_DC, st, nsys);
-      k_dc_factor<TF><<<nsys, 256, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(), P.alpha.as<double>(),
-                                                 P.ky2.as<double>(), P.jk.as<unsigned>(), sys0, P.fac.as<TF>(),
-                                                 P.status.as<int>());
+      const bool tm = c.timer.begin(KK_DC_FACTOR, st, nsys);
+      k_dc_factor<TF><<<nsys, DC_FACTOR_THREADS, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(),
+                                                               P.alpha.as<double>(), P.ky2.as<double>(),
+                                                               P.tiles.as<unsigned>(), sys0, P.fac.as<TF>(),
+                                                               P.status.as<int>());
       c.timer.end(tm, st);
       ++c.launches;
     }

@@ -79,8 +79,15 @@ class WSolverBase {
   virtual ~WSolverBase() = default;
 };
 
+// Kernel kinds reported by gj_kernel_time().
+enum KernelKind {
+  KK_FWD_STEP = 0, KK_REF_STEP = 1, KK_ADJ_STEP = 2, KK_IO = 3, KK_PLAIN = 4, KK_DC_FACTOR = 5, KK_IMAGE = 6,
+  KK_DC_PRECOND = 7
+};
+
 // Optional per-kernel device timing: CUDA events around sampled launches of
-// the hot kernels (every `stride`-th launch of each kind), also inside captured
+// the hot kernels (every `stride`-th launch of each kind; every launch of the
+// DC factor and substitution, which run a few times per call), also inside captured
 // CUDA graphs (external event-record nodes).  A Marks list belongs to one
 // launch sequence (a direct enqueue, or one captured graph that is replayed);
 // collect() adds its elapsed times after the stream has been synchronised.
@@ -112,7 +119,8 @@ struct KernelTimer {
     if (!on || !cur) return false;
     cur->launches[kind] += 1;
     cur->shot_launches[kind] += shots;
-    if ((seen[kind]++ % stride) != 0) return false;
+    const int every = (kind == KK_DC_FACTOR || kind == KK_DC_PRECOND) ? 1 : stride;
+    if ((seen[kind]++ % every) != 0) return false;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -143,8 +151,6 @@ struct KernelTimer {
   }
 };
 
-// Kernel kinds reported by gj_kernel_time().
-enum KernelKind { KK_FWD_STEP = 0, KK_REF_STEP = 1, KK_ADJ_STEP = 2, KK_IO = 3, KK_PLAIN = 4, KK_DC = 5, KK_IMAGE = 6 };
 
 struct Ctx {
   int device = 0;

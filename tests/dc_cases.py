@@ -4,7 +4,8 @@ import numpy as np
 from gerjoii_b200 import dc
 
 
-def small_dc(seed=0, n0=30, m0=10, robin=1, dx=0.25, n_el=12, pairs=3, levels=3, n_ky=6, blocks=True):
+def small_dc(seed=0, n0=30, m0=10, robin=1, dx=0.25, n_el=12, pairs=3, levels=3, n_ky=6, blocks=True, spacing=2,
+             first=2):
     X = np.arange(n0) * dx
     Z = np.arange(m0) * dx
     DX, DZ = dc.deltas(X, Z, robin)
@@ -16,7 +17,7 @@ def small_dc(seed=0, n0=30, m0=10, robin=1, dx=0.25, n_el=12, pairs=3, levels=3,
     SIG = dc.dc_robin(sig0, robin)
     n, m = SIG.shape
     kyw = dc.ky_weights(dx, n0 * dx, n_ky, dx=dx)
-    srcs = dc.dipole_dipole(n, m, robin, DX, DZ, n_electrodes=n_el, spacing_nodes=2, first_node=2, pairs=pairs,
+    srcs = dc.dipole_dipole(n, m, robin, DX, DZ, n_electrodes=n_el, spacing_nodes=spacing, first_node=first, pairs=pairs,
                             levels=levels, ky_w=kyw, rng=np.random.default_rng(seed + 1))
     return dict(SIG=SIG, DX=DX, DZ=DZ, robin=robin, srcs=srcs, n=n, m=m)
 

@@ -21,6 +21,24 @@ def test_dc_forward_matches_direct_solve(gpu_ctx):
     assert res["rel_residual"] <= 1e-10
 
 
+@pytest.mark.parametrize("shape", [
+    dict(n0=20, m0=2, n_el=6, spacing=2, first=2, levels=1, pairs=2),   # b = 3, depth fastest
+    dict(n0=4, m0=30, n_el=5, spacing=1, first=0, levels=1, pairs=2),   # b = 6, lateral fastest
+    dict(n0=150, m0=130, n_el=12, spacing=10, first=5, levels=2, pairs=1, n_ky=2),  # b = 131
+], ids=["b3", "b6", "b131"])
+def test_dc_forward_band_widths(gpu_ctx, shape):
+    """Band widths at the edges of the factor and substitution layouts: windows
+    narrower than the factor's panel (b = 3, 6; both unknown orderings) and a
+    band wider than 127, which takes the 256-position substitution window."""
+    import np_dc_oracle as dco
+    case = small_dc(seed=7, **shape)
+    res = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], want_u=True)
+    assert res["rel_residual"] <= 1e-10
+    for k, r in enumerate(oracle_forward(dco, case)):
+        assert rel_l2(res["d"][k], r[2]) < 1e-9
+        assert rel_l2(res["u"][k], r[0].reshape((case["n"], case["m"]), order="F")) < 1e-9
+
+
 def test_dc_gradient_matches_oracle(gpu_ctx):
     import np_dc_oracle as dco
     case = small_dc(seed=4)
