@@ -112,10 +112,14 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
 // block as S[c mod M][r mod Mr] = A(r, c), r = c .. c+b, with Mr = b + 1
 // rounded up to 4 so that four rows starting at a multiple of 4 are contiguous.
 // Per block of pivots q .. q+DC_NB-1:
-//   panel: for each pivot c0 = q+p: d = A(c0, c0), l_i = A(c0+i, c0) / d (written
-//     out); the rows below the panel go to U[p][r'] = l and Ud[p][r'] = l d
-//     (r' = row - q - DC_NB, zero outside the band); then the later panel
-//     columns take the rank-1 update.  Two barriers per pivot.
+//   panel: thread t holds row q+t of the DC_NB panel columns in registers.
+//     Warp 0 holds the pivot rows and runs the DC_NB pivots with shuffles
+//     (d = A(c0, c0), l = A(r, c0) / d, rank-1 update of the later panel
+//     columns), publishing d, 1 / d and the l of the pivot rows; after one
+//     barrier every other row applies the same DC_NB steps from those values.
+//     The l are written out; the rows below the panel also go to U[p][r'] = l
+//     and Ud[p][r'] = l d (r' = row - q - DC_NB, zero outside the band).
+//     Three barriers per block.
 //   trailing: the b x b lower triangle of columns q+DC_NB .. takes the
 //     rank-DC_NB update A(r, c) -= sum_p Ud[p][r'] U[p][c'], one 4 x 4 register
 //     tile per thread and pass (host-built tile list, column-major, so the lanes
@@ -147,7 +151,8 @@ __host__ __device__ inline DcFactorShape dc_factor_shape(int b) {
 template <class TF>
 __host__ __device__ inline size_t dc_factor_smem(int b) {
   const DcFactorShape f = dc_factor_shape(b);
-  return (size_t(f.M) * f.Mr + 2 * size_t(DC_NB) * f.BP + 4 * DC_NB) * sizeof(TF) + size_t(f.ntiles) * sizeof(unsigned);
+  return (size_t(f.M) * f.Mr + 2 * size_t(DC_NB) * f.BP + DC_NB * DC_NB + 5 * DC_NB) * sizeof(TF) +
+         size_t(f.ntiles) * sizeof(unsigned);
 }
 
 __device__ __forceinline__ void dc_ld4(const double* p, double v[4]) {
@@ -179,8 +184,10 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
   TF* S = reinterpret_cast<TF*>(shraw);
   TF* U = S + size_t(M) * Mr;  // [DC_NB][BP]
   TF* Ud = U + DC_NB * BP;     // [DC_NB][BP]
-  TF* lc = Ud + DC_NB * BP;    // l_j of the current pivot, j < DC_NB
-  TF* stg = lc + DC_NB;        // [3][DC_NB]: entering columns' diagonal, A(c+1, c), A(c+b, c)
+  TF* pd = Ud + DC_NB * BP;    // pivots d of the block
+  TF* pdinv = pd + DC_NB;      // 1 / d
+  TF* pl = pdinv + DC_NB;      // [DC_NB][DC_NB]: l of the panel's own rows, pl[p][c] = L(q+c, q+p)
+  TF* stg = pl + DC_NB * DC_NB;  // [3][DC_NB]: entering columns' diagonal, A(c+1, c), A(c+b, c)
   unsigned* tab = reinterpret_cast<unsigned*>(stg + 3 * DC_NB);
   const int sys = blockIdx.x, tid = threadIdx.x, nth = DC_FACTOR_THREADS;
   const double* al = alpha + size_t(sys0 + sys) * G.nb;
@@ -212,53 +219,70 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
     S[e] = column_value(c, k, dg, s1, s2);
   }
   const int Nn = (N + DC_NB - 1) / DC_NB * DC_NB;
-  const int i0 = tid + 1;  // this thread's row below the pivot (b < 256)
-  int sq = 0, rq = 0;      // q mod M, q mod Mr
+  int sq = 0, rq = 0;  // q mod M, q mod Mr
   __syncthreads();
   for (int q = 0; q < Nn; q += DC_NB) {
-    if (tid >= nth - DC_NB) {  // entering columns of this block (these threads have no panel row: b < 248)
+    if (tid >= nth - DC_NB) {  // entering columns of this block
       const int t = tid - (nth - DC_NB);
       TF dg, s1, s2;
       entering(q + M + t, dg, s1, s2);
       stg[t] = dg; stg[DC_NB + t] = s1; stg[2 * DC_NB + t] = s2;
     }
-    // ---- panel
-#pragma unroll 1
-    for (int p = 0; p < DC_NB; ++p) {
-      const int c0 = q + p;
-      int s0 = sq + p, rb0 = rq + p;
-      if (s0 >= M) s0 -= M;
-      while (rb0 >= Mr) rb0 -= Mr;  // Mr < DC_NB only for b < 7
-      const TF d = S[s0 * Mr + rb0];
-      const TF dinv = TF(1) / d;
-      int pos = rb0 + i0;
-      if (pos >= Mr) pos -= Mr;
-      TF ld = TF(0);
-      if (i0 <= b) {
-        const TF l = S[s0 * Mr + pos] * dinv;
-        ld = l * d;
-        if (c0 < N) F[size_t(c0) * wp + i0] = (c0 + i0 < N) ? l : TF(0);
-        if (i0 < DC_NB) lc[i0] = l;
-        if (i0 >= DC_NB - p) { U[p * BP + i0 - DC_NB + p] = l; Ud[p * BP + i0 - DC_NB + p] = ld; }
+    // ---- panel: thread t owns row q+t of the panel columns (t < DC_NB + BP) in registers
+    const bool row = tid < DC_NB + BP;
+    TF a[DC_NB];
+    {
+      const int pos = (rq + tid) % Mr;
+#pragma unroll
+      for (int c = 0; c < DC_NB; ++c) {
+        int sc = sq + c;
+        if (sc >= M) sc -= M;
+        a[c] = (row && tid >= c && tid - c <= b) ? S[sc * Mr + pos] : TF(0);
       }
-      for (int i = (i0 > b ? i0 : i0 + nth); i < BP + DC_NB - p; i += nth) {  // rows past the band
-        const int r = i - DC_NB + p;
-        if (r >= 0) { U[p * BP + r] = TF(0); Ud[p * BP + r] = TF(0); }
+    }
+    if (tid < 32) {  // warp 0 holds the pivot rows (lanes 0 .. DC_NB-1): the pivots by shuffles
+#pragma unroll
+      for (int p = 0; p < DC_NB; ++p) {
+        const TF dp = __shfl_sync(0xffffffffu, a[p], p);
+        const TF dinv = TF(1) / dp;
+        const TF l = tid > p ? a[p] * dinv : TF(0);
+        const TF ld = l * dp;
+        if (tid == 0) { pd[p] = dp; pdinv[p] = dinv; }
+#pragma unroll
+        for (int c = p + 1; c < DC_NB; ++c) {
+          const TF lc_ = __shfl_sync(0xffffffffu, l, c);
+          if (tid == 0) pl[p * DC_NB + c] = lc_;
+          a[c] -= ld * lc_;
+        }
+        a[p] = l;
       }
-      if (tid == 0 && c0 < N) {
-        F[size_t(c0) * wp] = dinv;
-        if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
+    }
+    __syncthreads();  // pivots published
+    if (tid >= 32 && row) {
+#pragma unroll
+      for (int p = 0; p < DC_NB; ++p) {
+        const TF l = a[p] * pdinv[p];
+        const TF ld = l * pd[p];
+#pragma unroll
+        for (int c = p + 1; c < DC_NB; ++c) a[c] -= ld * pl[p * DC_NB + c];
+        a[p] = l;
       }
-      if (p + 1 == DC_NB) break;
-      __syncthreads();
-      if (i0 <= b) {
-        int sj = s0;
-        for (int j = 1; j < DC_NB - p; ++j) {
-          if (++sj >= M) sj -= M;
-          if (i0 >= j) S[sj * Mr + pos] -= ld * lc[j];
+    }
+    if (row) {  // a[p] = l of row q+t for pivot q+p
+#pragma unroll
+      for (int p = 0; p < DC_NB; ++p) {
+        const int c0 = q + p, i = tid - p;
+        if (c0 < N && i >= 1 && i <= b) F[size_t(c0) * wp + i] = (q + tid < N) ? a[p] : TF(0);
+        if (tid >= DC_NB) {
+          U[p * BP + tid - DC_NB] = a[p];
+          Ud[p * BP + tid - DC_NB] = a[p] * pd[p];
         }
       }
-      __syncthreads();
+    }
+    if (tid < DC_NB && q + tid < N) {
+      const TF d = pd[tid];
+      F[size_t(q + tid) * wp] = pdinv[tid];
+      if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
     }
     __syncthreads();
     // ---- trailing rank-DC_NB update
