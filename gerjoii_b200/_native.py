@@ -14,7 +14,7 @@ from . import build as _build
 GJ_OK, GJ_EINVAL, GJ_ENOMEM, GJ_ENUMERIC, GJ_ETIMEOUT, GJ_ECUDA, GJ_EUNSUPPORTED = range(7)
 GJ_F32, GJ_F64 = 0, 1
 GJ_ADJ_REFERENCE, GJ_ADJ_EXACT = 0, 1
-GJ_MISFIT_L2, GJ_MISFIT_ENV_L2 = 0, 1
+GJ_MISFIT_L2, GJ_MISFIT_ENV_L2, GJ_MISFIT_PHASE_L2, GJ_MISFIT_ENV_L22, GJ_MISFIT_ENV_LOG = 0, 1, 2, 3, 4
 
 STATUS_NAMES = {0: "GJ_OK", 1: "GJ_EINVAL", 2: "GJ_ENOMEM", 3: "GJ_ENUMERIC", 4: "GJ_ETIMEOUT",
                 5: "GJ_ECUDA", 6: "GJ_EUNSUPPORTED"}

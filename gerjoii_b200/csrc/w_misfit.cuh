@@ -1,9 +1,16 @@
-// Envelope (env_L2) adjoint source and misfit on the device (w_bozdag.m:51-60,
-// instant_.m:14-20, w_E.m with d and d_o replaced by their envelopes,
-// w_update_e.m:75-76):
-//   E = |analytic(d)|, Eo = |analytic(d_o)|, Hd = imag(analytic(d))
-//   f = (E - Eo) / E,  e = d f - imag(analytic(f Hd)),  e(NaN) = 0
-//   misfit = 0.5 sum (E - Eo)^2 / sum Eo^2.
+// Envelope and phase adjoint sources and misfits on the device (w_bozdag.m:16-54,
+// instant_.m:14-20; w_E.m:7-16 on the envelopes or phases that w_fwd.m:34-35
+// stores in place of d and d_o; normalised as w_update_e.m:75-76):
+//   E = |analytic(d)|, Eo = |analytic(d_o)|, Hd = imag(analytic(d)),
+//   phi, phi_o the angles of the analytic signals, H = imag(analytic(.))
+//   env_L2  : f = (E - Eo) / E,        e = d f - H(f Hd),          e(NaN) = 0,
+//             misfit 0.5 sum (E - Eo)^2 / sum Eo^2
+//   phase_L2: g = (phi - phi_o) / E^2, e = -g + H(g d),
+//             misfit 0.5 sum (phi - phi_o)^2 / sum phi_o^2
+//   env_L22 : f = E^2 - Eo^2,          e = d f - H(f Hd),
+//             misfit 0.5 sum (E^2 - Eo^2)^2 / sum Eo^2
+//   env_LOG : f = log(Eo / E),         e = -f d / E^2 + H(f Hd / E^2), e(NaN) = 0,
+//             misfit 0.5 sum (log E - log Eo)^2 / sum Eo^2
 // The analytic signal follows MATLAB's hilbert: FFT along time, keep DC and
 // Nyquist, double positive frequencies, zero negative ones, inverse FFT.
 #pragma once
@@ -12,6 +19,9 @@
 #include <cufft.h>
 
 namespace gj {
+
+// misfit kinds, as gj_misfit_kind
+constexpr int MK_ENV_L2 = 1, MK_PHASE_L2 = 2, MK_ENV_L22 = 3, MK_ENV_LOG = 4;
 
 template <class T> struct CplxT;
 template <> struct CplxT<float> { using type = cuComplex; };
@@ -47,11 +57,12 @@ __global__ void k_env_mask(C* X, int nt, size_t ntr) {
   }
 }
 
-// From the analytic signals of d (A) and d_o (Ao): f into F, f*Hd into G
-// (complex, for the second Hilbert transform), misfit sums per shot.
+// From the traces d and the analytic signals of d (A) and d_o (Ao): the
+// pointwise factor into F and the operand of the second Hilbert transform into
+// G (complex), misfit sums per shot; `kind` as gj_misfit_kind.
 template <class T, class C>
-__global__ void k_env_mid(const C* A, const C* Ao, T* F, C* G, int nt, int ntr_per_shot, int nshots,
-                          double* sums) {
+__global__ void k_env_mid(const T* d, const C* A, const C* Ao, T* F, C* G, int nt, int ntr_per_shot, int nshots,
+                          int kind, double* sums) {
   const int s = blockIdx.y;
   if (s >= nshots) return;
   const size_t per = size_t(nt) * ntr_per_shot, base = size_t(s) * per;
@@ -60,11 +71,33 @@ __global__ void k_env_mid(const C* A, const C* Ao, T* F, C* G, int nt, int ntr_p
     const C a = A[base + i], ao = Ao[base + i];
     const T E = sqrt(cre(a) * cre(a) + cim(a) * cim(a));
     const T Eo = sqrt(cre(ao) * cre(ao) + cim(ao) * cim(ao));
-    const T f = (E - Eo) / E;  // NaN where E = 0 (zeroed at the end, w_bozdag.m:60)
+    T f, g;
+    double r;
+    if (kind == MK_PHASE_L2) {
+      const T ph = atan2(cim(a), cre(a)), pho = atan2(cim(ao), cre(ao));
+      f = (ph - pho) / (E * E);
+      g = f * d[base + i];
+      r = double(ph - pho);
+      den += double(pho) * double(pho);
+    } else {
+      if (kind == MK_ENV_L22) {
+        f = E * E - Eo * Eo;
+        g = f * cim(a);
+        r = double(f);
+      } else if (kind == MK_ENV_LOG) {
+        f = log(Eo / E) / (E * E);  // NaN / inf where E = 0 (zeroed at the end, w_bozdag.m:54)
+        g = f * cim(a);
+        r = double(log(E)) - double(log(Eo));
+      } else {
+        f = (E - Eo) / E;  // NaN where E = 0 (zeroed at the end, w_bozdag.m:25)
+        g = f * cim(a);
+        r = double(E - Eo);
+      }
+      den += double(Eo) * double(Eo);
+    }
     F[base + i] = f;
-    cset(G[base + i], f * cim(a), T(0));
-    num += double(E - Eo) * double(E - Eo);
-    den += double(Eo) * double(Eo);
+    cset(G[base + i], g, T(0));
+    num += r * r;
   }
   for (int o = 16; o > 0; o >>= 1) {
     num += __shfl_down_sync(0xffffffffu, num, o);
@@ -76,12 +109,21 @@ __global__ void k_env_mid(const C* A, const C* Ao, T* F, C* G, int nt, int ntr_p
   }
 }
 
-// e = d f - imag(analytic(f Hd)), NaN -> 0
+// The adjoint source from F and HG = analytic(G) (formulas above).
 template <class T, class C>
-__global__ void k_env_final(const T* d, const T* F, const C* HG, T* e, size_t n) {
+__global__ void k_env_final(const T* d, const T* F, const C* HG, T* e, size_t n, int kind) {
   for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < n; i += size_t(blockDim.x) * gridDim.x) {
-    const T v = d[i] * F[i] - cim(HG[i]);
-    e[i] = isnan(v) ? T(0) : v;
+    if (kind == MK_PHASE_L2) {
+      e[i] = -F[i] + cim(HG[i]);
+    } else if (kind == MK_ENV_L22) {
+      e[i] = d[i] * F[i] - cim(HG[i]);
+    } else if (kind == MK_ENV_LOG) {
+      const T v = -F[i] * d[i] + cim(HG[i]);
+      e[i] = isnan(v) ? T(0) : v;
+    } else {
+      const T v = d[i] * F[i] - cim(HG[i]);
+      e[i] = isnan(v) ? T(0) : v;
+    }
   }
 }
 

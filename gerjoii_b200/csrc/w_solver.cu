@@ -59,7 +59,7 @@ __global__ void k_cezj(const CoefBuild c, const TM* eps, const TM* sig, const in
 }
 
 // Residual e = d - d_obs and the two sums of the normalised L2 misfit
-// (w_bozdag.m:49, w_E.m:15-16, w_update_e.m:75-76).
+// (w_bozdag.m:14, w_E.m:15-16, w_update_e.m:75-76).
 template <class T>
 __global__ void k_residual(const T* d, const T* dobs, T* e, size_t per_shot, double* sums) {
   const int s = blockIdx.y;
@@ -681,8 +681,8 @@ class WSolver : public WSolverBase {
       c.launches += 1 + last_kernels;
       std::swap(A, B);
     }
-    if (mk == GJ_MISFIT_ENV_L2) {
-      GJ_TRY(env_residual(err, c, 0, nshots, st));
+    if (mk != GJ_MISFIT_L2) {
+      GJ_TRY(env_residual(err, c, 0, nshots, mk, st));
     } else {
       k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr,
                                                       sums.as<double>());
@@ -861,8 +861,8 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
-  // env_L2 residual and misfit sums for shots [g0, g0+gn) (w_bozdag.m:51-60).
-  gj_status env_residual(Err& err, Ctx& c, int g0, int gn, cudaStream_t st) {
+  // Envelope / phase residual and misfit sums for shots [g0, g0+gn) (w_bozdag.m:16-54).
+  gj_status env_residual(Err& err, Ctx& c, int g0, int gn, gj_misfit_kind mk, cudaStream_t st) {
     using C = typename CplxT<T>::type;
     const int nrr = std::max(nr, 1), nt = g.nt;
     const size_t tr = size_t(nrr) * nt, n = size_t(gn) * tr;
@@ -885,10 +885,11 @@ class WSolver : public WSolverBase {
     k_env_to_complex<T, C><<<512, 256, 0, st>>>(dob, envAo.as<C>(), n);
     GJ_TRY(analytic(err, envA.as<C>(), st));
     GJ_TRY(analytic(err, envAo.as<C>(), st));
-    k_env_mid<T, C><<<dim3(64, gn), 256, 0, st>>>(envA.as<C>(), envAo.as<C>(), envF.as<T>(), envG.as<C>(), nt, nrr,
-                                                 gn, sums.as<double>() + 2 * g0);
+    k_env_mid<T, C><<<dim3(64, gn), 256, 0, st>>>(d, envA.as<C>(), envAo.as<C>(), envF.as<T>(), envG.as<C>(), nt,
+                                                 nrr, gn, int(mk), sums.as<double>() + 2 * g0);
     GJ_TRY(analytic(err, envG.as<C>(), st));
-    k_env_final<T, C><<<512, 256, 0, st>>>(d, envF.as<T>(), envG.as<C>(), ebuf.as<T>() + size_t(g0) * tr, n);
+    k_env_final<T, C><<<512, 256, 0, st>>>(d, envF.as<T>(), envG.as<C>(), ebuf.as<T>() + size_t(g0) * tr, n,
+                                           int(mk));
     c.launches += 10;
     GJ_CUDA(err, cudaGetLastError());
     return GJ_OK;
@@ -1197,7 +1198,7 @@ class WSolver : public WSolverBase {
       if (o.filt_high > o.filt_low) return err.set(GJ_EUNSUPPORTED, "the plain form has no residual filter");
       return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
     }
-    const bool env = (mk == GJ_MISFIT_ENV_L2);
+    const bool env = (mk != GJ_MISFIT_L2);
     const bool filt = o.filt_high > o.filt_low;
     ring_on = ring_nth > 0 && !o.no_ring;
     // memory plan for one group
@@ -1255,7 +1256,7 @@ class WSolver : public WSolverBase {
         Marks m;
         c.timer.cur = &m;
         gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 1, !env);
-        if (rs == GJ_OK && env) rs = env_residual(err, c, g0, gn, st);
+        if (rs == GJ_OK && env) rs = env_residual(err, c, g0, gn, mk, st);
         if (rs == GJ_OK && filt) rs = filt_residual(err, c, o, g0, gn, st);
         if (rs == GJ_OK) rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 2, false);
         c.timer.cur = nullptr;
@@ -1531,7 +1532,7 @@ gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* 
                      bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
   if (!eps || !sig || !dobs || !geps || !gsig) return c.err.set(GJ_EINVAL, "null input or output pointer");
   if (mode != GJ_ADJ_REFERENCE && mode != GJ_ADJ_EXACT) return c.err.set(GJ_EINVAL, "unknown adjoint mode");
-  if (mk != GJ_MISFIT_L2 && mk != GJ_MISFIT_ENV_L2) return c.err.set(GJ_EINVAL, "unknown misfit kind");
+  if (mk < GJ_MISFIT_L2 || mk > GJ_MISFIT_ENV_LOG) return c.err.set(GJ_EINVAL, "unknown misfit kind");
   if (prec == GJ_F64) {
     WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
     return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, mk, o, geps, gsig, dev_out, misfit_out,
@@ -1545,7 +1546,7 @@ gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* 
 gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
                    const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out) {
   if (!eps || !sig || !dobs || !misfit_out) return c.err.set(GJ_EINVAL, "null input or output pointer");
-  if (mk != GJ_MISFIT_L2 && mk != GJ_MISFIT_ENV_L2) return c.err.set(GJ_EINVAL, "unknown misfit kind");
+  if (mk < GJ_MISFIT_L2 || mk > GJ_MISFIT_ENV_LOG) return c.err.set(GJ_EINVAL, "unknown misfit kind");
   if (prec == GJ_F64) {
     WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
     return s->misfit(c.err, c, eps, sig, dobs, mk, misfit_out, 0);

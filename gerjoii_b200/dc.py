@@ -144,3 +144,18 @@ def dipole_dipole(n: int, m: int, robin: int, DX: float, DZ: float, n_electrodes
         al = np.stack([alphas_compact(n, m, DX, DZ, la, lb, ky) for ky in ky_w[:, 0]])
         srcs.append(DcSource(la, lb, current, np.asarray(mn, np.int64), ky_w, al))
     return srcs
+
+
+def geometric_factor(ctx, shape: tuple[int, int], DX: float, DZ: float, robin: int, srcs, opts=None) -> list:
+    """Geometric factors of a survey (dc_geomefactor2_5d.m:44-49): the data of a
+    forward run on the Robin-padded grid with sigma = 1 everywhere, inverted,
+    k = 1 / d.  `ctx` is a Context (its dc_forward runs the GPU solver);
+    returns one array of nd factors per source."""
+    fw = ctx.dc_forward(np.ones(shape), DX, DZ, robin, srcs, opts=opts)
+    return [1.0 / np.asarray(d, np.float64) for d in fw["d"]]
+
+
+def apparent_resistivity(d: list, k: list) -> list:
+    """rho_a = k * d per datum (dc_geomefactor2_5d.m:36-43): the resistivity of
+    the homogeneous half-space that would produce the measured data."""
+    return [np.asarray(x, np.float64) * np.asarray(kk, np.float64) for x, kk in zip(d, k)]

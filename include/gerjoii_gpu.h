@@ -47,8 +47,13 @@ typedef enum gj_precision { GJ_F32 = 0, GJ_F64 = 1 } gj_precision;
  * gradient of 0.5*sum (d - d_obs)^2 with respect to eps_r and sigma. */
 typedef enum gj_adj_mode { GJ_ADJ_REFERENCE = 0, GJ_ADJ_EXACT = 1 } gj_adj_mode;
 
-/* Objective / adjoint source (w_bozdag.m:48-60). */
-typedef enum gj_misfit_kind { GJ_MISFIT_L2 = 0, GJ_MISFIT_ENV_L2 = 1 } gj_misfit_kind;
+/* Objective / adjoint source, the reference's obj_FNC (w_bozdag.m:13-54; misfits
+ * by w_E.m:7-16 on what w_fwd.m:34-35 stores): L2 on the traces, env_L2 on the
+ * envelopes, phase_L2 on the instantaneous phases, env_L22 on the squared
+ * envelopes, env_LOG on the log envelopes. */
+typedef enum gj_misfit_kind {
+  GJ_MISFIT_L2 = 0, GJ_MISFIT_ENV_L2 = 1, GJ_MISFIT_PHASE_L2 = 2, GJ_MISFIT_ENV_L22 = 3, GJ_MISFIT_ENV_LOG = 4
+} gj_misfit_kind;
 
 typedef struct gj_ctx gj_ctx;
 
@@ -139,7 +144,8 @@ gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precisi
 /* Forward runs and misfits only (no history, no adjoint): replaces the
  * objective evaluations of the step-length search, w_objs_e.m:24-65 as called
  * by w_stepparabola_e.m:20-41 for each trial model.  misfit_out: nshots
- * misfits normalised as in w_update_e.m:75-76 (L2) or of the envelopes (env_L2). */
+ * misfits normalised as in w_update_e.m:75-76, of the quantity the misfit kind
+ * compares (traces, envelopes, phases). */
 gj_status gj_w_misfit(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision,
                       const double* eps_r, const double* sigma, const gj_w_shot* shots,
                       int nshots, const double* d_obs, gj_misfit_kind misfit, double* misfit_out);

@@ -308,25 +308,59 @@ def instant_(u):
 
 
 def w_bozdag(d_o, d, obj_fnc="L2"):
-    """w_bozdag.m:48-60 (L2 and env_L2 branches). Returns (e, d_e, d_oe)."""
+    """w_bozdag.m:13-54: adjoint source for each objective (L2, env_L2,
+    phase_L2, env_L22, env_LOG). Returns (e, d_e, d_oe), the quantities whose
+    misfit w_E measures (w_fwd.m:34-35 stores d_e and d_oe in place of d and
+    d_o).  With hilbert's imaginary part H (an antisymmetric circulant):
+    env_L2 and env_LOG are the gradients of their misfits with respect to d,
+    env_L22 is half of it; phase_L2 is -g + H(g d), g = (phi - phi_o) / E^2, as
+    the reference writes it (w_bozdag.m:32-34)."""
     if obj_fnc == "L2":
         return d - d_o, d, d_o
-    if obj_fnc == "env_L2":
-        d_e, _, d_H = instant_(d)
-        d_oe, _, _ = instant_(d_o)
-        with np.errstate(divide="ignore", invalid="ignore"):
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if obj_fnc == "env_L2":
+            d_e, _, d_H = instant_(d)
+            d_oe, _, _ = instant_(d_o)
             dedoe = (d_e - d_oe) / d_e
-            e__ = np.imag(hilbert(dedoe * d_H, axis=0))
-            e_ = d * dedoe - e__
-        e_[np.isnan(e_)] = 0
-        return e_, d_e, d_oe
+            e_ = d * dedoe - np.imag(hilbert(dedoe * d_H, axis=0))
+            e_[np.isnan(e_)] = 0
+            return e_, d_e, d_oe
+        if obj_fnc == "phase_L2":
+            d_e, d_p, _ = instant_(d)
+            _, d_op, _ = instant_(d_o)
+            g = (d_p - d_op) / d_e ** 2
+            e_ = -g + np.imag(hilbert(g * d, axis=0))
+            return e_, d_p, d_op
+        if obj_fnc == "env_L22":
+            d_e, _, d_H = instant_(d)
+            d_oe, _, _ = instant_(d_o)
+            dedoe = d_e ** 2 - d_oe ** 2
+            e_ = d * dedoe - np.imag(hilbert(dedoe * d_H, axis=0))
+            return e_, d_e, d_oe
+        if obj_fnc == "env_LOG":
+            d_e, _, d_H = instant_(d)
+            d_oe, _, _ = instant_(d_o)
+            dedoe = np.real(np.log((d_oe / d_e).astype(np.complex128)))
+            e_ = -dedoe * (d / d_e ** 2) + np.imag(hilbert(dedoe * (d_H / d_e ** 2), axis=0))
+            e_[np.isnan(e_)] = 0
+            return e_, d_e, d_oe
     raise ValueError(obj_fnc)
 
 
-def w_E(d_o, d):
-    """w_E.m:7-16 with N = identity, normalised as w_update_e.m:75-76."""
-    e = (np.asarray(d, np.float64) - np.asarray(d_o, np.float64)).ravel()
+def w_E(d_o, d, obj_fnc="L2"):
+    """w_E.m:7-16 with N = identity (env_L22 squares, env_LOG takes logs of
+    both arguments), normalised by d_o.d_o as w_update_e.m:75-76; after
+    w_fwd.m:34-35 the arguments are w_bozdag's d_oe and d_e."""
+    d = np.asarray(d, np.float64).ravel()
     do = np.asarray(d_o, np.float64).ravel()
+    if obj_fnc == "env_L22":
+        a, b = d ** 2, do ** 2
+    elif obj_fnc == "env_LOG":
+        with np.errstate(divide="ignore"):
+            a, b = np.log(d), np.log(do)
+    else:
+        a, b = d, do
+    e = a - b
     return 0.5 * float(e @ e) / float(do @ do)
 
 

@@ -129,3 +129,19 @@ def test_dc_fp32_factor_option(gpu_ctx):
     assert b["iters"] <= a["iters"]
     for x, y in zip(a["d"], b["d"]):
         assert rel_l2(x, y) < 1e-9
+
+
+def test_geometric_factor_matches_oracle(gpu_ctx):
+    """dc_geomefactor2_5d.m through the GPU solver: k = 1 / d(sigma = 1)
+    against the oracle's direct solve, and the apparent resistivity k * d of a
+    homogeneous half-space equal to 1 / sigma."""
+    import np_dc_oracle as dco
+    from gerjoii_b200 import dc as dcm
+    case = small_dc(seed=9)
+    shape = case["SIG"].shape
+    k = dcm.geometric_factor(gpu_ctx, shape, case["DX"], case["DZ"], case["robin"], case["srcs"])
+    for kk, r in zip(k, oracle_forward(dco, case, np.ones(shape))):
+        assert rel_l2(kk, 1.0 / r[2]) < 1e-9
+    d = gpu_ctx.dc_forward(np.full(shape, 0.02), case["DX"], case["DZ"], case["robin"], case["srcs"])["d"]
+    for rho in dcm.apparent_resistivity(d, k):
+        assert np.allclose(rho, 50.0, rtol=1e-8)

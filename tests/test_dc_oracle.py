@@ -48,3 +48,31 @@ def test_reference_gradient_matches_finite_differences():
         Sm[l, h] -= hh
         fd = (J(Sp) - J(Sm)) / (2 * hh)
         assert abs(g[l - robin, h] - fd) <= 1e-5 * abs(fd), (l, h, g[l - robin, h], fd)
+
+
+class _OracleSolver:
+    """Stands in for a Context on CPU: dc_forward by the oracle's direct solves."""
+
+    def __init__(self, case):
+        self.case = case
+
+    def dc_forward(self, SIG, DX, DZ, robin, srcs, opts=None):
+        import np_dc_oracle as dco
+        from dc_cases import oracle_forward
+        return {"d": [r[2] for r in oracle_forward(dco, self.case, SIG)]}
+
+
+def test_geometric_factor_and_apparent_resistivity_of_a_half_space():
+    """dc_geomefactor2_5d.m: k = 1 / d(sigma = 1); over a homogeneous half-space
+    Lk scales with sigma (the Robin terms do not depend on it), so the apparent
+    resistivity k * d is exactly 1 / sigma."""
+    from dc_cases import small_dc
+    from gerjoii_b200 import dc as dcm
+    case = small_dc(seed=9)
+    solver = _OracleSolver(case)
+    shape = case["SIG"].shape
+    k = dcm.geometric_factor(solver, shape, case["DX"], case["DZ"], case["robin"], case["srcs"])
+    sigma0 = 0.02
+    d = solver.dc_forward(np.full(shape, sigma0), case["DX"], case["DZ"], case["robin"], case["srcs"])["d"]
+    for rho in dcm.apparent_resistivity(d, k):
+        assert np.allclose(rho, 1.0 / sigma0, rtol=1e-10)

@@ -107,3 +107,48 @@ def test_reference_adjoint_differs_from_exact_in_lossy_media(oracle):
     gr, _ = oracle.grad_reference(g, p.eps0, p.sig0, sh, e, u)
     c = float(np.sum(gr * gs) / (np.linalg.norm(gr) * np.linalg.norm(gs)))
     assert np.isfinite(c)
+
+
+def _smooth_traces(seed=3, nt=64, nr=3):
+    rng = np.random.default_rng(seed)
+    t = np.arange(nt)[:, None]
+    d = (np.sin(0.3 * t + rng.random(nr)) * np.exp(-((t - 30) / 15.0) ** 2)
+         + 0.3 * np.cos(0.11 * t + rng.random(nr)))
+    do = 0.9 * d + 0.05 * np.sin(0.2 * t)
+    return d, do
+
+
+@pytest.mark.parametrize("kind,scale", [("env_L2", 1.0), ("env_L22", 2.0), ("env_LOG", 1.0)])
+def test_envelope_adjoint_sources_are_misfit_gradients(kind, scale):
+    """w_bozdag.m's envelope adjoint sources are the derivatives of their
+    unnormalised misfits 0.5 sum (f(E) - f(Eo))^2 (f = identity, square, log;
+    w_E.m:8-16) with respect to the traces; env_L22's is half of it.  Central
+    differences on smooth traces pin the restatement without MATLAB."""
+    import np_oracle as npo
+    d, do = _smooth_traces()
+    f = {"env_L2": lambda v: v, "env_L22": lambda v: v ** 2, "env_LOG": np.log}[kind]
+
+    def J(x):
+        _, de, doe = npo.w_bozdag(do, x, kind)
+        r = f(de) - f(doe)
+        return 0.5 * float(np.sum(r * r))
+
+    e, _, _ = npo.w_bozdag(do, d, kind)
+    h = 1e-6
+    for (i, j) in [(5, 0), (30, 1), (47, 2), (63, 0)]:
+        dp, dm = d.copy(), d.copy()
+        dp[i, j] += h
+        dm[i, j] -= h
+        fd = (J(dp) - J(dm)) / (2 * h)
+        assert abs(scale * e[i, j] - fd) <= 1e-6 * max(abs(fd), np.abs(scale * e).max())
+
+
+@pytest.mark.parametrize("kind", ["L2", "env_L2", "phase_L2", "env_L22", "env_LOG"])
+def test_adjoint_sources_vanish_at_the_data(kind):
+    """Every objective's adjoint source and misfit are zero when the modelled
+    traces equal the observed ones (w_bozdag.m:13-54, w_E.m)."""
+    import np_oracle as npo
+    d, _ = _smooth_traces(seed=5)
+    e, de, doe = npo.w_bozdag(d, d, kind)
+    assert np.abs(e).max() <= 1e-12 * np.abs(d).max()
+    assert npo.w_E(doe, de, kind) == 0.0
