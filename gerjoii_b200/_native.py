@@ -15,6 +15,18 @@ GJ_OK, GJ_EINVAL, GJ_ENOMEM, GJ_ENUMERIC, GJ_ETIMEOUT, GJ_ECUDA, GJ_EUNSUPPORTED
 GJ_F32, GJ_F64 = 0, 1
 GJ_ADJ_REFERENCE, GJ_ADJ_EXACT = 0, 1
 GJ_MISFIT_L2, GJ_MISFIT_ENV_L2, GJ_MISFIT_PHASE_L2, GJ_MISFIT_ENV_L22, GJ_MISFIT_ENV_LOG = 0, 1, 2, 3, 4
+# the reference's obj_FNC names (w_bozdag.m:13-54); FREQstp is L2 there
+MISFIT_KINDS = {"L2": GJ_MISFIT_L2, "FREQstp": GJ_MISFIT_L2, "env_L2": GJ_MISFIT_ENV_L2,
+                "phase_L2": GJ_MISFIT_PHASE_L2, "env_L22": GJ_MISFIT_ENV_L22, "env_LOG": GJ_MISFIT_ENV_LOG}
+
+
+def misfit_kind(misfit) -> int:
+    """A gj_misfit_kind from its value or the reference's obj_FNC name."""
+    if isinstance(misfit, str):
+        if misfit not in MISFIT_KINDS:
+            raise ValueError(f"unknown obj_FNC {misfit!r}; one of {sorted(MISFIT_KINDS)}")
+        return MISFIT_KINDS[misfit]
+    return int(misfit)
 
 STATUS_NAMES = {0: "GJ_OK", 1: "GJ_EINVAL", 2: "GJ_ENOMEM", 3: "GJ_ENUMERIC", 4: "GJ_ETIMEOUT",
                 5: "GJ_ECUDA", 6: "GJ_EUNSUPPORTED"}
@@ -239,7 +251,7 @@ class Context:
         gc = grid_c(g)
         e, s = _f(eps), _f(sig)
         self._check(self.lib.gj_w_gradient(self.h, C.byref(gc), precision, _dp(e), _dp(s), sp.arr, sp.n,
-                                           _dp(dobs), int(mode), int(misfit), C.byref(o), _dp(ge), _dp(gs),
+                                           _dp(dobs), int(mode), misfit_kind(misfit), C.byref(o), _dp(ge), _dp(gs),
                                            _dp(mis), _dp(dd), _dp(ee)))
         shape = (g.m, g.n) if per == 1 else (per, g.m, g.n)
         res = {"g_eps": ge.reshape(shape, order="F") if per == 1 else
@@ -338,7 +350,7 @@ class Context:
         out = np.zeros(len(shots))
         e, s_ = _f(eps), _f(sig)
         self._check(self.lib.gj_w_misfit(self.h, C.byref(gc), precision, _dp(e), _dp(s_), sp.arr, sp.n, _dp(ob),
-                                          int(misfit), _dp(out)))
+                                          misfit_kind(misfit), _dp(out)))
         return out
 
     def w_gradient_dev(self, g, eps_t, sig_t, shots, dobs_t, ge_t, gs_t, mode=GJ_ADJ_REFERENCE,
@@ -351,7 +363,7 @@ class Context:
         mis = np.zeros(len(shots), np.float64)
         gc = grid_c(g)
         self._check(self.lib.gj_w_gradient_dev(self.h, C.byref(gc), prec, eps_t.data_ptr(), sig_t.data_ptr(),
-                                               sp.arr, sp.n, dobs_t.data_ptr(), int(mode), int(misfit),
+                                               sp.arr, sp.n, dobs_t.data_ptr(), int(mode), misfit_kind(misfit),
                                                C.byref(o), ge_t.data_ptr(), gs_t.data_ptr(), _dp(mis),
                                                C.c_void_p(stream)))
         return mis

@@ -55,6 +55,19 @@ static gj_w_grid wgrid(const mxArray* s) {
 }
 
 /* shot from s_w = [i j] (1-based), M (1-based linear Ez indices), wavelet */
+/* gerjoii_.w.obj_FNC (w_fwd.m:33) -> misfit kind; FREQstp is L2 (w_bozdag.m:13). */
+static gj_misfit_kind misfit_kind(const mxArray* a) {
+  char s[16];
+  if (mxGetString(a, s, sizeof s)) mexErrMsgIdAndTxt("gerjoii:arg", "obj_FNC must be a short string");
+  if (!strcmp(s, "L2") || !strcmp(s, "FREQstp")) return GJ_MISFIT_L2;
+  if (!strcmp(s, "env_L2")) return GJ_MISFIT_ENV_L2;
+  if (!strcmp(s, "phase_L2")) return GJ_MISFIT_PHASE_L2;
+  if (!strcmp(s, "env_L22")) return GJ_MISFIT_ENV_L22;
+  if (!strcmp(s, "env_LOG")) return GJ_MISFIT_ENV_LOG;
+  mexErrMsgIdAndTxt("gerjoii:arg", "unknown obj_FNC '%s'", s);
+  return GJ_MISFIT_L2;
+}
+
 static gj_w_shot wshot(const mxArray* s_w, const mxArray* M, const mxArray* wav, long** rec_out) {
   gj_w_shot q;
   const double* s = mxGetPr(s_w);
@@ -100,8 +113,9 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
                     mxGetPr(plhs[0]), am));
     mxFree(rec);
   } else if (!strcmp(cmd, "w_gradient")) {
-    /* [g_eps, g_sig, E] = gj_mex('w_gradient', eps, sigma, grid, S (ns x 2), Mcell, wavelet, dobs_cell, mode)
-       (w_update_es.m's w_fwd + w_grad pair for every shot at once) */
+    /* [g_eps, g_sig, E] = gj_mex('w_gradient', eps, sigma, grid, S (ns x 2), Mcell, wavelet, dobs_cell, mode,
+                                  obj_FNC)
+       (w_update_es.m's w_fwd + w_grad pair for every shot at once; obj_FNC 'L2' by default) */
     gj_w_grid g = wgrid(prhs[3]);
     const mxArray* S = prhs[4];
     const int ns = (int)mxGetM(S);
@@ -122,10 +136,11 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       o += (size_t)g.nt * shots[k].nr;
     }
     const gj_adj_mode mode = nrhs > 8 ? (gj_adj_mode)(int)mxGetScalar(prhs[8]) : GJ_ADJ_REFERENCE;
+    const gj_misfit_kind mk = nrhs > 9 ? misfit_kind(prhs[9]) : GJ_MISFIT_L2;
     plhs[0] = mxCreateDoubleMatrix(g.m, g.n, mxREAL);
     plhs[1] = mxCreateDoubleMatrix(g.m, g.n, mxREAL);
     plhs[2] = mxCreateDoubleMatrix(ns, 1, mxREAL);
-    check(gj_w_gradient(ctx(), &g, prec, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, dobs, mode, GJ_MISFIT_L2,
+    check(gj_w_gradient(ctx(), &g, prec, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, dobs, mode, mk,
                         NULL, mxGetPr(plhs[0]), mxGetPr(plhs[1]), mxGetPr(plhs[2]), NULL, NULL));
     for (int k = 0; k < ns; ++k) mxFree(recs[k]);
     mxFree(recs); mxFree(shots); mxFree(dobs);

@@ -1,0 +1,70 @@
+"""The reference's MAT-file formats (CPU): round trips of line<is>.mat,
+s_r(_).mat, s_i_r_d_std.mat and ky_w.mat through scipy.io in the reference's
+layouts, the shot indices of w_load.m, and a clear error for v7.3 files."""
+import numpy as np
+import pytest
+
+from gerjoii_b200 import matio, synth
+
+
+def test_radargram_round_trip(tmp_path):
+    rng = np.random.default_rng(1)
+    nt, nr = 50, 4
+    d = rng.standard_normal((nt, nr))
+    r = np.column_stack([0.5 + 0.25 * np.arange(nr), np.zeros(nr)])
+    s = np.array([0.1, 0.0])
+    p = str(tmp_path / "line1.mat")
+    matio.save_radargram(p, d, np.arange(nt) * 1e-10, 1e-10, 2.5e8, 0.02, r, s, np.sin(np.arange(nt)))
+    rg = matio.load_radargram(p)
+    assert np.array_equal(rg["d"], d)
+    assert rg["dt"] == 1e-10 and rg["fo"] == 2.5e8
+    assert rg["dr"] == 0.25 and rg["dsr"] == pytest.approx(0.4)  # w_natur_.m:56-57
+    assert rg["std_"].shape == (nt * nr, 1) and np.all(rg["std_"] == 1)
+
+
+def test_s_r_indices_map_to_the_shots_of_w_load(tmp_path):
+    """w_load.m:31-35: source [iz ix] -> Ez(pis + air + iz, pjs + ix) (1-based),
+    receivers [ix iz] -> (pis + air + iz, pjs + ix) through w_M."""
+    p = synth.small(m=20, n=30, pml=6, nt=40, free_top=True, seed=3)
+    g = p.grid
+    pairs = [(np.array([1, 5]), np.array([[3, 1], [7, 1], [11, 2]])),
+             (np.array([2, 9]), np.array([[4, 0], [8, 0]]))]
+    path = str(tmp_path / "s_r_.mat")
+    matio.save_s_r(path, pairs, indexed=True)
+    back = matio.load_s_r(path)
+    assert all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(pairs, back))
+    wv = np.random.default_rng(2).standard_normal((g.nt, 2))
+    shots = matio.shots_from_s_r_(g, back, wv)
+    for k, (s, r) in enumerate(pairs):
+        assert (shots[k].src_i, shots[k].src_j) == (g.dom_i0 + s[0], g.dom_j0 + s[1])
+        assert list(shots[k].rec) == [g.node(g.dom_i0 + iz, g.dom_j0 + ix) for ix, iz in r]
+        assert np.array_equal(shots[k].wavelet, wv[:, k])
+
+
+def test_dc_survey_and_ky_w_round_trip(tmp_path):
+    rng = np.random.default_rng(4)
+    gathers = [{"ab": np.array([3, 5]), "current": 0.5, "mn": np.array([[7, 9], [9, 11], [11, 13]]),
+                "d": rng.standard_normal(3), "std": np.full(3, 0.02)},
+               {"ab": np.array([4, 8]), "current": 1.0, "mn": np.array([[12, 16]]),
+                "d": rng.standard_normal(1), "std": np.full(1, 0.05)}]
+    p = str(tmp_path / "s_i_r_d_std.mat")
+    matio.save_dc_survey(p, gathers)
+    back = matio.load_dc_survey(p)
+    for a, b in zip(gathers, back):
+        assert np.array_equal(a["ab"], b["ab"]) and a["current"] == b["current"]
+        assert np.array_equal(a["mn"], b["mn"])
+        assert np.array_equal(a["d"], b["d"]) and np.array_equal(a["std"], b["std"])
+    kw = rng.random((6, 2, 2))
+    q = str(tmp_path / "ky_w.mat")
+    matio.save_ky_w(q, kw)
+    assert np.array_equal(matio.load_ky_w(q), kw)
+    matio.save_ky_w(q, kw[:, :, 0])
+    assert matio.load_ky_w(q).shape == (6, 2, 1)
+
+
+def test_v73_files_are_rejected_with_a_clear_error(tmp_path):
+    p = tmp_path / "line1.mat"
+    hdr = b"MATLAB 7.3 MAT-file, Platform: GLNXA64, Created on: Mon Jan  1 00:00:00 2024 HDF5 schema 1.00 ."
+    p.write_bytes(hdr.ljust(116, b" ") + b"\x00" * 8 + b"\x00\x02" + b"IM" + b"\x00" * 512)
+    with pytest.raises(ValueError, match="v7.3"):
+        matio.load_radargram(str(p))
