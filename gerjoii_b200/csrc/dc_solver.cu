@@ -76,7 +76,7 @@ __global__ void k_dc_stack(int N, int nky, int src0, int nsrc_b, const double* w
 struct DcPlan {
   DcGrid G{};
   int nky = 0, nsrc = 0, robin = 0;
-  DevBuf sig, faces, ky2, wts, alpha, ab, cur, mnoff, mnbuf, fac, vec, dots, done, status, gbuf, dbuf, ebuf, ubuf;
+  DevBuf sig, faces, ky2, wts, alpha, ab, cur, mnoff, mnbuf, dots, done, status, gbuf, dbuf, ebuf, ubuf;
   DevBuf tiles;  // the factor's trailing-update tiles, (ct << 16) | rt, column-major
   std::vector<long> off;
 };
@@ -102,7 +102,7 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   const double* sg = P.sig.as<double>();
   const double* al = P.alpha.as<double>();
   const double* k2 = P.ky2.as<double>();
-  const TF* F = P.fac.as<TF>();
+  const TF* F = c.dc_fac.as<TF>();
   const dim3 gv((N + 255) / 256 < 64 ? (N + 255) / 256 : 64, nsys);
   const size_t shp = dc_precond_smem<TF>(G.wp);
   auto precond = [&](double* rzv) {  // one warp per system; window of 32R >= b + 1 positions
@@ -251,13 +251,14 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   // ---- batch size from the memory budget: FP32 factor + 7 FP64 vectors + u_k per system
   size_t free_b = 0, total_b = 0;
   GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
-  const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.7 * double(free_b));
+  const size_t reusable = c.dc_fac.bytes + c.dc_vec.bytes;  // this context's DC buffers from earlier calls
+  const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.7 * double(free_b + reusable));
   const size_t per_sys = size_t(G.nq) * G.wp * sizeof(TF) + size_t(N) * 8 * sizeof(double) + 64;
   int srcs_per_batch = int(std::min<size_t>(nsrc, std::max<size_t>(1, budget / (per_sys * nky))));
   if (o.sources_per_batch > 0) srcs_per_batch = std::min(srcs_per_batch, o.sources_per_batch);
   const int nsys_b = srcs_per_batch * nky;
-  GJ_TRY(P.fac.alloc(err, size_t(nsys_b) * G.nq * G.wp * sizeof(TF)));
-  GJ_TRY(P.vec.alloc(err, size_t(nsys_b) * N * 7 * sizeof(double)));  // B, X, R, Z, P, AP, U
+  GJ_TRY(c.dc_fac.alloc(err, size_t(nsys_b) * G.nq * G.wp * sizeof(TF)));
+  GJ_TRY(c.dc_vec.alloc(err, size_t(nsys_b) * N * 7 * sizeof(double)));  // B, X, R, Z, P, AP, U
   GJ_TRY(P.dots.alloc(err, 6 * size_t(nsys_b) * sizeof(double)));
   GJ_TRY(P.done.alloc(err, nsys_b * sizeof(int)));
   const double tol = o.tol > 0 ? o.tol : 1e-10;
@@ -276,7 +277,7 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     GJ_TRY(P.tiles.alloc(err, ht.size() * sizeof(unsigned)));
     GJ_CUDA(err, cudaMemcpy(P.tiles.p, ht.data(), ht.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
   }
-  double* V = P.vec.as<double>();
+  double* V = c.dc_vec.as<double>();
   for (int s0 = 0; s0 < nsrc; s0 += srcs_per_batch) {
     const int nsb = std::min(srcs_per_batch, nsrc - s0);
     const int nsys = nsb * nky, sys0 = s0 * nky;
@@ -289,7 +290,7 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
       const bool tm = c.timer.begin(KK_DC_FACTOR, st, nsys);
       k_dc_factor<TF><<<nsys, DC_FACTOR_THREADS, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(),
                                                                P.alpha.as<double>(), P.ky2.as<double>(),
-                                                               P.tiles.as<unsigned>(), sys0, P.fac.as<TF>(),
+                                                               P.tiles.as<unsigned>(), sys0, c.dc_fac.as<TF>(),
                                                                P.status.as<int>());
       c.timer.end(tm, st);
       ++c.launches;

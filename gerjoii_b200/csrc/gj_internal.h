@@ -63,6 +63,11 @@ struct DevBuf {
     bytes = n;
     return GJ_OK;
   }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
@@ -158,6 +163,10 @@ struct Ctx {
   long launches = 0;
   KernelTimer timer;
   std::unique_ptr<WSolverBase> wsolver;  // cached radar plan
+  // DC band factors and CG vectors, kept between DC calls (tens of GB for a
+  // survey: allocating them costs milliseconds per GB); a radar call releases
+  // them before it plans its own memory.
+  DevBuf dc_fac, dc_vec;
   std::string wkey;
 };
 

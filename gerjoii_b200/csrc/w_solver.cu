@@ -1501,6 +1501,8 @@ class WSolver : public WSolverBase {
 
 template <class T>
 static gj_status get_solver(Ctx& c, const gj_w_grid& g, const gj_w_shot* shots, int ns, WSolver<T>*& out) {
+  c.dc_fac.release();  // the radar plan sizes itself from the free memory
+  c.dc_vec.release();
   std::string k = std::string(sizeof(T) == 8 ? "d" : "f") + WSolver<T>::key(g, shots, ns);
   if (c.wsolver && c.wkey == k) {
     out = static_cast<WSolver<T>*>(c.wsolver.get());
