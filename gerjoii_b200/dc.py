@@ -10,7 +10,9 @@ module prepares their inputs the way the reference's MATLAB does:
   private ``alphas`` (:820-960) in the compact layout of the C ABI;
 * :func:`ky_weights` designs wavenumbers and weights for the inverse cosine
   transform u = (2/pi) sum_k w_k u_k (a least-squares fit of the half-space
-  kernel, standing in for dc_kfourier.m's Gauss-Newton design).
+  kernel on fixed log-spaced wavenumbers);
+* :func:`kfourier` is the reference's own per-source design (dc_kfourier.m,
+  Gauss-Newton on the wavenumbers over the distances of :func:`coca_radius`).
 """
 from __future__ import annotations
 
@@ -159,3 +161,104 @@ def apparent_resistivity(d: list, k: list) -> list:
     """rho_a = k * d per datum (dc_geomefactor2_5d.m:36-43): the resistivity of
     the homogeneous half-space that would produce the measured data."""
     return [np.asarray(x, np.float64) * np.asarray(kk, np.float64) for x, kk in zip(d, k)]
+
+
+def coca_radius(n: int, m: int, DX: float, DZ: float, a_node: int, b_node: int):
+    """The distance pairs the wavenumber design fits (dc_coca.m:12-39,
+    dc_kfourier.m:43-65) on a uniform grid: for every node the distances r, r_
+    to the lower- and higher-index surface electrode (the lateral distance sums
+    the spacings over the inclusive index range, as dc_coca.m:18-21 does; the
+    depth of row h is h*DZ), unique pairs with both nonzero, then each of r and
+    r_ resampled on its own to fix(N^0.7) evenly spaced values, and
+    R = 1 / (1/r - 1/r_) where finite.  Returns (r, r_, R)."""
+    nodes = sorted(int(x) for x in (a_node, b_node))
+    if nodes[1] >= n:
+        raise ValueError("the wavenumber design needs both source electrodes on the surface row")
+    l = np.arange(n)
+    co = [np.where(l == s, 0.0, (np.abs(s - l) + 1) * DX) for s in nodes]
+    ca = np.arange(m) * DZ
+    r = np.sqrt(co[0][:, None] ** 2 + ca[None, :] ** 2).ravel(order="F")
+    r_ = np.sqrt(co[1][:, None] ** 2 + ca[None, :] ** 2).ravel(order="F")
+    RR = np.unique(np.column_stack([r, r_]), axis=0)
+    RR = RR[RR[:, 0] != 0]
+    RR = RR[RR[:, 1] != 0]
+    cnt = int(np.fix(10 ** (np.log10(len(RR)) * 0.7)))
+    r = np.linspace(RR[:, 0].min(), RR[:, 0].max(), cnt)
+    r_ = np.linspace(RR[:, 1].min(), RR[:, 1].max(), cnt)
+    with np.errstate(divide="ignore"):
+        R = 1.0 / (1.0 / r - 1.0 / r_)
+    keep = ~np.isinf(R)
+    if not keep.any():
+        # electrodes placed symmetrically in the grid give r and r_ the same
+        # range, so the two resampled lists coincide and every R is infinite;
+        # the reference's design is then left without distances (NaN weights)
+        raise ValueError("symmetric electrode placement: no distance pairs left for the wavenumber design")
+    return r[keep], r_[keep], R[keep]
+
+
+def _ridge_solve(A: np.ndarray, b: np.ndarray) -> np.ndarray:
+    try:
+        return np.linalg.solve(A, b)
+    except np.linalg.LinAlgError:  # MATLAB's backslash warns and returns Inf/NaN
+        return np.full(A.shape[1], np.nan)
+
+
+def kfourier(n: int, m: int, DX: float, DZ: float, a_node: int, b_node: int, n_ky: int, dx: float,
+             radius=None) -> np.ndarray:
+    """Wavenumbers and weights of the 2.5D inverse transform for one source, as
+    dc_kfourier.m:26-197 designs them.  K(ky) = (2/pi) R (K0(ky r) - K0(ky r_))
+    (the real part of besselk, which for a negative argument is K0 of its
+    magnitude); the fit v = K (K'K + 1e-8 I)^-1 K' 1 of the dipole kernel
+    should be 1.  From ky = logspace(-2, 0.5, n_ky) * dx, Gauss-Newton steps
+    (forward-difference Jacobian at 1.05 ky, ridge 1e-8, smallness 1e-8 ky)
+    with a 20-point line search over [0.01, 0.9] run while every objective so
+    far exceeds 1e-5, fewer than 25 iterations have run and each reduced the
+    objective by more than 5 %; an ill-conditioned K'K (reciprocal 1-norm
+    condition below 1e-15) or a NaN fit restores the previous ky and stops.
+    Weights w = (K'K + 5e-8 I)^-1 K' 1 at |ky|.  Returns [ky*dx, w] (n_ky x 2),
+    the reference's ky_w_.  `radius` = (r, r_, R) reuses the distances of an
+    earlier source, as the reference does once finite_.dc.radius is set
+    (dc_kfourier.m:43, 66-69)."""
+    r, r_, R = coca_radius(n, m, DX, DZ, a_node, b_node) if radius is None else radius
+    beta_v, beta_g, beta_dky, beta_wky = 1e-8, 1e-8, 1e-8, 5e-8
+    eye = np.eye(n_ky)
+    one = np.ones(len(r))
+
+    def kmat(ky):
+        with np.errstate(invalid="ignore"):
+            return (2 / np.pi) * R[:, None] * (ss.k0(np.abs(np.outer(r, ky))) - ss.k0(np.abs(np.outer(r_, ky))))
+
+    def fit(K):
+        return K @ _ridge_solve(K.T @ K + beta_v * eye, K.T @ one)
+
+    ky = np.logspace(-2, 0.5, n_ky) * dx
+    v = fit(kmat(ky))
+    obj = [float((1 - v) @ (1 - v))]
+    its, stopper, reduction = 1, False, 1.0
+    ls = np.linspace(0.01, 0.9, 20)
+    while all(o > 1e-5 for o in obj) and its < 25 and not stopper and reduction > 0.05:
+        ky_prev = ky.copy()
+        J = np.empty((len(r), n_ky))
+        for ii in range(n_ky):
+            k_ = ky.copy()
+            k_[ii] = 1.05 * k_[ii]
+            J[:, ii] = (fit(kmat(k_)) - v) / (k_[ii] - ky[ii])
+        grad = J.T @ (1 - v) + beta_g * ky
+        dky = _ridge_solve(J.T @ J + beta_dky * eye, grad)
+        res = np.array([float((1 - f) @ (1 - f)) for f in (fit(kmat(ky + a * dky)) for a in ls)])
+        jj = int(np.nanargmin(res)) if not np.isnan(res).all() else 0  # MATLAB min skips NaN
+        ky = ky + ls[jj] * dky
+        K = kmat(ky)
+        v = fit(K)
+        obj.append(float((1 - v) @ (1 - v)))
+        reduction = obj[its - 1] / obj[its] - 1
+        its += 1
+        with np.errstate(divide="ignore"):
+            rc = 1.0 / np.linalg.cond(K.T @ K, 1) if np.isfinite(K).all() else 0.0
+        if rc < 1e-15 or np.isnan(v).any():
+            ky = ky_prev
+            stopper = True
+    ky = np.abs(ky)
+    K = kmat(ky)
+    w = _ridge_solve(K.T @ K + beta_wky * eye, K.T @ one)
+    return np.column_stack([ky * dx, w])

@@ -2,6 +2,7 @@
 0.5*||d - d_obs||^2 (central differences), the host-side Robin coefficients
 match the oracle's, and the operator is symmetric positive definite."""
 import numpy as np
+import pytest
 
 from dc_cases import small_dc, oracle_alphas, oracle_forward
 
@@ -76,3 +77,65 @@ def test_geometric_factor_and_apparent_resistivity_of_a_half_space():
     d = solver.dc_forward(np.full(shape, sigma0), case["DX"], case["DZ"], case["robin"], case["srcs"])["d"]
     for rho in dcm.apparent_resistivity(d, k):
         assert np.allclose(rho, 1.0 / sigma0, rtol=1e-10)
+
+
+def _halfspace_grid():
+    from gerjoii_b200 import dc as dcm
+    n0, m0, robin, dx = 120, 40, 1, 0.25
+    DX, DZ = dcm.deltas(np.arange(n0) * dx, np.arange(m0) * dx, robin)
+    return n0 + 2 * robin, m0 + robin, DX, DZ, dx
+
+
+def test_kfourier_fits_the_dipole_kernel():
+    """dc_kfourier.m's design: with the final wavenumbers and weights,
+    (2/pi) R sum_k w_k (K0(ky_k r) - K0(ky_k r_)) reproduces 1 over the
+    distance pairs of dc_coca.m (rms misfit below 1 %)."""
+    import scipy.special as ss
+    from gerjoii_b200 import dc as dcm
+    n, m, DX, DZ, dx = _halfspace_grid()
+    la, lb = dcm.clean_electrode(41, 60)
+    r, r_, R = dcm.coca_radius(n, m, DX, DZ, la - 1, lb - 1)
+    kw = dcm.kfourier(n, m, DX, DZ, la - 1, lb - 1, 12, dx)
+    assert kw.shape == (12, 2) and np.isfinite(kw).all() and (kw[:, 0] > 0).all()
+    ky = kw[:, 0] / dx
+    v = (2 / np.pi) * R[:, None] * (ss.k0(np.outer(r, ky)) - ss.k0(np.outer(r_, ky))) @ kw[:, 1]
+    assert np.sqrt(np.mean((1 - v) ** 2)) < 0.01
+    # the reference reuses the first source's distances once finite_.dc.radius is set
+    assert np.array_equal(dcm.kfourier(n, m, DX, DZ, 0, 1, 12, dx, radius=(r, r_, R)), kw)
+
+
+def test_kfourier_halfspace_matches_analytic_potential():
+    """The 2.5D potential of a homogeneous half-space (oracle direct solves)
+    with dc_kfourier.m's wavenumbers and weights against dc_analhomo2_5d.m's
+    I/(2 pi sigma)(1/r_A - 1/r_B), away from the electrodes and the Robin
+    boundary (discretisation-limited)."""
+    import np_dc_oracle as dco
+    from gerjoii_b200 import dc as dcm
+    n, m, DX, DZ, dx = _halfspace_grid()
+    sigma = 0.01
+    SIG = np.full((n, m), sigma)
+    la, lb = dcm.clean_electrode(41, 60)
+    la, lb = la - 1, lb - 1
+    kyw = dcm.kfourier(n, m, DX, DZ, la, lb, 12, dx)
+    al = [dco.alphas(n, m, DX, DZ, dco.source_vector(n, m, la, lb)[:n], ky) for ky in kyw[:, 0]]
+    u = dco.dc_fwd2_5d(SIG, DX, DZ, dco.source_vector(n, m, la, lb, 1.0), al, kyw,
+                       dco.measuring_operator(n, m, np.array([[la + 5, la + 6]])), None)[0]
+    u = np.asarray(u).reshape((n, m), order="F")
+    ua = dco.analytic_halfspace(n, m, abs(DX), DZ, sigma, la, lb)
+    mask = np.zeros_like(u, bool)
+    mask[40:85, 2:15] = True
+    mask[abs(np.arange(n) - la)[:, None].repeat(m, 1) < 4] = False
+    mask[abs(np.arange(n) - lb)[:, None].repeat(m, 1) < 4] = False
+    err = np.abs(u[mask] - ua[mask]) / np.abs(ua[mask]).max()
+    assert err.max() < 0.10 and np.median(err) < 0.02, (err.max(), np.median(err))
+
+
+def test_kfourier_rejects_symmetric_electrodes():
+    """Electrodes placed symmetrically in the grid leave dc_kfourier.m's
+    resampled distances r and r_ identical (every R infinite): an error here,
+    where the reference would return NaN weights."""
+    from gerjoii_b200 import dc as dcm
+    n, m, DX, DZ, dx = _halfspace_grid()
+    la, lb = dcm.clean_electrode(51, 70)
+    with pytest.raises(ValueError, match="symmetric"):
+        dcm.kfourier(n, m, DX, DZ, la - 1, lb - 1, 12, dx)
