@@ -1,0 +1,86 @@
+"""Step length of the radar permittivity update, as the reference chooses it
+around its objective evaluations (w_stepparabola_e.m, w_boundstep2.m,
+w_objs_e.m:24-25).  The trial objectives are forward-only runs of all shots,
+which ``Context.w_misfit`` (gj_w_misfit) does on the GPU; this module holds the
+host logic around them.
+
+The reference's trial objective also band-filters the observed and modelled
+traces (w_objs_e.m:33-36) before the misfit; gj_w_misfit has no such filter, so
+with a band-limited inversion the trial misfits here are of the unfiltered
+traces.
+"""
+from __future__ import annotations
+
+import math
+from typing import Callable
+
+import numpy as np
+
+
+def perturb_eps(eps: np.ndarray, g_e: np.ndarray, ke: float) -> np.ndarray:
+    """The trial model eps * exp(-ke * eps * g_e) (w_objs_e.m:24-25)."""
+    eps = np.asarray(eps, np.float64)
+    return eps * np.exp(-ke * eps * np.asarray(g_e, np.float64))
+
+
+def _in_bounds(eps, deps, k, eps_max, eps_min) -> bool:
+    e = eps * np.exp(k * eps * deps)
+    return not (e.max() > eps_max or e.min() < eps_min)
+
+
+def boundstep2(eps, deps, eps_max: float, eps_min: float, k_) -> float:
+    """The largest step k for which eps * exp(k * eps * deps) stays within
+    [eps_min, eps_max] (w_boundstep2.m:5-23): a reverse search over 13
+    log-spaced steps from max(k_) down to min(k_) for the first one in bounds,
+    then a forward search over 20 linear steps between it and the previous,
+    out-of-bounds one, for the last one in bounds.  If even min(k_) is out of
+    bounds the first search ends there and its value is returned."""
+    eps = np.asarray(eps, np.float64).ravel()
+    deps = np.asarray(deps, np.float64).ravel()
+    k_ = np.atleast_1d(np.asarray(k_, np.float64))
+    k = np.logspace(math.log10(k_.max()), math.log10(k_.min()), 13)
+    ik = 0  # first in bounds, or the last entry (w_boundstep2.m:28-43)
+    while not _in_bounds(eps, deps, k[ik], eps_max, eps_min):
+        if ik + 1 >= len(k):
+            break
+        ik += 1
+    if ik == 0:
+        return float(k[0])
+    k = np.linspace(k[ik], k[ik - 1], 20)
+    ik = 0  # last in bounds (w_boundstep2.m:44-63)
+    while _in_bounds(eps, deps, k[ik], eps_max, eps_min):
+        if ik + 1 >= len(k):
+            return float(k[ik])
+        ik += 1
+    return float(k[max(ik - 1, 0)])
+
+
+def stepparabola(eps, g_e, objective: Callable[[float], float], E0: float, eps_max: float, eps_min: float,
+                 k_e, keprct_: float, keprct__: float, nparabo: int) -> tuple[float, np.ndarray, np.ndarray]:
+    """w_stepparabola_e.m: trial steps ke from -keprct_ * boundstep2(eps, g_e)
+    to keprct__ * boundstep2(eps, -g_e) (nparabo of them), their objectives
+    beside E0 at ke = 0, a least-squares parabola through the points and its
+    vertex as the step; a flat (zero or NaN) or negative vertex gives 0.
+    `objective(ke)` evaluates the trial model perturb_eps(eps, g_e, ke).
+    Returns (step, ke, E) with ke and E including the ke = 0 point first."""
+    ke_ = -boundstep2(eps, g_e, eps_max, eps_min, k_e) * keprct_
+    ke__ = boundstep2(eps, -np.asarray(g_e, np.float64), eps_max, eps_min, k_e) * keprct__
+    ks = np.linspace(ke_, ke__, nparabo)
+    E = np.array([float(E0)] + [float(objective(float(k))) for k in ks])
+    ke = np.concatenate([[0.0], ks])
+    with np.errstate(all="ignore"):
+        p = np.polyfit(ke, E, 2)
+        step = -p[1] / (2 * p[0])
+    if not np.isfinite(step) or step == 0 or step < 0:
+        step = 0.0
+    return float(step), ke, E
+
+
+def misfit_objective(ctx, grid, eps, sig, shots, d_obs, g_e, misfit=0, precision=0) -> Callable[[float], float]:
+    """The trial objective of w_objs_e.m on the GPU: the summed normalised
+    misfit of all shots for perturb_eps(eps, g_e, ke), one gj_w_misfit call
+    (forward runs only) per trial."""
+    def objective(ke: float) -> float:
+        return float(np.sum(ctx.w_misfit(grid, perturb_eps(eps, g_e, ke), sig, shots, d_obs, misfit=misfit,
+                                          precision=precision)))
+    return objective
