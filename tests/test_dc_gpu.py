@@ -145,3 +145,18 @@ def test_geometric_factor_matches_oracle(gpu_ctx):
     d = gpu_ctx.dc_forward(np.full(shape, 0.02), case["DX"], case["DZ"], case["robin"], case["srcs"])["d"]
     for rho in dcm.apparent_resistivity(d, k):
         assert np.allclose(rho, 50.0, rtol=1e-8)
+
+
+def test_dc_fp32_factor_wide_band(gpu_ctx):
+    """factor_fp32 = 1 on a band wider than 127 (b = 131): the FP32 factor
+    through the 256-position substitution window meets the FP64 tolerance and
+    agrees with the FP64-factor solution."""
+    case = small_dc(seed=7, n0=150, m0=130, n_el=12, spacing=10, first=5, levels=2, pairs=1, n_ky=2)
+    o = N.DcOptsC()
+    o.factor_fp32 = 1
+    o.max_iter = 200
+    a = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], opts=o)
+    b = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
+    assert a["rel_residual"] <= 1e-10 and b["rel_residual"] <= 1e-10
+    for x, y in zip(a["d"], b["d"]):
+        assert rel_l2(x, y) < 1e-9
