@@ -326,17 +326,11 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
       }
     }
     // ---- entering columns q+M .. q+M+DC_NB-1 into the panel's slots
-#pragma unroll 1
-    for (int t = 0; t < DC_NB; ++t) {
+    for (int e = tid; e < DC_NB * Mr; e += nth) {
+      const int t = e / Mr, k = e % Mr;
       int s_ = sq + t;
       if (s_ >= M) s_ -= M;
-      const int r0 = (q + M + t) % Mr;  // row slot of the diagonal (as column_value)
-      int r1 = r0 + 1, rb = r0 + b;
-      if (r1 >= Mr) r1 -= Mr;
-      if (rb >= Mr) rb -= Mr;
-      const TF dg = stg[t], s1 = stg[DC_NB + t], s2 = stg[2 * DC_NB + t];
-      TF* col = S + s_ * Mr;
-      for (int k = tid; k < Mr; k += nth) col[k] = k == r0 ? dg : (k == r1 ? s1 : (k == rb ? s2 : TF(0)));
+      S[s_ * Mr + k] = column_value(q + M + t, k, stg[t], stg[DC_NB + t], stg[2 * DC_NB + t]);
     }
     sq = sqn;
     rq = rqn;
