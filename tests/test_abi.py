@@ -41,3 +41,19 @@ def test_library_has_no_torch_dependency():
     with open(build.LIB, "rb") as f:
         blob = f.read()
     assert b"libtorch" not in blob and b"libc10" not in blob
+
+
+def test_python_constants_match_the_header_enums():
+    """The ctypes binding's misfit kinds, adjoint modes and precisions carry
+    the values include/gerjoii_gpu.h gives them, and every obj_FNC name maps
+    to a declared misfit kind."""
+    import re
+    from gerjoii_b200 import _native as N
+    hdr = open(os.path.join(ROOT, "include", "gerjoii_gpu.h")).read()
+    for name in ("GJ_MISFIT_L2", "GJ_MISFIT_ENV_L2", "GJ_MISFIT_PHASE_L2", "GJ_MISFIT_ENV_L22", "GJ_MISFIT_ENV_LOG",
+                 "GJ_ADJ_REFERENCE", "GJ_ADJ_EXACT", "GJ_F32", "GJ_F64"):
+        m = re.search(rf"\b{name}\s*=\s*(\d+)", hdr)
+        assert m, name
+        assert getattr(N, name) == int(m.group(1)), name
+    assert set(N.MISFIT_KINDS.values()) == {0, 1, 2, 3, 4}
+    assert N.misfit_kind("env_LOG") == N.GJ_MISFIT_ENV_LOG and N.misfit_kind(3) == 3
