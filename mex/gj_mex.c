@@ -84,6 +84,33 @@ static gj_w_shot wshot(const mxArray* s_w, const mxArray* M, const mxArray* wav,
   return q;
 }
 
+/* Shots of a batched call: S (ns x 2) source nodes, Mcell{k} receivers, one
+   wavelet for all, Dcell{k} nt x nr observed traces packed shot after shot.
+   The caller frees recs[k], recs, the shots and dobs with mxFree. */
+static gj_w_shot* pack_shots(const mxArray* S, const mxArray* Mcell, const mxArray* wav, const mxArray* Dcell, int nt,
+                             long*** recs_out, double** dobs_out, int* ns_out) {
+  const int ns = (int)mxGetM(S);
+  gj_w_shot* shots = (gj_w_shot*)mxMalloc(ns * sizeof(gj_w_shot));
+  long** recs = (long**)mxMalloc(ns * sizeof(long*));
+  size_t ntot = 0;
+  for (int k = 0; k < ns; ++k) ntot += (size_t)nt * mxGetNumberOfElements(mxGetCell(Mcell, k));
+  double* dobs = (double*)mxMalloc((ntot ? ntot : 1) * sizeof(double));
+  size_t o = 0;
+  for (int k = 0; k < ns; ++k) {
+    double sw[2] = {mxGetPr(S)[k], mxGetPr(S)[k + ns]};
+    mxArray* swa = mxCreateDoubleMatrix(1, 2, mxREAL);
+    memcpy(mxGetPr(swa), sw, sizeof sw);
+    shots[k] = wshot(swa, mxGetCell(Mcell, k), wav, &recs[k]);
+    mxDestroyArray(swa);
+    memcpy(dobs + o, mxGetPr(mxGetCell(Dcell, k)), (size_t)nt * shots[k].nr * sizeof(double));
+    o += (size_t)nt * shots[k].nr;
+  }
+  *recs_out = recs;
+  *dobs_out = dobs;
+  *ns_out = ns;
+  return shots;
+}
+
 void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   char cmd[64];
   if (nrhs < 1 || mxGetString(prhs[0], cmd, sizeof cmd)) mexErrMsgIdAndTxt("gerjoii:arg", "gj_mex(command, ...)");
@@ -117,24 +144,10 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
                                   obj_FNC)
        (w_update_es.m's w_fwd + w_grad pair for every shot at once; obj_FNC 'L2' by default) */
     gj_w_grid g = wgrid(prhs[3]);
-    const mxArray* S = prhs[4];
-    const int ns = (int)mxGetM(S);
-    gj_w_shot* shots = (gj_w_shot*)mxMalloc(ns * sizeof(gj_w_shot));
-    long** recs = (long**)mxMalloc(ns * sizeof(long*));
-    size_t ntot = 0;
-    for (int k = 0; k < ns; ++k) ntot += (size_t)g.nt * mxGetNumberOfElements(mxGetCell(prhs[5], k));
-    double* dobs = (double*)mxMalloc((ntot ? ntot : 1) * sizeof(double));
-    size_t o = 0;
-    for (int k = 0; k < ns; ++k) {
-      double sw[2] = {mxGetPr(S)[k], mxGetPr(S)[k + ns]};
-      mxArray* swa = mxCreateDoubleMatrix(1, 2, mxREAL);
-      memcpy(mxGetPr(swa), sw, sizeof sw);
-      shots[k] = wshot(swa, mxGetCell(prhs[5], k), prhs[6], &recs[k]);
-      mxDestroyArray(swa);
-      const mxArray* dk = mxGetCell(prhs[7], k);
-      memcpy(dobs + o, mxGetPr(dk), (size_t)g.nt * shots[k].nr * sizeof(double));
-      o += (size_t)g.nt * shots[k].nr;
-    }
+    long** recs;
+    double* dobs;
+    int ns;
+    gj_w_shot* shots = pack_shots(prhs[4], prhs[5], prhs[6], prhs[7], g.nt, &recs, &dobs, &ns);
     const gj_adj_mode mode = nrhs > 8 ? (gj_adj_mode)(int)mxGetScalar(prhs[8]) : GJ_ADJ_REFERENCE;
     const gj_misfit_kind mk = nrhs > 9 ? misfit_kind(prhs[9]) : GJ_MISFIT_L2;
     plhs[0] = mxCreateDoubleMatrix(g.m, g.n, mxREAL);
@@ -142,6 +155,19 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     plhs[2] = mxCreateDoubleMatrix(ns, 1, mxREAL);
     check(gj_w_gradient(ctx(), &g, prec, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, dobs, mode, mk,
                         NULL, mxGetPr(plhs[0]), mxGetPr(plhs[1]), mxGetPr(plhs[2]), NULL, NULL));
+    for (int k = 0; k < ns; ++k) mxFree(recs[k]);
+    mxFree(recs); mxFree(shots); mxFree(dobs);
+  } else if (!strcmp(cmd, "w_misfit")) {
+    /* E = gj_mex('w_misfit', eps, sigma, grid, S (ns x 2), Mcell, wavelet, dobs_cell, obj_FNC)
+       (the forward-only objective of every shot for a trial model, w_objs_e.m:24-65) */
+    gj_w_grid g = wgrid(prhs[3]);
+    long** recs;
+    double* dobs;
+    int ns;
+    gj_w_shot* shots = pack_shots(prhs[4], prhs[5], prhs[6], prhs[7], g.nt, &recs, &dobs, &ns);
+    const gj_misfit_kind mk = nrhs > 8 ? misfit_kind(prhs[8]) : GJ_MISFIT_L2;
+    plhs[0] = mxCreateDoubleMatrix(ns, 1, mxREAL);
+    check(gj_w_misfit(ctx(), &g, prec, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, dobs, mk, mxGetPr(plhs[0])));
     for (int k = 0; k < ns; ++k) mxFree(recs[k]);
     mxFree(recs); mxFree(shots); mxFree(dobs);
   } else if (!strcmp(cmd, "dc_fwd2_5d") || !strcmp(cmd, "dc_gradient2_5d")) {
