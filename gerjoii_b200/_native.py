@@ -99,6 +99,7 @@ SIGNATURES = {
                            C.POINTER(DcStatsC)]),
     "gj_dc_gradient": (_I, [_VP, C.POINTER(DcGridC), _DP, C.POINTER(DcSrcC), _I, C.POINTER(DcOptsC), _DP, _DP, _DP,
                             _DP, C.POINTER(DcStatsC)]),
+    "gj_dc_alphas": (_I, [C.POINTER(DcGridC), C.c_long, C.c_long, _DP, _DP]),
     "gj_w_forward_noalloc": (_I, [C.POINTER(GridC), _VP, _VP, _I, _I, _VP, _I, _VP, _VP, _VP, C.c_char_p,
                                   C.c_size_t]),
 }
@@ -367,3 +368,17 @@ class Context:
                                                C.byref(o), ge_t.data_ptr(), gs_t.data_ptr(), _dp(mis),
                                                C.c_void_p(stream)))
         return mis
+
+
+def dc_alphas(n: int, m: int, dx: float, dz: float, a_node: int, b_node: int, ky) -> np.ndarray:
+    """gj_dc_alphas: the Robin coefficients of one source (n_ky x GJ_DC_NALPHA,
+    the layout of DcSource.alpha), computed by the library on the host."""
+    lib = load()
+    ky = np.ascontiguousarray(ky, np.float64).ravel()
+    na = 2 * (m - 2) + (n - 2) + 4
+    out = np.zeros((len(ky), na))
+    g = DcGridC(n, m, 0, len(ky), dx, dz)
+    st = lib.gj_dc_alphas(C.byref(g), int(a_node), int(b_node), _dp(ky), _dp(out))
+    if st != 0:
+        raise ValueError(f"gj_dc_alphas failed with status {st}")
+    return out

@@ -240,6 +240,15 @@ gj_status gj_dc_gradient(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigm
                          double* g_out, double* d_out, double* e_out, double* misfit_out,
                          gj_dc_stats* stats);
 
+/* Robin coefficients of one source for every wavenumber, written to alpha_out
+ * in the layout gj_dc_src.alpha takes (n_ky x GJ_DC_NALPHA(n, m), ky-major):
+ * the private alphas of dc_Lk.m:820-960 (called by dc_Lk.m:236-520), which
+ * MATLAB code outside dc_Lk.m cannot call.  a_node, b_node are the source
+ * electrodes as in gj_dc_src (on the surface row); ky as gj_dc_src.ky.
+ * Computed on the host: needs no context and no GPU. */
+gj_status gj_dc_alphas(const gj_dc_grid* grid, long a_node, long b_node, const double* ky,
+                       double* alpha_out);
+
 /* Scratch limit of gj_w_forward_noalloc, in bytes (32 MiB): enough for a
  * padded grid of about 380 000 Ez nodes (for example 600 x 600). */
 #define GJ_W_NOALLOC_SCRATCH_BYTES (32u << 20)

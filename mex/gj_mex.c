@@ -172,6 +172,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     mxFree(recs); mxFree(shots); mxFree(dobs);
   } else if (!strcmp(cmd, "dc_fwd2_5d") || !strcmp(cmd, "dc_gradient2_5d")) {
     /* d = gj_mex('dc_fwd2_5d', sigma_robin, dcgrid, AB (ns x 2, 1-based), I, MNcell, kyw_cell, alpha_cell)
+       (alpha_cell = [] has the library compute dc_Lk.m's alphas, gj_dc_alphas)
        [g, d, e] = gj_mex('dc_gradient2_5d', ..., dobs_cell)   (dc_fwd2_5d.m, dc_gradient2_5d.m) */
     const int grad = !strcmp(cmd, "dc_gradient2_5d");
     gj_dc_grid g;
@@ -181,6 +182,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     const int ns = (int)mxGetM(AB);
     gj_dc_src* srcs = (gj_dc_src*)mxMalloc(ns * sizeof(gj_dc_src));
     long** mns = (long**)mxMalloc(ns * sizeof(long*));
+    double** als = (double**)mxMalloc(ns * sizeof(double*));
+    for (int k = 0; k < ns; ++k) als[k] = NULL;
     size_t nd = 0;
     for (int k = 0; k < ns; ++k) {
       const mxArray* MN = mxGetCell(prhs[5], k);
@@ -199,7 +202,13 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       srcs[k].mn = mns[k];
       srcs[k].ky = mxGetPr(kyw);
       srcs[k].w = mxGetPr(kyw) + g.n_ky;
-      srcs[k].alpha = mxGetPr(mxGetCell(prhs[7], k)); /* GJ_DC_NALPHA x n_ky, column per ky */
+      if (mxGetNumberOfElements(prhs[7]) > 0) {
+        srcs[k].alpha = mxGetPr(mxGetCell(prhs[7], k)); /* GJ_DC_NALPHA x n_ky, column per ky */
+      } else {  /* [] : the library computes dc_Lk.m's alphas for this source */
+        als[k] = (double*)mxMalloc((size_t)g.n_ky * GJ_DC_NALPHA(g.n, g.m) * sizeof(double));
+        check(gj_dc_alphas(&g, srcs[k].a, srcs[k].b, srcs[k].ky, als[k]));
+        srcs[k].alpha = als[k];
+      }
       srcs[k].d_obs = grad ? mxGetPr(mxGetCell(prhs[8], k)) : NULL;
       nd += ndk;
     }
@@ -213,8 +222,11 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       check(gj_dc_gradient(ctx(), &g, mxGetPr(prhs[1]), srcs, ns, NULL, mxGetPr(plhs[0]), mxGetPr(plhs[1]),
                            mxGetPr(plhs[2]), NULL, NULL));
     }
-    for (int k = 0; k < ns; ++k) mxFree(mns[k]);
-    mxFree(mns); mxFree(srcs);
+    for (int k = 0; k < ns; ++k) {
+      mxFree(mns[k]);
+      if (als[k]) mxFree(als[k]);
+    }
+    mxFree(mns); mxFree(als); mxFree(srcs);
   } else {
     mexErrMsgIdAndTxt("gerjoii:arg", "unknown command %s", cmd);
   }

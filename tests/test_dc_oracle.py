@@ -139,3 +139,23 @@ def test_kfourier_rejects_symmetric_electrodes():
     la, lb = dcm.clean_electrode(51, 70)
     with pytest.raises(ValueError, match="symmetric"):
         dcm.kfourier(n, m, DX, DZ, la - 1, lb - 1, 12, dx)
+
+
+def test_host_alphas_match_the_python_restatement():
+    """gj_dc_alphas (the library's host computation of dc_Lk.m's private alphas,
+    for callers that cannot reach it) equals dc.alphas_compact, across grids,
+    signed spacings and wavenumbers from ky dx = 2.5e-4 to arguments where
+    besselk underflows (large-argument expansion); a node midway between the
+    electrodes is 0/0 in both."""
+    from gerjoii_b200 import _native as N
+    from gerjoii_b200 import dc as dcm
+    ky = np.array([2.5e-4, 1e-3, 0.01, 0.1, 1.0, 3.0, 20.0, 80.0])
+    for (n, m, DX, DZ, a, b) in [(122, 41, -0.25, 0.25, 40, 59), (32, 11, 0.5, 0.25, 3, 9),
+                                 (402, 101, -0.25, 0.25, 100, 107), (7, 5, 1.0, 1.0, 1, 4)]:
+        with np.errstate(invalid="ignore"):
+            ref = np.stack([dcm.alphas_compact(n, m, DX, DZ, a, b, k) for k in ky])
+        got = N.dc_alphas(n, m, DX, DZ, a, b, ky)
+        assert got.shape == ref.shape
+        assert np.array_equal(np.isnan(got), np.isnan(ref))
+        ok = ~np.isnan(ref)
+        assert np.allclose(got[ok], ref[ok], rtol=1e-10, atol=0)
