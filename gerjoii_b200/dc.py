@@ -262,3 +262,20 @@ def kfourier(n: int, m: int, DX: float, DZ: float, a_node: int, b_node: int, n_k
     K = kmat(ky)
     w = _ridge_solve(K.T @ K + beta_wky * eye, K.T @ one)
     return np.column_stack([ky * dx, w])
+
+
+def redesign_sources(srcs, n: int, m: int, DX: float, DZ: float, n_ky: int, dx: float,
+                     reuse_first_radius: bool = True) -> list:
+    """The survey's sources with the reference's per-source wavenumbers and
+    weights (dc_kfourier.m for each source, as ky_w(:,:,i_e) of dc_load2_5d.m:33
+    holds them) and the matching Robin coefficients.  With reuse_first_radius
+    every source after the first uses the first source's distances, as the
+    reference does once finite_.dc.radius is set (dc_kfourier.m:43, 66-69)."""
+    out, radius = [], None
+    for q in srcs:
+        if radius is None or not reuse_first_radius:
+            radius = coca_radius(n, m, DX, DZ, q.a, q.b)
+        kyw = kfourier(n, m, DX, DZ, q.a, q.b, n_ky, dx, radius=radius)
+        al = np.stack([alphas_compact(n, m, DX, DZ, q.a, q.b, ky) for ky in kyw[:, 0]])
+        out.append(dataclasses.replace(q, ky_w=kyw, alpha=al))
+    return out

@@ -159,3 +159,23 @@ def test_host_alphas_match_the_python_restatement():
         assert np.array_equal(np.isnan(got), np.isnan(ref))
         ok = ~np.isnan(ref)
         assert np.allclose(got[ok], ref[ok], rtol=1e-10, atol=0)
+
+
+def test_redesigned_sources_carry_their_own_design():
+    """redesign_sources gives every source dc_kfourier.m's wavenumbers and
+    weights (the first source's equal a direct kfourier call) with Robin
+    coefficients for those wavenumbers, and the oracle solves the redesigned
+    survey to finite, nonzero data."""
+    import np_dc_oracle as dco
+    from dc_cases import small_dc
+    from gerjoii_b200 import dc as dcm
+    case = small_dc(seed=11, n0=40, m0=12, n_el=14, pairs=2, levels=2)
+    n, m = case["n"], case["m"]
+    srcs = dcm.redesign_sources(case["srcs"], n, m, case["DX"], case["DZ"], 8, 0.25)
+    assert all(q.ky_w.shape == (8, 2) and q.alpha.shape == (8, dcm.nalpha(n, m)) for q in srcs)
+    assert np.array_equal(srcs[0].ky_w, dcm.kfourier(n, m, case["DX"], case["DZ"], srcs[0].a, srcs[0].b, 8, 0.25))
+    for q in srcs:
+        al = [dco.alphas(n, m, case["DX"], case["DZ"], dco.source_vector(n, m, q.a, q.b)[:n], ky) for ky in q.ky_w[:, 0]]
+        d = dco.dc_fwd2_5d(case["SIG"], case["DX"], case["DZ"], dco.source_vector(n, m, q.a, q.b, q.current), al,
+                           q.ky_w, dco.measuring_operator(n, m, q.mn), None)[2]
+        assert np.isfinite(d).all() and np.abs(d).max() > 0
