@@ -207,12 +207,29 @@ def dc_gradient2_5d(SIG, DX, DZ, alphas_k, ky_w, Mop, uk, e, robin):
 
 
 def analytic_halfspace(n, m, DXabs, DZ, sigma, a_l, b_l, current=1.0):
-    """dc_analhomo2_5d.m:20-25 with dc_coca.m: surface dipole potential in a
-    homogeneous half-space, I/(2 pi sigma) (1/r_A - 1/r_B), at every node
-    (lateral index l, depth index h, 0-based), spacings taken positive."""
+    """dc_analhomo2_5d.m:20-25: surface dipole potential in a homogeneous
+    half-space, I/(2 pi sigma) (1/r_A - 1/r_B), at every node (lateral index l,
+    depth index h, 0-based), spacings taken positive.  Distances are the
+    physical ones, |l - l_A| dx; dc_coca.m's sum over the inclusive index range
+    would add one spacing."""
     l = np.arange(n)[:, None]
     h = np.arange(m)[None, :]
     rA = np.sqrt(((l - a_l) * DXabs) ** 2 + (h * DZ) ** 2)
     rB = np.sqrt(((l - b_l) * DXabs) ** 2 + (h * DZ) ** 2)
     with np.errstate(divide="ignore"):
         return current / (2 * np.pi * sigma) * (1 / rA - 1 / rB)
+
+
+def analytic_two_layer(n, DXabs, sigma1, sigma2, depth, a_l, b_l, current=1.0, terms=200):
+    """dc_analbi2_5d.m:23-44 on the surface row: the image series of a surface
+    dipole over a layer of conductivity sigma1 and thickness `depth` on a
+    half-space of sigma2, I/(2 pi sigma1) (a(r_A) - a(r_B)) with
+    a(r) = 1/r + sum_i 2 k^i / sqrt(r^2 + (2 i depth)^2), k = (sigma1 - sigma2) /
+    (sigma1 + sigma2); physical lateral distances (see analytic_halfspace)."""
+    l = np.arange(n)
+    k = (sigma1 - sigma2) / (sigma1 + sigma2)
+
+    def a(r):
+        with np.errstate(divide="ignore"):
+            return 1.0 / r + sum(2.0 * k ** i / np.sqrt(r ** 2 + (2.0 * i * depth) ** 2) for i in range(1, terms + 1))
+    return current / (2 * np.pi * sigma1) * (a(np.abs(l - a_l) * DXabs) - a(np.abs(l - b_l) * DXabs))

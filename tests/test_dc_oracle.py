@@ -179,3 +179,30 @@ def test_redesigned_sources_carry_their_own_design():
         d = dco.dc_fwd2_5d(case["SIG"], case["DX"], case["DZ"], dco.source_vector(n, m, q.a, q.b, q.current), al,
                            q.ky_w, dco.measuring_operator(n, m, q.mn), None)[2]
         assert np.isfinite(d).all() and np.abs(d).max() > 0
+
+
+@pytest.mark.parametrize("sig1,sig2", [(0.01, 0.05), (0.05, 0.01)], ids=["conductive", "resistive"])
+def test_two_layer_surface_potential_matches_image_series(sig1, sig2):
+    """dc_analbi2_5d.m's known answer: over a 2 m layer on a half-space, the
+    oracle's 2.5D surface potential (16 wavenumbers of ky_weights) against the
+    image series, away from the electrodes and the Robin boundary."""
+    import np_dc_oracle as dco
+    from gerjoii_b200 import dc as dcm
+    n0, m0, robin, dx, rows = 160, 60, 1, 0.25, 8
+    DX, DZ = dcm.deltas(np.arange(n0) * dx, np.arange(m0) * dx, robin)
+    sig0 = np.full((n0, m0), sig2)
+    sig0[:, :rows] = sig1
+    SIG = dcm.dc_robin(sig0, robin)
+    n, m = SIG.shape
+    la, lb = dcm.clean_electrode(61, 90)
+    la, lb = la - 1, lb - 1
+    kyw = dcm.ky_weights(dx, n0 * dx, 16, dx=dx)
+    al = [dco.alphas(n, m, DX, DZ, dco.source_vector(n, m, la, lb)[:n], ky) for ky in kyw[:, 0]]
+    u = dco.dc_fwd2_5d(SIG, DX, DZ, dco.source_vector(n, m, la, lb, 1.0), al, kyw,
+                       dco.measuring_operator(n, m, np.array([[la + 5, la + 6]])), None)[0]
+    u = np.asarray(u).reshape((n, m), order="F")[:, 0]
+    ua = dco.analytic_two_layer(n, dx, sig1, sig2, rows * dx, la, lb)
+    l = np.arange(n)
+    mask = (np.abs(l - la) >= 4) & (np.abs(l - lb) >= 4) & (l > 30) & (l < n - 30)
+    err = np.abs(u[mask] - ua[mask]) / np.abs(ua[mask]).max()
+    assert err.max() < 0.03 and np.median(err) < 0.005, (err.max(), np.median(err))
