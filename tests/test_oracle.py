@@ -152,3 +152,38 @@ def test_adjoint_sources_vanish_at_the_data(kind):
     e, de, doe = npo.w_bozdag(d, d, kind)
     assert np.abs(e).max() <= 1e-12 * np.abs(d).max()
     assert npo.w_E(doe, de, kind) == 0.0
+
+
+def test_forward_matches_the_2d_greens_function(oracle):
+    """Known answer: w_wavelet.m:15-18's 2D impulse response (1/2 pi) /
+    sqrt((v t)^2 - R^2) driven by the injected source.  The soft source adds
+    -dt/eps w(t) to one Ez node (Cezj, w_coeff.m), a line current w dx dy, so in
+    vacuum E(R, t) = -(mu dx dy / 2 pi) int_0^acosh(ct/R) w'(t - (R/c) cosh s) ds
+    (the substitution removes the singularity at t = R/c).  The oracle's traces
+    (reference layout, PML all round) at 15-35 cells equal it half a time step
+    later (the leapfrog staggering) to correlation 1 - 1e-5 and amplitude 0.5 %."""
+    import math
+    from gerjoii_b200.geometry import WGrid, Shot, w_wavelet, MU_0, C_0
+    m = n = 90
+    pml, air, dx, fo, nt = 20, 10, 0.05, 100e6, 520
+    dt = WGrid(m=m, n=n, pml=pml, pml_top=pml, air=air, nt=1, dx=dx, dy=dx, dt=1.0).cfl_dt(1.0, 0.95)
+    g = WGrid(m=m, n=n, pml=pml, pml_top=pml, air=air, nt=nt, dx=dx, dy=dx, dt=dt)
+    t = np.arange(nt) * dt
+    w = w_wavelet(t, 1e3, 1 / fo)
+    si, sj = g.model_node(45, 30)
+    cells = [(45, 50), (45, 65), (60, 30)]
+    rec = np.array([g.node(*g.model_node(a, b)) for a, b in cells])
+    d, _, _ = oracle.forward(g, np.ones((m, n)), np.zeros((m, n)), Shot(si, sj, w, rec))
+    tf = np.arange(-2000, 20 * nt) * (dt / 20)
+    wpf = np.gradient(w_wavelet(tf, 1e3, 1 / fo), tf)
+    for k, (a, b) in enumerate(cells):
+        R = math.hypot((a - 45) * dx, (b - 30) * dx)
+        an = np.zeros(nt)
+        for i, ti in enumerate(t + 0.5 * dt):
+            if C_0 * ti > R:
+                s = np.linspace(0.0, math.acosh(C_0 * ti / R), 4000)
+                an[i] = np.trapezoid(np.interp(ti - (R / C_0) * np.cosh(s), tf, wpf), s)
+        an *= -(MU_0 * dx * dx / (2 * math.pi))
+        cc = float(an @ d[:, k] / (np.linalg.norm(an) * np.linalg.norm(d[:, k])))
+        assert cc > 1 - 1e-5, (R, cc)
+        assert abs(np.abs(d[:, k]).max() / np.abs(an).max() - 1) < 5e-3, R
