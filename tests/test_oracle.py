@@ -222,3 +222,25 @@ def test_forward_matches_the_lossy_2d_solution(oracle, sigma):
         cc = float(an @ d[:, j] / (np.linalg.norm(an) * np.linalg.norm(d[:, j])))
         assert cc > 1 - 5e-4, (R, cc)
         assert abs(np.abs(d[:, j]).max() / np.abs(an).max() - 1) < 0.015, R
+
+
+@pytest.mark.parametrize("pml,bound", [(10, 2e-3), (20, 5e-4)])
+def test_pml_absorbs(oracle, pml, bound):
+    """The split-field PML of w_cpml.m (order 2, R0 = 1e-8, wdc_geom.m:98-99)
+    absorbs: traces 10 cells from the PML of a 60 x 60 model equal those of a
+    300 x 300 model (no boundary within reach during the record) to `bound` of
+    the direct wave's peak (measured 5e-4 at 10 cells, 1e-4 at 20)."""
+    from gerjoii_b200.geometry import WGrid, Shot, w_wavelet
+    dx, fo, air, nt = 0.05, 100e6, 10, 600
+
+    def run(m, n, src, recs):
+        dt = WGrid(m=m, n=n, pml=pml, pml_top=pml, air=air, nt=1, dx=dx, dy=dx, dt=1.0).cfl_dt(1.0, 0.95)
+        g = WGrid(m=m, n=n, pml=pml, pml_top=pml, air=air, nt=nt, dx=dx, dy=dx, dt=dt)
+        w = w_wavelet(np.arange(nt) * dt, 1e3, 1 / fo)
+        rec = np.array([g.node(*g.model_node(a, b)) for a, b in recs])
+        return oracle.forward(g, np.ones((m, n)), np.zeros((m, n)), Shot(*g.model_node(*src), w, rec))[0]
+
+    small = run(60, 60, (30, 20), [(30, 50), (50, 20)])
+    big = run(300, 300, (150, 140), [(150, 170), (170, 140)])
+    for j in range(2):
+        assert np.abs(small[:, j] - big[:, j]).max() <= bound * np.abs(big[:, j]).max()
