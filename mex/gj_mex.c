@@ -171,7 +171,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     for (int k = 0; k < ns; ++k) mxFree(recs[k]);
     mxFree(recs); mxFree(shots); mxFree(dobs);
   } else if (!strcmp(cmd, "dc_fwd2_5d") || !strcmp(cmd, "dc_gradient2_5d")) {
-    /* d = gj_mex('dc_fwd2_5d', sigma_robin, dcgrid, AB (ns x 2, 1-based), I, MNcell, kyw_cell, alpha_cell)
+    /* [d, u] = gj_mex('dc_fwd2_5d', sigma_robin, dcgrid, AB (ns x 2, 1-based), I, MNcell, kyw_cell, alpha_cell)
        (alpha_cell = [] has the library compute dc_Lk.m's alphas, gj_dc_alphas)
        [g, d, e] = gj_mex('dc_gradient2_5d', ..., dobs_cell)   (dc_fwd2_5d.m, dc_gradient2_5d.m) */
     const int grad = !strcmp(cmd, "dc_gradient2_5d");
@@ -214,7 +214,12 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     }
     if (!grad) {
       plhs[0] = mxCreateDoubleMatrix(nd, 1, mxREAL);
-      check(gj_dc_forward(ctx(), &g, mxGetPr(prhs[1]), srcs, ns, NULL, mxGetPr(plhs[0]), NULL, NULL));
+      double* u = NULL;
+      if (nlhs > 1) {  /* stacked potentials, n*m per source */
+        plhs[1] = mxCreateDoubleMatrix((size_t)g.n * g.m, ns, mxREAL);
+        u = mxGetPr(plhs[1]);
+      }
+      check(gj_dc_forward(ctx(), &g, mxGetPr(prhs[1]), srcs, ns, NULL, mxGetPr(plhs[0]), u, NULL));
     } else {
       plhs[0] = mxCreateDoubleMatrix(g.n - 2 * g.robin, g.m - g.robin, mxREAL);
       plhs[1] = mxCreateDoubleMatrix(nd, 1, mxREAL);
