@@ -281,3 +281,56 @@ def redesign_sources(srcs, n: int, m: int, DX: float, DZ: float, n_ky: int, dx: 
         al = np.stack([alphas_compact(n, m, DX, DZ, q.a, q.b, ky) for ky in kyw[:, 0]])
         out.append(dataclasses.replace(q, ky_w=kyw, alpha=al))
     return out
+
+
+def binning(x, r) -> np.ndarray:
+    """binning.m: for each value of r, the 1-based index of the nearest entry of
+    the sorted grid x; on a tie the lower index (its forward scan stops at the
+    first entry that is no nearer than the previous one)."""
+    x = np.asarray(x, np.float64)
+    r = np.atleast_1d(np.asarray(r, np.float64))
+    return np.array([int(np.argmin(np.abs(x - v))) + 1 for v in r], np.int64)
+
+
+def electrode_nodes(X, Z, electr_real, ab, mn, robin: int, n: int):
+    """dc_electrodes.m:29-52: electrode numbers (1-based rows of the coordinate
+    table electr_real, columns x and z) to grid nodes.  Coordinates are binned
+    onto the model grid X (lateral) and Z (depth), shifted by the Robin columns,
+    the source pair gets the parity clean (:66-75), and nodes are vectorised as
+    l + n (h - 1) (:76-83) with n the padded lateral size.  Returns 0-based
+    (a, b) and an (nd, 2) array of 0-based (M, N) nodes."""
+    E = np.asarray(electr_real, np.float64).reshape(-1, 2)
+
+    def nodes(nums):
+        nums = np.asarray(nums, np.int64).reshape(-1)
+        l = binning(X, E[nums - 1, 0]) + robin
+        h = binning(Z, E[nums - 1, 1])
+        return l, h
+
+    l, h = nodes(ab)
+    la, lb = clean_electrode(int(l[0]), int(l[1]))
+    a = (la - 1) + n * (int(h[0]) - 1)
+    b = (lb - 1) + n * (int(h[1]) - 1)
+    mn = np.asarray(mn, np.int64).reshape(-1, 2)
+    lm, hm = nodes(mn[:, 0])
+    ln, hn = nodes(mn[:, 1])
+    pairs = np.column_stack([(lm - 1) + n * (hm - 1), (ln - 1) + n * (hn - 1)])
+    return a, b, pairs
+
+
+def sources_from_survey(gathers, ky_w, X, Z, electr_real, robin: int, n: int, m: int, DX: float, DZ: float) -> list:
+    """DcSource list of a field survey: the gathers of s_i_r_d_std.mat
+    (matio.load_dc_survey), the per-source wavenumbers of ky_w.mat (n_ky x 2 x
+    nsrc, one shared when nsrc = 1) and the electrode coordinate table, as
+    dc_load2_5d.m:8-33 and dc_electrodes.m assemble them; observed data go to
+    d_obs and the Robin coefficients are computed for each source."""
+    kw = np.asarray(ky_w, np.float64)
+    if kw.ndim == 2:
+        kw = kw[:, :, None]
+    out = []
+    for ie, gth in enumerate(gathers):
+        a, b, pairs = electrode_nodes(X, Z, electr_real, gth["ab"], gth["mn"], robin, n)
+        k = kw[:, :, ie if kw.shape[2] > 1 else 0]
+        al = np.stack([alphas_compact(n, m, DX, DZ, a, b, ky) for ky in k[:, 0]])
+        out.append(DcSource(a, b, float(gth["current"]), pairs, k.copy(), al, np.asarray(gth["d"], np.float64)))
+    return out

@@ -68,3 +68,32 @@ def test_v73_files_are_rejected_with_a_clear_error(tmp_path):
     p.write_bytes(hdr.ljust(116, b" ") + b"\x00" * 8 + b"\x00\x02" + b"IM" + b"\x00" * 512)
     with pytest.raises(ValueError, match="v7.3"):
         matio.load_radargram(str(p))
+
+
+def test_dc_survey_files_to_sources(tmp_path):
+    """s_i_r_d_std.mat + ky_w.mat + an electrode table -> DcSource list as
+    dc_load2_5d.m and dc_electrodes.m assemble it: binning to the nearest grid
+    coordinate (ties to the lower index), Robin shift, parity clean of the
+    source pair only, vectorised nodes l + n (h - 1), data into d_obs."""
+    from gerjoii_b200 import dc
+    X = np.arange(40) * 0.25
+    Z = np.arange(12) * 0.25
+    robin = 1
+    n, m = 40 + 2 * robin, 12 + robin
+    elec = np.column_stack([0.25 * np.arange(2, 38, 2) + 0.01, np.zeros(18)])  # just off the grid points
+    assert list(dc.binning(X, [0.125, 0.126, 0.124, -1.0, 99.0])) == [1, 2, 1, 1, 40]
+    gathers = [{"ab": np.array([3, 5]), "current": 0.7, "mn": np.array([[7, 8], [9, 10]]),
+                "d": np.array([0.1, 0.05]), "std": np.array([0.01, 0.01])}]
+    kw = np.column_stack([np.geomspace(1e-3, 0.5, 6), np.ones(6)])
+    matio.save_dc_survey(str(tmp_path / "s.mat"), gathers)
+    matio.save_ky_w(str(tmp_path / "k.mat"), kw)
+    srcs = dc.sources_from_survey(matio.load_dc_survey(str(tmp_path / "s.mat")), matio.load_ky_w(str(tmp_path / "k.mat")),
+                                  X, Z, elec, robin, n, m, -0.25, 0.25)
+    q = srcs[0]
+    # electrode 3 sits at x = 1.51 -> grid index 7 (1-based), +1 Robin -> 8, even: kept
+    # electrode 5 sits at x = 2.51 -> 11, +1 -> 12, even -> 13 (the -I electrode goes odd)
+    assert (q.a, q.b) == (8 - 1, 13 - 1)
+    # receivers are not cleaned: electrode k -> padded lateral 2k + 2 (1-based) -> node 2k + 1
+    assert q.mn.tolist() == [[15, 17], [19, 21]]
+    assert q.current == 0.7 and np.array_equal(q.d_obs, [0.1, 0.05])
+    assert q.ky_w.shape == (6, 2) and q.alpha.shape == (6, dc.nalpha(n, m))
