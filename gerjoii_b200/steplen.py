@@ -1,6 +1,6 @@
-"""Step length of the radar permittivity update, as the reference chooses it
-around its objective evaluations (w_stepparabola_e.m, w_boundstep2.m,
-w_objs_e.m:24-25).  The trial objectives are forward-only runs of all shots,
+"""Step lengths of the radar permittivity and conductivity updates, as the
+reference chooses them around its objective evaluations (w_stepparabola_e.m,
+w_stepparabola_s.m, w_boundstep2.m, w_objs_e.m:24-25, w_objs_s.m:22-25).  The trial objectives are forward-only runs of all shots,
 which ``Context.w_misfit`` (gj_w_misfit) does on the GPU; this module holds the
 host logic around them.
 
@@ -76,11 +76,37 @@ def stepparabola(eps, g_e, objective: Callable[[float], float], E0: float, eps_m
     return float(step), ke, E
 
 
-def misfit_objective(ctx, grid, eps, sig, shots, d_obs, g_e, misfit=0, precision=0) -> Callable[[float], float]:
-    """The trial objective of w_objs_e.m on the GPU: the summed normalised
-    misfit of all shots for perturb_eps(eps, g_e, ke), one gj_w_misfit call
-    (forward runs only) per trial."""
-    def objective(ke: float) -> float:
-        return float(np.sum(ctx.w_misfit(grid, perturb_eps(eps, g_e, ke), sig, shots, d_obs, misfit=misfit,
-                                          precision=precision)))
+def stepparabola_s(sig, g_s, objective: Callable[[float], float], E0: float, sig_max: float, sig_min: float,
+                   k_s, ksprct_: float, ksprct__: float, nparabo: int) -> tuple[float, np.ndarray, np.ndarray]:
+    """w_stepparabola_s.m: the conductivity's trial steps all lie on the
+    positive side, from ksprct_ to ksprct__ times boundstep2(sig, -g_s)
+    (nparabo + 2 of them); the vertex of the least-squares parabola through
+    them and E0 at ks = 0 is the step, 0 when flat (zero or NaN).  Unlike the
+    permittivity's, a negative vertex is returned as it is (w_stepparabola_s.m
+    only reports it).  `objective(ks)` evaluates perturb_eps(sig, g_s, ks), the
+    same exponential update (w_objs_s.m:22-25)."""
+    kb = boundstep2(sig, -np.asarray(g_s, np.float64), sig_max, sig_min, k_s)
+    ks = np.linspace(kb * ksprct_, kb * ksprct__, nparabo + 2)
+    E = np.array([float(E0)] + [float(objective(float(k))) for k in ks])
+    k = np.concatenate([[0.0], ks])
+    with np.errstate(all="ignore"):
+        p = np.polyfit(k, E, 2)
+        step = -p[1] / (2 * p[0])
+    if not np.isfinite(step) or step == 0:
+        step = 0.0
+    return float(step), k, E
+
+
+def misfit_objective(ctx, grid, eps, sig, shots, d_obs, g, misfit=0, precision=0,
+                     which: str = "eps") -> Callable[[float], float]:
+    """The trial objective of w_objs_e.m (which = "eps") or w_objs_s.m
+    (which = "sig") on the GPU: the summed normalised misfit of all shots with
+    that parameter perturbed as x exp(-k x g), one gj_w_misfit call (forward
+    runs only) per trial."""
+    if which not in ("eps", "sig"):
+        raise ValueError("which must be 'eps' or 'sig'")
+
+    def objective(k: float) -> float:
+        e, s_ = (perturb_eps(eps, g, k), sig) if which == "eps" else (eps, perturb_eps(sig, g, k))
+        return float(np.sum(ctx.w_misfit(grid, e, s_, shots, d_obs, misfit=misfit, precision=precision)))
     return objective

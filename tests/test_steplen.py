@@ -38,3 +38,22 @@ def test_stepparabola_vertex_of_a_quadratic_objective():
     assert step == 0.0
     step, _, _ = steplen.stepparabola(eps, g, lambda k: 1.0 + k, 1.0, 20.0, 1.0, [1e-3, 10.0], 0.5, 0.5, 5)
     assert step == 0.0  # a line: no vertex
+
+
+def test_stepparabola_s_samples_positive_steps_and_keeps_a_negative_vertex():
+    """w_stepparabola_s.m: nparabo + 2 trial steps, all positive (both ends come
+    from boundstep2(sig, -g_s)); the vertex of a quadratic objective is the step,
+    and a negative vertex is returned rather than zeroed."""
+    sig = np.full((4, 4), 0.01)
+    g = np.full((4, 4), 1.0)
+
+    def obj(k, c):
+        return 1.0 + 2.0 * (k - c) ** 2
+
+    step, ks, E = steplen.stepparabola_s(sig, g, lambda k: obj(k, 0.2), obj(0.0, 0.2), 0.1, 1e-4, [1e-2, 1e3],
+                                         0.1, 0.9, 3)
+    assert len(ks) == 6 and ks[0] == 0.0 and (ks[1:] > 0).all()
+    assert abs(step - 0.2) < 1e-9
+    step, _, _ = steplen.stepparabola_s(sig, g, lambda k: obj(k, -0.3), obj(0.0, -0.3), 0.1, 1e-4, [1e-2, 1e3],
+                                        0.1, 0.9, 3)
+    assert abs(step + 0.3) < 1e-9
