@@ -110,3 +110,47 @@ def misfit_objective(ctx, grid, eps, sig, shots, d_obs, g, misfit=0, precision=0
         e, s_ = (perturb_eps(eps, g, k), sig) if which == "eps" else (eps, perturb_eps(sig, g, k))
         return float(np.sum(ctx.w_misfit(grid, e, s_, shots, d_obs, misfit=misfit, precision=precision)))
     return objective
+
+
+def dc_stepparabola(sig, g, objective: Callable[[float], float], E0: float, sig_max: float, sig_min: float,
+                    k_s, kprct_: float, kprct__: float) -> tuple[float, np.ndarray, np.ndarray]:
+    """dc_stepparabola2_5d.m: four trial steps from -kprct_ boundstep2(sig, g)
+    to kprct__ boundstep2(sig, -g) (dc_boundstep2.m is w_boundstep2.m), the
+    vertex of the least-squares parabola through them and E0 at k = 0; 0 when
+    flat (zero or NaN); a negative vertex falls back to the trial step of least
+    objective if that step is positive, else 0.  `objective(k)` evaluates the
+    model sig exp(-k sig g) (dc_objs2_5d.m)."""
+    g = np.asarray(g, np.float64)
+    k_ = -boundstep2(sig, g, sig_max, sig_min, k_s) * kprct_
+    k__ = boundstep2(sig, -g, sig_max, sig_min, k_s) * kprct__
+    ks = np.linspace(k_, k__, 4)
+    E = np.array([float(E0)] + [float(objective(float(k))) for k in ks])
+    k = np.concatenate([[0.0], ks])
+    with np.errstate(all="ignore"):
+        p = np.polyfit(k, E, 2)
+        step = -p[1] / (2 * p[0])
+    if not np.isfinite(step) or step == 0:
+        step = 0.0
+    if step < 0:
+        kb = k[int(np.argmin(E))]
+        step = float(kb) if kb > 0 else 0.0
+    return float(step), k, E
+
+
+def dc_misfit_objective(ctx, sig, robin: int, DX: float, DZ: float, srcs, g, std=None) -> Callable[[float], float]:
+    """The trial objective of dc_objs2_5d.m on the GPU: the model sig (n0 x m0,
+    before the Robin padding) perturbed as sig exp(-k sig g), padded (dc_robin),
+    one gj_dc_forward over the sources, and per source 0.5 sum std e^2 /
+    sum d_obs^2 (dc_E.m with N = diag(std_)), summed over the sources.  `std`
+    is a list of per-datum weights (ones when None)."""
+    from .dc import dc_robin
+
+    def objective(k: float) -> float:
+        d = ctx.dc_forward(dc_robin(perturb_eps(sig, g, k), robin), DX, DZ, robin, srcs)["d"]
+        total = 0.0
+        for j, (q, dj) in enumerate(zip(srcs, d)):
+            e = np.asarray(dj, np.float64) - np.asarray(q.d_obs, np.float64)
+            w = np.ones_like(e) if std is None else np.asarray(std[j], np.float64)
+            total += 0.5 * float(e @ (w * e)) / float(np.asarray(q.d_obs) @ np.asarray(q.d_obs))
+        return total
+    return objective

@@ -57,3 +57,54 @@ def test_stepparabola_s_samples_positive_steps_and_keeps_a_negative_vertex():
     step, _, _ = steplen.stepparabola_s(sig, g, lambda k: obj(k, -0.3), obj(0.0, -0.3), 0.1, 1e-4, [1e-2, 1e3],
                                         0.1, 0.9, 3)
     assert abs(step + 0.3) < 1e-9
+
+
+def test_dc_stepparabola_vertex_and_negative_fallback():
+    """dc_stepparabola2_5d.m: four trials around 0, the parabola vertex of a
+    quadratic objective; a negative vertex falls back to the best positive
+    trial step, or to 0 when the best trial is not positive."""
+    sig = np.full((5, 5), 0.01)
+    g = np.full((5, 5), 1.0)
+
+    def obj(k, c):
+        return 1.0 + 5.0 * (k - c) ** 2
+
+    step, k, E = steplen.dc_stepparabola(sig, g, lambda x: obj(x, 1.0), obj(0.0, 1.0), 0.1, 1e-4, [1e-2, 1e4],
+                                         0.5, 0.5)
+    assert len(k) == 5 and k.min() < 0 < k.max()
+    assert abs(step - 1.0) < 1e-9
+    step, k, E = steplen.dc_stepparabola(sig, g, lambda x: obj(x, -1.0), obj(0.0, -1.0), 0.1, 1e-4, [1e-2, 1e4],
+                                         0.5, 0.5)
+    assert step == 0.0  # vertex at -1, best trial negative
+    # a concave objective has a "vertex" that is a maximum; here on the negative side
+    step, k, E = steplen.dc_stepparabola(sig, g, lambda x: 10.0 - (x + 1.0) ** 2, 10.0 - 1.0, 0.1, 1e-4,
+                                         [1e-2, 1e4], 0.5, 0.5)
+    assert step == float(k[int(np.argmin(E))]) and step > 0
+
+
+def test_dc_misfit_objective_on_the_oracle():
+    """dc_objs2_5d.m's trial objective, with the oracle's direct solves standing
+    in for the GPU context: at k = 0 it is the normalised misfit of the model,
+    0.5 sum e^2 / sum d_obs^2 per source, and data weights scale it."""
+    import np_dc_oracle as dco
+    from dc_cases import small_dc, oracle_forward
+    from gerjoii_b200 import dc as dcm
+
+    case = small_dc(seed=13, pairs=2)
+    sig0 = case["SIG"][case["robin"]:-case["robin"], :-case["robin"]]
+    for q, r in zip(case["srcs"], oracle_forward(dco, case, case["SIG"] * 1.2)):
+        q.d_obs = r[2]
+
+    class Oracle:
+        def dc_forward(self, SIG, DX, DZ, robin, srcs):
+            return {"d": [r[2] for r in oracle_forward(dco, dict(case, srcs=srcs), SIG)]}
+
+    g = np.ones_like(sig0)
+    obj = steplen.dc_misfit_objective(Oracle(), sig0, case["robin"], case["DX"], case["DZ"], case["srcs"], g)
+    ref = sum(0.5 * float((r[2] - q.d_obs) @ (r[2] - q.d_obs)) / float(q.d_obs @ q.d_obs)
+              for q, r in zip(case["srcs"], oracle_forward(dco, case)))
+    assert abs(obj(0.0) - ref) <= 1e-12 * ref
+    w = [np.full(q.nd, 2.0) for q in case["srcs"]]
+    obj2 = steplen.dc_misfit_objective(Oracle(), sig0, case["robin"], case["DX"], case["DZ"], case["srcs"], g, std=w)
+    assert abs(obj2(0.0) - 2 * ref) <= 1e-12 * ref
+    assert np.isfinite(obj(1.0)) and obj(1.0) != obj(0.0)
