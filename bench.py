@@ -5,10 +5,17 @@ Workload (one "step" = one whole FWI gradient over all shots): the 1000 x 400
 radar model at dx = 0.02 m with 30 PML cells and a free top (padded 431 x 1060
 Yee grid), 6000 time steps, 250 MHz Ricker source, 30 surface sources and 200
 receivers, five-layer + blob permittivity, layered conductivity; seeded
-synthetic data (no field data).  Each step runs, for all 30 shots at once, the
-forward solve with checkpoints every K steps, the residual and misfit, the
-segment-by-segment recompute and the exact adjoint with the imaging condition
-(Kahan-compensated FP32 sums), and returns the epsilon and sigma gradients.
+synthetic data (no field data).  Each step runs the whole gradient of the 30
+shots: the forward solve (shots batched per launch; the u history kept in HBM
+in shot groups when it fits, else checkpoints every K steps and a segment
+recompute), the residual and misfit, the exact adjoint with the imaging
+condition (Kahan-compensated FP32 sums) and the PML-coefficient terms of the
+edge cells, and returns the epsilon and sigma gradients.
+
+The timed region runs with kernel timing off; the per-kernel figures and the
+roofline come from one more step run afterwards with sampled CUDA events on.
+A cfg3 leg times the checkpointed single-shot gradient on the 2000 x 800 grid
+(8000 steps, checkpoints every 90 steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -61,10 +68,12 @@ def workload(args, world=1):
     g = p.grid
     cfg = {"workload": f"radar FWI gradient, {g.n}x{g.m} model (padded {g.NX}x{g.NY} Yee grid), "
                        f"{args.nshots} shots x {len(p.shots[0].rec)} receivers, {g.nt} steps, FP32, "
-                       f"{args.mode} adjoint, checkpointed",
+                       f"{args.mode} adjoint",
            "grid": [g.NX, g.NY], "model": [g.m, g.n], "nt": g.nt, "shots": args.nshots,
            "receivers": len(p.shots[0].rec), "adjoint": args.mode,
-           "l2": "working set (fields, checkpoints, history ring) larger than the 126 MB L2; no flush needed"}
+           "l2": "working set (fields, checkpoints, history ring) larger than the 126 MB L2; no flush needed",
+           "memory_plan": "u history (and the PML band history of the exact adjoint) in HBM in shot groups when "
+                          "it fits the memory budget, else checkpoints + segment recompute"}
     return p, cfg
 
 
@@ -187,6 +196,45 @@ class CpuPool:
         self.pool.join()
 
 
+_DC_CASE = {}
+
+
+def _dc_cpu_worker(job):
+    """One DC source (all its wavenumbers) through the oracle's FP64 sparse
+    direct solves, in a worker process (one source per host core)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import np_dc_oracle as dco
+    from gerjoii_b200 import synth
+    n_sources, k = job
+    if n_sources not in _DC_CASE:
+        _DC_CASE[n_sources] = synth.cfg5(n_sources=n_sources)
+    c = _DC_CASE[n_sources]
+    q = c["srcs"][k]
+    n, m = c["n"], c["m"]
+    t0 = time.perf_counter()
+    al = [dco.alphas(n, m, c["DX"], c["DZ"], dco.source_vector(n, m, q.a, q.b)[:n], ky) for ky in q.ky_w[:, 0]]
+    dco.dc_fwd2_5d(c["SIG"], c["DX"], c["DZ"], dco.source_vector(n, m, q.a, q.b), al, q.ky_w,
+                   dco.measuring_operator(n, m, q.mn))
+    return time.perf_counter() - t0
+
+
+def dc_cpu_baseline(n_sources, threads):
+    """DC forward solves/s of the oracle on the host cores: `threads` spawned
+    workers, one source (x its wavenumbers) each, as BASELINE plans (one
+    source per core).  The first round starts the workers and builds the
+    survey in each; the second is timed."""
+    import multiprocessing as mp
+    pool = mp.get_context("spawn").Pool(threads)
+    jobs = [(n_sources, k % n_sources) for k in range(threads)]
+    pool.map(_dc_cpu_worker, jobs, chunksize=1)
+    t0 = time.perf_counter()
+    pool.map(_dc_cpu_worker, jobs, chunksize=1)
+    dt = time.perf_counter() - t0
+    pool.close()
+    pool.join()
+    return dt
+
+
 def dc_leg(ctx, n_sources=200):
     """Timed DC forward + sensitivity on the survey; accuracy on one source."""
     import torch
@@ -221,6 +269,12 @@ def dc_leg(ctx, n_sources=200):
                                     dco.measuring_operator(n, m, q.mn))
     t_cpu = time.perf_counter() - t0
     rel = float(np.linalg.norm(fw["d"][0] - d_ref) / np.linalg.norm(d_ref))
+    threads = min(os.cpu_count() or 1, 32)
+    t_par = dc_cpu_baseline(n_sources, threads)
+    dc_cpu = {"forward_solves_per_s": threads * nky / t_par, "cores": threads, "kind": "port",
+              "sample": f"{threads} sources x {nky} ky on {threads} worker processes (one source each), FP64 "
+                        f"sparse direct solves (scipy SuperLU) of the restated operator, operator assembly "
+                        f"included ({t_par:.1f} s); one source alone on one core: {nky / t_cpu:.2f} solves/s"}
     # per-kernel device time of the timed forward; algorithmic work per system:
     # factor b(b+1)/2 FMA per unknown, substitution reads the FP64 factor twice
     # (N rounded up to 32 columns of b+1 rounded up to even entries) and moves
@@ -252,10 +306,73 @@ def dc_leg(ctx, n_sources=200):
             "max_rel_residual": max(fw["rel_residual"], gr["rel_residual"]),
             "data_rel_err_vs_fp64_direct_solve": rel,
             "kernels": kern,
-            "cpu_baseline": {"forward_solves_per_s": nky / t_cpu, "cores": 1, "kind": "port",
-                             "sample": f"1 source x {nky} ky, FP64 sparse direct solves (scipy SuperLU) of the "
-                                       "restated operator, operator assembly included"},
+            "cpu_baseline": dc_cpu,
             "path": "gj_dc_forward / gj_dc_gradient, host buffers"}
+
+
+def cfg3_leg(ctx):
+    """cfg3: the single-shot FP32 exact gradient on the 2000 x 800 grid (30
+    PML cells, free top, 8000 steps, 250 MHz), with checkpoints every 90
+    steps and the segment recompute (the ~51 GB u history is never held).
+    Device-resident inputs, one call timed with CUDA events, kernel timing
+    off; then one instrumented call for the per-kernel averages.  Algorithmic
+    bytes per shot-gradient (shot-cells of the padded grid per step): forward
+    32 B + recompute 32 B + adjoint 32 B + imaging, u slots and adjoint ring
+    per model cell."""
+    import torch
+    from gerjoii_b200 import synth
+    from gerjoii_b200 import _native as N
+    p = synth.cfg3()
+    g = p.grid
+    dev = torch.device("cuda", 0)
+    d = ctx.w_forward(g, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F32)["d"]
+    dobs_t = torch.tensor(np.stack([x.T for x in d]), dtype=torch.float32, device=dev).contiguous()
+    eps_t = torch.tensor(np.asfortranarray(p.eps0).ravel(order="F"), dtype=torch.float32, device=dev)
+    sig_t = torch.tensor(np.asfortranarray(p.sig0).ravel(order="F"), dtype=torch.float32, device=dev)
+    ge = torch.zeros(g.m * g.n, dtype=torch.float32, device=dev)
+    gs = torch.zeros_like(ge)
+    o = N.OptsC()
+    o.ckpt_every = 90
+    st = torch.cuda.current_stream(dev)
+    run = lambda: ctx.w_gradient_dev(g, eps_t, sig_t, p.shots, dobs_t, ge, gs, mode=N.GJ_ADJ_EXACT, opts=o,
+                                     stream=st.cuda_stream)
+    ctx.set_kernel_timing(False)
+    run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    run()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    ctx.set_kernel_timing(True)
+    run()
+    torch.cuda.synchronize()
+    ctx.set_kernel_timing(True)
+    run()
+    torch.cuda.synchronize()
+    kt = {k: ctx.kernel_time(k) for k in ("fwd_step", "adj_step", "image")}
+    ctx.set_kernel_timing(False)
+    cells, mn = g.NX * g.NY, g.m * g.n
+    steps = kt["fwd_step"]["shot_launches"] + kt["adj_step"]["shot_launches"]
+    byts = (kt["fwd_step"]["shot_launches"] * (cells * 32.0 + mn * 4.0)
+            + kt["adj_step"]["shot_launches"] * (cells * 32.0 + mn * 4.0)
+            + kt["adj_step"]["shot_launches"] * mn * 8.0 + kt["image"]["shot_launches"] * mn * 36.0)
+    pk, pk_src = peaks()
+    per = {k: {"avg_launch_us": v["avg_us"], "launches": v["launches"]} for k, v in kt.items()}
+    return {"workload": f"radar FWI gradient, 1 shot, {g.n}x{g.m} model (padded {g.NX}x{g.NY}), {g.nt} steps, "
+                        "FP32, exact adjoint, checkpoints every 90 steps + segment recompute",
+            "shot_gradients_per_s": 1e3 / ms, "ms_per_gradient": ms,
+            "gcell_updates_per_s": steps * cells / (ms / 1e3) / 1e9,
+            "forward_plus_recompute_steps": kt["fwd_step"]["shot_launches"], "adjoint_steps": kt["adj_step"]["shot_launches"],
+            "recompute_overhead": kt["fwd_step"]["shot_launches"] / g.nt - 1.0,
+            "roofline": {"bound": "hbm", "achieved": byts / (ms / 1e3) / 1e9, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": byts / (ms / 1e3) / 1e9 / pk["hbm_gbs"], "peak_source": pk_src,
+                         "algorithmic_bytes_per_gradient": byts,
+                         "units": "per shot-step 32 B x NX*NY (forward, recompute, adjoint) + per model cell 4 B "
+                                  "(u slot, adjoint ring) + 8 B per imaged step + 36 B per imaging pass"},
+            "kernels": per}
 
 
 def cfg4_leg(args):
@@ -392,15 +509,14 @@ def main():
         if world > 1:
             shard.allreduce_sum([ge_t, gs_t])
 
-    # kernel timing is on during the warm-up as well: the CUDA graphs captured
-    # there (one per shot group, with the sampled timing events) are the ones
-    # the timed steps replay; switching it on again only clears the counters
-    ctx.set_kernel_timing(True)
+    # the warm-up captures the CUDA graphs (one per shot group) that the timed
+    # steps replay; kernel timing stays off for both, so the timed graphs hold
+    # no event nodes
+    ctx.set_kernel_timing(False)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     clocks = Clocks(local)
-    ctx.set_kernel_timing(True)
     launches = 0
     if world > 1:
         dist.barrier()
@@ -418,6 +534,18 @@ def main():
         dist.barrier()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
+    # instrumented pass after the timed region: one step (after one more that
+    # captures the graphs with the timing events) with CUDA events around
+    # every 8th launch of each step kernel; per-kernel averages and the
+    # roofline come from here
+    ctx.set_kernel_timing(True)
+    step()
+    torch.cuda.synchronize()
+    ctx.set_kernel_timing(True)  # clears the counters
+    isteps = 1
+    for _ in range(isteps):
+        step()
+    torch.cuda.synchronize()
     ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step", "image")}
     ktimes = {k: v for k, v in ktimes.items() if v["launches"] > 0}
     ctx.set_kernel_timing(False)
@@ -429,8 +557,9 @@ def main():
     value = shots_total / (ms / 1e3)
     cells = g.NX * g.NY
     mn = g.m * g.n
-    # cell-updates in the timed region: every forward, recompute and adjoint launch
-    upd = sum(ktimes[k]["shot_launches"] for k in ktimes if k != "image") * cells * world
+    # cell-updates in the timed region: every forward, recompute and adjoint
+    # launch (counted per step in the instrumented pass, which runs the same plan)
+    upd = sum(ktimes[k]["shot_launches"] for k in ktimes if k != "image") / isteps * args.steps * cells * world
     gcell = upd / (ms / 1e3) / 1e9
     # Algorithmic DRAM bytes of each kernel kind over the timed region.
     #  fwd_step (k_fwdw): read Ez, Hx, Hy, Ceze, Cezhy + write Ez, Hx, Hy = 32 B per
@@ -459,7 +588,7 @@ def main():
         tot_s = kt["avg_us"] * kt["launches"] / 1e6
         b = alg[kk](kt)
         kern[kk] = {"kernel": kname[kk], "launches": kt["launches"], "timed_launches": kt["sampled"],
-                    "avg_launch_us": kt["avg_us"], "ms_per_step": tot_s * 1e3 / args.steps,
+                    "avg_launch_us": kt["avg_us"], "ms_per_step": tot_s * 1e3 / isteps,
                     "algorithmic_bytes_per_launch": b / max(kt["launches"], 1),
                     "achieved_gbs": b / tot_s / 1e9 if tot_s > 0 else 0.0,
                     "frac_of_measured_hbm": (b / tot_s / 1e9) / pk["hbm_gbs"] if tot_s > 0 else 0.0}
@@ -478,14 +607,16 @@ def main():
                       "adj_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n adjoint-field ring write",
                       "image": "per imaged shot-step 8 B x m*n, per shot-launch 36 B x m*n",
                       "ref_step": "per shot: 32 B x NX*NY cells + 48 B x m*n (4 history reads, 4 sums r/w)"}[dom],
-            "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / ms}
+            "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / isteps / (ms / args.steps),
+            "pass": "separate instrumented step after the timed region (CUDA events around every 8th launch of "
+                    "each step kernel, also inside the graphs); the timed region itself runs without events"}
     line = {"metric": METRIC, "value": value, "unit": "shot-gradients/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded layered model, observed traces modelled on the device)",
             "config": cfg, "gcell_updates_per_s": gcell, "gpu_launches": launches,
             "clocks": clk, "roofline": roof,
-            "kernel_ms_per_step": {k: v["avg_us"] * v["launches"] / 1e3 / args.steps for k, v in ktimes.items()},
+            "kernel_ms_per_step": {k: v["avg_us"] * v["launches"] / 1e3 / isteps for k, v in ktimes.items()},
             "kernels": kern}
 
     if rank == 0 and not args.no_extras:
@@ -546,6 +677,7 @@ def main():
         # solve of the oracle on one source
         if not args.no_dc:
             line["dc"] = dc_leg(ctx)
+        line["cfg3"] = cfg3_leg(ctx)
         # CPU baseline (oracle) on the host cores, bounded sample
         threads = min(os.cpu_count() or 1, 32)
         nt_s = max(50, min(args.nt, 150))

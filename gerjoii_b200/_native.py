@@ -92,11 +92,17 @@ SIGNATURES = {
     "gj_w_gradient": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _I,
                            C.POINTER(OptsC), _DP, _DP, _DP, _DP, _DP]),
     "gj_w_misfit": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _DP]),
+    "gj_w_misfit_trials": (_I, [_VP, C.POINTER(GridC), _I, _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I,
+                                C.POINTER(OptsC), _DP]),
+    "gj_w_backward": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, C.POINTER(OptsC),
+                           _DP, _DP]),
     "gj_w_grad": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _DP, _DP, _DP, _DP]),
     "gj_w_gradient_dev": (_I, [_VP, C.POINTER(GridC), _I, _VP, _VP, C.POINTER(ShotC), _I, _VP, _I, _I,
                                C.POINTER(OptsC), _VP, _VP, _DP, _VP]),
     "gj_dc_forward": (_I, [_VP, C.POINTER(DcGridC), _DP, C.POINTER(DcSrcC), _I, C.POINTER(DcOptsC), _DP, _DP,
                            C.POINTER(DcStatsC)]),
+    "gj_dc_forward_k": (_I, [_VP, C.POINTER(DcGridC), _DP, C.POINTER(DcSrcC), _I, C.POINTER(DcOptsC), _DP, _DP,
+                             _DP, C.POINTER(DcStatsC)]),
     "gj_dc_gradient": (_I, [_VP, C.POINTER(DcGridC), _DP, C.POINTER(DcSrcC), _I, C.POINTER(DcOptsC), _DP, _DP, _DP,
                             _DP, C.POINTER(DcStatsC)]),
     "gj_dc_alphas": (_I, [C.POINTER(DcGridC), C.c_long, C.c_long, _DP, _DP]),
@@ -270,6 +276,27 @@ class Context:
             res["d"], res["e"] = outd, oute
         return res
 
+    def w_backward(self, g, eps, sig, shots, e, mode=GJ_ADJ_EXACT, precision=GJ_F32, opts=None):
+        """gj_w_backward: the adjoint of the forward map applied to the given
+        adjoint sources e (list of nt x nr arrays, one per shot): g_eps, g_sig
+        (summed over shots, or per shot with opts.per_shot)."""
+        sp = _ShotPack(shots, g.nt)
+        o = opts or OptsC()
+        per = len(shots) if o.per_shot else 1
+        ge = np.zeros(per * g.m * g.n, np.float64)
+        gs = np.zeros_like(ge)
+        ea = np.concatenate([_f(x).ravel(order="F") for x in e])
+        if ea.size != sum(g.nt * len(r) for r in sp.rec):
+            raise ValueError("e does not match the shots' receivers")
+        gc = grid_c(g)
+        self._check(self.lib.gj_w_backward(self.h, C.byref(gc), precision, _dp(_f(eps)), _dp(_f(sig)), sp.arr, sp.n,
+                                           _dp(ea), int(mode), C.byref(o), _dp(ge), _dp(gs)))
+        if per == 1:
+            return {"g_eps": ge.reshape((g.m, g.n), order="F"), "g_sig": gs.reshape((g.m, g.n), order="F")}
+        mn = g.m * g.n
+        return {"g_eps": np.stack([ge[k * mn:(k + 1) * mn].reshape((g.m, g.n), order="F") for k in range(per)]),
+                "g_sig": np.stack([gs[k * mn:(k + 1) * mn].reshape((g.m, g.n), order="F") for k in range(per)])}
+
     def w_grad(self, g, eps, sig, shot, e, u, precision=GJ_F32):
         """w_grad.m for one shot: (g, a_max)."""
         sp = _ShotPack([shot], g.nt)
@@ -300,18 +327,23 @@ class Context:
             arr[k].d_obs = do.ctypes.data_as(_DP) if do is not None else None
         return arr, keep
 
-    def dc_forward(self, sigma_robin, dx, dz, robin, srcs, opts=None, want_u=False):
-        """Data per source (list of nd arrays), optional stacked u (nsrc x n x m), stats."""
+    def dc_forward(self, sigma_robin, dx, dz, robin, srcs, opts=None, want_u=False, want_uk=False):
+        """Data per source (list of nd arrays), optional stacked u (nsrc x n x m),
+        optional per-wavenumber u_k (nsrc x N x n_ky, N = n*m in the vectorised
+        order l + h*n of dc_fwd2_5d.m:61), stats."""
         n, m = sigma_robin.shape
-        g = DcGridC(n, m, robin, len(srcs[0].ky_w), dx, dz)
+        nky = len(srcs[0].ky_w)
+        g = DcGridC(n, m, robin, nky, dx, dz)
         arr, keep = self._dc_pack(srcs, False)
         nd = sum(q.nd for q in srcs)
         d = np.zeros(max(nd, 1))
         u = np.zeros(len(srcs) * n * m) if want_u else None
+        uk = np.zeros(len(srcs) * nky * n * m) if want_uk else None
         st = DcStatsC()
         sg = np.asfortranarray(sigma_robin, np.float64)
-        self._check(self.lib.gj_dc_forward(self.h, C.byref(g), _dp(sg), arr, len(srcs),
-                                           C.byref(opts) if opts else None, _dp(d), _dp(u), C.byref(st)))
+        self._check(self.lib.gj_dc_forward_k(self.h, C.byref(g), _dp(sg), arr, len(srcs),
+                                             C.byref(opts) if opts else None, _dp(d), _dp(u), _dp(uk),
+                                             C.byref(st)))
         out, o = [], 0
         for q in srcs:
             out.append(d[o:o + q.nd].copy())
@@ -319,6 +351,8 @@ class Context:
         res = {"d": out, "iters": st.max_iterations, "rel_residual": st.max_rel_residual}
         if want_u:
             res["u"] = u.reshape((len(srcs), m, n)).transpose(0, 2, 1)
+        if want_uk:
+            res["u_k"] = uk.reshape((len(srcs), nky, n * m)).transpose(0, 2, 1)
         return res
 
     def dc_gradient(self, sigma_robin, dx, dz, robin, srcs, opts=None):
@@ -353,6 +387,26 @@ class Context:
         self._check(self.lib.gj_w_misfit(self.h, C.byref(gc), precision, _dp(e), _dp(s_), sp.arr, sp.n, _dp(ob),
                                           misfit_kind(misfit), _dp(out)))
         return out
+
+    def w_misfit_trials(self, g, eps_list, sig_list, shots, dobs, misfit=GJ_MISFIT_L2, precision=GJ_F32,
+                        filt=None, steep=0):
+        """gj_w_misfit_trials: misfits (ntrial x nshots) of several trial
+        models; filt = (f_low, f_high) band-filters both trace sets first
+        (w_objs_e.m:33-36)."""
+        sp = _ShotPack(shots, g.nt)
+        gc = grid_c(g)
+        ob = np.concatenate([_f(d).ravel(order="F") for d in dobs])
+        nt_ = len(eps_list)
+        e = np.concatenate([_f(x).ravel(order="F") for x in eps_list])
+        s_ = np.concatenate([_f(x).ravel(order="F") for x in sig_list])
+        o = OptsC()
+        if filt is not None:
+            o.filt_low, o.filt_high = filt
+            o.filt_steep = steep
+        out = np.zeros(nt_ * len(shots))
+        self._check(self.lib.gj_w_misfit_trials(self.h, C.byref(gc), precision, nt_, _dp(e), _dp(s_), sp.arr, sp.n,
+                                                _dp(ob), misfit_kind(misfit), C.byref(o), _dp(out)))
+        return out.reshape(nt_, len(shots))
 
     def w_gradient_dev(self, g, eps_t, sig_t, shots, dobs_t, ge_t, gs_t, mode=GJ_ADJ_REFERENCE,
                        misfit=GJ_MISFIT_L2, opts=None, stream=0):

@@ -90,12 +90,31 @@ gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precisi
                         o, g_eps, g_sig, false, misfit_out, d_out, e_out, 0);
 }
 
+gj_status gj_w_backward(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const double* eps_r,
+                        const double* sigma, const gj_w_shot* shots, int nshots, const double* e, gj_adj_mode mode,
+                        const gj_w_opts* opts, double* g_eps, double* g_sig) {
+  GJ_TRY(guard_ctx(ctx));
+  if (!grid) return ctx->c.err.set(GJ_EINVAL, "null grid");
+  gj_w_opts o{};
+  if (opts) o = *opts;
+  return gj::w_gradient(ctx->c, *grid, precision, eps_r, sigma, false, shots, nshots, e, false, mode, GJ_MISFIT_L2,
+                        o, g_eps, g_sig, false, nullptr, nullptr, nullptr, 0, true);
+}
+
 gj_status gj_w_misfit(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const double* eps_r,
                       const double* sigma, const gj_w_shot* shots, int nshots, const double* d_obs,
                       gj_misfit_kind misfit, double* misfit_out) {
   GJ_TRY(guard_ctx(ctx));
   if (!grid) return ctx->c.err.set(GJ_EINVAL, "null grid");
   return gj::w_misfit(ctx->c, *grid, precision, eps_r, sigma, shots, nshots, d_obs, misfit, misfit_out);
+}
+
+gj_status gj_w_misfit_trials(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, int ntrial,
+                             const double* eps_r, const double* sigma, const gj_w_shot* shots, int nshots,
+                             const double* d_obs, gj_misfit_kind misfit, const gj_w_opts* opts, double* misfit_out) {
+  GJ_TRY(guard_ctx(ctx));
+  if (!grid) return ctx->c.err.set(GJ_EINVAL, "null grid");
+  return gj::w_misfit(ctx->c, *grid, precision, eps_r, sigma, shots, nshots, d_obs, misfit, misfit_out, ntrial, opts);
 }
 
 gj_status gj_w_gradient_dev(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const void* eps_r_dev,
@@ -126,6 +145,17 @@ gj_status gj_dc_forward(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma
   gj_dc_opts o{};
   if (opts) o = *opts;
   return gj::dc_run(ctx->c, *grid, sigma, srcs, nsrc, false, o, d_out, nullptr, u_out, nullptr, nullptr, stats);
+}
+
+gj_status gj_dc_forward_k(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma, const gj_dc_src* srcs,
+                          int nsrc, const gj_dc_opts* opts, double* d_out, double* u_out, double* uk_out,
+                          gj_dc_stats* stats) {
+  GJ_TRY(guard_ctx(ctx));
+  if (!grid) return ctx->c.err.set(GJ_EINVAL, "null grid");
+  gj_dc_opts o{};
+  if (opts) o = *opts;
+  return gj::dc_run(ctx->c, *grid, sigma, srcs, nsrc, false, o, d_out, nullptr, u_out, nullptr, nullptr, stats,
+                    uk_out);
 }
 
 gj_status gj_dc_gradient(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma, const gj_dc_src* srcs, int nsrc,

@@ -163,7 +163,7 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
 template <class TF>
 static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_src* srcs, int nsrc,
                           bool grad, const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
-                          double* misfit_out, gj_dc_stats* stats) {
+                          double* misfit_out, gj_dc_stats* stats, double* uk_out) {
   Err& err = c.err;
   if (!sigma || !srcs || nsrc < 1) return err.set(GJ_EINVAL, "null sigma/sources or nsrc < 1");
   if (gg.n < 3 || gg.m < 3 || gg.n_ky < 1 || gg.robin < 0 || 2 * gg.robin >= gg.n || gg.robin >= gg.m)
@@ -303,6 +303,10 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
     it_max = std::max(it_max, iters); rel_max = std::max(rel_max, rel);
     GJ_CUDA(err, cudaMemcpyAsync(U, X, vn * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    // per-wavenumber potentials u_k of the batch's sources: [source][ky][node], the
+    // column-major N x n_ky u_k of dc_fwd2_5d.m:61 per source
+    if (uk_out)
+      GJ_CUDA(err, cudaMemcpyAsync(uk_out + size_t(sys0) * N, U, vn * sizeof(double), cudaMemcpyDeviceToHost, st));
     k_dc_data<<<dim3(4, nsb), 256, 0, st>>>(N, nky, s0, nsb, P.mnoff.as<long>(), P.mnbuf.as<long>(), P.wts.as<double>(),
                                              U, P.dbuf.as<double>());
     ++c.launches;
@@ -376,10 +380,10 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
 
 gj_status dc_run(Ctx& c, const gj_dc_grid& gg, const double* sigma, const gj_dc_src* srcs, int nsrc, bool grad,
                  const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
-                 double* misfit_out, gj_dc_stats* stats) {
+                 double* misfit_out, gj_dc_stats* stats, double* uk_out) {
   if (o.factor_fp32)
-    return dc_run_t<float>(c, gg, sigma, srcs, nsrc, grad, o, d_out, e_out, u_out, g_out, misfit_out, stats);
-  return dc_run_t<double>(c, gg, sigma, srcs, nsrc, grad, o, d_out, e_out, u_out, g_out, misfit_out, stats);
+    return dc_run_t<float>(c, gg, sigma, srcs, nsrc, grad, o, d_out, e_out, u_out, g_out, misfit_out, stats, uk_out);
+  return dc_run_t<double>(c, gg, sigma, srcs, nsrc, grad, o, d_out, e_out, u_out, g_out, misfit_out, stats, uk_out);
 }
 
 }  // namespace gj

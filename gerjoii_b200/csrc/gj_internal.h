@@ -178,9 +178,11 @@ gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* 
                      const void* sig, bool dev_inputs, const gj_w_shot* shots, int nshots,
                      const void* d_obs, bool dev_dobs, gj_adj_mode mode, gj_misfit_kind mk,
                      const gj_w_opts& o, void* g_eps, void* g_sig, bool dev_out,
-                     double* misfit_out, double* d_out, double* e_out, cudaStream_t stream);
+                     double* misfit_out, double* d_out, double* e_out, cudaStream_t stream,
+                     bool e_given = false);
 gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
-                   const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out);
+                   const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out,
+                   int ntrial = 1, const gj_w_opts* opts = nullptr);
 gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps,
                       const double* sig, const gj_w_shot& shot, const double* e, const double* u,
                       double* gout, double* amax);
@@ -188,6 +190,6 @@ gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const doubl
 // DC entry point implemented in dc_solver.cu.
 gj_status dc_run(Ctx& c, const gj_dc_grid& g, const double* sigma, const gj_dc_src* srcs, int nsrc, bool grad,
                  const gj_dc_opts& o, double* d_out, double* e_out, double* u_out, double* g_out,
-                 double* misfit_out, gj_dc_stats* stats);
+                 double* misfit_out, gj_dc_stats* stats, double* uk_out = nullptr);
 
 }  // namespace gj

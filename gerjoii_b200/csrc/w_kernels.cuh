@@ -22,6 +22,7 @@ enum Field { F_EZ = 0, F_HX = 1, F_HY = 2, F_EZX = 3, F_EZY = 4, NFIELDS = 5 };
 template <class T>
 struct WDev {
   int NX, NY, ld, P, Pt, m, n, di0, dj0;
+  int hr0, hld;            // rows [hr0, hr0 + hld) of the domain-node layout (the model rows, 4-aligned)
   int ei0, ei1, ej0, ej1;  // interior Ez nodes (w_solve.m:201)
   int hyi0, hyi1;          // interior Hy rows (w_solve.m:146)
   int hxj0, hxj1;          // interior Hx columns (w_solve.m:144)
@@ -31,6 +32,13 @@ struct WDev {
   const T* chy;            // Cezhy, interior nodes
   const T* ax; const T* bx; const T* ay; const T* by;      // split-field PML (band nodes)
   const T* hxa; const T* hxb; const T* hya; const T* hyb;  // H in the PML strips
+  // Band frame (w_band.cuh): the PML nodes whose update coefficients depend on
+  // the edge-replicated eps_r, stored per time step in two row-contiguous
+  // rectangles: lateral (rows [0, bRB), columns [0, P] and [NY-P, NY]; planes
+  // Ezx, Ezy, Hx) and bottom (rows [bR0, bRB), columns [0, NY]; planes Ezx,
+  // Ezy, Hy).  E planes of rows >= bR0 live in the bottom rectangle.
+  int bR0, bRB, bBh;       // bottom rows [bR0, bRB) (multiples of 4), bBh = bRB - bR0
+  long bLsz, bBsz, bsz;    // lateral plane, bottom plane, whole slot (3 bLsz + 3 bBsz)
 };
 
 // Per-launch arguments of the fused step kernels.
@@ -56,6 +64,7 @@ struct StepArgs {
   const T* uk;                            // u(k) slot
   T* acc; size_t astride;                 // accumulators [shot][4][dstride]: sumE, compE, sumS, compS
   int kahan;
+  T* band;             // ring forward: band history slot of this step (w.bsz per shot), or nullptr
 };
 
 __device__ __forceinline__ size_t nidx(int i, int j, int ld) { return size_t(i) + size_t(j) * size_t(ld); }
@@ -278,24 +287,40 @@ __global__ void k_inject_add(T* state, size_t sstride, const long* rec, int nr, 
 }
 
 // History slots and imaging accumulators use the "domain-node" layout: per
-// shot ld x n elements, element (i, j) of a model column j in [dj0, dj0+n) at
-// (j - dj0)*ld + i, so the marching kernels read and write them with the same
+// shot hld x n elements, element (i, j) of a model column j in [dj0, dj0+n)
+// and a row i in [hr0, hr0 + hld) at (j - dj0)*hld + (i - hr0).  hr0 and hld
+// are multiples of 4, so a lane's 16-byte row vector is either wholly inside
+// or wholly outside, and the kernels read and write the layout with the same
 // aligned vector accesses as the fields.  Rows outside the model are unused.
-__device__ __forceinline__ size_t dnode(int i, int j, int ld, int dj0) {
-  return size_t(j - dj0) * size_t(ld) + size_t(i);
+template <class T>
+__device__ __forceinline__ size_t dnode(const WDev<T>& w, int i, int j) {
+  return size_t(j - w.dj0) * size_t(w.hld) + size_t(i - w.hr0);
 }
+template <class T>
+__device__ __forceinline__ bool drow(const WDev<T>& w, int i) { return i >= w.hr0 && i < w.hr0 + w.hld; }
 
 // Copies the model columns of Ez (state) into a history slot (the checkpoint's u).
 template <class T>
 __global__ void k_domain_copy(const WDev<T> w, const T* state, size_t sstride, T* hist,
                               size_t hstride, int nshots) {
-  const size_t dn = size_t(w.ld) * w.n;
+  const size_t dn = size_t(w.hld) * w.n;
   const int s = blockIdx.y;
   if (s >= nshots) return;
   for (size_t q = threadIdx.x + size_t(blockIdx.x) * blockDim.x; q < dn; q += size_t(blockDim.x) * gridDim.x) {
-    const int I = int(q % w.ld), b = int(q / w.ld);
+    const int I = w.hr0 + int(q % w.hld), b = int(q / w.hld);
     hist[size_t(s) * hstride + q] = state[size_t(s) * sstride + nidx(I, w.dj0 + b, w.ld)];
   }
+}
+
+// Counts the non-finite values of x[0, n) into *count (NaN / Inf detection of
+// results; the reference's caller zeroes NaN gradients, w_update_e.m:131-137).
+template <class T>
+__global__ void k_count_nonfinite(const T* x, size_t n, unsigned* count) {
+  unsigned c = 0;
+  for (size_t i = threadIdx.x + size_t(blockIdx.x) * blockDim.x; i < n; i += size_t(blockDim.x) * gridDim.x)
+    c += isfinite(x[i]) ? 0u : 1u;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
 
 // Final gradient: out[p] = scale(p) * sum over shots of acc, in double.
@@ -307,7 +332,7 @@ __global__ void k_finish(const WDev<T> w, const T* acc, size_t astride, int nsho
                          int kind, double dt, double eps0, const double* eps_m, const double* sig_m,
                          double* geps, double* gsig) {
   const size_t mn = size_t(w.m) * w.n;
-  const size_t dn = size_t(w.ld) * w.n;
+  const size_t dn = size_t(w.hld) * w.n;
   for (size_t p = threadIdx.x + size_t(blockIdx.x) * blockDim.x; p < mn; p += size_t(blockDim.x) * gridDim.x) {
     double fe, fs;
     if (kind == 0) { fe = dt; fs = dt; }
@@ -315,7 +340,7 @@ __global__ void k_finish(const WDev<T> w, const T* acc, size_t astride, int nsho
       const double D = 2.0 * eps_m[p] * eps0 + dt * sig_m[p];
       fe = -2.0 * eps0 / D; fs = -dt / D;
     }
-    const size_t q = dnode(w.di0 + int(p % w.m), w.dj0 + int(p / w.m), w.ld, w.dj0);
+    const size_t q = dnode(w, w.di0 + int(p % w.m), w.dj0 + int(p / w.m));
     double se = 0, ss = 0;
     for (int s = 0; s < nshots; ++s) {
       const T* A = acc + size_t(s) * astride;
@@ -363,7 +388,7 @@ __global__ void k_plain_e(const WDev<T> w, T* st, size_t fs, long src, T sval, T
     Ex[k] = ex; Ey[k] = ey; e = ex + ey;
   }
   Ez[k] = e;
-  if (hist && J >= w.dj0 && J < w.dj0 + w.n) hist[dnode(I, J, w.ld, w.dj0)] = e;
+  if (hist && J >= w.dj0 && J < w.dj0 + w.n && drow(w, I)) hist[dnode(w, I, J)] = e;
 }
 
 // Plain reference-adjoint imaging: g -= du*a, g -= u*a (separate pass).
@@ -371,10 +396,10 @@ template <class T>
 __global__ void k_plain_img_ref(const WDev<T> w, const T* st, const T* u0, const T* u1, const T* u2,
                                 T c0, T c1, T c2, const T* uk, T* acc) {
   const size_t mn = size_t(w.m) * w.n;
-  const size_t dn = size_t(w.ld) * w.n;
+  const size_t dn = size_t(w.hld) * w.n;
   for (size_t p = threadIdx.x + size_t(blockIdx.x) * blockDim.x; p < mn; p += size_t(blockDim.x) * gridDim.x) {
     const int I = w.di0 + int(p % w.m), J = w.dj0 + int(p / w.m);
-    const size_t q = dnode(I, J, w.ld, w.dj0);
+    const size_t q = dnode(w, I, J);
     const T av = st[nidx(I, J, w.ld)];
     acc[q] -= (c0 * u0[q] + c1 * u1[q] + c2 * u2[q]) * av;
     acc[2 * dn + q] -= uk[q] * av;
@@ -400,8 +425,8 @@ __global__ void k_plain_adj_e(const WDev<T> w, T* st, size_t fs, T* px, T* py, T
     Sx[k] = w.ax[k] * lx; Sy[k] = w.ay[k] * ly;
   }
   if (interior && I >= w.di0 && I < w.di0 + w.m && J >= w.dj0 && J < w.dj0 + w.n) {
-    const size_t q = dnode(I, J, w.ld, w.dj0);
-    const size_t dn = size_t(w.ld) * w.n;
+    const size_t q = dnode(w, I, J);
+    const size_t dn = size_t(w.hld) * w.n;
     acc[q] += l * (ek[q] - ekm1[q]);
     acc[2 * dn + q] += l * (ek[q] + ekm1[q]);
   }

@@ -22,6 +22,7 @@
 // streaming pass.
 #pragma once
 #include "w_kernels_vec.cuh"
+#include "w_band.cuh"
 
 namespace gj {
 
@@ -364,9 +365,20 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
         vst(EzB + k, e_new);
         if (anyBand) { vst(ExB + k, exo); vst(EyB + k, eyo); }
       }
+      // band history of the exact adjoint (w_band.cuh): the split fields at
+      // the band nodes (zero elsewhere) and the strip H fields after the step
+      if (a.band && live && I0 < w.bRB) {
+        T* bs = a.band + size_t(zl) * w.bsz;
+        const long oe = band_off_e(w, I0, J, 0);
+        if (oe >= 0) { vst(bs + oe, exo); vst(bs + oe + (I0 >= w.bR0 ? w.bBsz : w.bLsz), eyo); }
+        const long ox = band_off_hx(w, I0, J);
+        if (ox >= 0) vst(bs + ox, hx_new);
+        const long oy = band_off_hy(w, I0, J);
+        if (oy >= 0) vst(bs + oy, hy_new);
+      }
     }
-    if (live && a.hist && J >= w.dj0 && J < w.dj0 + w.n)
-      vst(a.hist + size_t(zl) * a.hstride + dnode(I0, J, ld, w.dj0), e_new);
+    if (live && a.hist && J >= w.dj0 && J < w.dj0 + w.n && drow(w, I0))
+      vst(a.hist + size_t(zl) * a.hstride + dnode(w, I0, J), e_new);
     while (rJ == J) {  // d(it, r) = Ez(receiver) after the step (w_solve.m:100)
       const int I = __shfl_sync(0xffffffffu, wI, widx), r = __shfl_sync(0xffffffffu, wR, widx);
       if (I >= I0 && I < I0 + V) {
@@ -449,6 +461,7 @@ struct AdjRingArgs {
   const T* A; T* B; size_t fstride, sstride;
   int shot0;
   T* lout; size_t hstride;
+  T* band;  // adjoint band slot of this step (w.bsz per shot, w_band.cuh), or nullptr
 };
 
 template <class T, int S, bool FAST>
@@ -723,7 +736,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
                                       slast<T>(H + HA_BXUP));
         }
       }
-      T qy[V];
+      T qy[V], ltx[V], lty[V];
       const bool hxCol = J <= NY - 1;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
@@ -731,12 +744,25 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
         const T lt = lxo[v] + py_c[v] - py_n[v];
         lxn[v] = rx ? hxa_[v] * lt : T(0);
         qx[v] = rx ? hxb_[v] * lt : T(0);
+        ltx[v] = rx ? lt : T(0);
         const bool ry = (mHy >> v) & 1u, hin = (mHyInt >> v) & 1u;
         const T ha = hin ? T(1) : hya_[v], hb = hin ? w.chyez : hyb_[v];
         const T pdn = (v < V - 1) ? px_c[v < V - 1 ? v + 1 : v] : px_dn;
         const T lt2 = lyo[v] + px_c[v] - pdn;
         lyn[v] = ry ? ha * lt2 : T(0);
         qy[v] = ry ? hb * lt2 : T(0);
+        lty[v] = ry ? lt2 : T(0);
+      }
+      // adjoint band values (w_band.cuh): lx, ly at the band nodes, the
+      // transposed strip H values
+      if (a.band && live && I0 < w.bRB) {
+        T* bs = a.band + size_t(zl) * w.bsz;
+        const long oe = band_off_e(w, I0, J, 0);
+        if (oe >= 0) { vst(bs + oe, lx_c); vst(bs + oe + (I0 >= w.bR0 ? w.bBsz : w.bLsz), ly_c); }
+        const long ox = band_off_hx(w, I0, J);
+        if (ox >= 0) vst(bs + ox, ltx);
+        const long oy = band_off_hy(w, I0, J);
+        if (oy >= 0) vst(bs + oy, lty);
       }
       if (live) { vst(LxB + k, lxn); vst(LyB + k, lyn); }
       T qy_up = __shfl_up_sync(0xffffffffu, qy[V - 1], 1);
@@ -770,7 +796,8 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
         if (anyBand) { vst(SxB + k, sxn); vst(SyB + k, syn); }
       }
     }
-    if (live && J >= w.dj0 && J < w.dj0 + w.n) vst(a.lout + size_t(zl) * a.hstride + dnode(I0, J, ld, w.dj0), img);
+    if (live && J >= w.dj0 && J < w.dj0 + w.n && drow(w, I0))
+      vst(a.lout + size_t(zl) * a.hstride + dnode(w, I0, J), img);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       qx_prev[v] = qx[v];
@@ -800,10 +827,10 @@ __global__ void __launch_bounds__(256) k_image(const WDev<T> w, const T* lring, 
   const int g0 = w.di0 / V, g1 = (w.di0 + w.m - 1) / V;  // row groups meeting the model
   const int ng = g1 - g0 + 1;
   const size_t total = size_t(ng) * w.n;
-  const size_t dn = size_t(w.ld) * size_t(w.n);
+  const size_t dn = size_t(w.hld) * size_t(w.n);
   for (size_t t = threadIdx.x + size_t(blockIdx.x) * blockDim.x; t < total; t += size_t(blockDim.x) * gridDim.x) {
     const int gi = int(t % ng), b = int(t / ng);
-    const size_t q = size_t(b) * w.ld + size_t(g0 + gi) * V;
+    const size_t q = size_t(b) * w.hld + size_t((g0 + gi) * V - w.hr0);
     const T* L = lring + size_t(zl) * hstride + q;
     const T* E = Ek0 + size_t(zl) * hstride + q;
     T eh[V], s1[V], s2[V];
@@ -856,10 +883,10 @@ __global__ void __launch_bounds__(256) k_image_ref(const WDev<T> w, const T* lri
   const int g0 = w.di0 / V, g1 = (w.di0 + w.m - 1) / V;
   const int ng = g1 - g0 + 1;
   const size_t total = size_t(ng) * w.n;
-  const size_t dn = size_t(w.ld) * size_t(w.n);
+  const size_t dn = size_t(w.hld) * size_t(w.n);
   for (size_t t = threadIdx.x + size_t(blockIdx.x) * blockDim.x; t < total; t += size_t(blockDim.x) * gridDim.x) {
     const int gi = int(t % ng), b = int(t / ng);
-    const size_t q = size_t(b) * w.ld + size_t(g0 + gi) * V;
+    const size_t q = size_t(b) * w.hld + size_t((g0 + gi) * V - w.hr0);
     const T* L = lring + size_t(zl) * hstride + q;
     const T* U = H + size_t(zl) * hstride + q;
     T s1[V], s2[V];

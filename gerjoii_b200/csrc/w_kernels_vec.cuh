@@ -203,16 +203,16 @@ __global__ void __launch_bounds__(128, GJ_MINB_STEP) k_stepv(const WDev<T> w, co
     if (live) {
       vst(EzB + k, e_new);
       if (anyBand) { vst(ExB + k, exo); vst(EyB + k, eyo); }
-      if (J >= w.dj0 && J < w.dj0 + w.n) {
+      if (J >= w.dj0 && J < w.dj0 + w.n && drow(w, I0)) {
         // history / imaging in the domain-node layout (aligned vectors)
-        const size_t q = size_t(zl) * a.hstride + dnode(I0, J, ld, w.dj0);
+        const size_t q = size_t(zl) * a.hstride + dnode(w, I0, J);
         if (MODE == 0) {
           if (a.hist) vst(a.hist + q, e_new);
         } else {
           T u0[V], u1[V], u2[V], uk[V];
           vldw(a.u0 + q, u0); vldw(a.u1 + q, u1); vldw(a.u2 + q, u2); vldw(a.uk + q, uk);
-          const size_t dn = size_t(ld) * size_t(w.n);
-          T* acc = a.acc + size_t(s) * a.astride + dnode(I0, J, ld, w.dj0);
+          const size_t dn = size_t(w.hld) * size_t(w.n);
+          T* acc = a.acc + size_t(s) * a.astride + dnode(w, I0, J);
           T sE[V], cE[V], sS[V], cS[V];
           vldw(acc, sE); vldw(acc + 2 * dn, sS);
           if (a.kahan) { vldw(acc + dn, cE); vldw(acc + 3 * dn, cS); }
@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(128, GJ_MINB_ADJ) k_adj_stepv(const WDev<T> w,
       anyBand = anyBand || (e && !(colInt && I >= w.ei0 && I <= w.ei1));
     }
     if (live && anyBand) { vld(w.ax + k, axv); vld(w.ay + k, ayv); }
-    const bool dom = live && J >= w.dj0 && J < w.dj0 + w.n && colInt;
+    const bool dom = live && J >= w.dj0 && J < w.dj0 + w.n && colInt && drow(w, I0);
     T img1[V], img2[V];
     vzero<T, V>(img1); vzero<T, V>(img2);
 #pragma unroll
@@ -418,11 +418,11 @@ __global__ void __launch_bounds__(128, GJ_MINB_ADJ) k_adj_stepv(const WDev<T> w,
     }
     if (dom) {
       // imaging at interior model nodes, domain-node layout (aligned vectors)
-      const size_t q = size_t(zl) * a.hstride + dnode(I0, J, ld, w.dj0);
+      const size_t q = size_t(zl) * a.hstride + dnode(w, I0, J);
       T e1[V], e0[V];
       vldw(a.ek + q, e1); vldw(a.ekm1 + q, e0);
-      const size_t dn = size_t(ld) * size_t(w.n);
-      T* acc = a.acc + size_t(s) * a.astride + dnode(I0, J, ld, w.dj0);
+      const size_t dn = size_t(w.hld) * size_t(w.n);
+      T* acc = a.acc + size_t(s) * a.astride + dnode(w, I0, J);
       T sE[V], cE[V], sS[V], cS[V];
       vldw(acc, sE); vldw(acc + 2 * dn, sS);
       if (a.kahan) { vldw(acc + dn, cE); vldw(acc + 3 * dn, cS); }

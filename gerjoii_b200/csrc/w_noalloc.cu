@@ -24,7 +24,10 @@ namespace {
 constexpr size_t kNoallocScratchBytes = size_t(GJ_W_NOALLOC_SCRATCH_BYTES);
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once.
+// Device address of g_noalloc_scratch per device.  It is looked up again on
+// every call made outside stream capture (so a context re-created after
+// cudaDeviceReset gets its own address); a call made while `stream` is being
+// captured uses the address of the last uncaptured call on that device.
 constexpr int kMaxDevices = 64;
 std::mutex g_mtx;
 void* g_addr[kMaxDevices] = {nullptr};
@@ -38,13 +41,22 @@ void set_err(char* buf, size_t len, const char* msg) {
 
 // Host code cannot use the array's name as a device address; resolve it with
 // the right device current.
-gj_status scratch_address(int dev, void** out, char* eb, size_t el) {
+gj_status scratch_address(int dev, cudaStream_t st, void** out, char* eb, size_t el) {
   if (dev < 0 || dev >= kMaxDevices) {
     set_err(eb, el, "device ordinal out of range");
     return GJ_EINVAL;
   }
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    cs = cudaStreamCaptureStatusActive;  // treat as captured: use the cached address
+  }
   std::lock_guard<std::mutex> lk(g_mtx);
-  if (!g_addr[dev]) {
+  if (cs == cudaStreamCaptureStatusActive && !g_addr[dev]) {
+    set_err(eb, el, "first call on this device made during stream capture: call once outside capture first");
+    return GJ_EINVAL;
+  }
+  if (cs != cudaStreamCaptureStatusActive) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -98,12 +110,27 @@ __global__ void k_noalloc_cezj(CoefBuild c, const float* eps, const float* sig, 
 }
 
 // d[it + r*nt] = Ez(rec[r]); rec holds 0-based (NX+1)-linear node indices.
-__global__ void k_noalloc_record(const float* Ez, int NX1, int ld, const long* rec, int nr, int it, int nt,
-                                 float* d) {
+// A receiver outside the nnodes = (NX+1)(NY+1) Ez nodes is never read: its
+// trace gets NaN (the host rejects such receivers before the time loop, so
+// this guard only matters if the caller changes rec_dev during the call).
+__global__ void k_noalloc_record(const float* Ez, int NX1, long nnodes, int ld, const long* rec, int nr, int it,
+                                 int nt, float* d) {
   for (int r = threadIdx.x + blockIdx.x * blockDim.x; r < nr; r += blockDim.x * gridDim.x) {
     const long L = rec[r];
-    d[size_t(it) + size_t(r) * nt] = Ez[(L % NX1) + (L / NX1) * ld];
+    d[size_t(it) + size_t(r) * nt] = (L >= 0 && L < nnodes) ? Ez[(L % NX1) + (L / NX1) * ld] : __int_as_float(0x7fc00000);
   }
+}
+
+// Counts receivers outside [0, nnodes) into *bad.
+__global__ void k_noalloc_check_rec(const long* rec, int nr, long nnodes, int* bad) {
+  for (int r = threadIdx.x + blockIdx.x * blockDim.x; r < nr; r += blockDim.x * gridDim.x)
+    if (rec[r] < 0 || rec[r] >= nnodes) atomicAdd(bad, 1);
+}
+
+// NaN into every sample of the nt x nr traces (the output of a rejected call).
+__global__ void k_noalloc_fill_nan(float* d, size_t n) {
+  for (size_t q = threadIdx.x + size_t(blockIdx.x) * blockDim.x; q < n; q += size_t(blockDim.x) * gridDim.x)
+    d[q] = __int_as_float(0x7fc00000);
 }
 
 inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
@@ -140,7 +167,7 @@ extern "C" gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* ep
   const size_t b_coef = align256(12 * fstride * sizeof(float));
   const size_t b_state = align256(sstride * sizeof(float));
   const size_t b_prof = align256(size_t(2 * (NX + 2) + 2 * (NY + 2)) * sizeof(double));
-  const size_t need = b_coef + 2 * b_state + b_prof + 256;
+  const size_t need = b_coef + 2 * b_state + b_prof + 512;
   if (need > kNoallocScratchBytes) {
     char m[256];
     snprintf(m, sizeof m, "grid needs %zu bytes of scratch, above the %zu-byte limit of gj_w_forward_noalloc",
@@ -154,9 +181,9 @@ extern "C" gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* ep
     return GJ_ECUDA;
   }
   void* base = nullptr;
-  gj_status st0 = scratch_address(dev, &base, errbuf, errlen);
-  if (st0 != GJ_OK) return st0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  gj_status st0 = scratch_address(dev, st, &base, errbuf, errlen);
+  if (st0 != GJ_OK) return st0;
   unsigned char* p = static_cast<unsigned char*>(base);
   float* coef = reinterpret_cast<float*>(p);
   float* stA = reinterpret_cast<float*>(p + b_coef);
@@ -164,6 +191,33 @@ extern "C" gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* ep
   double* prof = reinterpret_cast<double*>(p + b_coef + 2 * b_state);
   long* d_src = reinterpret_cast<long*>(p + b_coef + 2 * b_state + b_prof);
   float* d_cezj = reinterpret_cast<float*>(d_src + 1);
+  int* d_bad = reinterpret_cast<int*>(p + b_coef + 2 * b_state + b_prof + 256);
+  const long nnodes = long(NX + 1) * long(NY + 1);
+
+  // Receivers must be Ez nodes of the padded grid.  They are device data, so
+  // they are checked on the device and the count read back (this waits for
+  // the work already queued on `stream`).  Rejected calls return GJ_EINVAL
+  // with NaN in every trace sample.
+  if (nr > 0) {
+    int bad = 0;
+    if (cudaMemsetAsync(d_bad, 0, sizeof(int), st) != cudaSuccess) {
+      set_err(errbuf, errlen, "cudaMemsetAsync on the scratch array failed");
+      return GJ_ECUDA;
+    }
+    k_noalloc_check_rec<<<(nr + 255) / 256, 256, 0, st>>>(rec_dev, nr, nnodes, d_bad);
+    if (cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      set_err(errbuf, errlen, "reading the receiver check back failed");
+      return GJ_ECUDA;
+    }
+    if (bad > 0) {
+      k_noalloc_fill_nan<<<64, 256, 0, st>>>(d_out_dev, size_t(nr) * size_t(g.nt));
+      char m[256];
+      snprintf(m, sizeof m, "%d receiver(s) outside the (NX+1)x(NY+1) = %ld Ez nodes", bad, nnodes);
+      set_err(errbuf, errlen, m);
+      return GJ_EINVAL;
+    }
+  }
 
   // Everything that must start at zero is cleared on every call: the array
   // keeps whatever the previous call left in it.
@@ -174,6 +228,7 @@ extern "C" gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* ep
   WDev<float> w{};
   w.NX = NX; w.NY = NY; w.ld = ld; w.P = g.pml; w.Pt = g.pml_top; w.m = g.m; w.n = g.n;
   w.di0 = g.pml_top + g.air; w.dj0 = g.pml;
+  w.hr0 = w.di0 / 4 * 4; w.hld = (w.di0 + g.m + 3) / 4 * 4 - w.hr0;
   w.ei0 = g.pml_top + 1; w.ei1 = NX - g.pml - 1; w.ej0 = g.pml + 1; w.ej1 = NY - g.pml - 1;
   w.hyi0 = g.pml_top; w.hyi1 = NX - g.pml - 1; w.hxj0 = g.pml; w.hxj1 = NY - g.pml - 1;
   w.chxez = float(-(2 * g.dt / g.dy) / (2 * g.mu0));
@@ -212,7 +267,8 @@ extern "C" gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* ep
     a.A = A; a.B = B; a.fstride = fstride; a.sstride = sstride; a.shot0 = 0; a.tj = tj; a.it = it;
     a.src = d_src; a.cezj = d_cezj; a.wav = wavelet_dev; a.nt = g.nt; a.hist = nullptr; a.kahan = 1;
     k_step<float, 0><<<grd, bx, 0, st>>>(w, a);
-    if (nr > 0) k_noalloc_record<<<(nr + 127) / 128, 128, 0, st>>>(B, NX + 1, ld, rec_dev, nr, it, g.nt, d_out_dev);
+    if (nr > 0)
+      k_noalloc_record<<<(nr + 127) / 128, 128, 0, st>>>(B, NX + 1, nnodes, ld, rec_dev, nr, it, g.nt, d_out_dev);
     float* t = A; A = B; B = t;
   }
   cudaError_t e = cudaGetLastError();

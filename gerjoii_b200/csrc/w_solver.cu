@@ -16,6 +16,7 @@
 #include "w_kernels_ring.cuh"
 #include "w_misfit.cuh"
 #include "w_condition.cuh"
+#include "w_band.cuh"
 
 namespace gj {
 
@@ -92,6 +93,7 @@ class WSolver : public WSolverBase {
  public:
   gj_w_grid g{};
   int NX = 0, NY = 0, ld = 0, nshots = 0, nr = 0;  // nr = max receivers per shot
+  int hr0 = 0, hld = 0;  // rows of the domain-node layout (history, accumulators, rings)
   size_t fstride = 0, sstride = 0, mn = 0, dn = 0;  // dn: domain-node elements per shot (ld*n)
   WDev<T> w{};   // forward coefficients
   WDev<T> wr{};  // reference-adjoint coefficients (sigma -> -sigma in the interior)
@@ -111,10 +113,27 @@ class WSolver : public WSolverBase {
   int bx = 128, tj = 16;
   // warp-task ring kernels (w_kernels_ring.cuh): threads per CTA (0 = not
   // available for T), ring stages, resident CTAs per SM, SMs; ring_on per call
-  int ring_nth = 0, ring_S = 0, ring_nb = 0, nsm = 148;
+  int ring_nth = 0, nsm = 148;
   bool ring_on = false;
   int Kd = 32;   // adjoint steps per imaging pass (slots of the l ring)
   DevBuf lring;
+  // exact adjoint: PML band history, adjoint band ring and band accumulators (w_band.cuh)
+  bool band_on = false;
+  DevBuf bhist, blam, bacc;
+  DevBuf nanbuf;  // non-finite counters of the results (GJ_ENUMERIC)
+
+  // Queues a count of the non-finite values of x[0, n) into counter q.
+  gj_status count_nonfinite_async(Err& err, const void* x, size_t n, bool dbl, int q, cudaStream_t st) {
+    GJ_TRY(nanbuf.alloc(err, 4 * sizeof(unsigned)));
+    unsigned* c = nanbuf.as<unsigned>() + q;
+    GJ_CUDA(err, cudaMemsetAsync(c, 0, sizeof(unsigned), st));
+    const int nb = int(std::min<size_t>((n + 255) / 256, 1024));
+    if (n == 0) return GJ_OK;
+    if (dbl) k_count_nonfinite<double><<<nb, 256, 0, st>>>(static_cast<const double*>(x), n, c);
+    else k_count_nonfinite<float><<<nb, 256, 0, st>>>(static_cast<const float*>(x), n, c);
+    GJ_CUDA(err, cudaGetLastError());
+    return GJ_OK;
+  }
 
 
   static std::string key(const gj_w_grid& g, const gj_w_shot* shots, int nshots) {
@@ -146,7 +165,9 @@ class WSolver : public WSolverBase {
     fstride = size_t(ld) * size_t(NY + 3);
     sstride = size_t(NFIELDS) * fstride;
     mn = size_t(g.m) * size_t(g.n);
-    dn = size_t(ld) * size_t(g.n);
+    hr0 = (g.pml_top + g.air) / 4 * 4;
+    hld = (g.pml_top + g.air + g.m + 3) / 4 * 4 - hr0;
+    dn = size_t(hld) * size_t(g.n);
     nshots = ns;
     nr = 0;
     sh.assign(ns, ShotHost{});
@@ -185,11 +206,13 @@ class WSolver : public WSolverBase {
     // device geometry
     w.NX = NX; w.NY = NY; w.ld = ld; w.P = g.pml; w.Pt = g.pml_top; w.m = g.m; w.n = g.n;
     w.di0 = g.pml_top + g.air; w.dj0 = g.pml;
+    w.hr0 = hr0; w.hld = hld;
     w.ei0 = g.pml_top + 1; w.ei1 = NX - g.pml - 1; w.ej0 = g.pml + 1; w.ej1 = NY - g.pml - 1;
     w.hyi0 = g.pml_top; w.hyi1 = NX - g.pml - 1; w.hxj0 = g.pml; w.hxj1 = NY - g.pml - 1;
     w.chxez = T(-(2 * g.dt / g.dy) / (2 * g.mu0));
     w.chyez = T((2 * g.dt / g.dx) / (2 * g.mu0));
     w.rxy = T(-g.dx / g.dy);
+    band_geometry(w);
     // coefficient arrays: 12 node arrays
     GJ_TRY(coef.alloc(err, 12 * fstride * sizeof(T)));
     GJ_CUDA(err, cudaMemset(coef.p, 0, 12 * fstride * sizeof(T)));
@@ -282,53 +305,64 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
-  // Launch shape of the warp-task ring kernels (w_kernels_ring.cuh): CTAs of
-  // RW warps, one task per warp.  Each step launches the fast-only kernel
-  // (interior blocks x interior columns, ring_SF stages) on the calling stream
-  // and the general kernel (the rest, ring_S stages) on a forked side stream.
+  // Launch shape of the warp-task ring kernels (w_kernels_ring.cuh).  Each
+  // step launches the fast-only kernel (interior blocks x interior columns) on
+  // the calling stream and the general kernel (the rest) on a forked side
+  // stream.  RingCfg holds the knobs: ring stages of the general (S) and fast
+  // (SF) kernels, warps per CTA of the general kernel (RWG; the fast one has
+  // RW), and the column chunk of a fast (tjF) and a general (tjS) warp task.
+  // The autotuner (autotune) times candidate configurations on the plan's own
+  // grid at the launch size and keeps the fastest per launch size; the
+  // GJ_RING_* environment variables fix a configuration instead.
   static constexpr int RW = 4;
-  int RWG = 4;  // warps per CTA of the general kernel (GJ_RING_CTA_WARPS)
-  int ring_SF = 3, nb_fast = 1;
+  struct RingCfg {
+    int S = 2, SF = 2, RWG = 4, tjF = 32, tjS = 16;
+    bool operator==(const RingCfg& o) const {
+      return S == o.S && SF == o.SF && RWG == o.RWG && tjF == o.tjF && tjS == o.tjS;
+    }
+  };
+  RingCfg rc;                    // configuration of the launches being enqueued
+  RingCfg rc_env;                // default, with the environment's overrides
+  bool env_fixed = false;        // a GJ_RING_* variable is set: no tuning
+  std::map<int, RingCfg> tuned;  // per launch size (shots per launch)
+  int maxsm_dyn = 0;
   const bool ring_serial = getenv("GJ_RING_SERIAL") != nullptr;
   int last_kernels = 0;  // kernels launched by the last launch_fwd / launch_adjr
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   template <int S, bool F>
-  gj_status ring_attr(Err& err, int& nb) {
-    const int rw = F ? RW : RWG;
-    const size_t sm = ring_smem(rw, S, F);
+  gj_status ring_attr(Err& err) {
+    const size_t sm = ring_smem(RW, S, F);  // the largest CTA of either kernel
+    if (sm > size_t(maxsm_dyn)) return GJ_OK;
     GJ_CUDA(err, cudaFuncSetAttribute(k_fwdw<T, S, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
     GJ_CUDA(err, cudaFuncSetAttribute(k_adjw<T, S, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)));
-    int n1 = 0, n2 = 0;
-    GJ_CUDA(err, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_fwdw<T, S, F>, 32 * rw, sm));
-    GJ_CUDA(err, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, k_adjw<T, S, F>, 32 * rw, sm));
-    nb = std::max(1, std::min(n1, n2));
     return GJ_OK;
-  }
-  template <bool F>
-  gj_status ring_attr_s(Err& err, int S, int& nb) {
-    if (S == 2) return ring_attr<2, F>(err, nb);
-    if (S == 3) return ring_attr<3, F>(err, nb);
-    return ring_attr<4, F>(err, nb);
   }
   gj_status ring_setup(Err& err) {
     ring_nth = 0;
     tasks.clear();
+    tuned.clear();
     if constexpr (VT<T>::V * sizeof(T) == 16) {
-      int dev = 0, maxsm = 0;
+      int dev = 0;
       GJ_CUDA(err, cudaGetDevice(&dev));
-      GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+      GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm_dyn, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
       GJ_CUDA(err, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-      int S = 2, SF = 2;
-      if (const char* e = getenv("GJ_RING_CTA_WARPS")) RWG = std::min(std::max(atoi(e), 1), 4);
-      if (const char* e = getenv("GJ_RING_STAGES")) S = std::min(std::max(atoi(e), 2), 4);
-      if (const char* e = getenv("GJ_RING_STAGES_FAST")) SF = std::min(std::max(atoi(e), 2), 4);
-      while (S > 2 && ring_smem(RWG, S, false) > size_t(maxsm)) --S;
-      if (ring_smem(RWG, S, false) > size_t(maxsm)) return GJ_OK;
-      ring_S = S;
-      ring_SF = SF;
-      GJ_TRY(ring_attr_s<false>(err, S, ring_nb));
-      GJ_TRY(ring_attr_s<true>(err, SF, nb_fast));
+      RingCfg d;
+      auto env = [&](const char* k, int& v, int lo, int hi) {
+        if (const char* e = getenv(k)) { v = std::min(std::max(atoi(e), lo), hi); env_fixed = true; }
+      };
+      env("GJ_RING_CTA_WARPS", d.RWG, 1, 4);
+      env("GJ_RING_STAGES", d.S, 2, 4);
+      env("GJ_RING_STAGES_FAST", d.SF, 2, 4);
+      env("GJ_RING_TJF", d.tjF, 2, 1 << 20);
+      env("GJ_RING_TJS", d.tjS, 2, 1 << 20);
+      if (const char* e = getenv("GJ_AUTOTUNE")) env_fixed = env_fixed || atoi(e) == 0;
+      if (ring_smem(RW, 2, false) > size_t(maxsm_dyn)) return GJ_OK;
+      while (d.S > 2 && ring_smem(RW, d.S, false) > size_t(maxsm_dyn)) --d.S;
+      GJ_TRY((ring_attr<2, false>(err))); GJ_TRY((ring_attr<3, false>(err))); GJ_TRY((ring_attr<4, false>(err)));
+      GJ_TRY((ring_attr<2, true>(err))); GJ_TRY((ring_attr<3, true>(err))); GJ_TRY((ring_attr<4, true>(err)));
+      rc_env = d;
+      rc = d;
       if (!side) GJ_CUDA(err, cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
       if (!ev_fork) GJ_CUDA(err, cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
       if (!ev_join) GJ_CUDA(err, cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
@@ -336,6 +370,11 @@ class WSolver : public WSolverBase {
       if (const char* e = getenv("GJ_IMAGE_WINDOW")) Kd = std::min(std::max(atoi(e), 1), 256);
     }
     return GJ_OK;
+  }
+  // The configuration for launches of gn shots: the tuned one when there is.
+  void select_cfg(int gn) {
+    auto it = tuned.find(gn);
+    rc = it != tuned.end() ? it->second : rc_env;
   }
   // Fast rows of the ring kernels: interior Ez rows (plus the free-top Ez = 0
   // row, whose Ceze/Cezhy are 1/0) that are also Hy interior rows.
@@ -347,9 +386,12 @@ class WSolver : public WSolverBase {
   // Task tables for launches of gn shots (built outside graph capture):
   // [0] forward fast, [1] forward general, [2] adjoint fast, [3] adjoint general.
   struct TaskTable { DevBuf buf[4]; int n[4] = {0, 0, 0, 0}; };
-  std::map<int, std::unique_ptr<TaskTable>> tasks;
+  std::map<long, std::unique_ptr<TaskTable>> tasks;
+  long task_key(int gn) const { return (long(gn) << 40) | (long(rc.tjF) << 20) | long(rc.tjS); }
+  const TaskTable& task_table(int gn) const { return *tasks.at(task_key(gn)); }
+  // Task tables of launches of gn shots for the column chunks of rc.
   gj_status prepare_tasks(Err& err, int gn) {
-    if (ring_nth == 0 || tasks.count(gn)) return GJ_OK;
+    if (ring_nth == 0 || tasks.count(task_key(gn))) return GJ_OK;
     constexpr int V = VT<T>::V;
     const int rows = 32 * V, nrb = (NX + 1 + rows - 1) / rows;
     std::vector<int> fast(nrb, 0);
@@ -361,19 +403,12 @@ class WSolver : public WSolverBase {
       fast[rb] = f ? 1 : 0;
       nF += fast[rb];
     }
-    // Column chunks: 32 columns per fast task and 16 per general task, the
-    // measured best for 10-shot launches of the 431 x 1060 grid (shorter chunks
-    // add per-task start-up and let the two kernels crowd each other);
-    // GJ_RING_TJF and GJ_RING_TJS override.
-    int tjS = 16;
-    if (const char* e = getenv("GJ_RING_TJS")) tjS = std::max(2, atoi(e));
+    const int tjS = rc.tjS;
     auto tt = std::make_unique<TaskTable>();
     for (int dir = 0; dir < 2; ++dir) {
       const int c0 = w.ej0, c1 = dir == 0 ? w.ej1 : w.ej1 - 1;  // fast columns
       const int ncol = std::max(c1 - c0 + 1, 0);
-      int tjF = 32;
-      if (const char* e = getenv("GJ_RING_TJF")) tjF = std::max(2, atoi(e));
-      tjF = std::min(tjF, std::max(ncol, 1));
+      const int tjF = std::min(rc.tjF, std::max(ncol, 1));
       std::vector<int4> hf, hg;
       auto chunks = [&](std::vector<int4>& h, int z, int r0, int a0, int a1, int tj) {
         for (int j0 = a0; j0 <= a1; j0 += tj) h.push_back(make_int4(r0, j0, std::min(j0 + tj - 1, a1), z << 1));
@@ -400,7 +435,7 @@ class WSolver : public WSolverBase {
                                 cudaMemcpyHostToDevice));
       }
     }
-    tasks.emplace(gn, std::move(tt));
+    tasks.emplace(task_key(gn), std::move(tt));
     return GJ_OK;
   }
 
@@ -443,9 +478,9 @@ class WSolver : public WSolverBase {
                        const WDev<T>* wsel = nullptr) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       if (ring_on) {
-        const TaskTable& tt = *tasks.at(gn);
+        const TaskTable& tt = task_table(gn);
         const WDev<T> wd = wsel ? *wsel : w;
-        const int S = ring_S, SF = ring_SF;
+        const int S = rc.S, SF = rc.SF;
         auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
           const dim3 grd((n + RW - 1) / RW);
           const size_t sm = ring_smem(RW, SF, true);
@@ -453,7 +488,7 @@ class WSolver : public WSolverBase {
           else if (SF == 3) k_fwdw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
           else k_fwdw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
         };
-        const int rw = RWG;
+        const int rw = rc.RWG;
         auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
           const dim3 grd((n + rw - 1) / rw);
           const size_t sm = ring_smem(rw, S, false);
@@ -474,9 +509,9 @@ class WSolver : public WSolverBase {
   // One exact adjoint step of gn shots with the l ring (ring kernels only).
   gj_status launch_adjr(Err& err, AdjRingArgs<T> a, int gn, cudaStream_t st, RecArgs<T> ra) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
-      const TaskTable& tt = *tasks.at(gn);
+      const TaskTable& tt = task_table(gn);
       const WDev<T> wd = w;
-      const int S = ring_S, SF = ring_SF;
+      const int S = rc.S, SF = rc.SF;
       auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
         const dim3 grd((n + RW - 1) / RW);
         const size_t sm = ring_smem(RW, SF, true);
@@ -484,7 +519,7 @@ class WSolver : public WSolverBase {
         else if (SF == 3) k_adjw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
         else k_adjw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
       };
-      const int rw = RWG;
+      const int rw = rc.RWG;
       auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
         const dim3 grd((n + rw - 1) / rw);
         const size_t sm = ring_smem(rw, S, false);
@@ -494,6 +529,93 @@ class WSolver : public WSolverBase {
       };
       return fork_join<AdjRingArgs<T>>(err, tt, 1, st, lf, lg);
     }
+    return GJ_OK;
+  }
+
+  // Autotuner: times candidate ring configurations for launches of gn shots
+  // on this grid (forward + exact-adjoint steps of zeroed states, no history)
+  // and keeps the fastest for gn.  Coordinate search: the fast kernel's
+  // stages x column chunk first, then the general kernel's stages x column
+  // chunk x CTA width.  Needs the states and the adjoint-field ring of the
+  // memory plan allocated for at least gn shots.
+  gj_status autotune(Err& err, int gn, cudaStream_t st) {
+    if (ring_nth == 0 || gn < 1) return GJ_OK;
+    if (env_fixed || tuned.count(gn)) { select_cfg(gn); return GJ_OK; }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GJ_CUDA(err, cudaEventCreate(&e0));
+    GJ_CUDA(err, cudaEventCreate(&e1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
+    const int warm = 2, reps = 6;
+    auto clear = [&]() -> gj_status {
+      GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      return GJ_OK;
+    };
+    auto time_cfg = [&](const RingCfg& cfg, float& ms) -> gj_status {
+      rc = cfg;
+      GJ_TRY(prepare_tasks(err, gn));
+      GJ_TRY(clear());
+      T* A = fwdA.as<T>() + ld;
+      T* B = fwdB.as<T>() + ld;
+      T* LA = adjA.as<T>() + ld;
+      T* LB = adjB.as<T>() + ld;
+      auto run = [&](int n) -> gj_status {
+        for (int i = 0; i < n; ++i) {
+          StepArgs<T> a = step_args(A, B, i % g.nt);
+          GJ_TRY(launch_fwd(err, a, gn, st));
+          std::swap(A, B);
+          AdjRingArgs<T> b{};
+          b.A = LA; b.B = LB; b.fstride = fstride; b.sstride = sstride; b.shot0 = 0;
+          b.lout = lring.as<T>(); b.hstride = dn;
+          GJ_TRY(launch_adjr(err, b, gn, st, rec_args(0)));
+          std::swap(LA, LB);
+        }
+        return GJ_OK;
+      };
+      GJ_TRY(run(warm));
+      GJ_CUDA(err, cudaEventRecord(e0, st));
+      GJ_TRY(run(reps));
+      GJ_CUDA(err, cudaEventRecord(e1, st));
+      GJ_CUDA(err, cudaEventSynchronize(e1));
+      GJ_CUDA(err, cudaEventElapsedTime(&ms, e0, e1));
+      GJ_CUDA(err, cudaGetLastError());
+      return GJ_OK;
+    };
+    RingCfg best = rc_env;
+    float tbest = 0.f;
+    GJ_TRY(time_cfg(best, tbest));
+    auto consider = [&](const RingCfg& q) -> gj_status {
+      if (q == best) return GJ_OK;
+      if (ring_smem(q.RWG, q.S, false) > size_t(maxsm_dyn) || ring_smem(RW, q.SF, true) > size_t(maxsm_dyn))
+        return GJ_OK;
+      float t = 0.f;
+      GJ_TRY(time_cfg(q, t));
+      if (t < tbest) { tbest = t; best = q; }
+      return GJ_OK;
+    };
+    for (int SF : {2, 3, 4})
+      for (int tjF : {16, 24, 32, 48}) {
+        RingCfg q = best;
+        q.SF = SF; q.tjF = tjF;
+        GJ_TRY(consider(q));
+      }
+    const RingCfg fast_best = best;
+    for (int S : {2, 3, 4})
+      for (int tjS : {8, 16, 32, 64})
+        for (int rw : {2, 4}) {
+          RingCfg q = fast_best;
+          q.S = S; q.tjS = tjS; q.RWG = rw;
+          GJ_TRY(consider(q));
+        }
+    GJ_TRY(clear());
+    tuned[gn] = best;
+    rc = best;
+    GJ_TRY(prepare_tasks(err, gn));
+    if (getenv("GJ_AUTOTUNE_VERBOSE"))
+      fprintf(stderr, "gerjoii_b200 autotune %dx%d, %d shots/launch: S=%d SF=%d RWG=%d tjF=%d tjS=%d, %.2f us/step\n",
+              NX, NY, gn, best.S, best.SF, best.RWG, best.tjF, best.tjS, 1e3f * tbest / reps);
     return GJ_OK;
   }
 
@@ -550,6 +672,7 @@ class WSolver : public WSolverBase {
     if (jz_out) GJ_TRY(jzb.alloc(err, size_t(nshots) * g.nt * sizeof(T)));
     if (u_out) GJ_TRY(ub.alloc(err, size_t(nshots) * dn * (g.nt + 1) * sizeof(T)));
     ring_on = ring_nth > 0;
+    select_cfg(nshots);
     GJ_TRY(prepare_tasks(err, nshots));
     for (int it = 0; it < g.nt; ++it) {
       StepArgs<T> a = step_args(A, B, it);
@@ -566,10 +689,13 @@ class WSolver : public WSolverBase {
     // copy out (per shot nt x nr, time fastest)
     std::vector<T> hd(size_t(nshots) * nrr * g.nt);
     GJ_CUDA(err, cudaMemcpy(hd.data(), dbuf.p, hd.size() * sizeof(T), cudaMemcpyDeviceToHost));
-    size_t o = 0;
+    size_t o = 0, nbad = 0;
     for (int s = 0; s < nshots; ++s)
       for (int r = 0; r < nrs[s]; ++r)
-        for (int t = 0; t < g.nt; ++t) d_out[o++] = double(hd[(size_t(s) * nrr + r) * g.nt + t]);
+        for (int t = 0; t < g.nt; ++t) {
+          d_out[o] = double(hd[(size_t(s) * nrr + r) * g.nt + t]);
+          nbad += std::isfinite(d_out[o++]) ? 0 : 1;
+        }
     if (jz_out) {
       std::vector<T> hj(size_t(nshots) * g.nt);
       GJ_CUDA(err, cudaMemcpy(hj.data(), jzb.p, hj.size() * sizeof(T), cudaMemcpyDeviceToHost));
@@ -585,8 +711,9 @@ class WSolver : public WSolverBase {
           for (int b = 0; b < g.n; ++b)
             for (int a_ = 0; a_ < g.m; ++a_)
               u_out[(size_t(s) * g.nt + t) * mn + size_t(b) * g.m + a_] =
-                  double(hu[(size_t(t) * nshots + s) * dn + size_t(b) * ld + di0 + a_]);
+                  double(hu[(size_t(t) * nshots + s) * dn + size_t(b) * hld + di0 - hr0 + a_]);
     }
+    if (nbad) return err.set(GJ_ENUMERIC, "%zu non-finite trace samples (outputs written)", nbad);
     return GJ_OK;
   }
 
@@ -661,13 +788,17 @@ class WSolver : public WSolverBase {
   // Forward runs and misfits of all shots, no history and no adjoint: the
   // objective evaluations of a step-length search (w_objs_e.m:24-65, called
   // by w_stepparabola_e.m:20-41 for each trial model).
+  // With opts->filt_high > filt_low both trace sets are band-filtered first
+  // (w_objs_e.m:33-36 / w_objs_s.m), so the misfit and its normaliser are
+  // those of the filtered traces.
   gj_status misfit(Err& err, Ctx& c, const double* eps, const double* sig, const double* dobs, gj_misfit_kind mk,
-                   double* misfit_out, cudaStream_t st) {
+                   double* misfit_out, cudaStream_t st, const gj_w_opts* opts = nullptr) {
     GJ_TRY(stage_inputs(err, c, eps, sig, false, dobs, false, st));
     GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     ring_on = ring_nth > 0;
+    select_cfg(nshots);
     GJ_TRY(prepare_tasks(err, nshots));
     T* A = fwdA.as<T>() + ld;
     T* B = fwdB.as<T>() + ld;
@@ -681,6 +812,10 @@ class WSolver : public WSolverBase {
       c.launches += 1 + last_kernels;
       std::swap(A, B);
     }
+    if (opts && opts->filt_high > opts->filt_low) {
+      GJ_TRY(filt_traces(err, c, *opts, dbuf.as<T>(), nshots, st));
+      GJ_TRY(filt_traces(err, c, *opts, dobsbuf.as<T>(), nshots, st));
+    }
     if (mk != GJ_MISFIT_L2) {
       GJ_TRY(env_residual(err, c, 0, nshots, mk, st));
     } else {
@@ -692,8 +827,12 @@ class WSolver : public WSolverBase {
     std::vector<double> hs(2 * nshots);
     GJ_CUDA(err, cudaMemcpyAsync(hs.data(), sums.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     GJ_CUDA(err, cudaStreamSynchronize(st));
-    for (int q = 0; q < nshots; ++q)
+    int nbad = 0;
+    for (int q = 0; q < nshots; ++q) {
       misfit_out[q] = hs[2 * q + 1] > 0 ? 0.5 * hs[2 * q] / hs[2 * q + 1] : 0.5 * hs[2 * q];
+      nbad += std::isfinite(misfit_out[q]) ? 0 : 1;
+    }
+    if (nbad) return err.set(GJ_ENUMERIC, "%d non-finite misfits (outputs written)", nbad);
     return GJ_OK;
   }
 
@@ -701,10 +840,11 @@ class WSolver : public WSolverBase {
   // Chooses K: the whole history when it fits, else checkpoints every K steps.
   void choose_k(const gj_w_opts& o, size_t free_bytes) {
     const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.8 * double(free_bytes));
-    const size_t per_slot = size_t(nshots) * dn * sizeof(T);
+    const size_t bnd = band_on ? size_t(w.bsz) : 0;  // band history per shot and slot
+    const size_t per_slot = size_t(nshots) * (dn + bnd) * sizeof(T);
     const size_t per_ck = size_t(nshots) * sstride * sizeof(T);
     if (o.ckpt_every > 0) { K = std::min(std::max(o.ckpt_every, 2), g.nt); return; }
-    const size_t extra = ring_on ? size_t(Kd) * per_slot : 0;  // the l ring
+    const size_t extra = ring_on ? size_t(Kd) * per_slot : 0;  // the l ring (and the band ring)
     if (size_t(g.nt + 1) * per_slot + extra <= budget) { K = g.nt; return; }
     double k = std::sqrt(double(g.nt) * double(per_ck) / double(per_slot));
     K = std::min(std::max(int(k), 2), g.nt);
@@ -770,6 +910,16 @@ class WSolver : public WSolverBase {
     else { k0 = k - 1; k1 = k; k2 = k + 1; c0 = -0.5 / dt; c1 = 0.0; c2 = 0.5 / dt; }
   }
 
+  // Band terms of the exact eps gradient added to gdev (double, per shot or summed).
+  void band_finish(Ctx& c, double* gdev, int per_shot, cudaStream_t st) {
+    BandFinish f;
+    f.dt = g.dt; f.eps0 = g.eps0; f.mu0 = g.mu0; f.Pt = g.pml_top; f.air = g.air; f.eps_m = eps_m;
+    const double* pp = prof.as<double>();
+    f.sex = pp; f.smx = pp + NX + 2; f.sey = pp + 2 * (NX + 2); f.smy = pp + 2 * (NX + 2) + NY + 2;
+    k_band_finish<T><<<64, 256, 0, st>>>(w, bacc.as<T>(), 2 * size_t(w.bsz), nshots, per_shot, f, gdev);
+    ++c.launches;
+  }
+
   // Final scaling, shot reduction and outputs.
   gj_status finish(Err& err, Ctx& c, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig, bool dev_out,
                    double* misfit_out, double* d_out, double* e_out, const std::vector<double>& hsums,
@@ -791,6 +941,7 @@ class WSolver : public WSolverBase {
       k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, nshots, 1, mode == GJ_ADJ_EXACT ? 1 : 0, g.dt,
                                        g.eps0, eps_m, sig_m, ce_, cs_);
       ++c.launches;
+      if (mode == GJ_ADJ_EXACT && band_on) band_finish(c, ce_, 1, st);
       GJ_TRY(condition(err, c, o, ce_, o.cond_ax, o.cond_az, st));
       GJ_TRY(condition(err, c, o, cs_, 2 * o.cond_ax, 2 * o.cond_az, st));
       if (o.per_shot) {
@@ -805,7 +956,13 @@ class WSolver : public WSolverBase {
       k_finish<T><<<256, 256, 0, st>>>(w, acc.as<T>(), 4 * dn, nshots, o.per_shot, mode == GJ_ADJ_EXACT ? 1 : 0,
                                        g.dt, g.eps0, eps_m, sig_m, ge_d, gs_d);
       ++c.launches;
+      if (mode == GJ_ADJ_EXACT && band_on) band_finish(c, ge_d, o.per_shot, st);
     }
+    GJ_TRY(count_nonfinite_async(err, ge_d, gsz, true, 0, st));
+    GJ_TRY(count_nonfinite_async(err, gs_d, gsz, true, 1, st));
+    unsigned hnan[2] = {0, 0};
+    GJ_CUDA(err, cudaMemcpyAsync(hnan, nanbuf.p, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    c.launches += 2;
     if (dev_out && sizeof(T) == 4) {
       k_convert<double, float><<<256, 256, 0, st>>>(ge_d, static_cast<float*>(geps), gsz);
       k_convert<double, float><<<256, 256, 0, st>>>(gs_d, static_cast<float*>(gsig), gsz);
@@ -831,6 +988,12 @@ class WSolver : public WSolverBase {
     };
     if (d_out) unpack(hd, d_out);
     if (e_out) unpack(he, e_out);
+    bool bad_mis = false;
+    for (int s = 0; s < nshots; ++s) bad_mis = bad_mis || !std::isfinite(hsums[2 * s]) || !std::isfinite(hsums[2 * s + 1]);
+    if (hnan[0] || hnan[1] || bad_mis)
+      return err.set(GJ_ENUMERIC, "non-finite results: %u of g_eps, %u of g_sig%s (outputs written; the reference "
+                     "zeroes such gradients, w_update_e.m:131-137, which opts.condition does)",
+                     hnan[0], hnan[1], bad_mis ? ", misfit" : "");
     return GJ_OK;
   }
 
@@ -902,6 +1065,10 @@ class WSolver : public WSolverBase {
   int filt_batch = 0, filt_ntp = 0;
   double filt_key[4] = {0, 0, 0, 0};
   gj_status filt_residual(Err& err, Ctx& c, const gj_w_opts& o, int g0, int gn, cudaStream_t st) {
+    return filt_traces(err, c, o, ebuf.as<T>() + size_t(g0) * std::max(nr, 1) * g.nt, gn, st);
+  }
+  // The same filter in place on gn shots of traces x ([shot][r][t]).
+  gj_status filt_traces(Err& err, Ctx& c, const gj_w_opts& o, T* x, int gn, cudaStream_t st) {
     using C = typename CplxT<T>::type;
     const int nrr = std::max(nr, 1), nt = g.nt;
     int ntp = 1;
@@ -944,7 +1111,7 @@ class WSolver : public WSolverBase {
       std::memcpy(filt_key, key, sizeof key);
     }
     GJ_TRY(filtX.alloc(err, size_t(batch) * ntp * sizeof(C)));
-    T* e = ebuf.as<T>() + size_t(g0) * nrr * nt;
+    T* e = x;
     C* X = filtX.as<C>();
     k_filt_pre<T, C><<<512, 256, 0, st>>>(e, filtW.as<T>(), X, nt, ntp, size_t(batch));
     cufftSetStream(filtplan, st);
@@ -992,7 +1159,8 @@ class WSolver : public WSolverBase {
     }
     if (o.ckpt_every > 0) return nshots;
     const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.8 * double(free_bytes));
-    const size_t per_shot = (size_t(g.nt + 1 + (ring_on ? Kd : 0)) * dn + 4 * sstride) * sizeof(T);
+    const size_t bnd = band_on ? size_t(w.bsz) : 0;
+    const size_t per_shot = (size_t(g.nt + 1 + (ring_on ? Kd : 0)) * (dn + bnd) + 4 * sstride) * sizeof(T);
     const int fit = int(std::min<size_t>(budget / std::max<size_t>(per_shot, 1), size_t(nshots)));
     if (fit >= nshots) return nshots;
     if (fit >= std::min(8, nshots)) {
@@ -1011,6 +1179,24 @@ class WSolver : public WSolverBase {
     return t;
   }
 
+  // Band kernels of the exact adjoint (w_band.cuh): band fields of a state
+  // into a band slot, the adjoint band values of a state, band imaging.
+  int band_blocks() const { return int(std::min<long>((w.bsz + 255) / 256, 4L * nsm)); }
+  void band_rec(const T* state, T* slot, int gn, cudaStream_t st, long& nl) {
+    k_band_rec<T><<<dim3(band_blocks(), gn), 256, 0, st>>>(w, state, sstride, fstride, slot);
+    ++nl;
+  }
+  void band_adj(const T* state, T* slot, int gn, cudaStream_t st, long& nl) {
+    k_band_adj<T><<<dim3(band_blocks(), gn), 256, 0, st>>>(w, state, sstride, fstride, slot);
+    ++nl;
+  }
+  void band_image(const T* lam, const T* Fk0, int cnt, int gn, int shot0, int kahan, cudaStream_t st, long& nl) {
+    const size_t sl = size_t(gn) * size_t(w.bsz);
+    k_image_band<T><<<dim3(band_blocks(), gn), 256, 0, st>>>(w, lam, sl, Fk0, sl, cnt, bacc.as<T>(),
+                                                             2 * size_t(w.bsz), shot0, kahan);
+    ++nl;
+  }
+
   // Enqueues the whole gradient of shots [g0, g0+gn) on stream st.
   // phase: 1 = forward (+ the L2 residual when l2), 2 = adjoint, 3 = both.
   gj_status enqueue_group(Err& err, Ctx& c, int g0, int gn, gj_adj_mode mode, int kahan,
@@ -1024,6 +1210,8 @@ class WSolver : public WSolverBase {
     T* H = hist.as<T>();
     const size_t hs = dn;
     auto slot_ptr = [&](long k, long base) { return H + size_t(k - base) * gn * hs; };
+    T* BH = bhist.as<T>();
+    auto bslot = [&](long k, long base) { return BH + size_t(k - base) * gn * size_t(w.bsz); };
     const long* rec = recbuf.as<long>() + size_t(g0) * nrr;
     const int* nrs_d = nrsbuf.as<int>() + g0;
     const int* sel = selbuf.as<int>() + size_t(g0) * nrr;
@@ -1036,6 +1224,7 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, gn * sstride * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, gn * sstride * sizeof(T), st));
     if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, gn * hs * sizeof(T), st));  // slot 0 = zero state
+    if (full && band_on) GJ_CUDA(err, cudaMemsetAsync(BH, 0, gn * size_t(w.bsz) * sizeof(T), st));
     size_t segi = 0;
     for (int it = 0; it < nt; ++it) {
       if (!full && segi < segs.size() && it == segs[segi].first) {
@@ -1049,9 +1238,11 @@ class WSolver : public WSolverBase {
       const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
       RecArgs<T> ra = rec_args(g0);
       if (ring_on && nr > 0) { ra.d = dgrp; ra.it = it; }  // receivers recorded inside the step
+      if (ring_on && full && band_on) a.band = bslot(it + 1, 0);  // band history written inside the step
       GJ_TRY(launch_fwd(err, a, gn, st, ra));
       c.timer.end(tm, st);
       nl += last_kernels;
+      if (!ring_on && full && band_on) band_rec(B, bslot(it + 1, 0), gn, st, nl);
       if (!ring_on) {
         k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, rec, nrr, nrs_d, it, nt, dgrp, d_src + g0,
                                                  static_cast<T*>(nullptr), gn);
@@ -1081,15 +1272,18 @@ class WSolver : public WSolverBase {
                                      cudaMemcpyDeviceToDevice, st));
         k_domain_copy<T><<<dim3(64, gn), 256, 0, st>>>(w, A, sstride, slot_ptr(s0, base), hs, gn);
         ++nl;
+        if (band_on) band_rec(A, bslot(s0, base), gn, st, nl);
         const int iend = std::min(s1 + 1, nt);
         for (int it = s0; it < iend; ++it) {
           StepArgs<T> a = step_args(A, B, it);
           a.shot0 = g0;
           a.hist = slot_ptr(it + 1, base); a.hstride = hs;
+          if (ring_on && band_on) a.band = bslot(it + 1, base);
           const bool tm = c.timer.begin(KK_FWD_STEP, st, gn);
           GJ_TRY(launch_fwd(err, a, gn, st));
           c.timer.end(tm, st);
           nl += last_kernels;
+          if (!ring_on && band_on) band_rec(B, bslot(it + 1, base), gn, st, nl);
           std::swap(A, B);
         }
       }
@@ -1153,6 +1347,7 @@ class WSolver : public WSolverBase {
           AdjRingArgs<T> a{};
           a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = g0;
           a.lout = lring.as<T>() + size_t(win) * gn * hs; a.hstride = hs;
+          if (band_on) a.band = blam.as<T>() + size_t(win) * gn * size_t(w.bsz);  // written inside the step
           const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
           GJ_TRY(launch_adjr(err, a, gn, st, ra));
           c.timer.end(tm, st);
@@ -1166,6 +1361,7 @@ class WSolver : public WSolverBase {
             k_image<T><<<dim3(nblk, gn), 256, 0, st>>>(w, lring.as<T>(), size_t(gn) * hs,
                                                        slot_ptr(k + win - 1, base), size_t(gn) * hs, win, hs,
                                                        acc.as<T>(), 4 * dn, g0, kahan);
+            if (band_on) band_image(blam.as<T>(), bslot(k + win - 1, base), win, gn, g0, kahan, st, nl);
             c.timer.end(ti, st);
             win = 0;
             ++nl;
@@ -1177,6 +1373,10 @@ class WSolver : public WSolverBase {
           a.A = LA; a.B = LB; a.fstride = fstride; a.sstride = sstride; a.shot0 = g0; a.tj = tjg;
           a.ek = slot_ptr(k, base); a.ekm1 = slot_ptr(k - 1, base); a.hstride = hs;
           a.acc = acc.as<T>(); a.astride = 4 * dn; a.kahan = kahan;
+          if (band_on) {
+            band_adj(LA, blam.as<T>(), gn, st, nl);
+            band_image(blam.as<T>(), bslot(k, base), 1, gn, g0, kahan, st, nl);
+          }
           const bool tm = c.timer.begin(KK_ADJ_STEP, st, gn);
           k_adj_stepv<T><<<grd, 128, 0, st>>>(w, a);
           c.timer.end(tm, st);
@@ -1189,22 +1389,28 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
+  // e_given: `dobs` holds the adjoint sources themselves (per shot nt x nr),
+  // the backward half of gj_w_backward: no residual, no misfit.
   gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
                      bool dev_dobs, gj_adj_mode mode, gj_misfit_kind mk, const gj_w_opts& o, void* geps,
-                     void* gsig, bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+                     void* gsig, bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st,
+                     bool e_given = false) {
     GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
+    if (e_given) mk = GJ_MISFIT_L2;
     if (o.plain) {
       if (mk != GJ_MISFIT_L2) return err.set(GJ_EUNSUPPORTED, "the plain form supports the L2 misfit only");
       if (o.filt_high > o.filt_low) return err.set(GJ_EUNSUPPORTED, "the plain form has no residual filter");
-      return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st);
+      return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st, e_given);
     }
     const bool env = (mk != GJ_MISFIT_L2);
     const bool filt = o.filt_high > o.filt_low;
     ring_on = ring_nth > 0 && !o.no_ring;
+    band_on = mode == GJ_ADJ_EXACT;
     // memory plan for one group
     size_t free_b = 0, total_b = 0;
     GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
-    const size_t owned = hist.bytes + ckpt.bytes + (G > 0 ? 4 * size_t(G) * sstride * sizeof(T) : 0);
+    const size_t owned = hist.bytes + ckpt.bytes + bhist.bytes + blam.bytes +
+                         (G > 0 ? 4 * size_t(G) * sstride * sizeof(T) : 0);
     const int Gnew = choose_group(o, free_b + owned);
     const int ns_save = nshots;
     nshots = Gnew;  // choose_k sizes buffers per group
@@ -1220,7 +1426,8 @@ class WSolver : public WSolverBase {
     hist_slots = full ? size_t(g.nt + 1) : size_t(maxlen + 3);
     const size_t hbytes = hist_slots * G * dn * sizeof(T);
     const size_t cbytes = full ? 0 : segs.size() * G * sstride * sizeof(T);
-    void* old[5] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p};
+    void* old[8] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p, bhist.p, blam.p, bacc.p};
+    if (!band_on) { bhist.release(); blam.release(); }
     GJ_TRY(hist.alloc(err, hbytes));
     if (!full) GJ_TRY(ckpt.alloc(err, cbytes));
     GJ_TRY(fwdA.alloc(err, size_t(G) * sstride * sizeof(T)));
@@ -1228,6 +1435,11 @@ class WSolver : public WSolverBase {
     GJ_TRY(adjA.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(adjB.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
+    if (band_on) {
+      GJ_TRY(bhist.alloc(err, hist_slots * G * size_t(w.bsz) * sizeof(T)));
+      GJ_TRY(blam.alloc(err, size_t(ring_on ? Kd : 1) * G * size_t(w.bsz) * sizeof(T)));
+      GJ_TRY(bacc.alloc(err, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T)));
+    }
     if (ring_on) {
       const void* lold = lring.p;
       GJ_TRY(lring.alloc(err, size_t(Kd) * G * dn * sizeof(T)));
@@ -1237,25 +1449,33 @@ class WSolver : public WSolverBase {
         GJ_CUDA(err, cudaMemsetAsync(lring.p, 0, size_t(Kd) * G * dn * sizeof(T), st));
       }
     }
-    void* nw[5] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p};
-    for (int q = 0; q < 5; ++q)
+    void* nw[8] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p, bhist.p, blam.p, bacc.p};
+    for (int q = 0; q < 8; ++q)
       if (old[q] != nw[q]) { drop_graphs(); break; }
     const int kahan = o.no_kahan ? 0 : 1;
     if (ring_on) {
-      GJ_TRY(prepare_tasks(err, G));
-      if (nshots % G) GJ_TRY(prepare_tasks(err, nshots % G));
+      GJ_TRY(autotune(err, G, st));
+      if (nshots % G) GJ_TRY(autotune(err, nshots % G, st));
     }
     GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
+    if (band_on) GJ_CUDA(err, cudaMemsetAsync(bacc.p, 0, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T), st));
     long nl = 0;
     for (int g0 = 0; g0 < nshots; g0 += G) {
       const int gn = std::min(G, nshots - g0);
-      if (env || filt) {
-        // forward, residual (envelope: cuFFT), band filter (cuFFT), adjoint:
-        // launched directly
+      if (ring_on) select_cfg(gn);
+      if (env || filt || e_given) {
+        // forward, residual (envelope: cuFFT) or the given adjoint sources,
+        // band filter (cuFFT), adjoint: launched directly
         Marks m;
         c.timer.cur = &m;
-        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 1, !env);
+        gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 1, !env && !e_given);
+        if (rs == GJ_OK && e_given) {
+          const size_t tr = size_t(std::max(nr, 1)) * g.nt;
+          if (cudaMemcpyAsync(ebuf.as<T>() + size_t(g0) * tr, dobsbuf.as<T>() + size_t(g0) * tr,
+                              size_t(gn) * tr * sizeof(T), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            rs = err.set(GJ_ECUDA, "copy of the adjoint sources failed");
+        }
         if (rs == GJ_OK && env) rs = env_residual(err, c, g0, gn, mk, st);
         if (rs == GJ_OK && filt) rs = filt_residual(err, c, o, g0, gn, st);
         if (rs == GJ_OK) rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 2, false);
@@ -1276,8 +1496,8 @@ class WSolver : public WSolverBase {
         continue;
       }
       char kb[96];
-      snprintf(kb, sizeof kb, "%d/%d/%d/%d/%d/%d/%d/%d/%d", g0, gn, int(mode), kahan, K, G, c.timer.on ? 1 : 0,
-               ring_on ? 1 : 0, Kd);
+      snprintf(kb, sizeof kb, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d.%d.%d.%d.%d", g0, gn, int(mode), kahan, K, G,
+               c.timer.on ? 1 : 0, ring_on ? 1 : 0, Kd, rc.S, rc.SF, rc.RWG, rc.tjF, rc.tjS);
       auto itg = graphs.find(kb);
       if (itg == graphs.end()) {
         auto rec = std::make_unique<GraphRec>();
@@ -1316,15 +1536,17 @@ class WSolver : public WSolverBase {
   // The plain form: one half-step per launch, one thread per node, one shot at a
   // time, full u history in HBM when it fits (else the same checkpointing).
   gj_status gradient_plain(Err& err, Ctx& c, gj_adj_mode mode, const gj_w_opts& o, void* geps, void* gsig,
-                           bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+                           bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st,
+                           bool e_given = false) {
     const int nrr = std::max(nr, 1), nt = g.nt;
     const size_t tr = size_t(nrr) * nt;
     size_t free_b = 0, total_b = 0;
     GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
     // per-shot sizing: pretend a single shot
+    band_on = mode == GJ_ADJ_EXACT;
     const int ns_save = nshots;
     nshots = 1;
-    choose_k(o, free_b + hist.bytes + ckpt.bytes);
+    choose_k(o, free_b + hist.bytes + ckpt.bytes + bhist.bytes + blam.bytes);
     nshots = ns_save;
     const bool full = (K >= nt);
     std::vector<std::pair<int, int>> segs = segments();
@@ -1336,6 +1558,12 @@ class WSolver : public WSolverBase {
     GJ_TRY(adjA.alloc(err, sstride * sizeof(T)));
     GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
     GJ_TRY(scratch.alloc(err, 5 * fstride * sizeof(T)));
+    if (band_on) {
+      GJ_TRY(bhist.alloc(err, hist_slots * size_t(w.bsz) * sizeof(T)));
+      GJ_TRY(blam.alloc(err, size_t(w.bsz) * sizeof(T)));
+      GJ_TRY(bacc.alloc(err, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T)));
+      GJ_CUDA(err, cudaMemsetAsync(bacc.p, 0, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T), st));
+    }
     GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(scratch.p, 0, 5 * fstride * sizeof(T), st));
     T* px = scratch.as<T>() + ld; T* py = px + fstride; T* lm = py + fstride; T* qx = lm + fstride; T* qy = qx + fstride;
@@ -1347,21 +1575,25 @@ class WSolver : public WSolverBase {
     const dim3 blk(32, 8), grd((NX + 1 + 31) / 32, (NY + 1 + 7) / 8);
     T* H = hist.as<T>();
     auto slot = [&](long k, long base) { return H + size_t(k - base) * dn; };
+    auto bslot = [&](long k, long base) { return band_on ? bhist.as<T>() + size_t(k - base) * size_t(w.bsz) : nullptr; };
+    long nlb = 0;  // band kernel launches
     T* S = fwdA.as<T>() + ld;  // shot state (in place)
     T* L = adjA.as<T>() + ld;
     Marks marks;
     c.timer.cur = &marks;
     for (int s = 0; s < nshots; ++s) {
       const long src = sh[s].src;
-      auto fwd_step = [&](int it, T* hslot) {
+      auto fwd_step = [&](int it, T* hslot, T* bsl) {
         const bool tm = c.timer.begin(KK_PLAIN, st);
         k_plain_h<T><<<grd, blk, 0, st>>>(w, S, fstride);
         k_plain_e<T><<<grd, blk, 0, st>>>(w, S, fstride, src, hcezj[s] * hwav[size_t(s) * nt + it], hslot);
+        if (bsl) band_rec(S, bsl, 1, st, nlb);
         c.timer.end(tm, st);
         c.launches += 2;
       };
       GJ_CUDA(err, cudaMemsetAsync(S - ld, 0, sstride * sizeof(T), st));
       if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, dn * sizeof(T), st));
+      if (full && band_on) GJ_CUDA(err, cudaMemsetAsync(bhist.p, 0, size_t(w.bsz) * sizeof(T), st));
       size_t segi = 0;
       for (int it = 0; it < nt; ++it) {
         if (!full && segi < segs.size() && it == segs[segi].first) {
@@ -1369,15 +1601,20 @@ class WSolver : public WSolverBase {
                                        cudaMemcpyDeviceToDevice, st));
           ++segi;
         }
-        fwd_step(it, full ? slot(it + 1, 0) : nullptr);
+        fwd_step(it, full ? slot(it + 1, 0) : nullptr, full ? bslot(it + 1, 0) : nullptr);
         k_record<T><<<dim3(1, 1), 128, 0, st>>>(S, sstride, recbuf.as<long>() + size_t(s) * nrr, nrr,
                                                 nrsbuf.as<int>() + s, it, nt, dbuf.as<T>() + size_t(s) * tr, d_src + s,
                                                 static_cast<T*>(nullptr), 1);
         ++c.launches;
       }
-      k_residual<T><<<dim3(64, 1), 256, 0, st>>>(dbuf.as<T>() + size_t(s) * tr, dobsbuf.as<T>() + size_t(s) * tr,
-                                                  ebuf.as<T>() + size_t(s) * tr, tr, sums.as<double>() + 2 * s);
-      ++c.launches;
+      if (e_given) {
+        GJ_CUDA(err, cudaMemcpyAsync(ebuf.as<T>() + size_t(s) * tr, dobsbuf.as<T>() + size_t(s) * tr,
+                                     tr * sizeof(T), cudaMemcpyDeviceToDevice, st));
+      } else {
+        k_residual<T><<<dim3(64, 1), 256, 0, st>>>(dbuf.as<T>() + size_t(s) * tr, dobsbuf.as<T>() + size_t(s) * tr,
+                                                    ebuf.as<T>() + size_t(s) * tr, tr, sums.as<double>() + 2 * s);
+        ++c.launches;
+      }
       GJ_CUDA(err, cudaMemsetAsync(L - ld, 0, sstride * sizeof(T), st));
       T* A_ = acc.as<T>() + size_t(s) * 4 * dn;
       for (int sidx = int(segs.size()) - 1; sidx >= 0; --sidx) {
@@ -1389,7 +1626,8 @@ class WSolver : public WSolverBase {
                                        cudaMemcpyDeviceToDevice, st));
           k_domain_copy<T><<<dim3(64, 1), 256, 0, st>>>(w, S, sstride, slot(s0, base), dn, 1);
           ++c.launches;
-          for (int it = s0; it < std::min(s1 + 1, nt); ++it) fwd_step(it, slot(it + 1, base));
+          if (band_on) band_rec(S, bslot(s0, base), 1, st, nlb);
+          for (int it = s0; it < std::min(s1 + 1, nt); ++it) fwd_step(it, slot(it + 1, base), bslot(it + 1, base));
         }
         for (int k = s1; k >= s0 + 1; --k) {
           const int itf = k - 1;
@@ -1408,6 +1646,10 @@ class WSolver : public WSolverBase {
           } else {
             k_inject_add<T><<<dim3(1, 1), 128, 0, st>>>(L, sstride, recbuf.as<long>() + size_t(s) * nrr, nrr,
                                                         nrsbuf.as<int>() + s, ebuf.as<T>() + size_t(s) * tr, itf, nt, 1);
+            if (band_on) {
+              band_adj(L, blam.as<T>(), 1, st, nlb);
+              band_image(blam.as<T>(), bslot(k, base), 1, 1, s, 0, st, nlb);
+            }
             k_plain_adj_e<T><<<grd, blk, 0, st>>>(w, L, fstride, px, py, lm, slot(k, base), slot(k - 1, base), A_);
             k_plain_adj_h<T><<<grd, blk, 0, st>>>(w, L, fstride, px, py, qx, qy);
             k_plain_adj_assemble<T><<<grd, blk, 0, st>>>(w, L, lm, qx, qy);
@@ -1418,6 +1660,7 @@ class WSolver : public WSolverBase {
       }
     }
     c.timer.cur = nullptr;
+    c.launches += nlb;
     GJ_CUDA(err, cudaGetLastError());
     std::vector<double> hsums(2 * nshots);
     GJ_CUDA(err, cudaMemcpyAsync(hsums.data(), sums.p, 2 * nshots * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1449,7 +1692,7 @@ class WSolver : public WSolverBase {
       for (int t = 0; t < nt; ++t)
         for (int b = 0; b < g.n; ++b)
           for (int a_ = 0; a_ < g.m; ++a_)
-            hu[size_t(t) * dn + size_t(b) * ld + w.di0 + a_] = T(u[size_t(t) * mn + size_t(b) * g.m + a_]);
+            hu[size_t(t) * dn + size_t(b) * hld + w.di0 - hr0 + a_] = T(u[size_t(t) * mn + size_t(b) * g.m + a_]);
       GJ_CUDA(err, cudaMemcpy(hist.as<T>() + dn, hu.data(), hu.size() * sizeof(T), cudaMemcpyHostToDevice));
     }
     GJ_TRY(adjA.alloc(err, sstride * sizeof(T)));
@@ -1531,30 +1774,37 @@ gj_status w_forward(Ctx& c, const gj_w_grid& g, gj_precision prec, const double*
 gj_status w_gradient(Ctx& c, const gj_w_grid& g, gj_precision prec, const void* eps, const void* sig,
                      bool dev_in, const gj_w_shot* shots, int nshots, const void* dobs, bool dev_dobs,
                      gj_adj_mode mode, gj_misfit_kind mk, const gj_w_opts& o, void* geps, void* gsig,
-                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st) {
+                     bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st, bool e_given) {
   if (!eps || !sig || !dobs || !geps || !gsig) return c.err.set(GJ_EINVAL, "null input or output pointer");
   if (mode != GJ_ADJ_REFERENCE && mode != GJ_ADJ_EXACT) return c.err.set(GJ_EINVAL, "unknown adjoint mode");
   if (mk < GJ_MISFIT_L2 || mk > GJ_MISFIT_ENV_LOG) return c.err.set(GJ_EINVAL, "unknown misfit kind");
   if (prec == GJ_F64) {
     WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
     return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, mk, o, geps, gsig, dev_out, misfit_out,
-                       d_out, e_out, st);
+                       d_out, e_out, st, e_given);
   }
   WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
   return s->gradient(c.err, c, eps, sig, dev_in, dobs, dev_dobs, mode, mk, o, geps, gsig, dev_out, misfit_out,
-                     d_out, e_out, st);
+                     d_out, e_out, st, e_given);
 }
 
 gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,
-                   const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out) {
+                   const gj_w_shot* shots, int nshots, const double* dobs, gj_misfit_kind mk, double* misfit_out,
+                   int ntrial, const gj_w_opts* opts) {
   if (!eps || !sig || !dobs || !misfit_out) return c.err.set(GJ_EINVAL, "null input or output pointer");
   if (mk < GJ_MISFIT_L2 || mk > GJ_MISFIT_ENV_LOG) return c.err.set(GJ_EINVAL, "unknown misfit kind");
-  if (prec == GJ_F64) {
-    WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
-    return s->misfit(c.err, c, eps, sig, dobs, mk, misfit_out, 0);
+  if (ntrial < 1) return c.err.set(GJ_EINVAL, "ntrial must be >= 1");
+  const size_t mn = size_t(g.m) * size_t(g.n);
+  for (int t = 0; t < ntrial; ++t) {
+    if (prec == GJ_F64) {
+      WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+      GJ_TRY(s->misfit(c.err, c, eps + t * mn, sig + t * mn, dobs, mk, misfit_out + size_t(t) * nshots, 0, opts));
+    } else {
+      WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+      GJ_TRY(s->misfit(c.err, c, eps + t * mn, sig + t * mn, dobs, mk, misfit_out + size_t(t) * nshots, 0, opts));
+    }
   }
-  WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
-  return s->misfit(c.err, c, eps, sig, dobs, mk, misfit_out, 0);
+  return GJ_OK;
 }
 
 gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps, const double* sig,

@@ -1,13 +1,10 @@
 """Step lengths of the radar permittivity and conductivity updates, as the
 reference chooses them around its objective evaluations (w_stepparabola_e.m,
-w_stepparabola_s.m, w_boundstep2.m, w_objs_e.m:24-25, w_objs_s.m:22-25).  The trial objectives are forward-only runs of all shots,
-which ``Context.w_misfit`` (gj_w_misfit) does on the GPU; this module holds the
-host logic around them.
-
-The reference's trial objective also band-filters the observed and modelled
-traces (w_objs_e.m:33-36) before the misfit; gj_w_misfit has no such filter, so
-with a band-limited inversion the trial misfits here are of the unfiltered
-traces.
+w_stepparabola_s.m, w_boundstep2.m, w_objs_e.m:24-25, w_objs_s.m:22-25).  The
+trial objectives are forward-only runs of all shots; all trial models of one
+search run in one ``Context.w_misfit_trials`` call (gj_w_misfit_trials), which
+band-filters the observed and modelled traces first as w_objs_e.m:33-36 does.
+This module holds the host logic around them.
 """
 from __future__ import annotations
 
@@ -66,7 +63,7 @@ def stepparabola(eps, g_e, objective: Callable[[float], float], E0: float, eps_m
     ke_ = -boundstep2(eps, g_e, eps_max, eps_min, k_e) * keprct_
     ke__ = boundstep2(eps, -np.asarray(g_e, np.float64), eps_max, eps_min, k_e) * keprct__
     ks = np.linspace(ke_, ke__, nparabo)
-    E = np.array([float(E0)] + [float(objective(float(k))) for k in ks])
+    E = np.concatenate([[float(E0)], _evaluate(objective, ks)])
     ke = np.concatenate([[0.0], ks])
     with np.errstate(all="ignore"):
         p = np.polyfit(ke, E, 2)
@@ -87,7 +84,7 @@ def stepparabola_s(sig, g_s, objective: Callable[[float], float], E0: float, sig
     same exponential update (w_objs_s.m:22-25)."""
     kb = boundstep2(sig, -np.asarray(g_s, np.float64), sig_max, sig_min, k_s)
     ks = np.linspace(kb * ksprct_, kb * ksprct__, nparabo + 2)
-    E = np.array([float(E0)] + [float(objective(float(k))) for k in ks])
+    E = np.concatenate([[float(E0)], _evaluate(objective, ks)])
     k = np.concatenate([[0.0], ks])
     with np.errstate(all="ignore"):
         p = np.polyfit(k, E, 2)
@@ -97,19 +94,50 @@ def stepparabola_s(sig, g_s, objective: Callable[[float], float], E0: float, sig
     return float(step), k, E
 
 
-def misfit_objective(ctx, grid, eps, sig, shots, d_obs, g, misfit=0, precision=0,
-                     which: str = "eps") -> Callable[[float], float]:
+def _evaluate(objective, ks) -> np.ndarray:
+    """Objective values at the trial steps ks: one batched call when the
+    objective offers ``many`` (all trial models in one GPU call), else one
+    call per step."""
+    many = getattr(objective, "many", None)
+    if many is not None:
+        return np.asarray(many(np.asarray(ks, np.float64)), np.float64)
+    return np.array([float(objective(float(k))) for k in ks])
+
+
+class MisfitObjective:
     """The trial objective of w_objs_e.m (which = "eps") or w_objs_s.m
     (which = "sig") on the GPU: the summed normalised misfit of all shots with
-    that parameter perturbed as x exp(-k x g), one gj_w_misfit call (forward
-    runs only) per trial."""
-    if which not in ("eps", "sig"):
-        raise ValueError("which must be 'eps' or 'sig'")
+    that parameter perturbed as x exp(-k x g).  ``many(ks)`` evaluates all
+    trial steps of a search in one gj_w_misfit_trials call (forward runs
+    only); calling the object evaluates one step.  ``filt = (f_, f__)`` are
+    regu.f_ and regu.f__ of w_objs_e.m:33-36: both trace sets are band-filtered
+    (filt_gauss.m, exponent 8) before the misfit."""
 
-    def objective(k: float) -> float:
-        e, s_ = (perturb_eps(eps, g, k), sig) if which == "eps" else (eps, perturb_eps(sig, g, k))
-        return float(np.sum(ctx.w_misfit(grid, e, s_, shots, d_obs, misfit=misfit, precision=precision)))
-    return objective
+    def __init__(self, ctx, grid, eps, sig, shots, d_obs, g, misfit=0, precision=0, which="eps", filt=None):
+        if which not in ("eps", "sig"):
+            raise ValueError("which must be 'eps' or 'sig'")
+        self.ctx, self.grid, self.eps, self.sig, self.shots, self.d_obs = ctx, grid, eps, sig, shots, d_obs
+        self.g, self.misfit, self.precision, self.which, self.filt = g, misfit, precision, which, filt
+
+    def _models(self, ks):
+        if self.which == "eps":
+            return [perturb_eps(self.eps, self.g, k) for k in ks], [self.sig] * len(ks)
+        return [self.eps] * len(ks), [perturb_eps(self.sig, self.g, k) for k in ks]
+
+    def many(self, ks) -> np.ndarray:
+        e, s_ = self._models(ks)
+        m = self.ctx.w_misfit_trials(self.grid, e, s_, self.shots, self.d_obs, misfit=self.misfit,
+                                     precision=self.precision, filt=self.filt)
+        return m.sum(axis=1)
+
+    def __call__(self, k: float) -> float:
+        return float(self.many([k])[0])
+
+
+def misfit_objective(ctx, grid, eps, sig, shots, d_obs, g, misfit=0, precision=0, which: str = "eps",
+                     filt=None) -> MisfitObjective:
+    """The trial objective of w_objs_e.m / w_objs_s.m (see MisfitObjective)."""
+    return MisfitObjective(ctx, grid, eps, sig, shots, d_obs, g, misfit, precision, which, filt)
 
 
 def dc_stepparabola(sig, g, objective: Callable[[float], float], E0: float, sig_max: float, sig_min: float,
@@ -124,7 +152,7 @@ def dc_stepparabola(sig, g, objective: Callable[[float], float], E0: float, sig_
     k_ = -boundstep2(sig, g, sig_max, sig_min, k_s) * kprct_
     k__ = boundstep2(sig, -g, sig_max, sig_min, k_s) * kprct__
     ks = np.linspace(k_, k__, 4)
-    E = np.array([float(E0)] + [float(objective(float(k))) for k in ks])
+    E = np.concatenate([[float(E0)], _evaluate(objective, ks)])
     k = np.concatenate([[0.0], ks])
     with np.errstate(all="ignore"):
         p = np.polyfit(k, E, 2)
@@ -137,20 +165,39 @@ def dc_stepparabola(sig, g, objective: Callable[[float], float], E0: float, sig_
     return float(step), k, E
 
 
-def dc_misfit_objective(ctx, sig, robin: int, DX: float, DZ: float, srcs, g, std=None) -> Callable[[float], float]:
+def dc_E(d_o, d, w=None, obj_fnc: str = "L2") -> float:
+    """dc_E.m: 0.5 e' N e with e = d - d_o, on the squared data for 'env_L22'
+    and on the log data for 'env_LOG'; N = diag(w) (ones when None)."""
+    d = np.asarray(d, np.float64).ravel()
+    d_o = np.asarray(d_o, np.float64).ravel()
+    if obj_fnc == "env_L22":
+        d, d_o = d ** 2, d_o ** 2
+    elif obj_fnc == "env_LOG":
+        d, d_o = np.log(d), np.log(d_o)
+    elif obj_fnc != "L2":
+        raise ValueError(f"unknown DC obj_FNC {obj_fnc!r}")
+    e = d - d_o
+    w = np.ones_like(e) if w is None else np.asarray(w, np.float64).ravel()
+    return 0.5 * float(e @ (w * e))
+
+
+def dc_misfit_objective(ctx, sig, robin: int, DX: float, DZ: float, srcs, g, std=None,
+                        obj_fnc: str = "L2") -> Callable[[float], float]:
     """The trial objective of dc_objs2_5d.m on the GPU: the model sig (n0 x m0,
     before the Robin padding) perturbed as sig exp(-k sig g), padded (dc_robin),
-    one gj_dc_forward over the sources, and per source 0.5 sum std e^2 /
-    sum d_obs^2 (dc_E.m with N = diag(std_)), summed over the sources.  `std`
-    is a list of per-datum weights (ones when None)."""
+    one gj_dc_forward over the sources, and per source dc_E(d_o, d, std,
+    obj_fnc) / (d_o' d_o) (the normaliser uses the untransformed data,
+    dc_objs2_5d.m).  The reference runs this search per source inside
+    dc_update2_5d(i_e); pass a one-source list for that; with several sources
+    the per-source objectives are summed.  `std` is a list of per-datum
+    weights (ones when None)."""
     from .dc import dc_robin
 
     def objective(k: float) -> float:
         d = ctx.dc_forward(dc_robin(perturb_eps(sig, g, k), robin), DX, DZ, robin, srcs)["d"]
         total = 0.0
         for j, (q, dj) in enumerate(zip(srcs, d)):
-            e = np.asarray(dj, np.float64) - np.asarray(q.d_obs, np.float64)
-            w = np.ones_like(e) if std is None else np.asarray(std[j], np.float64)
-            total += 0.5 * float(e @ (w * e)) / float(np.asarray(q.d_obs) @ np.asarray(q.d_obs))
+            do = np.asarray(q.d_obs, np.float64)
+            total += dc_E(do, dj, None if std is None else std[j], obj_fnc) / float(do @ do)
         return total
     return objective

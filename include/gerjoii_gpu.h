@@ -150,6 +150,43 @@ gj_status gj_w_misfit(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision
                       const double* eps_r, const double* sigma, const gj_w_shot* shots,
                       int nshots, const double* d_obs, gj_misfit_kind misfit, double* misfit_out);
 
+/* Objective values of several trial models for the step-length search:
+ * replaces the nparabo calls of w_objs_e.m:24-65 (and w_objs_s.m) that
+ * w_stepparabola_e.m:20-27 / w_stepparabola_s.m make, each a forward run of
+ * every shot followed by the misfit.
+ *   eps_r, sigma : ntrial models, m x n each, concatenated (the perturbed
+ *                  parame_.w.epsilon of w_objs_e.m:24-25)
+ *   opts         : may be NULL; filt_low < filt_high band-filters both the
+ *                  modelled and the observed traces first (filt_gauss.m with
+ *                  exponent filt_steep, 0 = 8), as w_objs_e.m:33-36 does with
+ *                  regu.f_ and regu.f__; the misfit and its d_o'd_o normaliser
+ *                  are then those of the filtered traces
+ *   misfit_out   : ntrial x nshots misfits, trial-major */
+gj_status gj_w_misfit_trials(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, int ntrial,
+                             const double* eps_r, const double* sigma, const gj_w_shot* shots, int nshots,
+                             const double* d_obs, gj_misfit_kind misfit, const gj_w_opts* opts,
+                             double* misfit_out);
+
+/* Backward half of the forward/backward pair gj_w_forward -> gj_w_backward:
+ * the adjoint of the forward map applied to given adjoint sources, the role of
+ * [g, a_max] = w_grad(u_w, ...) after w_fwd in the reference (w_grad.m:1,
+ * called by w_update_e.m:98 and w_update_s.m:77), for nshots shots at once.
+ *   e     : per shot nt x nr adjoint sources, shots concatenated (the residual
+ *           e_2d of w_fwd.m:34, or any dJ/dd)
+ *   mode  : GJ_ADJ_EXACT gives g = (dd/d eps_r)^T e and (dd/d sigma)^T e, the
+ *           PML-coefficient terms of the edge cells included; GJ_ADJ_REFERENCE
+ *           gives w_grad.m's g_eps = w_grad(d/dt u), g_sig = w_grad(u)
+ *   opts  : as gj_w_gradient (memory plan, per_shot, conditioning, band filter
+ *           of e); misfit options do not apply
+ * The forward wavefield is recomputed from the model inside the call with the
+ * same memory plan as gj_w_gradient (whole history or checkpoints): the exact
+ * adjoint needs the forward's PML split fields and strip H fields besides the
+ * model-domain u history that gj_w_forward returns.  For w_grad(u) on a
+ * caller-supplied u of one shot, see gj_w_grad. */
+gj_status gj_w_backward(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const double* eps_r,
+                        const double* sigma, const gj_w_shot* shots, int nshots, const double* e,
+                        gj_adj_mode mode, const gj_w_opts* opts, double* g_eps, double* g_sig);
+
 /* The adjoint half on its own: replaces [g, a_max] = w_grad(u, ...) (w_grad.m:1-115)
  * for one shot.  u is the m x n x nt history (or its time derivative), e the
  * nt x nr residual.  a_max may be NULL.  Reference semantics only. */
@@ -229,6 +266,15 @@ gj_status gj_dc_forward(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma
                         const gj_dc_src* srcs, int nsrc, const gj_dc_opts* opts,
                         double* d_out, double* u_out, gj_dc_stats* stats);
 
+/* gj_dc_forward that also returns the per-wavenumber potentials
+ * gerjoii_.dc.u_k of dc_fwd2_5d.m:61 (dc_fwd_k.m:43 for every ky).
+ *   uk_out : nsrc x n_ky x (n*m), per source the column-major (n*m) x n_ky u_k
+ *            (the potential of wavenumber ky_k in column k), may be NULL
+ * The other arguments are gj_dc_forward's. */
+gj_status gj_dc_forward_k(gj_ctx* ctx, const gj_dc_grid* grid, const double* sigma, const gj_dc_src* srcs,
+                          int nsrc, const gj_dc_opts* opts, double* d_out, double* u_out, double* uk_out,
+                          gj_dc_stats* stats);
+
 /* Sensitivity: replaces dc_fwd2_5d followed by
  * gerjoii_ = dc_gradient2_5d(parame_, finite_, gerjoii_) (dc_gradient2_5d.m:18-41).
  *   g_out  : (n - 2 robin) x (m - robin) gradient (sum over sources, or nsrc of
@@ -266,9 +312,16 @@ gj_status gj_dc_alphas(const gj_dc_grid* grid, long a_node, long b_node, const d
  *     GJ_W_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the
  *     library until the process exits.  Grids that need more are rejected with
  *     GJ_EINVAL and a message in errbuf (may be NULL).
- *   - The first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *   - Every call made outside stream capture looks up the array's device
+ *     address (cudaGetSymbolAddress) with the calling thread's current device,
+ *     so a context re-created after cudaDeviceReset (MATLAB's
+ *     reset(gpuDevice)) gets its own address; a call made while `stream` is
+ *     being captured reuses the address of the last uncaptured call on that
+ *     device, so make the first call on a device before any stream capture.
+ *   - Receivers must be Ez nodes, 0 <= rec < (NX+1)(NY+1).  They are checked
+ *     on the device before the time loop and the result read back, which
+ *     waits for the work already queued on `stream`; a call with a receiver
+ *     outside the grid returns GJ_EINVAL and fills d_out_dev with NaN.
  *   - Calls share the array: work is queued on `stream` (a cudaStream_t, NULL
  *     = legacy default stream), and calls that overlap on the GPU, from any
  *     thread or stream, race on it.  Each call clears the fields it needs. */

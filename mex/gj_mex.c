@@ -157,6 +157,22 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
                         NULL, mxGetPr(plhs[0]), mxGetPr(plhs[1]), mxGetPr(plhs[2]), NULL, NULL));
     for (int k = 0; k < ns; ++k) mxFree(recs[k]);
     mxFree(recs); mxFree(shots); mxFree(dobs);
+  } else if (!strcmp(cmd, "w_backward")) {
+    /* [g_eps, g_sig] = gj_mex('w_backward', eps, sigma, grid, S (ns x 2), Mcell, wavelet, e_cell, mode)
+       (the backward half of the pair w_solve -> w_backward: the adjoint of the forward map applied to
+        the residuals e_2d of every shot, w_grad.m:1 after w_fwd.m; mode 1 = exact adjoint, the default) */
+    gj_w_grid g = wgrid(prhs[3]);
+    long** recs;
+    double* e;
+    int ns;
+    gj_w_shot* shots = pack_shots(prhs[4], prhs[5], prhs[6], prhs[7], g.nt, &recs, &e, &ns);
+    const gj_adj_mode mode = nrhs > 8 ? (gj_adj_mode)(int)mxGetScalar(prhs[8]) : GJ_ADJ_EXACT;
+    plhs[0] = mxCreateDoubleMatrix(g.m, g.n, mxREAL);
+    plhs[1] = mxCreateDoubleMatrix(g.m, g.n, mxREAL);
+    check(gj_w_backward(ctx(), &g, prec, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, e, mode, NULL,
+                        mxGetPr(plhs[0]), mxGetPr(plhs[1])));
+    for (int k = 0; k < ns; ++k) mxFree(recs[k]);
+    mxFree(recs); mxFree(shots); mxFree(e);
   } else if (!strcmp(cmd, "w_misfit")) {
     /* E = gj_mex('w_misfit', eps, sigma, grid, S (ns x 2), Mcell, wavelet, dobs_cell, obj_FNC)
        (the forward-only objective of every shot for a trial model, w_objs_e.m:24-65) */
@@ -171,7 +187,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     for (int k = 0; k < ns; ++k) mxFree(recs[k]);
     mxFree(recs); mxFree(shots); mxFree(dobs);
   } else if (!strcmp(cmd, "dc_fwd2_5d") || !strcmp(cmd, "dc_gradient2_5d")) {
-    /* [d, u] = gj_mex('dc_fwd2_5d', sigma_robin, dcgrid, AB (ns x 2, 1-based), I, MNcell, kyw_cell, alpha_cell)
+    /* [d, u, u_k] = gj_mex('dc_fwd2_5d', sigma_robin, dcgrid, AB (ns x 2, 1-based), I, MNcell, kyw_cell,
+                            alpha_cell)   (u_k: (n*m) x n_ky x ns, gerjoii_.dc.u_k of dc_fwd2_5d.m:61)
        (alpha_cell = [] has the library compute dc_Lk.m's alphas, gj_dc_alphas)
        [g, d, e] = gj_mex('dc_gradient2_5d', ..., dobs_cell)   (dc_fwd2_5d.m, dc_gradient2_5d.m) */
     const int grad = !strcmp(cmd, "dc_gradient2_5d");
@@ -215,11 +232,17 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     if (!grad) {
       plhs[0] = mxCreateDoubleMatrix(nd, 1, mxREAL);
       double* u = NULL;
+      double* uk = NULL;
       if (nlhs > 1) {  /* stacked potentials, n*m per source */
         plhs[1] = mxCreateDoubleMatrix((size_t)g.n * g.m, ns, mxREAL);
         u = mxGetPr(plhs[1]);
       }
-      check(gj_dc_forward(ctx(), &g, mxGetPr(prhs[1]), srcs, ns, NULL, mxGetPr(plhs[0]), u, NULL));
+      if (nlhs > 2) {  /* per-wavenumber potentials, (n*m) x n_ky per source */
+        mwSize dk[3] = {(mwSize)g.n * g.m, (mwSize)g.n_ky, (mwSize)ns};
+        plhs[2] = mxCreateNumericArray(3, dk, mxDOUBLE_CLASS, mxREAL);
+        uk = mxGetPr(plhs[2]);
+      }
+      check(gj_dc_forward_k(ctx(), &g, mxGetPr(prhs[1]), srcs, ns, NULL, mxGetPr(plhs[0]), u, uk, NULL));
     } else {
       plhs[0] = mxCreateDoubleMatrix(g.n - 2 * g.robin, g.m - g.robin, mxREAL);
       plhs[1] = mxCreateDoubleMatrix(nd, 1, mxREAL);

@@ -45,6 +45,18 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
+def edge_cells(a):
+    """The model's edge cells (first and last row and column) of an m x n
+    array (or of the last two axes): the cells whose eps_r the PML replicates
+    (w_exp2pml.m:21-33), where the exact gradient collects the derivatives of
+    the PML coefficients."""
+    a = np.asarray(a)
+    m, n = a.shape[-2:]
+    msk = np.zeros((m, n), bool)
+    msk[0, :] = msk[-1, :] = msk[:, 0] = msk[:, -1] = True
+    return a[..., msk]
+
+
 def cosine(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()

@@ -11,13 +11,19 @@ pytestmark = pytest.mark.gpu
 
 
 def test_dc_forward_matches_direct_solve(gpu_ctx):
+    """Data, stacked potentials u and the per-wavenumber potentials u_k
+    (gerjoii_.dc.u_k of dc_fwd2_5d.m:61, through gj_dc_forward_k) against the
+    oracle's FP64 direct solves."""
     import np_dc_oracle as dco
     case = small_dc()
-    res = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], want_u=True)
+    res = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], want_u=True,
+                             want_uk=True)
     ref = oracle_forward(dco, case)
     for k, r in enumerate(ref):
         assert rel_l2(res["d"][k], r[2]) < 1e-9
         assert rel_l2(res["u"][k], r[0].reshape((case["n"], case["m"]), order="F")) < 1e-9
+        assert res["u_k"][k].shape == r[1].shape
+        assert rel_l2(res["u_k"][k], r[1]) < 1e-9
     assert res["rel_residual"] <= 1e-10
 
 

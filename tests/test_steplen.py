@@ -2,6 +2,7 @@
 w_stepparabola_e.m's parabola vertex, on models and objectives with known
 answers."""
 import numpy as np
+import pytest
 
 from gerjoii_b200 import steplen
 
@@ -108,3 +109,37 @@ def test_dc_misfit_objective_on_the_oracle():
     obj2 = steplen.dc_misfit_objective(Oracle(), sig0, case["robin"], case["DX"], case["DZ"], case["srcs"], g, std=w)
     assert abs(obj2(0.0) - 2 * ref) <= 1e-12 * ref
     assert np.isfinite(obj(1.0)) and obj(1.0) != obj(0.0)
+
+
+def test_dc_E_objective_transforms():
+    """dc_E.m: 0.5 e'Ne on the data, the squared data (env_L22) or the log
+    data (env_LOG)."""
+    rng = np.random.default_rng(3)
+    d_o = rng.uniform(0.5, 2.0, 20)
+    d = d_o * (1 + 0.1 * rng.standard_normal(20))
+    w = rng.uniform(0.5, 1.5, 20)
+    assert abs(steplen.dc_E(d_o, d, w) - 0.5 * np.sum(w * (d - d_o) ** 2)) < 1e-14
+    assert abs(steplen.dc_E(d_o, d, None, "env_L22") - 0.5 * np.sum((d ** 2 - d_o ** 2) ** 2)) < 1e-14
+    assert abs(steplen.dc_E(d_o, d, w, "env_LOG") - 0.5 * np.sum(w * (np.log(d) - np.log(d_o)) ** 2)) < 1e-14
+    with pytest.raises(ValueError):
+        steplen.dc_E(d_o, d, None, "L1")
+
+
+def test_batched_objective_is_used_by_the_searches():
+    """An objective with ``many`` is called once per search with all trial
+    steps (the batched GPU call) and gives the same step as per-step calls."""
+    eps = np.full((6, 7), 9.0)
+    g = np.full((6, 7), 0.01)
+    calls = []
+
+    class Obj:
+        def __call__(self, k):
+            return 1.0 + 3.0 * (k - 0.5) ** 2
+
+        def many(self, ks):
+            calls.append(len(ks))
+            return np.array([self(k) for k in ks])
+
+    s1, _, _ = steplen.stepparabola(eps, g, Obj(), 1.75, 25.0, 1.0, [1e-3, 1e2], 0.5, 0.9, 5)
+    s2, _, _ = steplen.stepparabola(eps, g, lambda k: Obj()(k), 1.75, 25.0, 1.0, [1e-3, 1e2], 0.5, 0.9, 5)
+    assert calls == [5] and s1 == s2

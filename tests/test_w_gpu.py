@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import rel_l2, cosine
+from conftest import rel_l2, cosine, edge_cells
 from gerjoii_b200 import synth
 from gerjoii_b200 import _native as N
 
@@ -63,18 +63,19 @@ def test_reference_gradient_matches_oracle(gpu_ctx, oracle, small_ft, prec, tol,
 
 @pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-10), (N.GJ_F32, 1e-4)])
 @pytest.mark.parametrize("ckpt", [0, 9])
-def test_exact_gradient_matches_oracle_interior(gpu_ctx, oracle, small_ft, prec, tol, ckpt):
-    p = small_ft
+@pytest.mark.parametrize("which", ["small_ft", "small_ref"])
+def test_exact_gradient_matches_oracle(gpu_ctx, oracle, which, request, prec, tol, ckpt):
+    """Every model cell, the edge cells (PML-coefficient terms) on their own too."""
+    p = request.getfixturevalue(which)
     g = p.grid
     dobs = _dobs(oracle, p)
     ge, gs, _ = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]), mode="exact")
     o = N.OptsC()
     o.ckpt_every = ckpt
     res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=prec, opts=o)
-    # interior model cells (edge cells also collect PML-coefficient terms)
-    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
-    assert rel_l2(res["g_eps"][sl], ge[sl]) < tol
-    assert rel_l2(res["g_sig"][sl], gs[sl]) < tol
+    assert rel_l2(res["g_eps"], ge) < tol
+    assert rel_l2(res["g_sig"], gs) < tol
+    assert rel_l2(edge_cells(res["g_eps"]), edge_cells(ge)) < 10 * tol
 
 
 def test_w_grad_matches_oracle(gpu_ctx, oracle, small_ref):
@@ -135,7 +136,8 @@ def test_autograd_harness_gradient_matches_finite_difference(gpu_ctx, oracle, sm
     sig = torch.tensor(p.sig0, dtype=torch.float64, device=dev, requires_grad=True)
     J = WGradient.apply(eps, sig, g, p.shots, do_t, gpu_ctx)
     J.backward()
-    for (a, b) in [(5, 10), (12, 20)]:
+    # interior cells and edge cells (the latter through the PML coefficients too)
+    for (a, b) in [(5, 10), (12, 20), (g.m - 1, 0), (g.m - 1, 17), (7, g.n - 1), (4, 0)]:
         h = 1e-5 * p.eps0[a, b]
         ep, em = p.eps0.copy(), p.eps0.copy()
         ep[a, b] += h
@@ -150,7 +152,7 @@ def test_autograd_harness_gradient_matches_finite_difference(gpu_ctx, oracle, sm
 def test_envelope_residual_and_exact_gradient_match_oracle(gpu_ctx, oracle, small_ft, prec, tol):
     """env_L2 (w_bozdag.m:16-25): residual against the numpy twin, misfit of the
     envelopes (w_E.m after w_fwd.m:34-35), exact gradient against the oracle's
-    exact adjoint driven by the same adjoint source (interior cells).  The
+    exact adjoint driven by the same adjoint source (all cells).  The
     residual divides by the envelope E, which magnifies the FP32 trace error
     (~1e-5) where E is small: hence the looser FP32 bound."""
     import np_oracle as npo
@@ -169,9 +171,8 @@ def test_envelope_residual_and_exact_gradient_match_oracle(gpu_ctx, oracle, smal
         a, b = oracle.grad_exact(g, p.eps0, p.sig0, sh, e)
         ge += a
         gs += b
-    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
-    assert rel_l2(res["g_eps"][sl], ge[sl]) < 10 * tol
-    assert rel_l2(res["g_sig"][sl], gs[sl]) < 10 * tol
+    assert rel_l2(res["g_eps"], ge) < 10 * tol
+    assert rel_l2(res["g_sig"], gs) < 10 * tol
 
 
 @pytest.mark.parametrize("kind", [N.GJ_MISFIT_PHASE_L2, N.GJ_MISFIT_ENV_L22, N.GJ_MISFIT_ENV_LOG],
@@ -204,9 +205,8 @@ def test_phase_and_envelope_variants_match_numpy_twin(gpu_ctx, oracle, small_ft,
         a, b = oracle.grad_exact(g, p.eps0, p.sig0, sh, res["e"][k])
         ge += a
         gs += b
-    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
-    assert rel_l2(res["g_eps"][sl], ge[sl]) < 1e-8
-    assert rel_l2(res["g_sig"][sl], gs[sl]) < 1e-8
+    assert rel_l2(res["g_eps"], ge) < 1e-8
+    assert rel_l2(res["g_sig"], gs) < 1e-8
 
 
 @pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-10), (N.GJ_F32, 2e-4)])
@@ -215,7 +215,7 @@ def test_band_filtered_residual_and_gradient_match_oracle(gpu_ctx, oracle, small
     """filt_gauss.m on the residual (w_update_e.m:69-70): the filtered residual
     against the numpy twin of filt_gauss, the misfit of the unfiltered residual,
     and the exact gradient against the oracle's exact adjoint driven by the
-    filtered residual (interior cells)."""
+    filtered residual (all cells)."""
     import np_oracle as npo
     p = small_ft
     g = p.grid
@@ -236,9 +236,8 @@ def test_band_filtered_residual_and_gradient_match_oracle(gpu_ctx, oracle, small
         a, b = oracle.grad_exact(g, p.eps0, p.sig0, sh, ef)
         ge += a
         gs += b
-    sl = (slice(0, g.m - 1), slice(1, g.n - 1))
-    assert rel_l2(res["g_eps"][sl], ge[sl]) < 10 * tol
-    assert rel_l2(res["g_sig"][sl], gs[sl]) < 10 * tol
+    assert rel_l2(res["g_eps"], ge) < 10 * tol
+    assert rel_l2(res["g_sig"], gs) < 10 * tol
 
 
 @pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-12), (N.GJ_F32, 1e-5)])
@@ -293,3 +292,114 @@ def test_gradient_conditioning_matches_numpy_twin(gpu_ctx, oracle, small_ft):
     assert rel_l2(cond["g_eps"], np.mean(te, axis=0)) < 1e-10
     assert rel_l2(cond["g_sig"], np.mean(ts, axis=0)) < 1e-10
     assert np.abs(cps["g_eps"]).max() == pytest.approx(1.0)
+
+
+def test_non_finite_results_return_enumeric(gpu_ctx, small_ft):
+    """NaN in the conductivity: forward, misfit-only and gradient calls (both
+    adjoint modes, FP32 and FP64) return GJ_ENUMERIC; with per-shot
+    conditioning the reference's NaN guard (w_update_e.m:131-137) zeroes the
+    gradients instead, and the context keeps working afterwards."""
+    p = small_ft
+    g = p.grid
+    sig = p.sig0.copy()
+    sig[5, 7] = np.nan
+    dobs = [np.zeros((g.nt, sh.nr)) for sh in p.shots]
+    for prec in (N.GJ_F32, N.GJ_F64):
+        with pytest.raises(N.GJError) as ei:
+            gpu_ctx.w_forward(g, p.eps0, sig, p.shots, precision=prec)
+        assert ei.value.status == N.GJ_ENUMERIC
+        with pytest.raises(N.GJError) as ei:
+            gpu_ctx.w_misfit(g, p.eps0, sig, p.shots, dobs, precision=prec)
+        assert ei.value.status == N.GJ_ENUMERIC
+        for mode in (N.GJ_ADJ_REFERENCE, N.GJ_ADJ_EXACT):
+            with pytest.raises(N.GJError) as ei:
+                gpu_ctx.w_gradient(g, p.eps0, sig, p.shots, dobs, mode=mode, precision=prec)
+            assert ei.value.status == N.GJ_ENUMERIC
+    o = N.OptsC()
+    o.condition, o.cond_fo, o.cond_ax, o.cond_az, o.per_shot = 1, 300e6, 0.2, 0.3, 1
+    with pytest.raises(N.GJError) as ei:  # the misfits themselves are still NaN
+        gpu_ctx.w_gradient(g, p.eps0, sig, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=o)
+    assert ei.value.status == N.GJ_ENUMERIC
+    r = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+    assert np.isfinite(r["g_eps"]).all()
+
+
+def test_small_memory_budget_checkpoints_with_the_same_result(gpu_ctx, oracle, small_ft):
+    """A memory budget too small for the whole u history makes the call
+    checkpoint and recompute (more launches) with the same FP64 gradient; a
+    grid whose fields cannot be allocated returns GJ_ENOMEM and leaves the
+    context usable."""
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    r1 = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+    n1 = gpu_ctx.last_launch_count
+    o = N.OptsC()
+    o.mem_budget_bytes = 4 << 20
+    o.no_graph = 1
+    r2 = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=o)
+    assert gpu_ctx.last_launch_count > n1
+    assert rel_l2(r2["g_eps"], r1["g_eps"]) < 1e-12 and rel_l2(r2["g_sig"], r1["g_sig"]) < 1e-12
+    import copy
+    huge = copy.copy(g)
+    huge.m, huge.n = 120000, 120000
+    with pytest.raises(N.GJError) as ei:
+        gpu_ctx.w_forward(huge, np.ones((3, 3)), np.ones((3, 3)), p.shots[:1])
+    assert ei.value.status in (N.GJ_ENOMEM, N.GJ_EINVAL)
+    r3 = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+    assert rel_l2(r3["g_eps"], r1["g_eps"]) < 1e-12
+
+
+@pytest.mark.parametrize("mode", [N.GJ_ADJ_EXACT, N.GJ_ADJ_REFERENCE])
+@pytest.mark.parametrize("plain", [0, 1])
+def test_forward_backward_pair_matches_gradient_and_oracle(gpu_ctx, oracle, small_ft, mode, plain):
+    """gj_w_forward -> residual on the host -> gj_w_backward (the MEX
+    forward/backward pair) equals the fused gj_w_gradient (FP64, 1e-12) and
+    the oracle's exact adjoint of the same adjoint sources (1e-10)."""
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    d = gpu_ctx.w_forward(g, p.eps0, p.sig0, p.shots, precision=N.GJ_F64)["d"]
+    e = [a - b for a, b in zip(d, dobs)]
+    o = N.OptsC()
+    o.plain = plain
+    bw = gpu_ctx.w_backward(g, p.eps0, p.sig0, p.shots, e, mode=mode, precision=N.GJ_F64, opts=o)
+    fu = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64, opts=o)
+    assert rel_l2(bw["g_eps"], fu["g_eps"]) < 1e-12
+    assert rel_l2(bw["g_sig"], fu["g_sig"]) < 1e-12
+    if mode == N.GJ_ADJ_EXACT:
+        ge, gs = np.zeros((g.m, g.n)), np.zeros((g.m, g.n))
+        for k, sh in enumerate(p.shots):
+            a, b = oracle.grad_exact(g, p.eps0, p.sig0, sh, e[k])
+            ge += a
+            gs += b
+        assert rel_l2(bw["g_eps"], ge) < 1e-10
+        assert rel_l2(bw["g_sig"], gs) < 1e-10
+
+
+@pytest.mark.parametrize("prec,tol", [(N.GJ_F64, 1e-10), (N.GJ_F32, 1e-4)])
+def test_misfit_trials_batched_and_band_filtered(gpu_ctx, oracle, small_ft, prec, tol):
+    """gj_w_misfit_trials: three trial models in one call equal three single
+    calls; with the band filter, each misfit is that of w_objs_e.m:33-36 on
+    the oracle's traces: both trace sets filtered (filt_gauss), then
+    0.5 |fd - fd_o|^2 / |fd_o|^2."""
+    import np_oracle as npo
+    p = small_ft
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    models = [p.eps0 * s for s in (0.97, 1.0, 1.04)]
+    sigs = [p.sig0] * 3
+    band = (80e6, 500e6)
+    many = gpu_ctx.w_misfit_trials(g, models, sigs, p.shots, dobs, precision=prec, filt=band)
+    assert many.shape == (3, len(p.shots))
+    for t, eps in enumerate(models):
+        one = gpu_ctx.w_misfit_trials(g, [eps], [p.sig0], p.shots, dobs, precision=prec, filt=band)
+        assert np.allclose(one[0], many[t], rtol=1e-12)
+        for k, sh in enumerate(p.shots):
+            d, _, _ = oracle.forward(g, eps, p.sig0, sh)
+            fd = npo.filt_gauss(d, g.dt, band[0], band[1], 8)
+            fo = npo.filt_gauss(dobs[k], g.dt, band[0], band[1], 8)
+            ref = 0.5 * np.sum((fd - fo) ** 2) / np.sum(fo ** 2)
+            assert abs(many[t, k] - ref) <= tol * ref
+    plain = gpu_ctx.w_misfit_trials(g, models, sigs, p.shots, dobs, precision=prec)
+    assert np.allclose(plain[1], gpu_ctx.w_misfit(g, models[1], p.sig0, p.shots, dobs, precision=prec), rtol=1e-12)

@@ -5,8 +5,9 @@ up front).  Its buffers live in a fixed per-device array inside the library.
 
 The test hands it device buffers it allocated itself, calls it twice in a row
 through the C ABI and compares each result with gj_w_forward, the allocating
-entry point.  The file name sorts last so a run that stops at the first failure
-has already run every other test.
+entry point, and with the oracle; a receiver outside the grid is rejected.
+The file name sorts last so a run that stops at the first failure has already
+run every other test.
 """
 import ctypes as C
 
@@ -69,3 +70,57 @@ def test_noalloc_rejects_grids_above_its_scratch_limit(gpu_ctx):
     st, msg = _call_noalloc(lib, g, eps_t, eps_t, shot, wav_t, rec_t, d_t)
     assert st == N.GJ_EINVAL
     assert "limit" in msg
+
+
+def test_noalloc_forward_matches_oracle_with_last_node_receiver(gpu_ctx, oracle):
+    """Traces against the FP64 oracle (FP32 bound 1e-5 rel-L2), with one
+    receiver on the last Ez node of the padded grid ((NX+1)(NY+1) - 1, on the
+    PEC corner: an all-zero trace) beside surface receivers."""
+    import torch
+    from gerjoii_b200.geometry import Shot
+    p = synth.small(m=24, n=40, pml=8, nt=300, free_top=True, seed=34)
+    g = p.grid
+    last = (g.NX + 1) * (g.NY + 1) - 1
+    sh = p.shots[0]
+    shot = Shot(sh.src_i, sh.src_j, sh.wavelet, np.concatenate([np.asarray(sh.rec, np.int64), [last]]))
+    d_ref, _, _ = oracle.forward(g, p.eps0, p.sig0, shot)
+    dev = torch.device("cuda", 0)
+    eps_t = torch.tensor(np.asfortranarray(p.eps0).ravel(order="F"), dtype=torch.float32, device=dev)
+    sig_t = torch.tensor(np.asfortranarray(p.sig0).ravel(order="F"), dtype=torch.float32, device=dev)
+    wav_t = torch.tensor(shot.wavelet[:g.nt], dtype=torch.float32, device=dev)
+    rec_t = torch.tensor(np.asarray(shot.rec, np.int64), dtype=torch.int64, device=dev)
+    for _ in range(2):
+        d_t = torch.full((shot.nr, g.nt), float("nan"), dtype=torch.float32, device=dev)
+        st, msg = _call_noalloc(N.load(), g, eps_t, sig_t, shot, wav_t, rec_t, d_t)
+        assert st == N.GJ_OK, msg
+        d = d_t.cpu().numpy().T
+        assert rel_l2(d, d_ref) < 1e-5
+        assert np.all(d[:, -1] == 0)
+
+
+def test_noalloc_rejects_receivers_outside_the_grid(gpu_ctx):
+    """A receiver index past the last Ez node (or negative) is never read:
+    the call returns GJ_EINVAL and every trace sample is NaN; the next call
+    with valid receivers works again."""
+    import torch
+    p = synth.small(m=24, n=40, pml=8, nt=60, free_top=True, seed=35)
+    g = p.grid
+    dev = torch.device("cuda", 0)
+    eps_t = torch.tensor(np.asfortranarray(p.eps0).ravel(order="F"), dtype=torch.float32, device=dev)
+    sig_t = torch.tensor(np.asfortranarray(p.sig0).ravel(order="F"), dtype=torch.float32, device=dev)
+    shot = p.shots[0]
+    wav_t = torch.tensor(shot.wavelet[:g.nt], dtype=torch.float32, device=dev)
+    lib = N.load()
+    for bad in ((g.NX + 1) * (g.NY + 1), -1):
+        rec = np.asarray(shot.rec, np.int64).copy()
+        rec[1] = bad
+        rec_t = torch.tensor(rec, dtype=torch.int64, device=dev)
+        d_t = torch.zeros((len(rec), g.nt), dtype=torch.float32, device=dev)
+        st, msg = _call_noalloc(lib, g, eps_t, sig_t, shot, wav_t, rec_t, d_t)
+        assert st == N.GJ_EINVAL and "outside" in msg, msg
+        assert torch.isnan(d_t).all()
+    rec_t = torch.tensor(np.asarray(shot.rec, np.int64), dtype=torch.int64, device=dev)
+    d_t = torch.zeros((shot.nr, g.nt), dtype=torch.float32, device=dev)
+    st, msg = _call_noalloc(lib, g, eps_t, sig_t, shot, wav_t, rec_t, d_t)
+    assert st == N.GJ_OK, msg
+    assert torch.isfinite(d_t).all()
