@@ -63,7 +63,8 @@ class DcSrcC(C.Structure):
 
 class DcOptsC(C.Structure):
     _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("per_source", C.c_int),
-                ("sources_per_batch", C.c_int), ("mem_budget_bytes", C.c_size_t), ("factor_fp32", C.c_int)]
+                ("sources_per_batch", C.c_int), ("mem_budget_bytes", C.c_size_t), ("factor_fp32", C.c_int),
+                ("precond", C.c_int)]
 
 
 class DcStatsC(C.Structure):

@@ -484,6 +484,93 @@ __global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac
   if (lane == 0) rz[sys] = acc;
 }
 
+// --------------------------------------------------------------------------
+// FP32 incomplete-Cholesky preconditioner IC(0) in red-black ordering (the
+// option beside the band factor).  With the nodes coloured by (l + h) & 1 the
+// 5-point operator is A = [Dr B; B' Db] (no red-red or black-black
+// couplings), and IC(0), which keeps only A's own pattern, is
+//   L = [Dr^1/2, 0; B' Dr^-1/2, Sb^1/2],  Sb = diag(Db - B' Dr^-1 B),
+// so M^-1 r takes two sweeps:
+//   black: z_b = (r_b - sum_red A(b, r) r_r / D_r) / Sb_b
+//   red:   z_r = (r_r - sum_black A(r, b) z_b) / D_r.
+// dinv[sys][t] holds 1 / D_r at the red nodes and 1 / Sb at the black ones,
+// in FP32; the sweeps run in FP32 and return z in FP64 for the FP64 flexible
+// CG, whose iteration refines the FP32-preconditioned solve to the FP64
+// tolerance.
+// --------------------------------------------------------------------------
+__global__ void k_dc_ic0_setup(const DcGrid G, const double* ox, const double* oz, const double* dbase,
+                               const double* sig, const double* alpha, const double* ky2, int sys0, int nsys,
+                               float* dinv, int* status) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys) return;
+  const double* al = alpha + size_t(sys0 + sys) * G.nb;
+  const double k2 = ky2[sys0 + sys];
+  float* Dv = dinv + size_t(sys) * G.N;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < G.N; t += blockDim.x * gridDim.x) {
+    const int l = t % G.n, h = t / G.n;
+    double d = dc_diag(G, dbase, sig, al, k2, l, h);
+    if ((l + h) & 1) {  // black: Schur diagonal over the red neighbours
+      if (l + 1 < G.n) d -= ox[t] * ox[t] / dc_diag(G, dbase, sig, al, k2, l + 1, h);
+      if (l >= 1) d -= ox[t - 1] * ox[t - 1] / dc_diag(G, dbase, sig, al, k2, l - 1, h);
+      if (h + 1 < G.m) d -= oz[t] * oz[t] / dc_diag(G, dbase, sig, al, k2, l, h + 1);
+      if (h >= 1) d -= oz[t - G.n] * oz[t - G.n] / dc_diag(G, dbase, sig, al, k2, l, h - 1);
+    }
+    if (!(d > 0.0) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
+    Dv[t] = float(1.0 / d);
+  }
+}
+
+// Black sweep: z_b, and r.z over the black nodes into rz[sys].
+__global__ void k_dc_ic0_black(const DcGrid G, const float* dinv, const double* ox, const double* oz,
+                               const double* r, double* z, double* rz, int nsys, const int* done) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys || (done && done[sys])) return;
+  const size_t o = size_t(sys) * G.N;
+  const float* Dv = dinv + o;
+  const double* R = r + o;
+  double part = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < G.N; t += blockDim.x * gridDim.x) {
+    const int l = t % G.n, h = t / G.n;
+    if (!((l + h) & 1)) continue;
+    float v = float(R[t]);
+    if (l + 1 < G.n) v -= float(ox[t]) * (float(R[t + 1]) * Dv[t + 1]);
+    if (l >= 1) v -= float(ox[t - 1]) * (float(R[t - 1]) * Dv[t - 1]);
+    if (h + 1 < G.m) v -= float(oz[t]) * (float(R[t + G.n]) * Dv[t + G.n]);
+    if (h >= 1) v -= float(oz[t - G.n]) * (float(R[t - G.n]) * Dv[t - G.n]);
+    const double zb = double(v * Dv[t]);
+    z[o + t] = zb;
+    part += R[t] * zb;
+  }
+  for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(rz + sys, part);
+}
+
+// Red sweep after the black one: z_r, and r.z over the red nodes into rz[sys].
+__global__ void k_dc_ic0_red(const DcGrid G, const float* dinv, const double* ox, const double* oz,
+                             const double* r, double* z, double* rz, int nsys, const int* done) {
+  const int sys = blockIdx.y;
+  if (sys >= nsys || (done && done[sys])) return;
+  const size_t o = size_t(sys) * G.N;
+  const float* Dv = dinv + o;
+  const double* R = r + o;
+  const double* Z = z + o;
+  double part = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < G.N; t += blockDim.x * gridDim.x) {
+    const int l = t % G.n, h = t / G.n;
+    if ((l + h) & 1) continue;
+    float v = float(R[t]);
+    if (l + 1 < G.n) v -= float(ox[t]) * float(Z[t + 1]);
+    if (l >= 1) v -= float(ox[t - 1]) * float(Z[t - 1]);
+    if (h + 1 < G.m) v -= float(oz[t]) * float(Z[t + G.n]);
+    if (h >= 1) v -= float(oz[t - G.n]) * float(Z[t - G.n]);
+    const double zr = double(v * Dv[t]);
+    z[o + t] = zr;
+    part += R[t] * zr;
+  }
+  for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(rz + sys, part);
+}
+
 // y = Lk x for every system (FP64), optional dot x.y into dot[sys].
 __global__ void k_dc_apply(const DcGrid G, const double* ox, const double* oz, const double* dbase,
                            const double* sig, const double* alpha, const double* ky2, int sys0,

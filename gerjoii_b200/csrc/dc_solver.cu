@@ -6,7 +6,8 @@
 // g = (2/pi) sum_k w_k g_k trimmed of the Robin padding (dc_gradient2_5d.m).
 // All systems of a batch of sources are solved together by FP64 CG
 // preconditioned with the band LDL^T factor of each system (FP64 by default,
-// FP32 on request).
+// FP32 on request), or, as an option, with the FP32 red-black IC(0)
+// preconditioner (k_dc_ic0_*).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -83,7 +84,7 @@ struct DcPlan {
 
 template <class TF>
 static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B, double* X, double tol, int maxit,
-                     int& iters, double& relmax, cudaStream_t st) {
+                     int& iters, double& relmax, cudaStream_t st, bool ic0 = false) {
   const DcGrid& G = P.G;
   const int N = G.N;
   const size_t vn = size_t(nsys) * N;
@@ -107,7 +108,13 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   const size_t shp = dc_precond_smem<TF>(G.wp);
   auto precond = [&](double* rzv) {  // one warp per system; window of 32R >= b + 1 positions
     const bool tm = c.timer.begin(KK_DC_PRECOND, st, nsys);
-    if (G.b < 128) k_dc_precond<TF, 4><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
+    if (ic0) {  // two FP32 sweeps of the red-black IC(0) factor
+      cudaMemsetAsync(rzv, 0, nsys * sizeof(double), st);
+      const float* Dv = c.dc_fac.as<float>();
+      k_dc_ic0_black<<<gv, 256, 0, st>>>(G, Dv, ox, oz, R, Z, rzv, nsys, done);
+      k_dc_ic0_red<<<gv, 256, 0, st>>>(G, Dv, ox, oz, R, Z, rzv, nsys, done);
+      c.launches += 1;
+    } else if (G.b < 128) k_dc_precond<TF, 4><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
     else k_dc_precond<TF, 8><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
     c.timer.end(tm, st);
   };
@@ -253,16 +260,18 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
   const size_t reusable = c.dc_fac.bytes + c.dc_vec.bytes;  // this context's DC buffers from earlier calls
   const size_t budget = o.mem_budget_bytes ? o.mem_budget_bytes : size_t(0.7 * double(free_b + reusable));
-  const size_t per_sys = size_t(G.nq) * G.wp * sizeof(TF) + size_t(N) * 8 * sizeof(double) + 64;
+  const bool ic0 = o.precond == 1;
+  const size_t fac_sys = ic0 ? size_t(N) * sizeof(float) : size_t(G.nq) * G.wp * sizeof(TF);
+  const size_t per_sys = fac_sys + size_t(N) * 8 * sizeof(double) + 64;
   int srcs_per_batch = int(std::min<size_t>(nsrc, std::max<size_t>(1, budget / (per_sys * nky))));
   if (o.sources_per_batch > 0) srcs_per_batch = std::min(srcs_per_batch, o.sources_per_batch);
   const int nsys_b = srcs_per_batch * nky;
-  GJ_TRY(c.dc_fac.alloc(err, size_t(nsys_b) * G.nq * G.wp * sizeof(TF)));
+  GJ_TRY(c.dc_fac.alloc(err, size_t(nsys_b) * fac_sys));
   GJ_TRY(c.dc_vec.alloc(err, size_t(nsys_b) * N * 7 * sizeof(double)));  // B, X, R, Z, P, AP, U
   GJ_TRY(P.dots.alloc(err, 6 * size_t(nsys_b) * sizeof(double)));
   GJ_TRY(P.done.alloc(err, nsys_b * sizeof(int)));
   const double tol = o.tol > 0 ? o.tol : 1e-10;
-  const int maxit = o.max_iter > 0 ? o.max_iter : 50;
+  const int maxit = o.max_iter > 0 ? o.max_iter : (ic0 ? 20000 : 50);
   int it_max = 0;
   double rel_max = 0;
   const size_t smem_f = dc_factor_smem<TF>(G.b);
@@ -285,13 +294,20 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     double* B = V;
     double* X = B + vn;  // X, R, Z, P, AP follow (pcg layout)
     double* U = X + 5 * vn;
-    // factor
+    // factor (band LDL^T), or the IC(0) diagonals
     {
       const bool tm = c.timer.begin(KK_DC_FACTOR, st, nsys);
-      k_dc_factor<TF><<<nsys, DC_FACTOR_THREADS, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(),
-                                                               P.alpha.as<double>(), P.ky2.as<double>(),
-                                                               P.tiles.as<unsigned>(), sys0, c.dc_fac.as<TF>(),
-                                                               P.status.as<int>());
+      if (ic0) {
+        const dim3 gv((N + 255) / 256 < 64 ? (N + 255) / 256 : 64, nsys);
+        k_dc_ic0_setup<<<gv, 256, 0, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(), P.alpha.as<double>(),
+                                           P.ky2.as<double>(), sys0, nsys, c.dc_fac.as<float>(),
+                                           P.status.as<int>());
+      } else {
+        k_dc_factor<TF><<<nsys, DC_FACTOR_THREADS, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(),
+                                                                 P.alpha.as<double>(), P.ky2.as<double>(),
+                                                                 P.tiles.as<unsigned>(), sys0, c.dc_fac.as<TF>(),
+                                                                 P.status.as<int>());
+      }
       c.timer.end(tm, st);
       ++c.launches;
     }
@@ -300,7 +316,7 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     k_dc_rhs_src<<<(nsys + 127) / 128, 128, 0, st>>>(N, P.ab.as<long>(), P.cur.as<double>(), nky, sys0, nsys, B);
     ++c.launches;
     int iters = 0; double rel = 0;
-    GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
+    GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st, ic0));
     it_max = std::max(it_max, iters); rel_max = std::max(rel_max, rel);
     GJ_CUDA(err, cudaMemcpyAsync(U, X, vn * sizeof(double), cudaMemcpyDeviceToDevice, st));
     // per-wavenumber potentials u_k of the batch's sources: [source][ky][node], the
@@ -331,7 +347,7 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
       k_dc_rhs_adj<<<dim3(1, nsb), 256, 0, st>>>(N, nky, s0, nsb, P.mnoff.as<long>(), P.mnbuf.as<long>(),
                                                  P.ebuf.as<double>(), B);
       ++c.launches;
-      GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st));
+      GJ_TRY(pcg<TF>(err, c, P, sys0, nsys, B, X, tol, maxit, iters, rel, st, ic0));
       it_max = std::max(it_max, iters); rel_max = std::max(rel_max, rel);
       k_dc_sens<<<dim3(64, nsys), 256, 0, st>>>(G, P.sig.as<double>(), P.alpha.as<double>(), P.ky2.as<double>(),
                                                 P.wts.as<double>(), sys0, nky, U, X, P.gbuf.as<double>(), nsys);
@@ -345,7 +361,8 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   std::vector<int> hst(nsys_all);
   GJ_CUDA(err, cudaMemcpy(hst.data(), P.status.p, nsys_all * sizeof(int), cudaMemcpyDeviceToHost));
   for (int s = 0; s < nsys_all; ++s)
-    if (hst[s]) return err.set(GJ_ENUMERIC, "zero or non-finite pivot in the band factor of system %d", s);
+    if (hst[s]) return err.set(GJ_ENUMERIC, "zero or non-finite pivot in the %s of system %d",
+                               ic0 ? "IC(0) factor" : "band factor", s);
   if (stats) { stats->max_iterations = it_max; stats->max_rel_residual = rel_max; }
   if (rel_max > tol * 10)
     return err.set(GJ_ENUMERIC, "CG reached relative residual %.3e > %.1e after %d iterations", rel_max, tol, it_max);

@@ -249,6 +249,10 @@ typedef struct gj_dc_opts {
   size_t mem_budget_bytes; /* 0 = 70% of free device memory */
   int factor_fp32;         /* 1 = FP32 band factor as the preconditioner (half the memory;
                               converges slowly for the smallest ky), else FP64 */
+  int precond;             /* 0 = band LDL^T factor of each system (FP64, or FP32 with
+                              factor_fp32); 1 = FP32 incomplete Cholesky IC(0) in red-black
+                              ordering (no factorisation pass, N floats per system; many
+                              more CG iterations); the CG itself is FP64 in both cases */
 } gj_dc_opts;
 
 typedef struct gj_dc_stats {

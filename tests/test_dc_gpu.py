@@ -166,3 +166,24 @@ def test_dc_fp32_factor_wide_band(gpu_ctx):
     assert a["rel_residual"] <= 1e-10 and b["rel_residual"] <= 1e-10
     for x, y in zip(a["d"], b["d"]):
         assert rel_l2(x, y) < 1e-9
+
+
+def test_dc_ic0_preconditioner_option_matches_direct_solve(gpu_ctx):
+    """The FP32 red-black IC(0) preconditioner option (gj_dc_opts.precond = 1):
+    FP64 CG refines to the same 1e-10 relative residual, so data, potentials
+    and the gradient equal the FP64 direct solve and the band-factor path; it
+    needs many more iterations than the band factor's one."""
+    import np_dc_oracle as dco
+    case = small_dc(seed=11)
+    o = N.DcOptsC()
+    o.precond = 1
+    res = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], opts=o, want_u=True)
+    assert res["rel_residual"] <= 1e-10 and res["iters"] > 1
+    for k, r in enumerate(oracle_forward(dco, case)):
+        assert rel_l2(res["d"][k], r[2]) < 1e-9
+        assert rel_l2(res["u"][k], r[0].reshape((case["n"], case["m"]), order="F")) < 1e-9
+    for q, r in zip(case["srcs"], oracle_forward(dco, case, case["SIG"] * 1.2)):
+        q.d_obs = r[2]
+    g1 = gpu_ctx.dc_gradient(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], opts=o)
+    g0 = gpu_ctx.dc_gradient(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
+    assert rel_l2(g1["g"], g0["g"]) < 1e-8
