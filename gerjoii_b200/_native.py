@@ -85,6 +85,7 @@ SIGNATURES = {
     "gj_version": (C.c_char_p, []),
     "gj_context_create": (_I, [C.POINTER(_VP), _I]),
     "gj_context_destroy": (_I, [_VP]),
+    "gj_context_release": (_I, [_VP]),
     "gj_last_error": (C.c_char_p, [_VP]),
     "gj_last_launch_count": (_L, [_VP]),
     "gj_set_kernel_timing": (_I, [_VP, _I]),
@@ -192,6 +193,10 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def release(self):
+        """gj_context_release: free the cached plans and DC buffers."""
+        self._check(self.lib.gj_context_release(self.h))
 
     def _check(self, st):
         if st != GJ_OK:

@@ -48,6 +48,16 @@ gj_status gj_context_destroy(gj_ctx* ctx) {
   return GJ_OK;
 }
 
+gj_status gj_context_release(gj_ctx* ctx) {
+  GJ_TRY(guard_ctx(ctx));
+  cudaDeviceSynchronize();
+  ctx->c.wsolver.reset();
+  ctx->c.wkey.clear();
+  ctx->c.dc_fac.release();
+  ctx->c.dc_vec.release();
+  return GJ_OK;
+}
+
 const char* gj_last_error(const gj_ctx* ctx) { return ctx ? ctx->c.err.msg.c_str() : "null context"; }
 
 long gj_last_launch_count(const gj_ctx* ctx) { return ctx ? ctx->c.launches : 0; }

@@ -187,3 +187,19 @@ def test_dc_ic0_preconditioner_option_matches_direct_solve(gpu_ctx):
     g1 = gpu_ctx.dc_gradient(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"], opts=o)
     g0 = gpu_ctx.dc_gradient(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
     assert rel_l2(g1["g"], g0["g"]) < 1e-8
+
+
+def test_context_release_frees_cached_buffers_and_keeps_working(gpu_ctx):
+    """gj_context_release frees the DC factors and CG vectors the context keeps
+    between calls (device memory comes back) and the next call works."""
+    import torch
+    case = small_dc(seed=12, n0=150, m0=60, pairs=6)
+    r1 = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    gpu_ctx.release()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 > free0
+    r2 = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
+    for a, b in zip(r1["d"], r2["d"]):
+        assert rel_l2(a, b) < 1e-12
