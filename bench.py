@@ -131,6 +131,17 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def band_counts(g):
+    """PML band Ez nodes (split fields) and band-frame entries per shot-step
+    (the band history of the exact adjoint, csrc/w_band.cuh band_geometry)."""
+    NX, NY, P, Pt = g.NX, g.NY, g.pml, g.pml_top
+    interior = (NX - P - 1 - Pt) * (NY - 2 * P - 1)
+    bnodes = (NX - 1) * (NY - 1) - interior
+    bR0, bRB = (NX - P) // 4 * 4, (NX + 3) // 4 * 4
+    bsz = 3 * (bRB * 2 * (P + 1) + (bRB - bR0) * (NY + 1))
+    return bnodes, bsz
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
@@ -392,12 +403,13 @@ def cfg3_leg(ctx):
 
 
 def cfg4_leg(args):
-    """48 uneven problems (grids 256..1536 x 128..512, dx 0.02..0.05 m, 1500..5000
-    steps, 4..24 shots; blob / layer models): every problem is one gradient call
-    (FP32, exact adjoint, Kahan sums, shot groups and graphs chosen per problem).
-    Timed: one whole pass over the 48 problems after a warm-up pass (the warm-up
-    builds each problem's plan and CUDA graphs).  Baseline: the plain per-shot
-    FP64 form on one shot of every 12th problem, compared per cell-update."""
+    """cfg4: 48 uneven problems (grids 256..1536 x 128..512, dx 0.02..0.05 m,
+    1500..5000 steps, 4..24 shots; blob / layer models), FP32 exact gradients
+    with Kahan sums, all of them in one gj_w_gradient_batch call: the problems
+    run concurrently in memory-budgeted waves, each wave one CUDA graph launch.
+    Timed: one call after a warm-up call (which plans, tunes and captures the
+    wave graphs).  Baseline: the plain per-shot FP64 form on one shot of
+    every 12th problem, compared per cell-update."""
     import torch
     from gerjoii_b200 import synth
     from gerjoii_b200 import _native as N
@@ -407,21 +419,23 @@ def cfg4_leg(args):
     for p in probs:
         d = ctx.w_forward(p.grid, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F32)["d"]
         data.append(d)
-
-    def one_pass():
-        t0 = time.perf_counter()
-        for p, d in zip(probs, data):
-            ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, d, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)
-        torch.cuda.synchronize()
-        return time.perf_counter() - t0
-
-    one_pass()
+    ctx.release()
+    batch = [(p.grid, p.eps0, p.sig0, p.shots, d) for p, d in zip(probs, data)]
+    t0 = time.perf_counter()
+    ctx.w_gradient_batch(batch, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)
+    torch.cuda.synchronize()
+    t_first = time.perf_counter() - t0
     clocks = Clocks(0)
     clocks.start()
-    t = one_pass()
+    t0 = time.perf_counter()
+    _, nwaves = ctx.w_gradient_batch(batch, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
     clk = clocks.stop()
+    launches = ctx.last_launch_count
     shots = sum(len(p.shots) for p in probs)
     upd = sum(2 * len(p.shots) * p.grid.nt * p.grid.NX * p.grid.NY for p in probs)
+    ctx.release()
     # plain FP64 sample
     o = N.OptsC()
     o.plain = 1
@@ -440,9 +454,10 @@ def cfg4_leg(args):
             "unit": "shot-gradients/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded blob / layer models, observed traces modelled on the device)",
-            "config": {"workload": "48 uneven problems (cfg4), one gradient call each, exact adjoint, FP32",
-                       "problems": len(probs), "shots": shots, "cell_updates": upd},
-            "gcell_updates_per_s": upd / t / 1e9, "clocks": clk,
+            "config": {"workload": "48 uneven problems (cfg4), one gj_w_gradient_batch call, exact adjoint, FP32",
+                       "problems": len(probs), "shots": shots, "cell_updates": upd, "waves": nwaves,
+                       "first_call_s": t_first},
+            "gcell_updates_per_s": upd / t / 1e9, "gpu_launches": launches, "clocks": clk,
             "plain_fp64_sample": {"gcell_updates_per_s": s_upd / s_t / 1e9,
                                   "sample": "1 shot of problems 0, 12, 24, 36, plain per-shot FP64 form",
                                   "speedup_fp32_over_plain_fp64": (upd / t) / (s_upd / s_t)}}
@@ -573,25 +588,32 @@ def main():
     value = shots_total / (ms / 1e3)
     cells = g.NX * g.NY
     mn = g.m * g.n
+    bnodes, bsz = band_counts(g)
     # cell-updates in the timed region: every forward, recompute and adjoint
     # launch (counted per step in the instrumented pass, which runs the same plan)
     upd = sum(ktimes[k]["shot_launches"] for k in ktimes if k != "image") / isteps * args.steps * cells * world
     gcell = upd / (ms / 1e3) / 1e9
     # Algorithmic DRAM bytes of each kernel kind over the timed region.
     #  fwd_step (k_fwdw): read Ez, Hx, Hy, Ceze, Cezhy + write Ez, Hx, Hy = 32 B per
-    #    padded cell, + 4 B per model node for the history write.
+    #    padded cell, + 4 B per model node for the history write, + 16 B per PML
+    #    band node (split fields Ezx, Ezy read and written), + 4 B per band-frame
+    #    entry for the band history write (exact adjoint).
     #  adj_step (k_adjw): the transposed stencil, 32 B per padded cell, + 4 B per
-    #    model node for the adjoint-field ring write.
-    #  image (k_image): per imaged step 8 B per model node (adjoint field + E
-    #    history), per launch 36 B per model node (one more E slot, the four
+    #    model node for the adjoint-field ring write, + 16 B per band node (split
+    #    adjoints), + 4 B per band-frame entry (adjoint band ring write).
+    #  image (k_image + k_image_band): per imaged step 8 B per model node and 8 B
+    #    per band-frame entry (adjoint ring + history), per launch 36 B per model
+    #    node and 20 B per band-frame entry (one more history slot, the
     #    compensated accumulators read and written).
     #  ref_step (k_stepv<float,1>): 32 B per cell + 48 B per model node (4 history
     #    reads, 4 accumulators read and written).
     adj_sl = ktimes.get("adj_step", {}).get("shot_launches", 0)
+    exact = args.mode == "exact"
+    bz = bsz if exact else 0
     alg = {
-        "fwd_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0),
-        "adj_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0),
-        "image": lambda k: adj_sl * mn * 8.0 + k["shot_launches"] * mn * 36.0,
+        "fwd_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0 + bnodes * 16.0 + bz * 4.0),
+        "adj_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0 + bnodes * 16.0 + bz * 4.0),
+        "image": lambda k: adj_sl * (mn + bz) * 8.0 + k["shot_launches"] * (mn * 36.0 + bz * 20.0),
         "ref_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 48.0),
     }
     # (a forward or adjoint "launch" is one step: the fast-only and the general
@@ -619,9 +641,12 @@ def main():
             "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes_per_launch"],
             "shots_per_launch": shots_per_launch,
             "launches": kt["launches"], "timed_launches": kt["sampled"], "avg_launch_us": kt["avg_us"],
-            "units": {"fwd_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n history write",
-                      "adj_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n adjoint-field ring write",
-                      "image": "per imaged shot-step 8 B x m*n, per shot-launch 36 B x m*n",
+            "units": {"fwd_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n history write + 16 B x PML "
+                                  "band nodes (split fields) + 4 B x band-frame entries (band history)",
+                      "adj_step": "per shot: 32 B x NX*NY cells (stencil) + 4 B x m*n adjoint-field ring write + 16 B "
+                                  "x PML band nodes + 4 B x band-frame entries (adjoint band ring)",
+                      "image": "per imaged shot-step 8 B x (m*n + band-frame entries), per shot-launch 36 B x m*n + "
+                               "20 B x band-frame entries",
                       "ref_step": "per shot: 32 B x NX*NY cells + 48 B x m*n (4 history reads, 4 sums r/w)"}[dom],
             "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / isteps / (ms / args.steps),
             "pass": "separate instrumented step after the timed region (CUDA events around every 8th launch of "

@@ -79,6 +79,14 @@ class OptsC(C.Structure):
                 ("condition", C.c_int), ("cond_fo", C.c_double), ("cond_ax", C.c_double), ("cond_az", C.c_double)]
 
 
+_DP_ = C.POINTER(C.c_double)
+
+
+class ProblemC(C.Structure):
+    _fields_ = [("grid", GridC), ("eps_r", _DP_), ("sigma", _DP_), ("shots", C.c_void_p), ("nshots", C.c_int),
+                ("d_obs", _DP_), ("g_eps", _DP_), ("g_sig", _DP_), ("misfit", _DP_)]
+
+
 # Every symbol the header declares, with its signature.
 _VP, _DP, _I, _L = C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_long
 SIGNATURES = {
@@ -96,6 +104,7 @@ SIGNATURES = {
     "gj_w_misfit": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, _DP]),
     "gj_w_misfit_trials": (_I, [_VP, C.POINTER(GridC), _I, _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I,
                                 C.POINTER(OptsC), _DP]),
+    "gj_w_gradient_batch": (_I, [_VP, _I, C.POINTER(ProblemC), _I, _I, C.POINTER(OptsC), C.POINTER(C.c_int)]),
     "gj_w_backward": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _I, _DP, _I, C.POINTER(OptsC),
                            _DP, _DP]),
     "gj_w_grad": (_I, [_VP, C.POINTER(GridC), _I, _DP, _DP, C.POINTER(ShotC), _DP, _DP, _DP, _DP]),
@@ -413,6 +422,34 @@ class Context:
         self._check(self.lib.gj_w_misfit_trials(self.h, C.byref(gc), precision, nt_, _dp(e), _dp(s_), sp.arr, sp.n,
                                                 _dp(ob), misfit_kind(misfit), C.byref(o), _dp(out)))
         return out.reshape(nt_, len(shots))
+
+    def w_gradient_batch(self, problems, mode=GJ_ADJ_EXACT, precision=GJ_F32, opts=None):
+        """gj_w_gradient_batch: problems is a list of (grid, eps, sig, shots,
+        d_obs) tuples (d_obs: list of nt x nr arrays); returns a list of
+        {"g_eps", "g_sig", "misfit"} and the number of waves used."""
+        keep, arr = [], (ProblemC * len(problems))()
+        outs = []
+        for k, (g, eps, sig, shots, dobs) in enumerate(problems):
+            sp = _ShotPack(shots, g.nt)
+            e, s_ = _f(eps), _f(sig)
+            ob = np.concatenate([_f(d).ravel(order="F") for d in dobs])
+            ge = np.zeros(g.m * g.n)
+            gs = np.zeros(g.m * g.n)
+            mis = np.zeros(len(shots))
+            keep += [sp, e, s_, ob]
+            arr[k].grid = grid_c(g)
+            arr[k].eps_r, arr[k].sigma = _dp(e), _dp(s_)
+            arr[k].shots = C.cast(sp.arr, C.c_void_p)
+            arr[k].nshots = len(shots)
+            arr[k].d_obs = _dp(ob)
+            arr[k].g_eps, arr[k].g_sig, arr[k].misfit = _dp(ge), _dp(gs), _dp(mis)
+            outs.append((g, ge, gs, mis))
+        nw = C.c_int(0)
+        self._check(self.lib.gj_w_gradient_batch(self.h, precision, arr, len(problems), int(mode),
+                                                 C.byref(opts) if opts else None, C.byref(nw)))
+        res = [{"g_eps": ge.reshape((g.m, g.n), order="F"), "g_sig": gs.reshape((g.m, g.n), order="F"),
+                "misfit": mis} for (g, ge, gs, mis) in outs]
+        return res, nw.value
 
     def w_gradient_dev(self, g, eps_t, sig_t, shots, dobs_t, ge_t, gs_t, mode=GJ_ADJ_REFERENCE,
                        misfit=GJ_MISFIT_L2, opts=None, stream=0):

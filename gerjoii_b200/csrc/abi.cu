@@ -100,6 +100,14 @@ gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precisi
                         o, g_eps, g_sig, false, misfit_out, d_out, e_out, 0);
 }
 
+gj_status gj_w_gradient_batch(gj_ctx* ctx, gj_precision precision, const gj_w_problem* probs, int nprob,
+                              gj_adj_mode mode, const gj_w_opts* opts, int* nwaves) {
+  GJ_TRY(guard_ctx(ctx));
+  gj_w_opts o{};
+  if (opts) o = *opts;
+  return gj::w_gradient_batch(ctx->c, precision, probs, nprob, mode, o, nwaves);
+}
+
 gj_status gj_w_backward(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, const double* eps_r,
                         const double* sigma, const gj_w_shot* shots, int nshots, const double* e, gj_adj_mode mode,
                         const gj_w_opts* opts, double* g_eps, double* g_sig) {

@@ -42,17 +42,24 @@ struct Err {
     if (s_ != GJ_OK) return s_;      \
   } while (0)
 
-// Owned device allocation.
+// Device allocation, owned (cudaMalloc) or borrowed from a caller-owned pool.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  bool owned = true;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() { if (p) cudaFree(p); }
+  ~DevBuf() { if (p && owned) cudaFree(p); }
+  // Points at n bytes of memory owned elsewhere (never freed here).
+  void borrow(void* q, size_t n) {
+    if (p && owned) cudaFree(p);
+    p = q; bytes = n; owned = false;
+  }
   gj_status alloc(Err& err, size_t n) {
-    if (n <= bytes && p) return GJ_OK;
-    if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+    if (n <= bytes && p && owned) return GJ_OK;
+    if (p && owned) cudaFree(p);
+    p = nullptr; bytes = 0; owned = true;
     if (n == 0) return GJ_OK;
     cudaError_t e = cudaMalloc(&p, n);
     if (e != cudaSuccess) {
@@ -64,9 +71,10 @@ struct DevBuf {
     return GJ_OK;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
     p = nullptr;
     bytes = 0;
+    owned = true;
   }
   template <class T> T* as() const { return static_cast<T*>(p); }
 };
@@ -82,6 +90,12 @@ struct ShotHost {
 class WSolverBase {
  public:
   virtual ~WSolverBase() = default;
+};
+
+// Cached state of gj_w_gradient_batch (plans, pool, wave graphs).
+class WBatchBase {
+ public:
+  virtual ~WBatchBase() = default;
 };
 
 // Kernel kinds reported by gj_kernel_time().
@@ -168,6 +182,7 @@ struct Ctx {
   // them before it plans its own memory.
   DevBuf dc_fac, dc_vec;
   std::string wkey;
+  std::unique_ptr<WBatchBase> wbatch;  // gj_w_gradient_batch's plans and wave graphs
 };
 
 // Radar entry points implemented in w_solver.cu.
@@ -186,6 +201,9 @@ gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* 
 gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* eps,
                       const double* sig, const gj_w_shot& shot, const double* e, const double* u,
                       double* gout, double* amax);
+
+gj_status w_gradient_batch(Ctx& c, gj_precision prec, const gj_w_problem* probs, int nprob, gj_adj_mode mode,
+                           const gj_w_opts& o, int* nwaves_out);
 
 // DC entry point implemented in dc_solver.cu.
 gj_status dc_run(Ctx& c, const gj_dc_grid& g, const double* sigma, const gj_dc_src* srcs, int nsrc, bool grad,

@@ -322,6 +322,7 @@ class WSolver : public WSolverBase {
     }
   };
   RingCfg rc;                    // configuration of the launches being enqueued
+  bool light_tune = false;       // batch plans: a smaller candidate set
   RingCfg rc_env;                // default, with the environment's overrides
   bool env_fixed = false;        // a GJ_RING_* variable is set: no tuning
   std::map<int, RingCfg> tuned;  // per launch size (shots per launch)
@@ -533,8 +534,10 @@ class WSolver : public WSolverBase {
   }
 
   // Autotuner: times candidate ring configurations for launches of gn shots
-  // on this grid (forward + exact-adjoint steps of zeroed states, no history)
-  // and keeps the fastest for gn.  Coordinate search: the fast kernel's
+  // on this grid (forward + exact-adjoint steps of zeroed states with the
+  // work of a real step: history and band-history writes, receiver record,
+  // adjoint-source injection, adjoint-field and band rings) and keeps the
+  // fastest for gn.  Coordinate search: the fast kernel's
   // stages x column chunk first, then the general kernel's stages x column
   // chunk x CTA width.  Needs the states and the adjoint-field ring of the
   // memory plan allocated for at least gn shots.
@@ -564,12 +567,19 @@ class WSolver : public WSolverBase {
       auto run = [&](int n) -> gj_status {
         for (int i = 0; i < n; ++i) {
           StepArgs<T> a = step_args(A, B, i % g.nt);
-          GJ_TRY(launch_fwd(err, a, gn, st));
+          if (hist.p && hist_slots > 1) { a.hist = hist.as<T>() + size_t(gn) * dn; a.hstride = dn; }
+          if (band_on && bhist.p && hist_slots > 1) a.band = bhist.as<T>() + size_t(gn) * size_t(w.bsz);
+          RecArgs<T> ra = rec_args(0);
+          if (nr > 0) { ra.d = dbuf.as<T>(); ra.it = i % g.nt; }
+          GJ_TRY(launch_fwd(err, a, gn, st, ra));
           std::swap(A, B);
           AdjRingArgs<T> b{};
           b.A = LA; b.B = LB; b.fstride = fstride; b.sstride = sstride; b.shot0 = 0;
           b.lout = lring.as<T>(); b.hstride = dn;
-          GJ_TRY(launch_adjr(err, b, gn, st, rec_args(0)));
+          if (band_on && blam.p) b.band = blam.as<T>();
+          RecArgs<T> rb = rec_args(0);
+          if (nr > 0) { rb.e = ebuf.as<T>(); rb.kinj = i % g.nt; }
+          GJ_TRY(launch_adjr(err, b, gn, st, rb));
           std::swap(LA, LB);
         }
         return GJ_OK;
@@ -595,16 +605,21 @@ class WSolver : public WSolverBase {
       if (t < tbest) { tbest = t; best = q; }
       return GJ_OK;
     };
-    for (int SF : {2, 3, 4})
-      for (int tjF : {16, 24, 32, 48}) {
+    const std::vector<int> SFs = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
+    const std::vector<int> tjFs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{16, 24, 32, 48};
+    const std::vector<int> Ss = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
+    const std::vector<int> tjSs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{8, 16, 32, 64};
+    const std::vector<int> rws = light_tune ? std::vector<int>{4} : std::vector<int>{2, 4};
+    for (int SF : SFs)
+      for (int tjF : tjFs) {
         RingCfg q = best;
         q.SF = SF; q.tjF = tjF;
         GJ_TRY(consider(q));
       }
     const RingCfg fast_best = best;
-    for (int S : {2, 3, 4})
-      for (int tjS : {8, 16, 32, 64})
-        for (int rw : {2, 4}) {
+    for (int S : Ss)
+      for (int tjS : tjSs)
+        for (int rw : rws) {
           RingCfg q = fast_best;
           q.S = S; q.tjS = tjS; q.RWG = rw;
           GJ_TRY(consider(q));
@@ -1389,26 +1404,26 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
-  // e_given: `dobs` holds the adjoint sources themselves (per shot nt x nr),
-  // the backward half of gj_w_backward: no residual, no misfit.
-  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
-                     bool dev_dobs, gj_adj_mode mode, gj_misfit_kind mk, const gj_w_opts& o, void* geps,
-                     void* gsig, bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st,
-                     bool e_given = false) {
-    GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
-    if (e_given) mk = GJ_MISFIT_L2;
-    if (o.plain) {
-      if (mk != GJ_MISFIT_L2) return err.set(GJ_EUNSUPPORTED, "the plain form supports the L2 misfit only");
-      if (o.filt_high > o.filt_low) return err.set(GJ_EUNSUPPORTED, "the plain form has no residual filter");
-      return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st, e_given);
-    }
-    const bool env = (mk != GJ_MISFIT_L2);
-    const bool filt = o.filt_high > o.filt_low;
+  // Memory plan of a gradient call: shot groups G, checkpoint interval K,
+  // and the history, checkpoint, adjoint-state and ring buffers (carved from
+  // the pool when pool_p is set, as gj_w_gradient_batch does); then the
+  // autotuner for the launch sizes.  avail = 0 measures the free memory.
+  std::vector<std::pair<int, int>> segs_;
+  bool full_ = false;
+  unsigned char* pool_p = nullptr;  // batch: next free byte of the shared pool
+  gj_status take(Err& err, DevBuf& b, size_t bytes) {
+    if (!pool_p) return b.alloc(err, bytes);
+    b.borrow(pool_p, bytes);
+    pool_p += (bytes + 255) / 256 * 256;
+    return GJ_OK;
+  }
+  gj_status plan_buffers(Err& err, const gj_w_opts& o, size_t avail, gj_adj_mode mode, cudaStream_t st) {
     ring_on = ring_nth > 0 && !o.no_ring;
     band_on = mode == GJ_ADJ_EXACT;
     // memory plan for one group
-    size_t free_b = 0, total_b = 0;
-    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
+    size_t free_b = avail, total_b = 0;
+    (void)total_b;
+    if (!avail) GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
     const size_t owned = hist.bytes + ckpt.bytes + bhist.bytes + blam.bytes +
                          (G > 0 ? 4 * size_t(G) * sstride * sizeof(T) : 0);
     const int Gnew = choose_group(o, free_b + owned);
@@ -1428,21 +1443,21 @@ class WSolver : public WSolverBase {
     const size_t cbytes = full ? 0 : segs.size() * G * sstride * sizeof(T);
     void* old[8] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p, bhist.p, blam.p, bacc.p};
     if (!band_on) { bhist.release(); blam.release(); }
-    GJ_TRY(hist.alloc(err, hbytes));
-    if (!full) GJ_TRY(ckpt.alloc(err, cbytes));
+    GJ_TRY(take(err, hist, hbytes));
+    if (!full) GJ_TRY(take(err, ckpt, cbytes));
     GJ_TRY(fwdA.alloc(err, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(fwdB.alloc(err, size_t(G) * sstride * sizeof(T)));
-    GJ_TRY(adjA.alloc(err, size_t(G) * sstride * sizeof(T)));
-    GJ_TRY(adjB.alloc(err, size_t(G) * sstride * sizeof(T)));
+    GJ_TRY(take(err, adjA, size_t(G) * sstride * sizeof(T)));
+    GJ_TRY(take(err, adjB, size_t(G) * sstride * sizeof(T)));
     GJ_TRY(acc.alloc(err, size_t(nshots) * 4 * dn * sizeof(T)));
     if (band_on) {
-      GJ_TRY(bhist.alloc(err, hist_slots * G * size_t(w.bsz) * sizeof(T)));
-      GJ_TRY(blam.alloc(err, size_t(ring_on ? Kd : 1) * G * size_t(w.bsz) * sizeof(T)));
+      GJ_TRY(take(err, bhist, hist_slots * G * size_t(w.bsz) * sizeof(T)));
+      GJ_TRY(take(err, blam, size_t(ring_on ? Kd : 1) * G * size_t(w.bsz) * sizeof(T)));
       GJ_TRY(bacc.alloc(err, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T)));
     }
     if (ring_on) {
       const void* lold = lring.p;
-      GJ_TRY(lring.alloc(err, size_t(Kd) * G * dn * sizeof(T)));
+      GJ_TRY(take(err, lring, size_t(Kd) * G * dn * sizeof(T)));
       if (lring.p != lold) {
         drop_graphs();
         // rows that no lane writes stay zero
@@ -1452,11 +1467,72 @@ class WSolver : public WSolverBase {
     void* nw[8] = {hist.p, ckpt.p, fwdA.p, adjA.p, acc.p, bhist.p, blam.p, bacc.p};
     for (int q = 0; q < 8; ++q)
       if (old[q] != nw[q]) { drop_graphs(); break; }
-    const int kahan = o.no_kahan ? 0 : 1;
     if (ring_on) {
       GJ_TRY(autotune(err, G, st));
       if (nshots % G) GJ_TRY(autotune(err, nshots % G, st));
     }
+    segs_ = segs;
+    full_ = full;
+    return GJ_OK;
+  }
+
+  // ------------------------------------------------------------ batch
+  // The whole gradient of all shots after plan_buffers (L2, no residual
+  // filter): accumulators cleared, then every shot group; capturable.
+  gj_status enqueue_all(Err& err, Ctx& c, gj_adj_mode mode, int kahan, cudaStream_t st, long& nl) {
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+    GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
+    if (band_on) GJ_CUDA(err, cudaMemsetAsync(bacc.p, 0, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T), st));
+    for (int g0 = 0; g0 < nshots; g0 += G) {
+      const int gn = std::min(G, nshots - g0);
+      if (ring_on) select_cfg(gn);
+      GJ_TRY(enqueue_group(err, c, g0, gn, mode, kahan, segs_, full_, nl, st));
+    }
+    return GJ_OK;
+  }
+  // Pool bytes plan_buffers carves with all shots in one group and
+  // checkpoint interval Kc (Kc >= nt: the whole history kept).
+  size_t pool_need(int Kc, bool exact) const {
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t Gs = size_t(nshots), sz = sizeof(T), bs = exact ? size_t(w.bsz) : 0;
+    const bool full = Kc >= g.nt;
+    const size_t nseg = full ? 0 : size_t((g.nt + Kc - 1) / Kc);
+    const size_t slots = full ? size_t(g.nt + 1) : size_t(Kc + 4);
+    size_t b = al(slots * Gs * dn * sz) + al(nseg * Gs * sstride * sz) + 2 * al(Gs * sstride * sz) +
+               al(size_t(Kd) * Gs * dn * sz);
+    if (exact) b += al(slots * Gs * bs * sz) + al(size_t(Kd) * Gs * bs * sz);
+    return b + 4096;
+  }
+  // Checkpoint interval of least pool memory.
+  int best_k(bool exact) const {
+    int kb = g.nt;
+    size_t nb = pool_need(g.nt, exact);
+    for (int k = 8; k < g.nt; k += std::max(1, k / 8)) {
+      const size_t b = pool_need(k, exact);
+      if (b < nb) { nb = b; kb = k; }
+    }
+    return kb;
+  }
+
+  // e_given: `dobs` holds the adjoint sources themselves (per shot nt x nr),
+  // the backward half of gj_w_backward: no residual, no misfit.
+  gj_status gradient(Err& err, Ctx& c, const void* eps, const void* sig, bool dev_in, const void* dobs,
+                     bool dev_dobs, gj_adj_mode mode, gj_misfit_kind mk, const gj_w_opts& o, void* geps,
+                     void* gsig, bool dev_out, double* misfit_out, double* d_out, double* e_out, cudaStream_t st,
+                     bool e_given = false) {
+    GJ_TRY(stage_inputs(err, c, eps, sig, dev_in, dobs, dev_dobs, st));
+    if (e_given) mk = GJ_MISFIT_L2;
+    if (o.plain) {
+      if (mk != GJ_MISFIT_L2) return err.set(GJ_EUNSUPPORTED, "the plain form supports the L2 misfit only");
+      if (o.filt_high > o.filt_low) return err.set(GJ_EUNSUPPORTED, "the plain form has no residual filter");
+      return gradient_plain(err, c, mode, o, geps, gsig, dev_out, misfit_out, d_out, e_out, st, e_given);
+    }
+    const bool env = (mk != GJ_MISFIT_L2);
+    const bool filt = o.filt_high > o.filt_low;
+    GJ_TRY(plan_buffers(err, o, 0, mode, st));
+    const std::vector<std::pair<int, int>> segs = segs_;
+    const bool full = full_;
+    const int kahan = o.no_kahan ? 0 : 1;
     GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
     if (band_on) GJ_CUDA(err, cudaMemsetAsync(bacc.p, 0, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T), st));
@@ -1816,6 +1892,196 @@ gj_status w_grad_only(Ctx& c, const gj_w_grid& g, gj_precision prec, const doubl
   }
   WSolver<float>* s; GJ_TRY(get_solver(c, g, &shot, 1, s));
   return s->grad_only(c.err, c, eps, sig, e, u, gout, amax);
+}
+
+// ------------------------------------------------------------------ batch
+// gj_w_gradient_batch: many independent problems (grids, shots, step counts
+// all different), their whole gradients run concurrently.  Each problem's
+// plan is cached; its large buffers (adjoint states, u and band history,
+// checkpoints, rings) are carved from one pool at offsets that repeat from
+// call to call, so the captured graphs stay valid.  The problems are packed
+// into waves by their smallest pool footprint (checkpointed at the interval
+// of least memory); a wave's spare memory lets problems keep more history
+// (the whole of it when it fits, which saves the recompute).  Every wave is
+// one CUDA graph whose child graphs (one per problem: forward, residual,
+// recompute, adjoint, imaging of all its shots) have no dependencies on one
+// another, launched once.
+template <class T>
+struct WBatch : WBatchBase {
+  std::vector<std::string> keys;
+  std::vector<std::unique_ptr<WSolver<T>>> plans;
+  std::vector<int> kc;  // checkpoint interval per problem (nt: whole history)
+  DevBuf pool;
+  std::vector<std::vector<int>> waves;
+  std::vector<cudaGraphExec_t> execs;
+  std::vector<long> launches;
+  int mode = -1, kahan = -1;
+  ~WBatch() override {
+    for (auto e : execs)
+      if (e) cudaGraphExecDestroy(e);
+  }
+};
+
+template <class T>
+static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj_mode mode, const gj_w_opts& o0,
+                                  int* nwaves_out) {
+  Err& err = c.err;
+  const int kahan = o0.no_kahan ? 0 : 1;
+  c.wsolver.reset();  // the single-call plan and the DC buffers give their memory back
+  c.wkey.clear();
+  c.dc_fac.release();
+  c.dc_vec.release();
+  std::vector<std::string> keys(np);
+  for (int p = 0; p < np; ++p)
+    keys[p] = std::string(sizeof(T) == 8 ? "d" : "f") + WSolver<T>::key(pr[p].grid, pr[p].shots, pr[p].nshots);
+  auto* B = dynamic_cast<WBatch<T>*>(c.wbatch.get());
+  if (!B || B->keys != keys || B->mode != int(mode) || B->kahan != kahan) {
+    c.wbatch.reset();
+    auto nb = std::make_unique<WBatch<T>>();
+    nb->keys = keys;
+    nb->mode = int(mode);
+    nb->kahan = kahan;
+    for (int p = 0; p < np; ++p) {
+      auto sv = std::make_unique<WSolver<T>>();
+      gj_status r = sv->setup(err, pr[p].grid, pr[p].shots, pr[p].nshots);
+      if (r != GJ_OK) return err.set(r, "problem %d: %s", p, err.msg.c_str());
+      if (sv->ring_nth == 0) return err.set(GJ_EUNSUPPORTED, "problem %d: the batch runs the ring kernels only", p);
+      sv->light_tune = true;
+      nb->plans.push_back(std::move(sv));
+    }
+    B = nb.get();
+    c.wbatch = std::move(nb);
+  }
+  cudaStream_t st = 0;
+  for (int p = 0; p < np; ++p) {
+    if (!pr[p].eps_r || !pr[p].sigma || !pr[p].d_obs || !pr[p].g_eps || !pr[p].g_sig)
+      return err.set(GJ_EINVAL, "problem %d: null input or output pointer", p);
+    gj_status r = B->plans[p]->stage_inputs(err, c, pr[p].eps_r, pr[p].sigma, false, pr[p].d_obs, false, st);
+    if (r != GJ_OK) return r;
+  }
+  const bool exact = mode == GJ_ADJ_EXACT;
+  if (B->waves.empty()) {
+    // per-problem memory outside the pool (accumulators, final gradients) and the pool budget
+    size_t owned = 0;
+    for (auto& q : B->plans)
+      owned += size_t(q->nshots) * (4 * q->dn + (exact ? 2 * size_t(q->w.bsz) : 0)) * sizeof(T) +
+               4 * q->mn * sizeof(double);
+    size_t free_b = 0, total_b = 0;
+    GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
+    const size_t avail = free_b > owned ? free_b - owned : 0;
+    const size_t budget = o0.mem_budget_bytes ? o0.mem_budget_bytes : size_t(0.8 * double(avail));
+    std::vector<size_t> nmin(np), nfull(np);
+    std::vector<int> kmin(np);
+    for (int p = 0; p < np; ++p) {
+      kmin[p] = B->plans[p]->best_k(exact);
+      nmin[p] = B->plans[p]->pool_need(kmin[p], exact);
+      nfull[p] = B->plans[p]->pool_need(B->plans[p]->g.nt, exact);
+      if (nmin[p] > budget) return err.set(GJ_ENOMEM, "problem %d needs %zu bytes, above the budget %zu", p, nmin[p], budget);
+    }
+    // pack by work, largest first
+    std::vector<int> order(np);
+    for (int p = 0; p < np; ++p) order[p] = p;
+    auto work = [&](int p) {
+      return double(B->plans[p]->nshots) * B->plans[p]->g.nt * double(B->plans[p]->NX) * B->plans[p]->NY;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+    std::vector<int> cur;
+    size_t used = 0;
+    for (int p : order) {
+      if (!cur.empty() && used + nmin[p] > budget) {
+        B->waves.push_back(cur);
+        cur.clear();
+        used = 0;
+      }
+      cur.push_back(p);
+      used += nmin[p];
+    }
+    if (!cur.empty()) B->waves.push_back(cur);
+    // spare memory of a wave: whole histories first for the cheapest upgrades,
+    // then longer checkpoint intervals for the rest
+    B->kc = kmin;
+    size_t pool = 0;
+    for (auto& wv : B->waves) {
+      size_t u = 0;
+      for (int p : wv) u += nmin[p];
+      std::vector<int> up(wv);
+      std::sort(up.begin(), up.end(), [&](int a, int b) { return nfull[a] - nmin[a] < nfull[b] - nmin[b]; });
+      for (int p : up)
+        if (u - nmin[p] + nfull[p] <= budget) { u += nfull[p] - nmin[p]; B->kc[p] = B->plans[p]->g.nt; }
+      pool = std::max(pool, u);
+    }
+    GJ_TRY(B->pool.alloc(err, pool));
+    B->execs.assign(B->waves.size(), nullptr);
+    B->launches.assign(B->waves.size(), 0);
+  }
+  if (nwaves_out) *nwaves_out = int(B->waves.size());
+  for (size_t wi = 0; wi < B->waves.size(); ++wi) {
+    const auto& wv = B->waves[wi];
+    if (!B->execs[wi]) {
+      unsigned char* cursor = B->pool.template as<unsigned char>();
+      cudaGraph_t wave = nullptr;
+      GJ_CUDA(err, cudaGraphCreate(&wave, 0));
+      struct GraphGuard { cudaGraph_t g; ~GraphGuard() { if (g) cudaGraphDestroy(g); } } gg{wave};
+      long nl = 0;
+      for (int p : wv) {
+        WSolver<T>& q = *B->plans[p];
+        gj_w_opts op = o0;
+        op.shots_per_launch = q.nshots;
+        op.ckpt_every = B->kc[p] >= q.g.nt ? 0 : B->kc[p];
+        op.mem_budget_bytes = B->kc[p] >= q.g.nt ? size_t(-1) / 4 : 0;
+        q.pool_p = cursor;
+        gj_status r = q.plan_buffers(err, op, size_t(1) << 62, mode, st);
+        cursor = q.pool_p;
+        q.pool_p = nullptr;
+        if (r != GJ_OK) return r;
+        if (size_t(cursor - B->pool.template as<unsigned char>()) > B->pool.bytes)
+          return err.set(GJ_ENOMEM, "batch pool overrun (problem %d)", p);
+        cudaStream_t cs;
+        GJ_CUDA(err, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        GJ_CUDA(err, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        gj_status rs = q.enqueue_all(err, c, mode, kahan, cs, nl);
+        cudaGraph_t pg = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(cs, &pg);
+        cudaStreamDestroy(cs);
+        if (rs != GJ_OK) { if (pg) cudaGraphDestroy(pg); return rs; }
+        if (ce != cudaSuccess) return err.set(GJ_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        cudaGraphNode_t node;
+        ce = cudaGraphAddChildGraphNode(&node, wave, nullptr, 0, pg);
+        cudaGraphDestroy(pg);
+        if (ce != cudaSuccess) return err.set(GJ_ECUDA, "child graph: %s", cudaGetErrorString(ce));
+      }
+      cudaError_t ce = cudaGraphInstantiate(&B->execs[wi], wave, 0);
+      if (ce != cudaSuccess) {
+        B->execs[wi] = nullptr;
+        return err.set(GJ_ECUDA, "wave graph instantiate failed: %s", cudaGetErrorString(ce));
+      }
+      B->launches[wi] = nl;
+    }
+    GJ_CUDA(err, cudaGraphLaunch(B->execs[wi], st));
+    GJ_CUDA(err, cudaStreamSynchronize(st));
+    c.launches += B->launches[wi];
+    for (int p : wv) {
+      WSolver<T>& q = *B->plans[p];
+      std::vector<double> hs(2 * q.nshots);
+      GJ_CUDA(err, cudaMemcpy(hs.data(), q.sums.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      gj_w_opts op = o0;
+      op.per_shot = 0;
+      gj_status r = q.finish(err, c, mode, op, pr[p].g_eps, pr[p].g_sig, false, pr[p].misfit, nullptr, nullptr, hs, st);
+      if (r != GJ_OK) return err.set(r, "problem %d: %s", p, err.msg.c_str());
+    }
+  }
+  return GJ_OK;
+}
+
+gj_status w_gradient_batch(Ctx& c, gj_precision prec, const gj_w_problem* probs, int nprob, gj_adj_mode mode,
+                           const gj_w_opts& o, int* nwaves_out) {
+  if (nprob < 1 || !probs) return c.err.set(GJ_EINVAL, "need at least one problem");
+  if (mode != GJ_ADJ_REFERENCE && mode != GJ_ADJ_EXACT) return c.err.set(GJ_EINVAL, "unknown adjoint mode");
+  if (o.plain || o.no_ring || o.filt_high > o.filt_low || o.condition || o.per_shot)
+    return c.err.set(GJ_EUNSUPPORTED, "the batch supports the default ring path with the L2 misfit, summed "
+                                      "gradients and no residual filter or conditioning");
+  if (prec == GJ_F64) return gradient_batch_t<double>(c, probs, nprob, mode, o, nwaves_out);
+  return gradient_batch_t<float>(c, probs, nprob, mode, o, nwaves_out);
 }
 
 }  // namespace gj

@@ -147,6 +147,35 @@ gj_status gj_w_gradient(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precisi
                         gj_misfit_kind misfit, const gj_w_opts* opts, double* g_eps,
                         double* g_sig, double* misfit_out, double* d_out, double* e_out);
 
+/* One independent problem of gj_w_gradient_batch: its own grid, model,
+ * shots, observed traces and outputs (host arrays, as gj_w_gradient). */
+typedef struct gj_w_problem {
+  gj_w_grid grid;
+  const double* eps_r;     /* m x n */
+  const double* sigma;     /* m x n */
+  const gj_w_shot* shots;
+  int nshots;
+  const double* d_obs;     /* per shot nt x nr, shots concatenated */
+  double* g_eps;           /* m x n, summed over the problem's shots */
+  double* g_sig;           /* m x n */
+  double* misfit;          /* nshots normalised misfits, may be NULL */
+} gj_w_problem;
+
+/* Gradients of many independent problems of uneven sizes in one call: the
+ * reference runs such inversions as separate parfor workers and Slurm jobs
+ * (w_update_e_.m:32 per shot, one MATLAB process per field line).  The
+ * problems run concurrently in memory-budgeted waves, each wave one CUDA
+ * graph launch holding every problem's whole gradient (forward, residual,
+ * recompute, exact or reference adjoint, imaging; all its shots per launch);
+ * a problem keeps its whole u history when the wave's memory allows, else it
+ * checkpoints.  Plans, buffers and the wave graphs are cached in the context
+ * while the problems (grids and shots) repeat.  L2 misfit; opts: no_kahan and
+ * mem_budget_bytes (the pool budget, 0 = 80% of free memory) apply, the plain,
+ * no_ring, filter, conditioning and per_shot options do not (GJ_EUNSUPPORTED).
+ *   nwaves : number of waves used, may be NULL */
+gj_status gj_w_gradient_batch(gj_ctx* ctx, gj_precision precision, const gj_w_problem* probs, int nprob,
+                              gj_adj_mode mode, const gj_w_opts* opts, int* nwaves);
+
 /* Forward runs and misfits only (no history, no adjoint): replaces the
  * objective evaluations of the step-length search, w_objs_e.m:24-65 as called
  * by w_stepparabola_e.m:20-41 for each trial model.  misfit_out: nshots
