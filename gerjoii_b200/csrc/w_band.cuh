@@ -202,13 +202,19 @@ struct BandFinish {
 
 // Adds the band terms to g_eps (double, m x n per shot with per_shot, else
 // summed): every model cell on the edges gathers the nodes of its preimage
-// under w_exp2pml.m (the PML rows and columns that replicate it).
+// under w_exp2pml.m (the PML rows and columns that replicate it).  One warp
+// per model cell (warp-uniform skip of the cells off the edges); the lanes
+// stride over the preimage and a fixed-order shuffle reduction keeps the sum
+// deterministic.
 template <class T>
 __global__ void k_band_finish(const WDev<T> w, const T* bacc, size_t bstride, int nshots, int per_shot,
                               const BandFinish f, double* geps) {
   const int m = w.m, n = w.n, NX = w.NX, NY = w.NY, P = w.P;
   const size_t mn = size_t(m) * n;
-  for (size_t p = threadIdx.x + size_t(blockIdx.x) * blockDim.x; p < mn; p += size_t(blockDim.x) * gridDim.x) {
+  const int lane = threadIdx.x & 31;
+  const size_t warp = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const size_t nwarps = (size_t(gridDim.x) * blockDim.x) >> 5;
+  for (size_t p = warp; p < mn; p += nwarps) {
     const int a = int(p % m), b = int(p / m);
     const bool top = a == 0 && f.air == 0 && f.Pt > 0;
     if (!(b == 0 || b == n - 1 || a == m - 1 || top)) continue;
@@ -217,42 +223,47 @@ __global__ void k_band_finish(const WDev<T> w, const T* bacc, size_t bstride, in
     if (top) I0 = 0;
     if (b == 0) J0 = 0;
     if (b == n - 1) J1 = NY - 1;
+    const int ni = I1 - I0 + 1, cnt = ni * (J1 - J0 + 1);
     const double eps = f.eps_m[p], e0 = f.eps0, dt = f.dt, u0 = f.mu0;
     double tot = 0.0;
     for (int s = 0; s < nshots; ++s) {
       const T* A = bacc + size_t(s) * bstride;
       auto S = [&](long q) { return double(A[q]) - double(A[w.bsz + q]); };
       double g = 0.0;
-      for (int J = J0; J <= J1; ++J)
-        for (int I = I0; I <= I1; ++I) {
-          const bool xbot = I >= NX - P && I <= NX - 1;
-          const bool xtop = I >= 1 && I <= f.Pt;
-          const bool ystrip = (J >= 1 && J <= P) || (J >= NY - P && J <= NY - 1);
-          if (ez_bandnode(w, I, J)) {
-            double cx = 0.0, cy = 0.0;
-            if (xbot) cx = -2.0 * e0 / (2.0 * e0 * eps + dt * f.sex[I]);
-            else if (!xtop) cx = -1.0 / eps;
-            if (ystrip) cy = -2.0 * e0 / (2.0 * e0 * eps + dt * f.sey[J]);
-            else if (xbot) cy = -1.0 / eps;
-            const long ox = band_off_e(w, I, J, 0), oy = band_off_e(w, I, J, 1);
-            if (cx != 0.0 && ox >= 0) g += cx * S(ox);
-            if (cy != 0.0 && oy >= 0) g += cy * S(oy);
-          }
-          if (J <= NY - 1 && !(J >= w.hxj0 && J <= w.hxj1) && I >= 1 && I <= NX - 1) {
-            const double sm = f.smy[J] / eps;
-            const long o = band_off_hx(w, I, J);
-            if (o >= 0) g += dt * sm / (eps * (2.0 * u0 + dt * sm)) * S(o);
-          }
-          if (xbot && !(I >= w.hyi0 && I <= w.hyi1) && J >= 1 && J <= NY - 1) {
-            const double sm = f.smx[I] / eps;
-            const long o = band_off_hy(w, I, J);
-            if (o >= 0) g += dt * sm / (eps * (2.0 * u0 + dt * sm)) * S(o);
-          }
+      for (int q = lane; q < cnt; q += 32) {
+        const int I = I0 + q % ni, J = J0 + q / ni;
+        const bool xbot = I >= NX - P && I <= NX - 1;
+        const bool xtop = I >= 1 && I <= f.Pt;
+        const bool ystrip = (J >= 1 && J <= P) || (J >= NY - P && J <= NY - 1);
+        if (ez_bandnode(w, I, J)) {
+          double cx = 0.0, cy = 0.0;
+          if (xbot) cx = -2.0 * e0 / (2.0 * e0 * eps + dt * f.sex[I]);
+          else if (!xtop) cx = -1.0 / eps;
+          if (ystrip) cy = -2.0 * e0 / (2.0 * e0 * eps + dt * f.sey[J]);
+          else if (xbot) cy = -1.0 / eps;
+          const long ox = band_off_e(w, I, J, 0), oy = band_off_e(w, I, J, 1);
+          if (cx != 0.0 && ox >= 0) g += cx * S(ox);
+          if (cy != 0.0 && oy >= 0) g += cy * S(oy);
         }
-      if (per_shot) geps[size_t(s) * mn + p] += g;
-      else tot += g;
+        if (J <= NY - 1 && !(J >= w.hxj0 && J <= w.hxj1) && I >= 1 && I <= NX - 1) {
+          const double sm = f.smy[J] / eps;
+          const long o = band_off_hx(w, I, J);
+          if (o >= 0) g += dt * sm / (eps * (2.0 * u0 + dt * sm)) * S(o);
+        }
+        if (xbot && !(I >= w.hyi0 && I <= w.hyi1) && J >= 1 && J <= NY - 1) {
+          const double sm = f.smx[I] / eps;
+          const long o = band_off_hy(w, I, J);
+          if (o >= 0) g += dt * sm / (eps * (2.0 * u0 + dt * sm)) * S(o);
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) g += __shfl_down_sync(0xffffffffu, g, o);
+      if (per_shot) {
+        if (lane == 0) geps[size_t(s) * mn + p] += g;
+      } else {
+        tot += g;
+      }
     }
-    if (!per_shot) geps[p] += tot;
+    if (!per_shot && lane == 0) geps[p] += tot;
   }
 }
 

@@ -321,11 +321,12 @@ class WSolver : public WSolverBase {
       return S == o.S && SF == o.SF && RWG == o.RWG && tjF == o.tjF && tjS == o.tjS;
     }
   };
-  RingCfg rc;                    // configuration of the launches being enqueued
+  RingCfg rc;                    // configuration of the forward launches being enqueued
+  RingCfg rca;                   // and of the exact-adjoint launches
   bool light_tune = false;       // batch plans: a smaller candidate set
   RingCfg rc_env;                // default, with the environment's overrides
   bool env_fixed = false;        // a GJ_RING_* variable is set: no tuning
-  std::map<int, RingCfg> tuned;  // per launch size (shots per launch)
+  std::map<int, std::pair<RingCfg, RingCfg>> tuned;  // (forward, adjoint) per launch size
   int maxsm_dyn = 0;
   const bool ring_serial = getenv("GJ_RING_SERIAL") != nullptr;
   int last_kernels = 0;  // kernels launched by the last launch_fwd / launch_adjr
@@ -364,7 +365,17 @@ class WSolver : public WSolverBase {
       GJ_TRY((ring_attr<2, true>(err))); GJ_TRY((ring_attr<3, true>(err))); GJ_TRY((ring_attr<4, true>(err)));
       rc_env = d;
       rc = d;
-      if (!side) GJ_CUDA(err, cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+      rca = d;
+      // the general kernel (PML band) sets the step time: its stream gets the
+      // highest priority so its CTAs are dispatched before the fast kernel's
+      // (graphs honour the captured priority, cudaGraphInstantiateFlagUseNodePriority)
+      if (!side) {
+        int lo = 0, hi = 0;
+        GJ_CUDA(err, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        const char* e = getenv("GJ_SIDE_PRIORITY");
+        const bool prio = !(e && atoi(e) == 0);
+        GJ_CUDA(err, cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, prio ? hi : lo));
+      }
       if (!ev_fork) GJ_CUDA(err, cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
       if (!ev_join) GJ_CUDA(err, cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
       ring_nth = 32 * RW;
@@ -375,7 +386,8 @@ class WSolver : public WSolverBase {
   // The configuration for launches of gn shots: the tuned one when there is.
   void select_cfg(int gn) {
     auto it = tuned.find(gn);
-    rc = it != tuned.end() ? it->second : rc_env;
+    rc = it != tuned.end() ? it->second.first : rc_env;
+    rca = it != tuned.end() ? it->second.second : rc_env;
   }
   // Fast rows of the ring kernels: interior Ez rows (plus the free-top Ez = 0
   // row, whose Ceze/Cezhy are 1/0) that are also Hy interior rows.
@@ -388,11 +400,15 @@ class WSolver : public WSolverBase {
   // [0] forward fast, [1] forward general, [2] adjoint fast, [3] adjoint general.
   struct TaskTable { DevBuf buf[4]; int n[4] = {0, 0, 0, 0}; };
   std::map<long, std::unique_ptr<TaskTable>> tasks;
-  long task_key(int gn) const { return (long(gn) << 40) | (long(rc.tjF) << 20) | long(rc.tjS); }
-  const TaskTable& task_table(int gn) const { return *tasks.at(task_key(gn)); }
-  // Task tables of launches of gn shots for the column chunks of rc.
+  static long task_key(int gn, const RingCfg& q) { return (long(gn) << 40) | (long(q.tjF) << 20) | long(q.tjS); }
+  const TaskTable& task_table(int gn, const RingCfg& q) const { return *tasks.at(task_key(gn, q)); }
+  // Task tables of launches of gn shots for the column chunks of rc and rca.
   gj_status prepare_tasks(Err& err, int gn) {
-    if (ring_nth == 0 || tasks.count(task_key(gn))) return GJ_OK;
+    GJ_TRY(prepare_tasks_for(err, gn, rc));
+    return prepare_tasks_for(err, gn, rca);
+  }
+  gj_status prepare_tasks_for(Err& err, int gn, const RingCfg& q) {
+    if (ring_nth == 0 || tasks.count(task_key(gn, q))) return GJ_OK;
     constexpr int V = VT<T>::V;
     const int rows = 32 * V, nrb = (NX + 1 + rows - 1) / rows;
     std::vector<int> fast(nrb, 0);
@@ -404,12 +420,12 @@ class WSolver : public WSolverBase {
       fast[rb] = f ? 1 : 0;
       nF += fast[rb];
     }
-    const int tjS = rc.tjS;
+    const int tjS = q.tjS;
     auto tt = std::make_unique<TaskTable>();
     for (int dir = 0; dir < 2; ++dir) {
       const int c0 = w.ej0, c1 = dir == 0 ? w.ej1 : w.ej1 - 1;  // fast columns
       const int ncol = std::max(c1 - c0 + 1, 0);
-      const int tjF = std::min(rc.tjF, std::max(ncol, 1));
+      const int tjF = std::min(q.tjF, std::max(ncol, 1));
       std::vector<int4> hf, hg;
       auto chunks = [&](std::vector<int4>& h, int z, int r0, int a0, int a1, int tj) {
         for (int j0 = a0; j0 <= a1; j0 += tj) h.push_back(make_int4(r0, j0, std::min(j0 + tj - 1, a1), z << 1));
@@ -436,7 +452,7 @@ class WSolver : public WSolverBase {
                                 cudaMemcpyHostToDevice));
       }
     }
-    tasks.emplace(task_key(gn), std::move(tt));
+    tasks.emplace(task_key(gn, q), std::move(tt));
     return GJ_OK;
   }
 
@@ -479,7 +495,7 @@ class WSolver : public WSolverBase {
                        const WDev<T>* wsel = nullptr) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       if (ring_on) {
-        const TaskTable& tt = task_table(gn);
+        const TaskTable& tt = task_table(gn, rc);
         const WDev<T> wd = wsel ? *wsel : w;
         const int S = rc.S, SF = rc.SF;
         auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
@@ -510,9 +526,9 @@ class WSolver : public WSolverBase {
   // One exact adjoint step of gn shots with the l ring (ring kernels only).
   gj_status launch_adjr(Err& err, AdjRingArgs<T> a, int gn, cudaStream_t st, RecArgs<T> ra) {
     if constexpr (VT<T>::V * sizeof(T) == 16) {
-      const TaskTable& tt = task_table(gn);
+      const TaskTable& tt = task_table(gn, rca);
       const WDev<T> wd = w;
-      const int S = rc.S, SF = rc.SF;
+      const int S = rca.S, SF = rca.SF;
       auto lf = [&](const int4* tk, int n, cudaStream_t s_) {
         const dim3 grd((n + RW - 1) / RW);
         const size_t sm = ring_smem(RW, SF, true);
@@ -520,7 +536,7 @@ class WSolver : public WSolverBase {
         else if (SF == 3) k_adjw<T, 3, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
         else k_adjw<T, 4, true><<<grd, 32 * RW, sm, s_>>>(wd, a, tk, n, ra);
       };
-      const int rw = rc.RWG;
+      const int rw = rca.RWG;
       auto lg = [&](const int4* tk, int n, cudaStream_t s_) {
         const dim3 grd((n + rw - 1) / rw);
         const size_t sm = ring_smem(rw, S, false);
@@ -548,39 +564,47 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaEventCreate(&e0));
     GJ_CUDA(err, cudaEventCreate(&e1));
     struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
-    const int warm = 2, reps = 6;
+    const int warm = 2, reps = 12;
+    const bool adj_ok = lring.p != nullptr;
+    // history and band slots rotate over the buffers (strided), so their
+    // writes reach DRAM as in a real step instead of one L2-resident slot
+    const size_t nslot = hist_slots > 1 ? hist_slots : 1;
+    auto slot_of = [&](int i) { return nslot > 1 ? 1 + (size_t(i) * 97) % (nslot - 1) : size_t(0); };
     auto clear = [&]() -> gj_status {
       GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, size_t(gn) * sstride * sizeof(T), st));
       GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, size_t(gn) * sstride * sizeof(T), st));
-      GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, size_t(gn) * sstride * sizeof(T), st));
-      GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      if (adj_ok) {
+        GJ_CUDA(err, cudaMemsetAsync(adjA.p, 0, size_t(gn) * sstride * sizeof(T), st));
+        GJ_CUDA(err, cudaMemsetAsync(adjB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      }
       return GJ_OK;
     };
-    auto time_cfg = [&](const RingCfg& cfg, float& ms) -> gj_status {
-      rc = cfg;
-      GJ_TRY(prepare_tasks(err, gn));
+    // dir 0: forward steps with cfg as rc; dir 1: adjoint steps with cfg as rca
+    auto time_cfg = [&](int dir, const RingCfg& cfg, float& ms) -> gj_status {
+      if (dir == 0) rc = cfg; else rca = cfg;
+      GJ_TRY(prepare_tasks_for(err, gn, cfg));
       GJ_TRY(clear());
-      T* A = fwdA.as<T>() + ld;
-      T* B = fwdB.as<T>() + ld;
-      T* LA = adjA.as<T>() + ld;
-      T* LB = adjB.as<T>() + ld;
+      T* A = (dir == 0 ? fwdA : adjA).template as<T>() + ld;
+      T* B = (dir == 0 ? fwdB : adjB).template as<T>() + ld;
       auto run = [&](int n) -> gj_status {
         for (int i = 0; i < n; ++i) {
-          StepArgs<T> a = step_args(A, B, i % g.nt);
-          if (hist.p && hist_slots > 1) { a.hist = hist.as<T>() + size_t(gn) * dn; a.hstride = dn; }
-          if (band_on && bhist.p && hist_slots > 1) a.band = bhist.as<T>() + size_t(gn) * size_t(w.bsz);
-          RecArgs<T> ra = rec_args(0);
-          if (nr > 0) { ra.d = dbuf.as<T>(); ra.it = i % g.nt; }
-          GJ_TRY(launch_fwd(err, a, gn, st, ra));
+          if (dir == 0) {
+            StepArgs<T> a = step_args(A, B, i % g.nt);
+            if (hist.p && nslot > 1) { a.hist = hist.as<T>() + slot_of(i) * gn * dn; a.hstride = dn; }
+            if (band_on && bhist.p && nslot > 1) a.band = bhist.as<T>() + slot_of(i) * gn * size_t(w.bsz);
+            RecArgs<T> ra = rec_args(0);
+            if (nr > 0) { ra.d = dbuf.as<T>(); ra.it = i % g.nt; }
+            GJ_TRY(launch_fwd(err, a, gn, st, ra));
+          } else {
+            AdjRingArgs<T> b{};
+            b.A = A; b.B = B; b.fstride = fstride; b.sstride = sstride; b.shot0 = 0;
+            b.lout = lring.as<T>() + size_t(i % Kd) * gn * dn; b.hstride = dn;
+            if (band_on && blam.p) b.band = blam.as<T>() + size_t(i % Kd) * gn * size_t(w.bsz);
+            RecArgs<T> rb = rec_args(0);
+            if (nr > 0) { rb.e = ebuf.as<T>(); rb.kinj = i % g.nt; }
+            GJ_TRY(launch_adjr(err, b, gn, st, rb));
+          }
           std::swap(A, B);
-          AdjRingArgs<T> b{};
-          b.A = LA; b.B = LB; b.fstride = fstride; b.sstride = sstride; b.shot0 = 0;
-          b.lout = lring.as<T>(); b.hstride = dn;
-          if (band_on && blam.p) b.band = blam.as<T>();
-          RecArgs<T> rb = rec_args(0);
-          if (nr > 0) { rb.e = ebuf.as<T>(); rb.kinj = i % g.nt; }
-          GJ_TRY(launch_adjr(err, b, gn, st, rb));
-          std::swap(LA, LB);
         }
         return GJ_OK;
       };
@@ -593,44 +617,49 @@ class WSolver : public WSolverBase {
       GJ_CUDA(err, cudaGetLastError());
       return GJ_OK;
     };
-    RingCfg best = rc_env;
-    float tbest = 0.f;
-    GJ_TRY(time_cfg(best, tbest));
-    auto consider = [&](const RingCfg& q) -> gj_status {
-      if (q == best) return GJ_OK;
-      if (ring_smem(q.RWG, q.S, false) > size_t(maxsm_dyn) || ring_smem(RW, q.SF, true) > size_t(maxsm_dyn))
-        return GJ_OK;
-      float t = 0.f;
-      GJ_TRY(time_cfg(q, t));
-      if (t < tbest) { tbest = t; best = q; }
-      return GJ_OK;
-    };
     const std::vector<int> SFs = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
     const std::vector<int> tjFs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{16, 24, 32, 48};
     const std::vector<int> Ss = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
     const std::vector<int> tjSs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{8, 16, 32, 64};
-    const std::vector<int> rws = light_tune ? std::vector<int>{4} : std::vector<int>{2, 4};
-    for (int SF : SFs)
-      for (int tjF : tjFs) {
-        RingCfg q = best;
-        q.SF = SF; q.tjF = tjF;
-        GJ_TRY(consider(q));
-      }
-    const RingCfg fast_best = best;
-    for (int S : Ss)
-      for (int tjS : tjSs)
-        for (int rw : rws) {
-          RingCfg q = fast_best;
-          q.S = S; q.tjS = tjS; q.RWG = rw;
+    const std::vector<int> rws = light_tune ? std::vector<int>{2, 4} : std::vector<int>{2, 4};
+    RingCfg best[2] = {rc_env, rc_env};
+    float tb[2] = {0.f, 0.f};
+    for (int dir = 0; dir < (adj_ok ? 2 : 1); ++dir) {
+      GJ_TRY(time_cfg(dir, best[dir], tb[dir]));
+      auto consider = [&](const RingCfg& q) -> gj_status {
+        if (q == best[dir]) return GJ_OK;
+        if (ring_smem(q.RWG, q.S, false) > size_t(maxsm_dyn) || ring_smem(RW, q.SF, true) > size_t(maxsm_dyn))
+          return GJ_OK;
+        float t = 0.f;
+        GJ_TRY(time_cfg(dir, q, t));
+        if (t < tb[dir]) { tb[dir] = t; best[dir] = q; }
+        return GJ_OK;
+      };
+      for (int SF : SFs)
+        for (int tjF : tjFs) {
+          RingCfg q = best[dir];
+          q.SF = SF; q.tjF = tjF;
           GJ_TRY(consider(q));
         }
+      const RingCfg fast_best = best[dir];
+      for (int S : Ss)
+        for (int tjS : tjSs)
+          for (int rw : rws) {
+            RingCfg q = fast_best;
+            q.S = S; q.tjS = tjS; q.RWG = rw;
+            GJ_TRY(consider(q));
+          }
+    }
     GJ_TRY(clear());
-    tuned[gn] = best;
-    rc = best;
+    tuned[gn] = {best[0], best[1]};
+    select_cfg(gn);
     GJ_TRY(prepare_tasks(err, gn));
     if (getenv("GJ_AUTOTUNE_VERBOSE"))
-      fprintf(stderr, "gerjoii_b200 autotune %dx%d, %d shots/launch: S=%d SF=%d RWG=%d tjF=%d tjS=%d, %.2f us/step\n",
-              NX, NY, gn, best.S, best.SF, best.RWG, best.tjF, best.tjS, 1e3f * tbest / reps);
+      fprintf(stderr,
+              "gerjoii_b200 autotune %dx%d, %d shots/launch: forward S=%d SF=%d RWG=%d tjF=%d tjS=%d %.2f us/step; "
+              "adjoint S=%d SF=%d RWG=%d tjF=%d tjS=%d %.2f us/step\n",
+              NX, NY, gn, best[0].S, best[0].SF, best[0].RWG, best[0].tjF, best[0].tjS, 1e3f * tb[0] / reps,
+              best[1].S, best[1].SF, best[1].RWG, best[1].tjF, best[1].tjS, 1e3f * tb[1] / reps);
     return GJ_OK;
   }
 
@@ -931,7 +960,7 @@ class WSolver : public WSolverBase {
     f.dt = g.dt; f.eps0 = g.eps0; f.mu0 = g.mu0; f.Pt = g.pml_top; f.air = g.air; f.eps_m = eps_m;
     const double* pp = prof.as<double>();
     f.sex = pp; f.smx = pp + NX + 2; f.sey = pp + 2 * (NX + 2); f.smy = pp + 2 * (NX + 2) + NY + 2;
-    k_band_finish<T><<<64, 256, 0, st>>>(w, bacc.as<T>(), 2 * size_t(w.bsz), nshots, per_shot, f, gdev);
+    k_band_finish<T><<<2 * nsm, 256, 0, st>>>(w, bacc.as<T>(), 2 * size_t(w.bsz), nshots, per_shot, f, gdev);
     ++c.launches;
   }
 
@@ -1571,9 +1600,10 @@ class WSolver : public WSolverBase {
         c.timer.collect(m);
         continue;
       }
-      char kb[96];
+      char kb[160];
       snprintf(kb, sizeof kb, "%d/%d/%d/%d/%d/%d/%d/%d/%d/%d.%d.%d.%d.%d", g0, gn, int(mode), kahan, K, G,
                c.timer.on ? 1 : 0, ring_on ? 1 : 0, Kd, rc.S, rc.SF, rc.RWG, rc.tjF, rc.tjS);
+      snprintf(kb + strlen(kb), sizeof kb - strlen(kb), "/%d.%d.%d.%d.%d", rca.S, rca.SF, rca.RWG, rca.tjF, rca.tjS);
       auto itg = graphs.find(kb);
       if (itg == graphs.end()) {
         auto rec = std::make_unique<GraphRec>();
@@ -1590,7 +1620,7 @@ class WSolver : public WSolverBase {
         cudaStreamDestroy(cs);
         GJ_TRY(rs);
         if (ce != cudaSuccess) return err.set(GJ_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&rec->exec, graph, 0);
+        ce = cudaGraphInstantiate(&rec->exec, graph, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(graph);
         if (ce != cudaSuccess) return err.set(GJ_ECUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
         rec->launches = cnt;
@@ -1916,10 +1946,15 @@ struct WBatch : WBatchBase {
   std::vector<cudaGraphExec_t> execs;
   std::vector<long> launches;
   int mode = -1, kahan = -1;
-  ~WBatch() override {
+  size_t budget_opt = 0;  // opts.mem_budget_bytes the waves were planned for
+  void drop_waves() {
     for (auto e : execs)
       if (e) cudaGraphExecDestroy(e);
+    execs.clear();
+    waves.clear();
+    launches.clear();
   }
+  ~WBatch() override { drop_waves(); }
 };
 
 template <class T>
@@ -1951,6 +1986,10 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
     }
     B = nb.get();
     c.wbatch = std::move(nb);
+  }
+  if (B->budget_opt != o0.mem_budget_bytes) {
+    B->drop_waves();
+    B->budget_opt = o0.mem_budget_bytes;
   }
   cudaStream_t st = 0;
   for (int p = 0; p < np; ++p) {
@@ -2050,7 +2089,7 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
         cudaGraphDestroy(pg);
         if (ce != cudaSuccess) return err.set(GJ_ECUDA, "child graph: %s", cudaGetErrorString(ce));
       }
-      cudaError_t ce = cudaGraphInstantiate(&B->execs[wi], wave, 0);
+      cudaError_t ce = cudaGraphInstantiate(&B->execs[wi], wave, cudaGraphInstantiateFlagUseNodePriority);
       if (ce != cudaSuccess) {
         B->execs[wi] = nullptr;
         return err.set(GJ_ECUDA, "wave graph instantiate failed: %s", cudaGetErrorString(ce));
