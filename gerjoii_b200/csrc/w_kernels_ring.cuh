@@ -126,11 +126,20 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
   if (t >= ntask) return;  // whole warp; the kernel has no CTA barrier
   const int4 tk = tasks[t];
   const int ld = w.ld, NX = w.NX, NY = w.NY;
-  const int I0 = tk.x + lane * V;
+  // split task (general kernel, bottom block): lanes 0-15 run shot z, lanes
+  // 16-31 shot z+1 over the same 64 rows; a half's first lane loads its own
+  // up-halo (second half: halo entries shifted by 5, past the first half's
+  // five), its last lane reads the zero padding below NX
+  const bool split = !FAST && ((tk.w >> 1) & 1);
+  const int half = split ? (lane >> 4) : 0;
+  const int hl = split ? (lane & 15) : lane;
+  const bool upl = hl == 0, dnl = split ? hl == 15 : lane == 31;
+  const int hoff = half ? 5 : 0;
+  const int I0 = tk.x + hl * V;
   const int j0 = tk.y, j1 = tk.z;
   const bool fastRows = (tk.w & 1) != 0;
   const bool live = I0 <= NX;
-  const int zl = tk.w >> 1;
+  const int zl = (tk.w >> 2) + half;
   const int s = a.shot0 + zl;
   const size_t off = size_t(zl) * a.sstride, fs = a.fstride;
   const T* EzA = a.A + off;
@@ -188,8 +197,8 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       cp16(L + RF_CE * 32, w.ce + k);
       cp16(L + RF_CH * 32, w.chy + k);
       uint4* H = R + SLOTS * 32;
-      if (lane == 31) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
-      if (lane == 0 && I0 >= 1) {
+      if (dnl) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
+      if (upl && I0 >= 1) {
         const size_t ku = nidx(I0 - V, J, ld);
         cp16(H + HF_EZUP, EzA + ku);
         cp16(H + HF_HYUP, HyA + ku);
@@ -208,9 +217,9 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
         cp16(L + RF_AY * 32, w.ay + k); cp16(L + RF_BY * 32, w.by + k);
         cp16(L + RF_EX * 32, ExA + k); cp16(L + RF_EY * 32, EyA + k);
       }
-      uint4* H = R + SLOTS * 32;
-      if (lane == 31 && I0 + V <= NX) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
-      if (lane == 0 && I0 >= 1) {
+      uint4* H = R + SLOTS * 32 + hoff;
+      if (dnl && I0 + V <= NX) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
+      if (upl && I0 >= 1) {
         const size_t ku = nidx(I0 - V, J, ld);
         cp16(H + HF_EZUP, EzA + ku);
         cp16(H + HF_HYUP, HyA + ku);
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
   // receiver window (fused k_record): lane q holds receiver rp + q of this
   // shot's column-sorted list, from the first one at column >= j0
   const int* rsl = ra.rs + size_t(zl) * 3 * ra.nrr;
-  const int rn = ra.d ? ra.nrs[zl] : 0;
+  const int rn = (ra.d && !split) ? ra.nrs[zl] : 0;  // split tasks hold no receivers
   int rp = rn ? rec_first(rsl, rn, j0) : 0;
   int wJ = 0x7fffffff, wI = 0, wR = 0, widx = 0;
   auto rec_window = [&]() {
@@ -262,7 +271,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
     cp_wait<S - 1>();
     const uint4* R = ring + size_t(it % S) * STAGE;
     const uint4* L = R + lane;
-    const uint4* H = R + SLOTS * 32;
+    const uint4* H = R + SLOTS * 32 + hoff;
     const size_t k = nidx(I0, J, ld);
     T ez_n[V], hxo[V], hyo[V], hx_new[V], hy_new[V], e_new[V];
     if (FAST || (fastRows && J >= w.ej0 && J <= w.ej1)) {
@@ -271,7 +280,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       sld(L + RF_EZN * 32, ez_n); sld(L + RF_HX * 32, hxo); sld(L + RF_HY * 32, hyo);
       sld(L + RF_CE * 32, ce_); sld(L + RF_CH * 32, ch_);
       T nxt = __shfl_down_sync(0xffffffffu, ez_c[0], 1);
-      if (lane == 31) nxt = sfirst<T>(H + HF_EZDN);
+      if (dnl) nxt = sfirst<T>(H + HF_EZDN);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         hx_new[v] = T(1) * hxo[v] + w.chxez * (ez_n[v] - ez_c[v]);
@@ -280,7 +289,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       }
       vst(HxB + k, hx_new); vst(HyB + k, hy_new);
       T hy_up = __shfl_up_sync(0xffffffffu, hy_new[V - 1], 1);
-      if (lane == 0) {
+      if (upl) {
         hy_up = T(0);
         if (I0 >= 1) hy_up = T(1) * slast<T>(H + HF_HYUP) + w.chyez * (ez_c[0] - slast<T>(H + HF_EZUP));
       }
@@ -310,7 +319,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       vzero<T, V>(hya_); vzero<T, V>(hyb_);
       if (live && hyStrip) { sld(L + RF_HYA * 32, hya_); sld(L + RF_HYB * 32, hyb_); }
       T nxt = __shfl_down_sync(0xffffffffu, ez_c[0], 1);
-      if (lane == 31) nxt = (I0 + V <= NX) ? sfirst<T>(H + HF_EZDN) : T(0);
+      if (dnl) nxt = (I0 + V <= NX) ? sfirst<T>(H + HF_EZDN) : T(0);
       const bool hxCol = J <= NY - 1;
 #pragma unroll
       for (int v = 0; v < V; ++v) {
@@ -324,7 +333,7 @@ __global__ void __launch_bounds__(128) k_fwdw(const WDev<T> w, const StepArgs<T>
       }
       if (live) { vst(HxB + k, hx_new); vst(HyB + k, hy_new); }
       T hy_up = __shfl_up_sync(0xffffffffu, hy_new[V - 1], 1);
-      if (lane == 0) {
+      if (upl) {
         hy_up = T(0);
         if (live && I0 >= 1 && Iup <= NX - 1) {
           T ha = T(1), hb = w.chyez;
@@ -476,11 +485,20 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
   if (t >= ntask) return;
   const int4 tk = tasks[t];
   const int ld = w.ld, NX = w.NX, NY = w.NY;
-  const int I0 = tk.x + lane * V;
+  // split task (general kernel, bottom block): lanes 0-15 run shot z, lanes
+  // 16-31 shot z+1 (see k_fwdw); the second half's halo entries are shifted
+  // by 6.  Its down-halo entries (6-9) would overlap the first half's up-halo
+  // ones, but a split task's last lanes have Idn > NX and load no down-halo.
+  const bool split = !FAST && ((tk.w >> 1) & 1);
+  const int half = split ? (lane >> 4) : 0;
+  const int hl = split ? (lane & 15) : lane;
+  const bool upl = hl == 0, dnl = split ? hl == 15 : lane == 31;
+  const int hoff = half ? 6 : 0;
+  const int I0 = tk.x + hl * V;
   const int j0 = tk.y, j1 = tk.z;
   const bool fastRows = (tk.w & 1) != 0;
   const bool live = I0 <= NX;
-  const int zl = tk.w >> 1;
+  const int zl = (tk.w >> 2) + half;
   const size_t off = size_t(zl) * a.sstride, fs = a.fstride;
   const T* LA = a.A + off;
   const T* LxA = LA + fs;
@@ -537,12 +555,12 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       cp16(L + RF_CE * 32, w.ce + kn);      // slot 3: Ceze(J+1)
       cp16(L + RF_CH * 32, w.chy + kn);     // slot 4: Cezhy(J+1)
       uint4* H = R + SLOTS * 32;
-      if (lane == 31) {
+      if (dnl) {
         const size_t kd = nidx(Idn, J, ld);
         cp16(H + 0, LA + kd);
         cp16(H + 1, w.chy + kd);
       }
-      if (lane == 0 && I0 >= 1) {
+      if (upl && I0 >= 1) {
         const size_t ku = nidx(I0 - V, J, ld);
         cp16(H + 2, LA + ku);
         cp16(H + 3, w.chy + ku);
@@ -564,15 +582,15 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       cp16(L + RA_LY * 32, LyA + k);
       if (!(J >= w.hxj0 && J <= w.hxj1)) { cp16(L + RA_HXA * 32, w.hxa + k); cp16(L + RA_HXB * 32, w.hxb + k); }
       if (hyStrip) { cp16(L + RA_HYA * 32, w.hya + k); cp16(L + RA_HYB * 32, w.hyb + k); }
-      uint4* H = R + SLOTS * 32;
-      if (lane == 31 && Idn <= NX) {
+      uint4* H = R + SLOTS * 32 + hoff;
+      if (dnl && Idn <= NX) {
         const size_t kd = nidx(Idn, J, ld);
         const int cls = adj_class(w, Idn, J);
         if (cls) cp16(H + HA_LDN, LA + kd);
         if (cls == 1) cp16(H + HA_CHDN, w.chy + kd);
         if (cls == 2) { cp16(H + HA_SXDN, SxA + kd); cp16(H + HA_BXDN, w.bx + kd); }
       }
-      if (lane == 0 && I0 >= 1) {
+      if (upl && I0 >= 1) {
         const size_t ku = nidx(I0 - V, J, ld);
         const int cls = adj_class(w, Iup, J);
         if (cls) cp16(H + HA_LUP, LA + ku);
@@ -617,7 +635,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
   // receiver window (fused injection of the next step's adjoint source):
   // lane q holds receiver rp + q of this shot's column-sorted list and its e
   const int* rsl = ra.rs + size_t(zl) * 3 * ra.nrr;
-  const int rn = ra.kinj >= 0 ? ra.nrs[zl] : 0;
+  const int rn = (ra.kinj >= 0 && !split) ? ra.nrs[zl] : 0;  // split tasks hold no receivers
   int rp = rn ? rec_first(rsl, rn, j0) : 0;
   int wJ = 0x7fffffff, wI = 0, widx = 0;
   T wE = T(0);
@@ -653,7 +671,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
     cp_wait<S - 1>();
     const uint4* R = ring + size_t(it % S) * STAGE;
     const uint4* L = R + lane;
-    const uint4* H = R + SLOTS * 32;
+    const uint4* H = R + SLOTS * 32 + hoff;
     const size_t k = nidx(I0, J, ld);
     T l_n[V], px_n[V], py_n[V], lm_n[V], lx_n[V], ly_n[V], ax_n[V], ay_n[V], lxo[V], lyo[V];
     T lxn[V], lyn[V], qx[V], le[V], img[V];
@@ -679,8 +697,8 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       }
       T px_dn = __shfl_down_sync(0xffffffffu, px_c[0], 1);
       T px_up = __shfl_up_sync(0xffffffffu, px_c[V - 1], 1);
-      if (lane == 31) px_dn = chdn * ldn;
-      if (lane == 0) px_up = (I0 >= 1) ? chup * lup : T(0);
+      if (dnl) px_dn = chdn * ldn;
+      if (upl) px_up = (I0 >= 1) ? chup * lup : T(0);
       T qy[V];
 #pragma unroll
       for (int v = 0; v < V; ++v) {
@@ -694,7 +712,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       }
       vst(LxB + k, lxn); vst(LyB + k, lyn);
       T qy_up = __shfl_up_sync(0xffffffffu, qy[V - 1], 1);
-      if (lane == 0) qy_up = (I0 >= 1) ? w.chyez * (lyup + px_up - px_c[0]) : T(0);
+      if (upl) qy_up = (I0 >= 1) ? w.chyez * (lyup + px_up - px_c[0]) : T(0);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         const T qym = (v > 0) ? qy[v > 0 ? v - 1 : 0] : qy_up;
@@ -720,7 +738,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       if (live && hyStrip) { sld(L + RA_HYA * 32, hya_); sld(L + RA_HYB * 32, hyb_); }
       T px_dn = __shfl_down_sync(0xffffffffu, px_c[0], 1);
       T px_up = __shfl_up_sync(0xffffffffu, px_c[V - 1], 1);
-      if (lane == 31) {
+      if (dnl) {
         px_dn = T(0);
         if (live && Idn <= NX) {
           const int cls = adj_class(w, Idn, J);
@@ -728,7 +746,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
                                       sfirst<T>(H + HA_BXDN));
         }
       }
-      if (lane == 0) {
+      if (upl) {
         px_up = T(0);
         if (live && I0 >= 1) {
           const int cls = adj_class(w, Iup, J);
@@ -766,7 +784,7 @@ __global__ void __launch_bounds__(128) k_adjw(const WDev<T> w, const AdjRingArgs
       }
       if (live) { vst(LxB + k, lxn); vst(LyB + k, lyn); }
       T qy_up = __shfl_up_sync(0xffffffffu, qy[V - 1], 1);
-      if (lane == 0) {
+      if (upl) {
         qy_up = T(0);
         if (live && I0 >= 1) {
           const T hb = upStrip ? slast<T>(H + HA_HYBUP) : w.chyez;

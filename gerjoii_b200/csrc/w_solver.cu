@@ -170,6 +170,7 @@ class WSolver : public WSolverBase {
     dn = size_t(hld) * size_t(g.n);
     nshots = ns;
     nr = 0;
+    max_rec_row = -1;
     sh.assign(ns, ShotHost{});
     sh_src_i.assign(ns, 0);
     sh_src_j.assign(ns, 0);
@@ -196,6 +197,7 @@ class WSolver : public WSolverBase {
         const long i = L % (NX + 1), j = L / (NX + 1);
         sh[s].rec[r] = i + j * ld;
         last[sh[s].rec[r]] = r;
+        max_rec_row = std::max(max_rec_row, int(i));
       }
       for (int r = 0; r < q.nr; ++r)
         if (last[sh[s].rec[r]] == r) sh[s].sel.push_back(r);
@@ -324,6 +326,8 @@ class WSolver : public WSolverBase {
   RingCfg rc;                    // configuration of the forward launches being enqueued
   RingCfg rca;                   // and of the exact-adjoint launches
   bool light_tune = false;       // batch plans: a smaller candidate set
+  const bool no_split = getenv("GJ_NO_SPLIT") != nullptr;  // one shot per general task everywhere
+  int max_rec_row = -1;          // largest receiver row over all shots (split tasks hold none)
   RingCfg rc_env;                // default, with the environment's overrides
   bool env_fixed = false;        // a GJ_RING_* variable is set: no tuning
   std::map<int, std::pair<RingCfg, RingCfg>> tuned;  // (forward, adjoint) per launch size
@@ -427,18 +431,29 @@ class WSolver : public WSolverBase {
       const int ncol = std::max(c1 - c0 + 1, 0);
       const int tjF = std::min(q.tjF, std::max(ncol, 1));
       std::vector<int4> hf, hg;
-      auto chunks = [&](std::vector<int4>& h, int z, int r0, int a0, int a1, int tj) {
-        for (int j0 = a0; j0 <= a1; j0 += tj) h.push_back(make_int4(r0, j0, std::min(j0 + tj - 1, a1), z << 1));
+      // task word: (shot << 2) | (split << 1) | fast
+      auto chunks = [&](std::vector<int4>& h, int z, int r0, int a0, int a1, int tj, int split) {
+        for (int j0 = a0; j0 <= a1; j0 += tj)
+          h.push_back(make_int4(r0, j0, std::min(j0 + tj - 1, a1), (z << 2) | (split << 1)));
+      };
+      // Split general tasks: a block whose live rows fit 16 lanes (r0 + 16 V > NX)
+      // runs two shots per warp, when no receiver of any shot lies in its rows
+      // (split tasks skip the fused receiver record and injection).
+      auto splittable = [&](int rb) {
+        const int r0 = rb * rows;
+        return !no_split && !fast[rb] && r0 + 16 * V > NX && max_rec_row < r0;
       };
       for (int z = 0; z < gn; ++z)
         for (int rb = 0; rb < nrb; ++rb) {
           const int r0 = rb * rows;
           if (fast[rb] && ncol > 0) {
-            chunks(hf, z, r0, c0, c1, tjF);
-            if (c0 > 0) chunks(hg, z, r0, 0, c0 - 1, tjS);
-            if (c1 < NY) chunks(hg, z, r0, c1 + 1, NY, tjS);
-          } else {
-            chunks(hg, z, r0, 0, NY, tjS);
+            chunks(hf, z, r0, c0, c1, tjF, 0);
+            if (c0 > 0) chunks(hg, z, r0, 0, c0 - 1, tjS, 0);
+            if (c1 < NY) chunks(hg, z, r0, c1 + 1, NY, tjS, 0);
+          } else if (!splittable(rb)) {
+            chunks(hg, z, r0, 0, NY, tjS, 0);
+          } else if (z % 2 == 0) {
+            chunks(hg, z, r0, 0, NY, tjS, z + 1 < gn ? 1 : 0);
           }
         }
       for (auto& q : hf) q.w |= 1;
@@ -559,7 +574,7 @@ class WSolver : public WSolverBase {
   // memory plan allocated for at least gn shots.
   gj_status autotune(Err& err, int gn, cudaStream_t st) {
     if (ring_nth == 0 || gn < 1) return GJ_OK;
-    if (env_fixed || tuned.count(gn)) { select_cfg(gn); return GJ_OK; }
+    if (env_fixed || tuned.count(gn)) { select_cfg(gn); return prepare_tasks(err, gn); }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     GJ_CUDA(err, cudaEventCreate(&e0));
     GJ_CUDA(err, cudaEventCreate(&e1));
@@ -618,20 +633,32 @@ class WSolver : public WSolverBase {
       return GJ_OK;
     };
     const std::vector<int> SFs = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
-    const std::vector<int> tjFs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{16, 24, 32, 48};
+    // small launches (few shots) need short column chunks to spread over the SMs
+    const bool small = long(gn) * ((NX + 1 + 127) / 128) * ((NY + 31) / 32) < 8L * nsm;
+    std::vector<int> tjFs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{16, 24, 32, 48};
     const std::vector<int> Ss = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
-    const std::vector<int> tjSs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{8, 16, 32, 64};
+    std::vector<int> tjSs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{8, 16, 32, 64};
+    if (small) { tjFs.insert(tjFs.begin(), 8); tjSs.insert(tjSs.begin(), 4); }
     const std::vector<int> rws = light_tune ? std::vector<int>{2, 4} : std::vector<int>{2, 4};
     RingCfg best[2] = {rc_env, rc_env};
     float tb[2] = {0.f, 0.f};
+    const char* vb = getenv("GJ_AUTOTUNE_VERBOSE");
+    const bool every = vb && atoi(vb) >= 2;  // print every candidate's time
+    auto show = [&](int dir, const RingCfg& q, float t) {
+      if (every)
+        fprintf(stderr, "gerjoii_b200 autotune candidate %s S=%d SF=%d RWG=%d tjF=%d tjS=%d %.2f us/step\n",
+                dir ? "adjoint" : "forward", q.S, q.SF, q.RWG, q.tjF, q.tjS, 1e3f * t / reps);
+    };
     for (int dir = 0; dir < (adj_ok ? 2 : 1); ++dir) {
       GJ_TRY(time_cfg(dir, best[dir], tb[dir]));
+      show(dir, best[dir], tb[dir]);
       auto consider = [&](const RingCfg& q) -> gj_status {
         if (q == best[dir]) return GJ_OK;
         if (ring_smem(q.RWG, q.S, false) > size_t(maxsm_dyn) || ring_smem(RW, q.SF, true) > size_t(maxsm_dyn))
           return GJ_OK;
         float t = 0.f;
         GJ_TRY(time_cfg(dir, q, t));
+        show(dir, q, t);
         if (t < tb[dir]) { tb[dir] = t; best[dir] = q; }
         return GJ_OK;
       };
@@ -654,7 +681,7 @@ class WSolver : public WSolverBase {
     tuned[gn] = {best[0], best[1]};
     select_cfg(gn);
     GJ_TRY(prepare_tasks(err, gn));
-    if (getenv("GJ_AUTOTUNE_VERBOSE"))
+    if (vb)
       fprintf(stderr,
               "gerjoii_b200 autotune %dx%d, %d shots/launch: forward S=%d SF=%d RWG=%d tjF=%d tjS=%d %.2f us/step; "
               "adjoint S=%d SF=%d RWG=%d tjF=%d tjS=%d %.2f us/step\n",
