@@ -406,9 +406,9 @@ def cfg4_leg(args):
     """cfg4: 48 uneven problems (grids 256..1536 x 128..512, dx 0.02..0.05 m,
     1500..5000 steps, 4..24 shots; blob / layer models), FP32 exact gradients
     with Kahan sums, all of them in one gj_w_gradient_batch call: the problems
-    run concurrently in memory-budgeted waves, each wave one CUDA graph launch.
+    run concurrently in memory-budgeted waves, all waves one CUDA graph launch.
     Timed: one call after a warm-up call (which plans, tunes and captures the
-    wave graphs).  Baseline: the plain per-shot FP64 form on one shot of
+    graph).  Baseline: the plain per-shot FP64 form on one shot of
     every 12th problem, compared per cell-update."""
     import torch
     from gerjoii_b200 import synth

@@ -318,7 +318,7 @@ class WSolver : public WSolverBase {
   // GJ_RING_* environment variables fix a configuration instead.
   static constexpr int RW = 4;
   struct RingCfg {
-    int S = 2, SF = 2, RWG = 4, tjF = 32, tjS = 16;
+    int S = 2, SF = 3, RWG = 2, tjF = 32, tjS = 8;
     bool operator==(const RingCfg& o) const {
       return S == o.S && SF == o.SF && RWG == o.RWG && tjF == o.tjF && tjS == o.tjS;
     }
@@ -579,7 +579,7 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaEventCreate(&e0));
     GJ_CUDA(err, cudaEventCreate(&e1));
     struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
-    const int warm = 2, reps = 12;
+    const int warm = 2, reps = 10, trials = 3;
     const bool adj_ok = lring.p != nullptr;
     // history and band slots rotate over the buffers (strided), so their
     // writes reach DRAM as in a real step instead of one L2-resident slot
@@ -624,22 +624,31 @@ class WSolver : public WSolverBase {
         return GJ_OK;
       };
       GJ_TRY(run(warm));
-      GJ_CUDA(err, cudaEventRecord(e0, st));
-      GJ_TRY(run(reps));
-      GJ_CUDA(err, cudaEventRecord(e1, st));
-      GJ_CUDA(err, cudaEventSynchronize(e1));
-      GJ_CUDA(err, cudaEventElapsedTime(&ms, e0, e1));
+      // the least of a few timed runs (others' launches and clock changes
+      // only ever add time)
+      ms = 0.f;
+      for (int trial = 0; trial < trials; ++trial) {
+        GJ_CUDA(err, cudaEventRecord(e0, st));
+        GJ_TRY(run(reps));
+        GJ_CUDA(err, cudaEventRecord(e1, st));
+        GJ_CUDA(err, cudaEventSynchronize(e1));
+        float t = 0.f;
+        GJ_CUDA(err, cudaEventElapsedTime(&t, e0, e1));
+        ms = trial ? std::min(ms, t) : t;
+      }
       GJ_CUDA(err, cudaGetLastError());
       return GJ_OK;
     };
-    const std::vector<int> SFs = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
+    const std::vector<int> SFs = light_tune ? std::vector<int>{2, 3} : std::vector<int>{2, 3, 4};
     // small launches (few shots) need short column chunks to spread over the SMs
     const bool small = long(gn) * ((NX + 1 + 127) / 128) * ((NY + 31) / 32) < 8L * nsm;
     std::vector<int> tjFs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{16, 24, 32, 48};
-    const std::vector<int> Ss = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3, 4};
-    std::vector<int> tjSs = light_tune ? std::vector<int>{16, 32} : std::vector<int>{8, 16, 32, 64};
-    if (small) { tjFs.insert(tjFs.begin(), 8); tjSs.insert(tjSs.begin(), 4); }
-    const std::vector<int> rws = light_tune ? std::vector<int>{2, 4} : std::vector<int>{2, 4};
+    const std::vector<int> Ss = light_tune ? std::vector<int>{2} : std::vector<int>{2, 3};
+    // the general kernel runs in about one wave, its time about proportional
+    // to the column chunk of a task: short chunks first
+    const std::vector<int> tjSs = light_tune ? std::vector<int>{4, 8, 16} : std::vector<int>{4, 6, 8, 12, 16, 32};
+    if (small) tjFs.insert(tjFs.begin(), 8);
+    const std::vector<int> rws = {2, 4};
     RingCfg best[2] = {rc_env, rc_env};
     float tb[2] = {0.f, 0.f};
     const char* vb = getenv("GJ_AUTOTUNE_VERBOSE");
@@ -650,6 +659,7 @@ class WSolver : public WSolverBase {
                 dir ? "adjoint" : "forward", q.S, q.SF, q.RWG, q.tjF, q.tjS, 1e3f * t / reps);
     };
     for (int dir = 0; dir < (adj_ok ? 2 : 1); ++dir) {
+      if (dir == 0) GJ_TRY(time_cfg(dir, best[dir], tb[dir]));  // clocks up before the first timing
       GJ_TRY(time_cfg(dir, best[dir], tb[dir]));
       show(dir, best[dir], tb[dir]);
       auto consider = [&](const RingCfg& q) -> gj_status {
@@ -659,23 +669,33 @@ class WSolver : public WSolverBase {
         float t = 0.f;
         GJ_TRY(time_cfg(dir, q, t));
         show(dir, q, t);
-        if (t < tb[dir]) { tb[dir] = t; best[dir] = q; }
+        if (t < 0.98f * tb[dir]) { tb[dir] = t; best[dir] = q; }  // a clear gain, not timing noise
         return GJ_OK;
       };
+      // The two kernels of a step run concurrently and the step takes about
+      // the longer of them, so the general kernel's knobs go first (with the
+      // fast kernel's default), then the fast kernel's, then the general
+      // kernel's again when the fast ones changed.
+      auto general = [&]() -> gj_status {
+        const RingCfg from = best[dir];
+        for (int S : Ss)
+          for (int tjS : tjSs)
+            for (int rw : rws) {
+              RingCfg q = from;
+              q.S = S; q.tjS = tjS; q.RWG = rw;
+              GJ_TRY(consider(q));
+            }
+        return GJ_OK;
+      };
+      GJ_TRY(general());
+      const RingCfg before = best[dir];
       for (int SF : SFs)
         for (int tjF : tjFs) {
-          RingCfg q = best[dir];
+          RingCfg q = before;
           q.SF = SF; q.tjF = tjF;
           GJ_TRY(consider(q));
         }
-      const RingCfg fast_best = best[dir];
-      for (int S : Ss)
-        for (int tjS : tjSs)
-          for (int rw : rws) {
-            RingCfg q = fast_best;
-            q.S = S; q.tjS = tjS; q.RWG = rw;
-            GJ_TRY(consider(q));
-          }
+      if (!(best[dir] == before)) GJ_TRY(general());
     }
     GJ_TRY(clear());
     tuned[gn] = {best[0], best[1]};
@@ -1536,6 +1556,8 @@ class WSolver : public WSolverBase {
   // The whole gradient of all shots after plan_buffers (L2, no residual
   // filter): accumulators cleared, then every shot group; capturable.
   gj_status enqueue_all(Err& err, Ctx& c, gj_adj_mode mode, int kahan, cudaStream_t st, long& nl) {
+    // a ring in a shared pool holds what the pool's previous user left there
+    if (ring_on && !lring.owned) GJ_CUDA(err, cudaMemsetAsync(lring.p, 0, size_t(Kd) * G * dn * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     GJ_CUDA(err, cudaMemsetAsync(acc.p, 0, nshots * 4 * dn * sizeof(T), st));
     if (band_on) GJ_CUDA(err, cudaMemsetAsync(bacc.p, 0, size_t(nshots) * 2 * size_t(w.bsz) * sizeof(T), st));
@@ -1970,16 +1992,15 @@ struct WBatch : WBatchBase {
   std::vector<int> kc;  // checkpoint interval per problem (nt: whole history)
   DevBuf pool;
   std::vector<std::vector<int>> waves;
-  std::vector<cudaGraphExec_t> execs;
-  std::vector<long> launches;
+  cudaGraphExec_t exec = nullptr;  // every wave, one after the other, in one graph
+  long launches = 0;               // kernel launches inside it
   int mode = -1, kahan = -1;
   size_t budget_opt = 0;  // opts.mem_budget_bytes the waves were planned for
   void drop_waves() {
-    for (auto e : execs)
-      if (e) cudaGraphExecDestroy(e);
-    execs.clear();
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
     waves.clear();
-    launches.clear();
+    launches = 0;
   }
   ~WBatch() override { drop_waves(); }
 };
@@ -2027,10 +2048,10 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
   }
   const bool exact = mode == GJ_ADJ_EXACT;
   if (B->waves.empty()) {
-    // per-problem memory outside the pool (accumulators, final gradients) and the pool budget
+    // per-problem memory outside the pool (accumulators, forward states, final gradients) and the pool budget
     size_t owned = 0;
     for (auto& q : B->plans)
-      owned += size_t(q->nshots) * (4 * q->dn + (exact ? 2 * size_t(q->w.bsz) : 0)) * sizeof(T) +
+      owned += size_t(q->nshots) * (4 * q->dn + 2 * q->sstride + (exact ? 2 * size_t(q->w.bsz) : 0)) * sizeof(T) +
                4 * q->mn * sizeof(double);
     size_t free_b = 0, total_b = 0;
     GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
@@ -2077,18 +2098,20 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
       pool = std::max(pool, u);
     }
     GJ_TRY(B->pool.alloc(err, pool));
-    B->execs.assign(B->waves.size(), nullptr);
-    B->launches.assign(B->waves.size(), 0);
   }
   if (nwaves_out) *nwaves_out = int(B->waves.size());
-  for (size_t wi = 0; wi < B->waves.size(); ++wi) {
-    const auto& wv = B->waves[wi];
-    if (!B->execs[wi]) {
+  if (!B->exec) {
+    // One graph: per wave, one child graph per problem (no dependencies
+    // between them); each wave after the previous one, whose pool it reuses.
+    cudaGraph_t all = nullptr;
+    GJ_CUDA(err, cudaGraphCreate(&all, 0));
+    struct GraphGuard { cudaGraph_t g; ~GraphGuard() { if (g) cudaGraphDestroy(g); } } ga{all};
+    std::vector<cudaGraphNode_t> prev;  // the previous wave's nodes
+    long nl = 0;
+    for (size_t wi = 0; wi < B->waves.size(); ++wi) {
+      const auto& wv = B->waves[wi];
       unsigned char* cursor = B->pool.template as<unsigned char>();
-      cudaGraph_t wave = nullptr;
-      GJ_CUDA(err, cudaGraphCreate(&wave, 0));
-      struct GraphGuard { cudaGraph_t g; ~GraphGuard() { if (g) cudaGraphDestroy(g); } } gg{wave};
-      long nl = 0;
+      std::vector<cudaGraphNode_t> cur;
       for (int p : wv) {
         WSolver<T>& q = *B->plans[p];
         gj_w_opts op = o0;
@@ -2112,21 +2135,27 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
         if (rs != GJ_OK) { if (pg) cudaGraphDestroy(pg); return rs; }
         if (ce != cudaSuccess) return err.set(GJ_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce));
         cudaGraphNode_t node;
-        ce = cudaGraphAddChildGraphNode(&node, wave, nullptr, 0, pg);
+        ce = cudaGraphAddChildGraphNode(&node, all, prev.data(), prev.size(), pg);
         cudaGraphDestroy(pg);
         if (ce != cudaSuccess) return err.set(GJ_ECUDA, "child graph: %s", cudaGetErrorString(ce));
+        cur.push_back(node);
       }
-      cudaError_t ce = cudaGraphInstantiate(&B->execs[wi], wave, cudaGraphInstantiateFlagUseNodePriority);
-      if (ce != cudaSuccess) {
-        B->execs[wi] = nullptr;
-        return err.set(GJ_ECUDA, "wave graph instantiate failed: %s", cudaGetErrorString(ce));
-      }
-      B->launches[wi] = nl;
+      prev = std::move(cur);
     }
-    GJ_CUDA(err, cudaGraphLaunch(B->execs[wi], st));
-    GJ_CUDA(err, cudaStreamSynchronize(st));
-    c.launches += B->launches[wi];
-    for (int p : wv) {
+    cudaError_t ce = cudaGraphInstantiate(&B->exec, all, cudaGraphInstantiateFlagUseNodePriority);
+    if (ce != cudaSuccess) {
+      B->exec = nullptr;
+      return err.set(GJ_ECUDA, "batch graph instantiate failed: %s", cudaGetErrorString(ce));
+    }
+    B->launches = nl;
+  }
+  GJ_CUDA(err, cudaGraphLaunch(B->exec, st));
+  GJ_CUDA(err, cudaStreamSynchronize(st));
+  c.launches += B->launches;
+  // every problem's accumulators, sums and traces are its own (outside the
+  // pool), so the finishing steps follow the whole graph
+  for (int p = 0; p < np; ++p) {
+    {
       WSolver<T>& q = *B->plans[p];
       std::vector<double> hs(2 * q.nshots);
       GJ_CUDA(err, cudaMemcpy(hs.data(), q.sums.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost));

@@ -164,11 +164,13 @@ typedef struct gj_w_problem {
 /* Gradients of many independent problems of uneven sizes in one call: the
  * reference runs such inversions as separate parfor workers and Slurm jobs
  * (w_update_e_.m:32 per shot, one MATLAB process per field line).  The
- * problems run concurrently in memory-budgeted waves, each wave one CUDA
- * graph launch holding every problem's whole gradient (forward, residual,
- * recompute, exact or reference adjoint, imaging; all its shots per launch);
- * a problem keeps its whole u history when the wave's memory allows, else it
- * checkpoints.  Plans, buffers and the wave graphs are cached in the context
+ * problems run concurrently in memory-budgeted waves (a wave's problems
+ * share one device pool; the next wave starts when the previous one ends),
+ * and all waves are one CUDA graph launch holding every problem's whole
+ * gradient (forward, residual, recompute, exact or reference adjoint,
+ * imaging; all its shots per launch); a problem keeps its whole u history
+ * when its wave's memory allows, else it checkpoints.  Plans, buffers and the
+ * graph are cached in the context
  * while the problems (grids and shots) repeat.  L2 misfit; opts: no_kahan and
  * mem_budget_bytes (the pool budget, 0 = 80% of free memory) apply, the plain,
  * no_ring, filter, conditioning and per_shot options do not (GJ_EUNSUPPORTED).

@@ -1,5 +1,5 @@
 """gj_w_gradient_batch: independent problems of uneven grids, shot counts and
-step counts in memory-budgeted waves, each wave one CUDA graph launch.  Every
+step counts in memory-budgeted waves, all waves one CUDA graph launch.  Every
 problem's gradient must equal its own gj_w_gradient call (FP64), with whole
 histories and with a pool budget small enough to force several waves (and
 checkpointing where a wave's spare memory cannot hold whole histories), and
