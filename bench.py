@@ -566,9 +566,10 @@ def main():
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     # instrumented pass after the timed region: one step (after one more that
-    # captures the graphs with the timing events) with CUDA events around
-    # every 8th launch of each step kernel; per-kernel averages and the
-    # roofline come from here
+    # captures the graphs with the timing events) with CUDA events around runs
+    # of 8 consecutive launches of a step kernel (one run per 16 launches) and
+    # single imaging launches; per-kernel averages and the roofline come from
+    # here
     ctx.set_kernel_timing(True)
     step()
     torch.cuda.synchronize()
@@ -649,8 +650,9 @@ def main():
                                "20 B x band-frame entries",
                       "ref_step": "per shot: 32 B x NX*NY cells + 48 B x m*n (4 history reads, 4 sums r/w)"}[dom],
             "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / isteps / (ms / args.steps),
-            "pass": "separate instrumented step after the timed region (CUDA events around every 8th launch of "
-                    "each step kernel, also inside the graphs); the timed region itself runs without events"}
+            "pass": "separate instrumented step after the timed region (CUDA events around runs of 8 consecutive "
+                    "launches of each step kernel, one run per 16 launches, also inside the graphs; runs that the "
+                    "imaging kernel interrupts are dropped); the timed region itself runs without events"}
     line = {"metric": METRIC, "value": value, "unit": "shot-gradients/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -105,14 +105,20 @@ enum KernelKind {
 };
 
 // Optional per-kernel device timing: CUDA events around sampled launches of
-// the hot kernels (every `stride`-th launch of each kind; every launch of the
-// DC factor and substitution, which run a few times per call), also inside captured
-// CUDA graphs (external event-record nodes).  A Marks list belongs to one
-// launch sequence (a direct enqueue, or one captured graph that is replayed);
-// collect() adds its elapsed times after the stream has been synchronised.
+// the hot kernels, also inside captured CUDA graphs (external event-record
+// nodes).  The step kernels are timed in runs of `span` consecutive launches
+// (one run starts at every `stride`-th launch of a kind), so the cost of the
+// event records is spread over the run; a run that another timed kernel
+// interrupts (the imaging kernel between adjoint steps) is dropped.  Other
+// kinds are timed one launch at a time (every `stride`-th; every launch of
+// the DC factor and substitution, which run a few times per call).  A Marks
+// list belongs to one launch sequence (a direct enqueue, or one captured graph
+// that is replayed); collect() adds its elapsed times after the stream has
+// been synchronised.
 struct Marks {
   std::vector<cudaEvent_t> ev;            // owned events, in pairs
-  std::vector<int> kind;                  // per pair
+  std::vector<int> kind;                  // per pair (-1: dropped run)
+  std::vector<int> count;                 // per pair: launches inside it
   long launches[8] = {0};                 // every launch of each kind in this sequence
   long shot_launches[8] = {0};            // sum of shots over those launches
   ~Marks() { for (auto e : ev) cudaEventDestroy(e); }
@@ -120,24 +126,33 @@ struct Marks {
 
 struct KernelTimer {
   bool on = false;
-  int stride = 8;
+  int stride = 16, span = 8;
   double ms[8] = {0};
   long sampled[8] = {0};
   long launches[8] = {0};
   long shot_launches[8] = {0};
   long seen[8] = {0};
   Marks* cur = nullptr;  // list receiving new marks
+  int open = -1;         // kind of the run being timed, or -1
+  int open_n = 0;        // launches in it so far
   static void rec(cudaEvent_t e, cudaStream_t st) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(st, &cs);
     if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
     else cudaEventRecord(e, st);
   }
+  static bool step_kind(int k) { return k == KK_FWD_STEP || k == KK_REF_STEP || k == KK_ADJ_STEP; }
   // begin/end bracket one launch of `shots` shots; begin returns whether it is timed.
   bool begin(int kind, cudaStream_t st, int shots = 1) {
     if (!on || !cur) return false;
     cur->launches[kind] += 1;
     cur->shot_launches[kind] += shots;
+    if (open >= 0 && open != kind) {  // another kernel inside the run: drop it
+      rec(cur->ev.back(), st);
+      cur->kind.back() = -1;
+      open = -1;
+    }
+    if (open == kind) return true;
     const int every = (kind == KK_DC_FACTOR || kind == KK_DC_PRECOND) ? 1 : stride;
     if ((seen[kind]++ % every) != 0) return false;
     cudaEvent_t a, b;
@@ -146,20 +161,33 @@ struct KernelTimer {
     cur->ev.push_back(a);
     cur->ev.push_back(b);
     cur->kind.push_back(kind);
+    cur->count.push_back(0);
     rec(a, st);
+    open = kind;
+    open_n = 0;
     return true;
   }
   void end(bool timed, cudaStream_t st) {
-    if (timed) rec(cur->ev.back(), st);
+    if (!timed || open < 0) return;
+    cur->count.back() += 1;
+    if (++open_n >= (step_kind(open) ? span : 1)) {
+      rec(cur->ev.back(), st);
+      open = -1;
+    }
+  }
+  // Ends an open run (shorter than span) before the sequence ends.
+  void close(cudaStream_t st) {
+    if (open >= 0 && cur) rec(cur->ev.back(), st);
+    open = -1;
   }
   // Adds one execution of the sequence `m` (after its stream has completed).
   void collect(const Marks& m) {
     if (!on) return;
     for (size_t q = 0; q < m.kind.size(); ++q) {
       float t = 0;
-      if (cudaEventElapsedTime(&t, m.ev[2 * q], m.ev[2 * q + 1]) == cudaSuccess) {
+      if (m.kind[q] >= 0 && m.count[q] > 0 && cudaEventElapsedTime(&t, m.ev[2 * q], m.ev[2 * q + 1]) == cudaSuccess) {
         ms[m.kind[q]] += t;
-        sampled[m.kind[q]] += 1;
+        sampled[m.kind[q]] += m.count[q];
       }
     }
     for (int k = 0; k < 8; ++k) { launches[k] += m.launches[k]; shot_launches[k] += m.shot_launches[k]; }
@@ -167,6 +195,7 @@ struct KernelTimer {
   }
   void reset() {
     for (int k = 0; k < 8; ++k) { ms[k] = 0; sampled[k] = 0; launches[k] = 0; shot_launches[k] = 0; seen[k] = 0; }
+    open = -1;
   }
 };
 

@@ -579,7 +579,7 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaEventCreate(&e0));
     GJ_CUDA(err, cudaEventCreate(&e1));
     struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
-    const int warm = 2, reps = 10, trials = 3;
+    const int reps = 10, trials = 3;
     const bool adj_ok = lring.p != nullptr;
     // history and band slots rotate over the buffers (strided), so their
     // writes reach DRAM as in a real step instead of one L2-resident slot
@@ -601,7 +601,7 @@ class WSolver : public WSolverBase {
       GJ_TRY(clear());
       T* A = (dir == 0 ? fwdA : adjA).template as<T>() + ld;
       T* B = (dir == 0 ? fwdB : adjB).template as<T>() + ld;
-      auto run = [&](int n) -> gj_status {
+      auto run = [&](int n, cudaStream_t rs) -> gj_status {
         for (int i = 0; i < n; ++i) {
           if (dir == 0) {
             StepArgs<T> a = step_args(A, B, i % g.nt);
@@ -609,7 +609,7 @@ class WSolver : public WSolverBase {
             if (band_on && bhist.p && nslot > 1) a.band = bhist.as<T>() + slot_of(i) * gn * size_t(w.bsz);
             RecArgs<T> ra = rec_args(0);
             if (nr > 0) { ra.d = dbuf.as<T>(); ra.it = i % g.nt; }
-            GJ_TRY(launch_fwd(err, a, gn, st, ra));
+            GJ_TRY(launch_fwd(err, a, gn, rs, ra));
           } else {
             AdjRingArgs<T> b{};
             b.A = A; b.B = B; b.fstride = fstride; b.sstride = sstride; b.shot0 = 0;
@@ -617,19 +617,37 @@ class WSolver : public WSolverBase {
             if (band_on && blam.p) b.band = blam.as<T>() + size_t(i % Kd) * gn * size_t(w.bsz);
             RecArgs<T> rb = rec_args(0);
             if (nr > 0) { rb.e = ebuf.as<T>(); rb.kinj = i % g.nt; }
-            GJ_TRY(launch_adjr(err, b, gn, st, rb));
+            GJ_TRY(launch_adjr(err, b, gn, rs, rb));
           }
           std::swap(A, B);
         }
         return GJ_OK;
       };
-      GJ_TRY(run(warm));
-      // the least of a few timed runs (others' launches and clock changes
+      // The steps run as the solver runs them: captured into a CUDA graph
+      // (node priorities kept) and replayed.  Launched one by one from a
+      // stream instead, configurations with larger general-kernel CTAs timed
+      // about as fast as the best and then ran twice as long inside graphs.
+      cudaStream_t cs = nullptr;
+      GJ_CUDA(err, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+      GJ_CUDA(err, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      gj_status rs = run(reps, cs);
+      cudaGraph_t gr = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(cs, &gr);
+      cudaStreamDestroy(cs);
+      if (rs != GJ_OK) { if (gr) cudaGraphDestroy(gr); return rs; }
+      if (ce != cudaSuccess) return err.set(GJ_ECUDA, "tuning graph capture failed: %s", cudaGetErrorString(ce));
+      cudaGraphExec_t ex = nullptr;
+      ce = cudaGraphInstantiate(&ex, gr, cudaGraphInstantiateFlagUseNodePriority);
+      cudaGraphDestroy(gr);
+      if (ce != cudaSuccess) return err.set(GJ_ECUDA, "tuning graph instantiate failed: %s", cudaGetErrorString(ce));
+      struct ExecGuard { cudaGraphExec_t e; ~ExecGuard() { cudaGraphExecDestroy(e); } } eg{ex};
+      GJ_CUDA(err, cudaGraphLaunch(ex, st));  // warm-up replay
+      // the least of a few timed replays (others' launches and clock changes
       // only ever add time)
       ms = 0.f;
       for (int trial = 0; trial < trials; ++trial) {
         GJ_CUDA(err, cudaEventRecord(e0, st));
-        GJ_TRY(run(reps));
+        GJ_CUDA(err, cudaGraphLaunch(ex, st));
         GJ_CUDA(err, cudaEventRecord(e1, st));
         GJ_CUDA(err, cudaEventSynchronize(e1));
         float t = 0.f;
@@ -1633,6 +1651,7 @@ class WSolver : public WSolverBase {
         if (rs == GJ_OK && env) rs = env_residual(err, c, g0, gn, mk, st);
         if (rs == GJ_OK && filt) rs = filt_residual(err, c, o, g0, gn, st);
         if (rs == GJ_OK) rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st, 2, false);
+        c.timer.close(st);
         c.timer.cur = nullptr;
         GJ_TRY(rs);
         GJ_CUDA(err, cudaStreamSynchronize(st));
@@ -1643,6 +1662,7 @@ class WSolver : public WSolverBase {
         Marks m;
         c.timer.cur = &m;
         gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, nl, st);
+        c.timer.close(st);
         c.timer.cur = nullptr;
         GJ_TRY(rs);
         GJ_CUDA(err, cudaStreamSynchronize(st));
@@ -1663,6 +1683,7 @@ class WSolver : public WSolverBase {
         c.timer.cur = rec->marks.get();
         long cnt = 0;
         gj_status rs = enqueue_group(err, c, g0, gn, mode, kahan, segs, full, cnt, cs);
+        c.timer.close(cs);
         c.timer.cur = nullptr;
         cudaGraph_t graph = nullptr;
         cudaError_t ce = cudaStreamEndCapture(cs, &graph);
@@ -1814,6 +1835,7 @@ class WSolver : public WSolverBase {
         }
       }
     }
+    c.timer.close(st);
     c.timer.cur = nullptr;
     c.launches += nlb;
     GJ_CUDA(err, cudaGetLastError());

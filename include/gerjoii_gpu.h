@@ -376,13 +376,15 @@ gj_status gj_w_forward_noalloc(const gj_w_grid* grid, const float* eps_dev, cons
 long gj_last_launch_count(const gj_ctx* ctx);
 
 /* Per-kernel device timing, accumulated over calls while enabled: CUDA events
- * around every 8th launch of each radar step kernel (inside captured graphs
- * too) and around every launch of the DC factor and substitution.
+ * around runs of 8 consecutive launches of each radar step kernel (one run per
+ * 16 launches; a run that another timed kernel interrupts is dropped), around
+ * every 16th launch of the other radar kernels (inside captured graphs too)
+ * and around every launch of the DC factor and substitution.
  * kind: 0 forward Yee step, 1 reference-adjoint step, 2 exact-adjoint step,
  * 3 receiver I/O, 4 plain kernels, 5 DC band factor, 6 radar imaging,
  * 7 DC band substitution (preconditioner apply).  gj_kernel_time returns the
- * summed milliseconds of the timed launches (ms / sampled is the average
- * launch duration), the number of launches of that kind, and the sum over
+ * summed milliseconds of the timed launches, their number (ms / sampled is
+ * the average launch duration), the number of launches of that kind, and the sum over
  * those launches of the shots each one advanced.  No counterpart in the
  * reference (MATLAB tic/toc around whole phases, w_begin_.m:74-76). */
 gj_status gj_set_kernel_timing(gj_ctx* ctx, int on);

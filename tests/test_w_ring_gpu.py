@@ -2,6 +2,8 @@
 against the register-marching kernels and the oracle, on grids tall enough
 for several row blocks per column, so the halo rows, the fast and general
 paths, the column chunks and the imaging windows are all exercised."""
+import os
+
 import numpy as np
 import pytest
 
@@ -126,3 +128,68 @@ def test_ring_reference_adjoint_matches_marching_and_oracle(gpu_ctx, oracle, tal
     ge, gs, _ = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]), mode="reference")
     assert rel_l2(r["g_eps"], ge) < 1e-9
     assert rel_l2(r["g_sig"], gs) < 1e-9
+
+
+@pytest.mark.parametrize("mode", ["exact", "reference"])
+@pytest.mark.parametrize("nsrc", [4, 5])
+def test_split_bottom_tasks_match_oracle(gpu_ctx, oracle, mode, nsrc):
+    """A grid whose bottom row block has few live rows (NX + 1 = 152: 24 rows
+    past the last full block of 128 (FP32) or 64 (FP64) rows), so that block
+    runs as split tasks, two shots per warp, in both precisions; an odd shot
+    count leaves the last shot of each launch unpaired."""
+    p = synth.small(m=140, n=44, pml=10, nt=200, nsrc=nsrc, nrec=9, seed=37)
+    g = p.grid
+    assert g.pml_top + g.air + g.m + g.pml + 1 == 152
+    dobs = _dobs(oracle, p)
+    ge, gs, mis = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]), mode=mode)
+    gm = N.GJ_ADJ_EXACT if mode == "exact" else N.GJ_ADJ_REFERENCE
+    r64 = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=gm, precision=N.GJ_F64)
+    assert rel_l2(r64["g_eps"], ge) < 1e-9
+    assert rel_l2(r64["g_sig"], gs) < 1e-9
+    assert rel_l2(edge_cells(r64["g_eps"]), edge_cells(ge)) < 1e-9
+    assert np.allclose(r64["misfit"], mis, rtol=1e-10)
+    # FP32: split tasks against one shot per task everywhere (GJ_NO_SPLIT),
+    # both with the same fixed ring configuration (the column chunks decide
+    # where a task recomputes its first Hx column, which moves FP32 rounding),
+    # in contexts whose plans are made with those variables set
+    fixed = {"GJ_RING_STAGES": "2", "GJ_RING_STAGES_FAST": "3", "GJ_RING_CTA_WARPS": "2",
+             "GJ_RING_TJF": "32", "GJ_RING_TJS": "8"}
+    res = []
+    for extra in ({}, {"GJ_NO_SPLIT": "1"}):
+        env = dict(fixed, **extra)
+        os.environ.update(env)
+        try:
+            ctx2 = N.Context(0)
+            try:
+                res.append(ctx2.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=gm, precision=N.GJ_F32))
+            finally:
+                ctx2.close()
+        finally:
+            for k in env:
+                del os.environ[k]
+    for key in ("g_eps", "g_sig"):
+        assert rel_l2(res[0][key], res[1][key]) < 1e-6, key
+
+
+def test_kernel_timing_counts_runs(gpu_ctx, oracle, tall):
+    """The optional device timing: every step launch is counted, runs of
+    consecutive step launches are sampled, and the average launch time lies
+    between zero and the call's wall time per step."""
+    import time
+    p = tall
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)  # plans, graphs
+    gpu_ctx.set_kernel_timing(True)
+    try:
+        t0 = time.perf_counter()
+        gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)
+        wall_ms = 1e3 * (time.perf_counter() - t0)
+        kt = {k: gpu_ctx.kernel_time(k) for k in ("fwd_step", "adj_step", "image")}
+    finally:
+        gpu_ctx.set_kernel_timing(False)
+    for k in ("fwd_step", "adj_step"):
+        assert kt[k]["launches"] >= g.nt
+        assert 0 < kt[k]["sampled"] <= kt[k]["launches"]
+        assert 0 < kt[k]["avg_us"] < 1e3 * wall_ms / g.nt
+    assert kt["image"]["launches"] >= 1
