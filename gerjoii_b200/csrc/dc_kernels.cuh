@@ -341,8 +341,10 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
 
 // z = (L D L^T)^{-1} r and rz = r.z for every system; one warp (one CTA) per
 // system.  r, z are FP64 vectors in the reference layout [sys][l + h*n].
-// Factor columns stream through a shared-memory ring of DC_NST chunks of DC_CH
-// columns (16-byte cp.async, DC_NST - 1 chunks ahead).  The substitution window
+// Factor columns stream through a shared-memory ring of NST chunks of CH
+// columns (16-byte cp.async, NST - 1 chunks ahead); a ring of 4 x 8 columns
+// (26.6 KB for b = 101 in FP64) lets 8 systems share an SM, where 4 x 16
+// columns allowed 4.  The substitution window
 // lives in registers: within the 32-step sub-block starting at band index qs,
 // slot u of lane t holds position qs + 32u + t (mod 32R), so slot 0 holds the
 // sub-block's own positions; the slots rotate by one between sub-blocks and
@@ -354,25 +356,25 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
 //            them; the DC_NEAR - 1 nearest terms come from registers, so the
 //            reduction of step q waits only for x_{q+DC_NEAR}, which enters the
 //            window DC_NEAR steps after it is computed.
-constexpr int DC_CH = 16, DC_NST = 4, DC_NEAR = 4;
+constexpr int DC_NEAR = 4;
 
 template <class TF>
-__host__ __device__ inline size_t dc_precond_smem(int wp) {
-  return size_t(DC_NST) * DC_CH * wp * sizeof(TF);
+__host__ __device__ inline size_t dc_precond_smem(int wp, int ch, int nst) {
+  return size_t(nst) * ch * wp * sizeof(TF);
 }
 
 __device__ __forceinline__ unsigned dc_smem_addr(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
-// Copies factor chunk c (columns c*DC_CH ..) into ring slot c mod DC_NST as one
+// Copies factor chunk c (columns c*CH ..) into ring slot c mod NST as one
 // commit group (an empty group when c is outside [0, nch)).
-template <class TF>
+template <class TF, int CH, int NST>
 __device__ __forceinline__ void dc_chunk_async(TF* ring, const TF* F, int c, int nch, int wp, int lane) {
   if (c >= 0 && c < nch) {
-    const int pieces = DC_CH * wp * int(sizeof(TF)) / 16;
-    const char* src = reinterpret_cast<const char*>(F + size_t(c) * DC_CH * wp);
-    const unsigned dst = dc_smem_addr(ring + (c & (DC_NST - 1)) * DC_CH * wp);
+    const int pieces = CH * wp * int(sizeof(TF)) / 16;
+    const char* src = reinterpret_cast<const char*>(F + size_t(c) * CH * wp);
+    const unsigned dst = dc_smem_addr(ring + (c & (NST - 1)) * CH * wp);
     for (int p = lane; p < pieces; p += 32)
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16u * unsigned(p)),
                    "l"(src + 16 * size_t(p))
@@ -381,7 +383,7 @@ __device__ __forceinline__ void dc_chunk_async(TF* ring, const TF* F, int c, int
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }
 
-template <class TF, int R>
+template <class TF, int R, int CH, int NST>
 __global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac, const double* r, double* z,
                                                    double* rz, int nsys, const int* done) {
   extern __shared__ __align__(16) unsigned char shpraw[];
@@ -390,7 +392,8 @@ __global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac
   const int sys = blockIdx.x, lane = threadIdx.x & 31;
   if (sys >= nsys || (done && done[sys])) return;
   const int N = G.N, b = G.b, wp = G.wp, nq = G.nq;
-  const int nch = nq / DC_CH;
+  static_assert((CH == 4 || CH == 8 || CH == 16) && (NST == 4 || NST == 8), "power-of-two ring shapes");
+  const int nch = nq / CH;
   const TF* F = fac + size_t(sys) * nq * wp;
   const double* Rv = r + size_t(sys) * N;
   double* Z = z + size_t(sys) * N;
@@ -398,23 +401,23 @@ __global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac
   auto rld = [&](const double* v, int a) { return (a >= 0 && a < N) ? v[ref(a)] : 0.0; };
   auto chunk_wait = [&](int c_issue) {
     __syncwarp();  // every lane is done with the slot being refilled
-    dc_chunk_async(ring, F, c_issue, nch, wp, lane);
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(DC_NST - 1) : "memory");
+    dc_chunk_async<TF, CH, NST>(ring, F, c_issue, nch, wp, lane);
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NST - 1) : "memory");
     __syncwarp();
   };
-  auto column = [&](int q) { return ring + (((q / DC_CH) & (DC_NST - 1)) * DC_CH + (q & (DC_CH - 1))) * wp; };
+  auto column = [&](int q) { return ring + (((q / CH) & (NST - 1)) * CH + (q & (CH - 1))) * wp; };
   // ---- forward sweep
   TF w[R];
 #pragma unroll
   for (int u = 0; u < R; ++u) w[u] = TF(rld(Rv, 32 * u + lane));
   double rn = rld(Rv, WIN + lane);  // refills of the sub-block's slot 0
-  for (int c = 0; c < DC_NST - 1; ++c) dc_chunk_async(ring, F, c, nch, wp, lane);
+  for (int c = 0; c < NST - 1; ++c) dc_chunk_async<TF, CH, NST>(ring, F, c, nch, wp, lane);
   for (int qs = 0; qs < nq; qs += 32) {
     const double rnn = rld(Rv, qs + 32 + WIN + lane);
     TF zv = TF(0);
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
-      if ((j & (DC_CH - 1)) == 0) chunk_wait((qs + j) / DC_CH + DC_NST - 1);
+      if ((j & (CH - 1)) == 0) chunk_wait((qs + j) / CH + NST - 1);
       const TF* col = column(qs + j);
       const TF y = __shfl_sync(0xffffffffu, w[0], j);
       if (lane == j) { zv = y * col[0]; w[0] = TF(rn); }
@@ -439,7 +442,7 @@ __global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac
   TF nx[DC_NEAR];  // nx[k] = x_{q+1+k}
 #pragma unroll
   for (int k = 0; k < DC_NEAR; ++k) nx[k] = TF(0);
-  for (int c = 0; c < DC_NST - 1; ++c) dc_chunk_async(ring, F, nch - 1 - c, nch, wp, lane);
+  for (int c = 0; c < NST - 1; ++c) dc_chunk_async<TF, CH, NST>(ring, F, nch - 1 - c, nch, wp, lane);
   double zc = rld(Z, nq - 32 + lane), rc = rld(Rv, nq - 32 + lane);
   double acc = 0.0;
   for (int qs = nq - 32; qs >= 0; qs -= 32) {
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(32) k_dc_precond(const DcGrid G, const TF* fac
     TF xv = TF(0);
 #pragma unroll
     for (int j = 31; j >= 0; --j) {
-      if ((j & (DC_CH - 1)) == DC_CH - 1) chunk_wait((qs + j) / DC_CH - (DC_NST - 1));
+      if ((j & (CH - 1)) == CH - 1) chunk_wait((qs + j) / CH - (NST - 1));
       const TF* col = column(qs + j);
       if (j + DC_NEAR < 32) { if (lane == j + DC_NEAR) w[0] = nx[DC_NEAR - 1]; }
       else if (lane == j + DC_NEAR - 32) w[1] = nx[DC_NEAR - 1];

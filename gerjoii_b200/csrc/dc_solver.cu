@@ -10,12 +10,38 @@
 // preconditioner (k_dc_ic0_*).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "dc_kernels.cuh"
 #include "gj_internal.h"
 
 namespace gj {
+
+// Shape of the substitution's shared-memory ring: chunks of `ch` factor
+// columns, `nst` chunks (8 x 4 by default; GJ_DC_RING=CHxNST picks 4x4, 4x8,
+// 8x4 or 16x4).
+struct DcRing { int ch = 8, nst = 4; };
+static DcRing dc_ring() {
+  DcRing r;
+  if (const char* e = getenv("GJ_DC_RING")) {
+    int a = 0, b = 0;
+    if (sscanf(e, "%dx%d", &a, &b) == 2 &&
+        ((a == 4 && (b == 4 || b == 8)) || (a == 8 && b == 4) || (a == 16 && b == 4))) { r.ch = a; r.nst = b; }
+  }
+  return r;
+}
+// The substitution kernel of a window of 32 R band positions and a ring shape.
+template <class TF>
+static void (*dc_precond_kernel(int b, DcRing r))(const DcGrid, const TF*, const double*, double*, double*, int,
+                                                   const int*) {
+  const bool wide = b >= 128;
+  if (r.ch == 4 && r.nst == 4) return wide ? k_dc_precond<TF, 8, 4, 4> : k_dc_precond<TF, 4, 4, 4>;
+  if (r.ch == 4) return wide ? k_dc_precond<TF, 8, 4, 8> : k_dc_precond<TF, 4, 4, 8>;
+  if (r.ch == 16) return wide ? k_dc_precond<TF, 8, 16, 4> : k_dc_precond<TF, 4, 16, 4>;
+  return wide ? k_dc_precond<TF, 8, 8, 4> : k_dc_precond<TF, 4, 8, 4>;
+}
 
 namespace {
 
@@ -105,7 +131,9 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
   const double* k2 = P.ky2.as<double>();
   const TF* F = c.dc_fac.as<TF>();
   const dim3 gv((N + 255) / 256 < 64 ? (N + 255) / 256 : 64, nsys);
-  const size_t shp = dc_precond_smem<TF>(G.wp);
+  const DcRing ring = dc_ring();
+  const size_t shp = dc_precond_smem<TF>(G.wp, ring.ch, ring.nst);
+  const auto kpre = dc_precond_kernel<TF>(G.b, ring);
   auto precond = [&](double* rzv) {  // one warp per system; window of 32R >= b + 1 positions
     const bool tm = c.timer.begin(KK_DC_PRECOND, st, nsys);
     if (ic0) {  // two FP32 sweeps of the red-black IC(0) factor
@@ -114,8 +142,9 @@ static gj_status pcg(Err& err, Ctx& c, DcPlan& P, int sys0, int nsys, double* B,
       k_dc_ic0_black<<<gv, 256, 0, st>>>(G, Dv, ox, oz, R, Z, rzv, nsys, done);
       k_dc_ic0_red<<<gv, 256, 0, st>>>(G, Dv, ox, oz, R, Z, rzv, nsys, done);
       c.launches += 1;
-    } else if (G.b < 128) k_dc_precond<TF, 4><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
-    else k_dc_precond<TF, 8><<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
+    } else {
+      kpre<<<nsys, 32, shp, st>>>(G, F, R, Z, rzv, nsys, done);
+    }
     c.timer.end(tm, st);
   };
   GJ_CUDA(err, cudaMemsetAsync(X, 0, vn * sizeof(double), st));
@@ -193,7 +222,7 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
     GJ_CUDA(err, cudaGetDevice(&dev));
     GJ_CUDA(err, cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (G.b > DC_FACTOR_THREADS - DC_NB - 1 || dc_factor_smem<TF>(G.b) > size_t(maxsm) ||
-        dc_precond_smem<TF>(G.wp) > size_t(maxsm))
+        dc_precond_smem<TF>(G.wp, dc_ring().ch, dc_ring().nst) > size_t(maxsm))
       return err.set(GJ_EUNSUPPORTED, "band width min(n, m) = %d: the factor window needs %zu bytes of shared memory "
                                       "(limit %d)", G.b, dc_factor_smem<TF>(G.b), maxsm);
   }
@@ -276,8 +305,11 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   double rel_max = 0;
   const size_t smem_f = dc_factor_smem<TF>(G.b);
   GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
-  GJ_CUDA(err, cudaFuncSetAttribute(G.b < 128 ? k_dc_precond<TF, 4> : k_dc_precond<TF, 8>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(dc_precond_smem<TF>(G.wp))));
+  {
+    const DcRing ring = dc_ring();
+    GJ_CUDA(err, cudaFuncSetAttribute(dc_precond_kernel<TF>(G.b, ring), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(dc_precond_smem<TF>(G.wp, ring.ch, ring.nst))));
+  }
   {
     const int nt = dc_factor_shape(G.b).BP / 4;
     std::vector<unsigned> ht;
