@@ -133,6 +133,7 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
 // are zero.
 constexpr int DC_NB = 8;
 constexpr int DC_FACTOR_THREADS = 256;
+static_assert(DC_FACTOR_THREADS == 32 * DC_NB, "one warp per entering column");
 
 struct DcFactorShape {
   int M, Mr, BP, ntiles;
@@ -325,12 +326,24 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
           }
       }
     }
-    // ---- entering columns q+M .. q+M+DC_NB-1 into the panel's slots
-    for (int e = tid; e < DC_NB * Mr; e += nth) {
-      const int t = e / Mr, k = e % Mr;
+    // ---- entering columns q+M .. q+M+DC_NB-1 into the panel's slots: warp t
+    // zeroes slot column t with 16-byte stores, then writes its three entries
+    // (diagonal, A(c+1, c), A(c+b, c))
+    {
+      const int t = tid >> 5, lane = tid & 31;
       int s_ = sq + t;
       if (s_ >= M) s_ -= M;
-      S[s_ * Mr + k] = column_value(q + M + t, k, stg[t], stg[DC_NB + t], stg[2 * DC_NB + t]);
+      TF* col = S + s_ * Mr;
+      const int nvec = Mr * int(sizeof(TF)) / 16;
+      for (int v = lane; v < nvec; v += 32) reinterpret_cast<uint4*>(col)[v] = make_uint4(0u, 0u, 0u, 0u);
+      __syncwarp();
+      if (lane < 3) {
+        const int c = q + M + t, r0 = c % Mr;
+        int k = r0 + (lane == 0 ? 0 : (lane == 1 ? 1 : b));
+        if (k >= Mr) k -= Mr;
+        // b = 1 makes lanes 1 and 2 write the same entry, the same value
+        col[k] = stg[lane * DC_NB + t];
+      }
     }
     sq = sqn;
     rq = rqn;
