@@ -121,9 +121,11 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
 //     and Ud[p][r'] = l d (r' = row - q - DC_NB, zero outside the band).
 //     Three barriers per block.
 //   trailing: the b x b lower triangle of columns q+DC_NB .. takes the
-//     rank-DC_NB update A(r, c) -= sum_p Ud[p][r'] U[p][c'], one 4 x 4 register
-//     tile per thread and pass (host-built tile list, column-major, so the lanes
-//     of a warp share the U operand and read contiguous rows of one column);
+//     rank-DC_NB update A(r, c) -= sum_p Ud[p][r'] U[p][c'], one register tile
+//     of 4 rows x TC columns per thread and pass (host-built tile list,
+//     column-major, so the lanes of a warp share the U operand and read
+//     contiguous rows of one column; TC = 8 covers b = 101 in one pass of 182
+//     tiles over the 256 threads, where 4 x 4 tiles take two, the second with 95);
 //   the DC_NB columns entering the window (original entries: diagonal,
 //     A(c+1, c), A(c+b, c), fetched during the panel by the last DC_NB threads)
 //     take the panel's slots.
@@ -136,7 +138,7 @@ constexpr int DC_FACTOR_THREADS = 256;
 static_assert(DC_FACTOR_THREADS == 32 * DC_NB, "one warp per entering column");
 
 struct DcFactorShape {
-  int M, Mr, BP, ntiles;
+  int M, Mr, BP, BPU, ntiles;
 };
 
 __host__ __device__ inline DcFactorShape dc_factor_shape(int b) {
@@ -144,6 +146,7 @@ __host__ __device__ inline DcFactorShape dc_factor_shape(int b) {
   f.M = b + DC_NB;
   f.Mr = (b + 1 + 3) / 4 * 4;
   f.BP = (b + 3) / 4 * 4;
+  f.BPU = (f.BP + 7) / 8 * 8;  // row stride of U, Ud: whole 8-column tiles
   const int nt = f.BP / 4;
   f.ntiles = nt * (nt + 1) / 2;
   return f;
@@ -152,7 +155,7 @@ __host__ __device__ inline DcFactorShape dc_factor_shape(int b) {
 template <class TF>
 __host__ __device__ inline size_t dc_factor_smem(int b) {
   const DcFactorShape f = dc_factor_shape(b);
-  return (size_t(f.M) * f.Mr + 2 * size_t(DC_NB) * f.BP + DC_NB * DC_NB + 5 * DC_NB) * sizeof(TF) +
+  return (size_t(f.M) * f.Mr + 2 * size_t(DC_NB) * f.BPU + DC_NB * DC_NB + 5 * DC_NB) * sizeof(TF) +
          size_t(f.ntiles) * sizeof(unsigned);
 }
 
@@ -172,20 +175,21 @@ __device__ __forceinline__ void dc_st4(float* p, const float v[4]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-template <class TF>
-__global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G, const double* ox, const double* oz,
+template <class TF, int TC>
+__global__ void __launch_bounds__(DC_FACTOR_THREADS, 2) k_dc_factor(const DcGrid G, const double* ox, const double* oz,
                                                                  const double* dbase, const double* sig,
                                                                  const double* alpha, const double* ky2,
-                                                                 const unsigned* tiles, int sys0, TF* fac,
+                                                                 const unsigned* tiles, int ntiles, int sys0, TF* fac,
                                                                  int* status) {
   extern __shared__ __align__(16) unsigned char shraw[];
   const int N = G.N, b = G.b, wp = G.wp;
   const DcFactorShape fs = dc_factor_shape(b);
-  const int M = fs.M, Mr = fs.Mr, BP = fs.BP;
+  static_assert(TC == 4 || TC == 8, "trailing tiles of 4 rows x 4 or 8 columns");
+  const int M = fs.M, Mr = fs.Mr, BP = fs.BP, BPU = fs.BPU;
   TF* S = reinterpret_cast<TF*>(shraw);
-  TF* U = S + size_t(M) * Mr;  // [DC_NB][BP]
-  TF* Ud = U + DC_NB * BP;     // [DC_NB][BP]
-  TF* pd = Ud + DC_NB * BP;    // pivots d of the block
+  TF* U = S + size_t(M) * Mr;  // [DC_NB][BPU]
+  TF* Ud = U + DC_NB * BPU;    // [DC_NB][BPU]
+  TF* pd = Ud + DC_NB * BPU;   // pivots d of the block
   TF* pdinv = pd + DC_NB;      // 1 / d
   TF* pl = pdinv + DC_NB;      // [DC_NB][DC_NB]: l of the panel's own rows, pl[p][c] = L(q+c, q+p)
   TF* stg = pl + DC_NB * DC_NB;  // [3][DC_NB]: entering columns' diagonal, A(c+1, c), A(c+b, c)
@@ -212,7 +216,9 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
     if (rb >= Mr) rb -= Mr;
     return k == r0 ? dg : (k == r1 ? s1 : (k == rb ? s2 : TF(0)));
   };
-  for (int e = tid; e < fs.ntiles; e += nth) tab[e] = tiles[e];
+  // ntiles (the host list's length, at most fs.ntiles, the 4 x 4 count that
+  // sizes tab) tiles of 4 rows x TC columns
+  for (int e = tid; e < ntiles; e += nth) tab[e] = tiles[e];
   for (int e = tid; e < M * Mr; e += nth) {  // columns 0 .. M-1
     const int c = e / Mr, k = e % Mr;
     TF dg, s1, s2;
@@ -275,8 +281,8 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
         const int c0 = q + p, i = tid - p;
         if (c0 < N && i >= 1 && i <= b) F[size_t(c0) * wp + i] = (q + tid < N) ? a[p] : TF(0);
         if (tid >= DC_NB) {
-          U[p * BP + tid - DC_NB] = a[p];
-          Ud[p * BP + tid - DC_NB] = a[p] * pd[p];
+          U[p * BPU + tid - DC_NB] = a[p];
+          Ud[p * BPU + tid - DC_NB] = a[p] * pd[p];
         }
       }
     }
@@ -289,39 +295,40 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS) k_dc_factor(const DcGrid G,
     // ---- trailing rank-DC_NB update
     int sqn = sq + DC_NB, rqn = (rq + DC_NB) % Mr;
     if (sqn >= M) sqn -= M;
-    for (int e = tid; e < fs.ntiles; e += nth) {
+    for (int e = tid; e < ntiles; e += nth) {
       const unsigned tv = tab[e];
       const int rt = int(tv & 0xffffu), ct = int(tv >> 16);
       int rbase = rqn + 4 * rt;
       if (rbase >= Mr) rbase -= Mr;
-      TF acc[4][4];
-      int sc[4];
+      TF acc[TC][4];
+      int sc[TC];
 #pragma unroll
-      for (int kc = 0; kc < 4; ++kc) {
-        int s_ = sqn + 4 * ct + kc;
+      for (int kc = 0; kc < TC; ++kc) {
+        int s_ = sqn + TC * ct + kc;  // TC * ct + kc < BPU <= M
         if (s_ >= M) s_ -= M;
         sc[kc] = s_;
         dc_ld4(S + s_ * Mr + rbase, acc[kc]);
       }
 #pragma unroll
       for (int p = 0; p < DC_NB; ++p) {
-        TF av[4], bv[4];
-        dc_ld4(Ud + p * BP + 4 * rt, av);
-        dc_ld4(U + p * BP + 4 * ct, bv);
+        TF av[4], bv[TC];
+        dc_ld4(Ud + p * BPU + 4 * rt, av);
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc)
+        for (int h = 0; h < TC / 4; ++h) dc_ld4(U + p * BPU + TC * ct + 4 * h, bv + 4 * h);
+#pragma unroll
+        for (int kc = 0; kc < TC; ++kc)
 #pragma unroll
           for (int kr = 0; kr < 4; ++kr) acc[kc][kr] -= av[kr] * bv[kc];
       }
-      if (rt > ct && 4 * rt + 3 < b) {
+      if (4 * rt > TC * ct + TC - 1 && 4 * rt + 3 < b) {  // strictly below the diagonal, inside the band
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc) dc_st4(S + sc[kc] * Mr + rbase, acc[kc]);
+        for (int kc = 0; kc < TC; ++kc) dc_st4(S + sc[kc] * Mr + rbase, acc[kc]);
       } else {
 #pragma unroll
-        for (int kc = 0; kc < 4; ++kc)
+        for (int kc = 0; kc < TC; ++kc)
 #pragma unroll
           for (int kr = 0; kr < 4; ++kr) {
-            const int rp = 4 * rt + kr, cp = 4 * ct + kc;
+            const int rp = 4 * rt + kr, cp = TC * ct + kc;
             if (rp >= cp && rp < b) S[sc[kc] * Mr + rbase + kr] = acc[kc][kr];
           }
       }

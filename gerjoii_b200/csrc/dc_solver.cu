@@ -19,6 +19,12 @@
 
 namespace gj {
 
+// Columns of the factor's trailing-update register tiles (4 rows x 8 columns
+// by default; GJ_DC_TILE=4 selects 4 x 4).
+static int dc_tile_cols() {
+  const char* e = getenv("GJ_DC_TILE");
+  return (e && atoi(e) == 4) ? 4 : 8;
+}
 // Shape of the substitution's shared-memory ring: chunks of `ch` factor
 // columns, `nst` chunks (8 x 4 by default; GJ_DC_RING=CHxNST picks 4x4, 4x8,
 // 8x4 or 16x4).
@@ -105,6 +111,7 @@ struct DcPlan {
   int nky = 0, nsrc = 0, robin = 0;
   DevBuf sig, faces, ky2, wts, alpha, ab, cur, mnoff, mnbuf, dots, done, status, gbuf, dbuf, ebuf, ubuf;
   DevBuf tiles;  // the factor's trailing-update tiles, (ct << 16) | rt, column-major
+  int ntiles = 0;
   std::vector<long> off;
 };
 
@@ -304,17 +311,23 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
   int it_max = 0;
   double rel_max = 0;
   const size_t smem_f = dc_factor_smem<TF>(G.b);
-  GJ_CUDA(err, cudaFuncSetAttribute(k_dc_factor<TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
+  const int tc = dc_tile_cols();
+  const auto kfac = tc == 8 ? k_dc_factor<TF, 8> : k_dc_factor<TF, 4>;
+  GJ_CUDA(err, cudaFuncSetAttribute(kfac, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f)));
   {
     const DcRing ring = dc_ring();
     GJ_CUDA(err, cudaFuncSetAttribute(dc_precond_kernel<TF>(G.b, ring), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(dc_precond_smem<TF>(G.wp, ring.ch, ring.nst))));
   }
   {
-    const int nt = dc_factor_shape(G.b).BP / 4;
+    // tiles of 4 rows x tc columns on or below the diagonal, column-major
+    const DcFactorShape fs = dc_factor_shape(G.b);
+    const int nt = fs.BP / 4, nct = (tc == 8 ? fs.BPU : fs.BP) / tc;
     std::vector<unsigned> ht;
-    for (int ct = 0; ct < nt; ++ct)
-      for (int rt = ct; rt < nt; ++rt) ht.push_back((unsigned(ct) << 16) | unsigned(rt));
+    for (int ct = 0; ct < nct; ++ct)
+      for (int rt = tc * ct / 4; rt < nt; ++rt) ht.push_back((unsigned(ct) << 16) | unsigned(rt));
+    if (ht.size() > size_t(fs.ntiles)) return err.set(GJ_EINVAL, "factor tile list longer than its shared-memory table");
+    P.ntiles = int(ht.size());
     GJ_TRY(P.tiles.alloc(err, ht.size() * sizeof(unsigned)));
     GJ_CUDA(err, cudaMemcpy(P.tiles.p, ht.data(), ht.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
   }
@@ -335,10 +348,10 @@ static gj_status dc_run_t(Ctx& c, const gj_dc_grid& gg, const double* sigma, con
                                            P.ky2.as<double>(), sys0, nsys, c.dc_fac.as<float>(),
                                            P.status.as<int>());
       } else {
-        k_dc_factor<TF><<<nsys, DC_FACTOR_THREADS, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(),
-                                                                 P.alpha.as<double>(), P.ky2.as<double>(),
-                                                                 P.tiles.as<unsigned>(), sys0, c.dc_fac.as<TF>(),
-                                                                 P.status.as<int>());
+        kfac<<<nsys, DC_FACTOR_THREADS, smem_f, st>>>(G, ox, ox + N, ox + 2 * N, P.sig.as<double>(),
+                                                      P.alpha.as<double>(), P.ky2.as<double>(),
+                                                      P.tiles.as<unsigned>(), P.ntiles, sys0, c.dc_fac.as<TF>(),
+                                                      P.status.as<int>());
       }
       c.timer.end(tm, st);
       ++c.launches;
