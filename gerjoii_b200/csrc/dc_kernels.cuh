@@ -174,6 +174,13 @@ __device__ __forceinline__ void dc_st4(double* p, const double v[4]) {
 __device__ __forceinline__ void dc_st4(float* p, const float v[4]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
+// 16 bytes of entries to a 16-byte aligned address
+__device__ __forceinline__ void dc_st16(double* p, const double (&v)[2]) {
+  *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+}
+__device__ __forceinline__ void dc_st16(float* p, const float (&v)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
 
 template <class TF, int TC>
 __global__ void __launch_bounds__(DC_FACTOR_THREADS, 2) k_dc_factor(const DcGrid G, const double* ox, const double* oz,
@@ -275,23 +282,43 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS, 2) k_dc_factor(const DcGrid
         a[p] = l;
       }
     }
-    if (row) {  // a[p] = l of row q+t for pivot q+p
+    if (row && tid >= DC_NB) {  // a[p] = l of row q+t for pivot q+p, rows below the panel
 #pragma unroll
       for (int p = 0; p < DC_NB; ++p) {
-        const int c0 = q + p, i = tid - p;
-        if (c0 < N && i >= 1 && i <= b) F[size_t(c0) * wp + i] = (q + tid < N) ? a[p] : TF(0);
-        if (tid >= DC_NB) {
-          U[p * BPU + tid - DC_NB] = a[p];
-          Ud[p * BPU + tid - DC_NB] = a[p] * pd[p];
-        }
+        U[p * BPU + tid - DC_NB] = a[p];
+        Ud[p * BPU + tid - DC_NB] = a[p] * pd[p];
       }
     }
     if (tid < DC_NB && q + tid < N) {
       const TF d = pd[tid];
-      F[size_t(q + tid) * wp] = pdinv[tid];
       if (!(d != TF(0)) || !isfinite(d)) atomicExch(status + sys0 + sys, 1);
     }
     __syncthreads();
+    // ---- factor columns q .. q+DC_NB-1: warp p writes column q+p,
+    // [1 / d, l_{q+p+1,q+p} .. l_{q+p+b,q+p}] (0 for rows at or past N and in
+    // the padding past b), 16 bytes per lane, from the published pivots, the
+    // panel rows' l (pl) and the rows below the panel (U); the stores overlap
+    // the trailing update.  wp is a multiple of the entries per store, so the
+    // last store of a column ends inside it.
+    {
+      const int p = tid >> 5, lane = tid & 31;
+      const int c0 = q + p;
+      if (c0 < N) {
+        TF* Fc = F + size_t(c0) * wp;
+        constexpr int EV = 16 / int(sizeof(TF));
+        for (int v = lane; v * EV <= b; v += 32) {
+          TF e[EV];
+#pragma unroll
+          for (int u = 0; u < EV; ++u) {
+            const int i = v * EV + u;
+            e[u] = i == 0 ? pdinv[p]
+                 : (i > b || c0 + i >= N) ? TF(0)
+                 : (i < DC_NB - p ? pl[p * DC_NB + p + i] : U[p * BPU + i + p - DC_NB]);
+          }
+          dc_st16(Fc + v * EV, e);
+        }
+      }
+    }
     // ---- trailing rank-DC_NB update
     int sqn = sq + DC_NB, rqn = (rq + DC_NB) % Mr;
     if (sqn >= M) sqn -= M;
