@@ -124,8 +124,8 @@ __device__ __forceinline__ void dc_lh(const DcGrid& G, int q, int& l, int& h) {
 //     rank-DC_NB update A(r, c) -= sum_p Ud[p][r'] U[p][c'], one register tile
 //     of 4 rows x TC columns per thread and pass (host-built tile list,
 //     column-major, so the lanes of a warp share the U operand and read
-//     contiguous rows of one column; TC = 8 covers b = 101 in one pass of 182
-//     tiles over the 256 threads, where 4 x 4 tiles take two, the second with 95);
+//     contiguous rows of one column); TC = 4 by default (351 tiles, two passes
+//     at b = 101), TC = 8 covers b = 101 in one pass of 182 tiles but spills;
 //   the DC_NB columns entering the window (original entries: diagonal,
 //     A(c+1, c), A(c+b, c), fetched during the panel by the last DC_NB threads)
 //     take the panel's slots.
@@ -174,6 +174,20 @@ __device__ __forceinline__ void dc_st4(double* p, const double v[4]) {
 __device__ __forceinline__ void dc_st4(float* p, const float v[4]) {
   *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
 }
+// Four entries at p in the order (2h, 2h+1, 2-2h, 3-2h), h = 0 or 1: two
+// 16-byte halves, the one at p + 2h first (FP64); FP32 entries are one
+// 16-byte vector and h = 0.
+__device__ __forceinline__ void dc_ld4h(const double* p, int h, double v[4]) {
+  const double2 a = *reinterpret_cast<const double2*>(p + 2 * h);
+  const double2 c = *reinterpret_cast<const double2*>(p + 2 - 2 * h);
+  v[0] = a.x; v[1] = a.y; v[2] = c.x; v[3] = c.y;
+}
+__device__ __forceinline__ void dc_ld4h(const float* p, int, float v[4]) { dc_ld4(p, v); }
+__device__ __forceinline__ void dc_st4h(double* p, int h, const double v[4]) {
+  *reinterpret_cast<double2*>(p + 2 * h) = make_double2(v[0], v[1]);
+  *reinterpret_cast<double2*>(p + 2 - 2 * h) = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void dc_st4h(float* p, int, const float v[4]) { dc_st4(p, v); }
 // 16 bytes of entries to a 16-byte aligned address
 __device__ __forceinline__ void dc_st16(double* p, const double (&v)[2]) {
   *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
@@ -319,7 +333,15 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS, 2) k_dc_factor(const DcGrid
         }
       }
     }
-    // ---- trailing rank-DC_NB update
+    // ---- trailing rank-DC_NB update.  A lane's 4 rows are 32 bytes (FP64),
+    // and the lanes of a warp hold consecutive row blocks of one column, so a
+    // 16-byte load of the same half by every lane spans 1 KB with every
+    // second 16 bytes unused (two shared wavefronts per 128 bytes).  Lanes
+    // with bit 2 set take their second half first (rows 2, 3, 0, 1): each 8
+    // lanes then cover all 32 banks once.  The lane keeps that row order for
+    // its accumulators, the Ud rows and the stores, so nothing moves between
+    // lanes.  FP32 rows are 16 bytes, contiguous across lanes already.
+    const int hs = sizeof(TF) == 8 ? (tid >> 2) & 1 : 0;  // row pair first in this lane's order
     int sqn = sq + DC_NB, rqn = (rq + DC_NB) % Mr;
     if (sqn >= M) sqn -= M;
     for (int e = tid; e < ntiles; e += nth) {
@@ -334,12 +356,12 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS, 2) k_dc_factor(const DcGrid
         int s_ = sqn + TC * ct + kc;  // TC * ct + kc < BPU <= M
         if (s_ >= M) s_ -= M;
         sc[kc] = s_;
-        dc_ld4(S + s_ * Mr + rbase, acc[kc]);
+        dc_ld4h(S + s_ * Mr + rbase, hs, acc[kc]);
       }
 #pragma unroll
       for (int p = 0; p < DC_NB; ++p) {
         TF av[4], bv[TC];
-        dc_ld4(Ud + p * BPU + 4 * rt, av);
+        dc_ld4h(Ud + p * BPU + 4 * rt, hs, av);
 #pragma unroll
         for (int h = 0; h < TC / 4; ++h) dc_ld4(U + p * BPU + TC * ct + 4 * h, bv + 4 * h);
 #pragma unroll
@@ -349,14 +371,15 @@ __global__ void __launch_bounds__(DC_FACTOR_THREADS, 2) k_dc_factor(const DcGrid
       }
       if (4 * rt > TC * ct + TC - 1 && 4 * rt + 3 < b) {  // strictly below the diagonal, inside the band
 #pragma unroll
-        for (int kc = 0; kc < TC; ++kc) dc_st4(S + sc[kc] * Mr + rbase, acc[kc]);
+        for (int kc = 0; kc < TC; ++kc) dc_st4h(S + sc[kc] * Mr + rbase, hs, acc[kc]);
       } else {
 #pragma unroll
         for (int kc = 0; kc < TC; ++kc)
 #pragma unroll
           for (int kr = 0; kr < 4; ++kr) {
-            const int rp = 4 * rt + kr, cp = TC * ct + kc;
-            if (rp >= cp && rp < b) S[sc[kc] * Mr + rbase + kr] = acc[kc][kr];
+            const int rr = kr ^ (2 * hs);  // the row of slot kr
+            const int rp = 4 * rt + rr, cp = TC * ct + kc;
+            if (rp >= cp && rp < b) S[sc[kc] * Mr + rbase + rr] = acc[kc][kr];
           }
       }
     }

@@ -19,11 +19,11 @@
 
 namespace gj {
 
-// Columns of the factor's trailing-update register tiles (4 rows x 8 columns
-// by default; GJ_DC_TILE=4 selects 4 x 4).
+// Columns of the factor's trailing-update register tiles (4 rows x 4 columns
+// by default; GJ_DC_TILE=8 selects 4 x 8, which spills at 128 registers).
 static int dc_tile_cols() {
   const char* e = getenv("GJ_DC_TILE");
-  return (e && atoi(e) == 4) ? 4 : 8;
+  return (e && atoi(e) == 8) ? 8 : 4;
 }
 // Shape of the substitution's shared-memory ring: chunks of `ch` factor
 // columns, `nst` chunks (8 x 4 by default; GJ_DC_RING=CHxNST picks 4x4, 4x8,

@@ -6,6 +6,7 @@ from conftest import rel_l2
 from dc_cases import small_dc, oracle_alphas, oracle_forward
 from gerjoii_b200 import _native as N
 from gerjoii_b200 import dc
+from gerjoii_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
@@ -203,3 +204,22 @@ def test_context_release_frees_cached_buffers_and_keeps_working(gpu_ctx):
     r2 = gpu_ctx.dc_forward(case["SIG"], case["DX"], case["DZ"], case["robin"], case["srcs"])
     for a, b in zip(r1["d"], r2["d"]):
         assert rel_l2(a, b) < 1e-12
+
+
+@pytest.mark.parametrize("env", [{"GJ_DC_TILE": "8"}, {"GJ_DC_RING": "16x4"}, {"GJ_DC_RING": "4x8"}],
+                         ids=["tile8", "ring16x4", "ring4x8"])
+def test_dc_kernel_variants_match_default(gpu_ctx, env):
+    """The factor's 4 x 8 trailing tiles and the substitution's other ring
+    shapes (chosen per call through the environment) give the default's data."""
+    import os
+    c = synth.cfg5(n_sources=3, n_ky=4)
+    ref = gpu_ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], c["srcs"])
+    os.environ.update(env)
+    try:
+        alt = gpu_ctx.dc_forward(c["SIG"], c["DX"], c["DZ"], c["robin"], c["srcs"])
+    finally:
+        for k in env:
+            del os.environ[k]
+    for a, b in zip(alt["d"], ref["d"]):
+        assert np.allclose(a, b, rtol=1e-9, atol=0)
+    assert alt["rel_residual"] <= 1e-10

@@ -3,7 +3,9 @@ grid (dx = 0.02 m, 30 PML cells, 8000 steps, 250 MHz).  The FP32 exact
 gradient, computed with checkpoints and segment recompute, is compared with
 the FP64 exact gradient (rel-L2 <= 1e-4, cosine >= 0.9999), the FP64 exact
 gradient with central differences of FP64 forward models at 20 seeded cells
-(h = 1e-3 relative), and the envelope (env_L2) variant is run as well."""
+(h = 1e-3 relative); the reference-semantics adjoint the same way (FP32
+checkpointed vs FP64, rel-L2 <= 1e-4 for both gradients), and the envelope
+(env_L2) variant is run as well."""
 import numpy as np
 import pytest
 
@@ -62,8 +64,9 @@ def test_cfg3_reference_adjoint_and_envelope_variant(gpu_ctx, cfg3_case):
     o.ckpt_every = 90
     ref32 = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_REFERENCE, precision=N.GJ_F32, opts=o)
     ref64 = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_REFERENCE, precision=N.GJ_F64)
-    assert rel_l2(ref32["g_sig"], ref64["g_sig"]) <= 1e-4
-    assert cosine(ref32["g_eps"], ref64["g_eps"]) >= 0.9999
+    for key in ("g_eps", "g_sig"):
+        assert rel_l2(ref32[key], ref64[key]) <= 1e-4, key  # measured 3.2e-5 for both
+        assert cosine(ref32[key], ref64[key]) >= 0.9999, key
     env = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, misfit=N.GJ_MISFIT_ENV_L2,
                              precision=N.GJ_F32, opts=o)
     assert np.isfinite(env["g_eps"]).all() and np.abs(env["g_eps"]).max() > 0
