@@ -193,3 +193,34 @@ def test_kernel_timing_counts_runs(gpu_ctx, oracle, tall):
         assert 0 < kt[k]["sampled"] <= kt[k]["launches"]
         assert 0 < kt[k]["avg_us"] < 1e3 * wall_ms / g.nt
     assert kt["image"]["launches"] >= 1
+
+
+@pytest.mark.parametrize("env", [
+    {"GJ_AUTOTUNE": "0"},
+    {"GJ_RING_CTA_WARPS": "4", "GJ_RING_STAGES": "3", "GJ_RING_STAGES_FAST": "4", "GJ_RING_TJF": "16",
+     "GJ_RING_TJS": "4"},
+    {"GJ_NO_SPLIT": "1", "GJ_SIDE_PRIORITY": "0"},
+], ids=["defaults", "fixed", "no_split_no_priority"])
+def test_ring_configurations_from_the_environment(gpu_ctx, oracle, tall, env):
+    """Plans made with the tuner off, with a fixed ring configuration, or with
+    split tasks and the priority stream off give the tuned plan's FP64
+    gradient.  The column chunks decide where a task recomputes its first Hx
+    column (a different rounding), which the eps imaging's cancellation turns
+    into about 1e-10 on this grid, as against the oracle."""
+    p = tall
+    g = p.grid
+    dobs = _dobs(oracle, p)
+    ref = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+    os.environ.update(env)
+    try:
+        ctx2 = N.Context(0)
+        try:
+            alt = ctx2.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+        finally:
+            ctx2.close()
+    finally:
+        for k in env:
+            del os.environ[k]
+    assert rel_l2(alt["g_eps"], ref["g_eps"]) < 1e-9
+    assert rel_l2(alt["g_sig"], ref["g_sig"]) < 1e-9
+    assert np.allclose(alt["misfit"], ref["misfit"], rtol=1e-12)
