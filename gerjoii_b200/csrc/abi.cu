@@ -53,6 +53,7 @@ gj_status gj_context_release(gj_ctx* ctx) {
   cudaDeviceSynchronize();
   ctx->c.wsolver.reset();
   ctx->c.wkey.clear();
+  ctx->c.wbatch.reset();
   ctx->c.dc_fac.release();
   ctx->c.dc_vec.release();
   return GJ_OK;

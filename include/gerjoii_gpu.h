@@ -110,8 +110,9 @@ typedef struct gj_w_opts {
 gj_status gj_context_create(gj_ctx** ctx, int device);
 gj_status gj_context_destroy(gj_ctx* ctx);
 /* Frees the device memory a context keeps between calls (the cached radar plan
- * with its history, checkpoints and graphs, and the DC band factors and CG
- * vectors, tens of GB for a large survey) and keeps the context usable; the
+ * with its history, checkpoints and graphs, the batch plans with their pool and
+ * graph, and the DC band factors and CG vectors, tens of GB for a large survey)
+ * and keeps the context usable; the
  * next call plans and allocates again.  No counterpart in the reference
  * (MATLAB's clear / reset between phases of an inversion). */
 gj_status gj_context_release(gj_ctx* ctx);

@@ -81,3 +81,20 @@ def test_batch_rejects_unsupported_options(gpu_ctx, problems):
     with pytest.raises(N.GJError) as ei:
         gpu_ctx.w_gradient_batch(probs, opts=o)
     assert ei.value.status == N.GJ_EUNSUPPORTED
+
+
+def test_release_frees_the_batch_pool(gpu_ctx, problems):
+    """gj_context_release gives the batch's pool and graph back; the next batch
+    call plans again and returns the same gradients."""
+    import torch
+    probs = [(p.grid, p.eps0, p.sig0, p.shots, d) for p, d in problems]
+    r1, _ = gpu_ctx.w_gradient_batch(probs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    gpu_ctx.release()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 > free0
+    r2, _ = gpu_ctx.w_gradient_batch(probs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+    for a, b in zip(r1, r2):
+        assert rel_l2(a["g_eps"], b["g_eps"]) < 1e-12
+        assert rel_l2(a["g_sig"], b["g_sig"]) < 1e-12
