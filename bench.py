@@ -15,7 +15,9 @@ edge cells, and returns the epsilon and sigma gradients.
 The timed region runs with kernel timing off; the per-kernel figures and the
 roofline come from one more step run afterwards with sampled CUDA events on.
 A cfg3 leg times the checkpointed single-shot gradient on the 2000 x 800 grid
-(8000 steps, checkpoints every 90 steps).
+(8000 steps, checkpoints every 90 steps), a cfg4 leg the 48 uneven problems in
+one gj_w_gradient_batch call (--no-cfg4 skips it; --cfg4 prints it as a line of
+its own), and a dc leg the 2.5D DC survey (--no-dc).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -55,6 +57,7 @@ def parse():
     ap.add_argument("--mode", default="exact", choices=["exact", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip the e2e, plain-FP64, DC and CPU legs")
     ap.add_argument("--no-dc", action="store_true", help="skip the DC leg")
+    ap.add_argument("--no-cfg4", action="store_true", help="skip the 48-problem batch leg")
     ap.add_argument("--dc-only", action="store_true", help="only the DC leg (JSON line of its own)")
     ap.add_argument("--dc-sources", type=int, default=200, help="DC sources (x 20 wavenumbers)")
     ap.add_argument("--cfg4", action="store_true",
@@ -402,19 +405,23 @@ def cfg3_leg(ctx):
             "kernels": per}
 
 
-def cfg4_leg(args):
+def cfg4_leg(ctx=None):
     """cfg4: 48 uneven problems (grids 256..1536 x 128..512, dx 0.02..0.05 m,
     1500..5000 steps, 4..24 shots; blob / layer models), FP32 exact gradients
     with Kahan sums, all of them in one gj_w_gradient_batch call: the problems
     run concurrently in memory-budgeted waves, all waves one CUDA graph launch.
     Timed: one call after a warm-up call (which plans, tunes and captures the
     graph).  Baseline: the plain per-shot FP64 form on one shot of
-    every 12th problem, compared per cell-update."""
+    every 12th problem, compared per cell-update.  Returns the figures as a
+    dict (the bench line's "cfg4" key, or a line of its own with --cfg4)."""
     import torch
     from gerjoii_b200 import synth
     from gerjoii_b200 import _native as N
     probs = synth.cfg4_problems()
-    ctx = N.Context(0)
+    own = ctx is None
+    if own:
+        ctx = N.Context(0)
+    ctx.release()  # the caller's cached plans give their memory back
     data = []
     for p in probs:
         d = ctx.w_forward(p.grid, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F32)["d"]
@@ -450,17 +457,28 @@ def cfg4_leg(args):
         torch.cuda.synchronize()
         s_t += time.perf_counter() - t0
         s_upd += 2 * p.grid.nt * p.grid.NX * p.grid.NY
-    line = {"metric": "cfg4: 48 uneven radar gradients, shot-gradients/s & Gcell-upd/s, 1 B200", "value": shots / t,
-            "unit": "shot-gradients/s", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": t * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded blob / layer models, observed traces modelled on the device)",
-            "config": {"workload": "48 uneven problems (cfg4), one gj_w_gradient_batch call, exact adjoint, FP32",
-                       "problems": len(probs), "shots": shots, "cell_updates": upd, "waves": nwaves,
-                       "first_call_s": t_first},
-            "gcell_updates_per_s": upd / t / 1e9, "gpu_launches": launches, "clocks": clk,
+    ctx.release()
+    if own:
+        ctx.close()
+    return {"workload": "48 uneven problems (cfg4), one gj_w_gradient_batch call, exact adjoint, FP32",
+            "shot_gradients_per_s": shots / t, "ms_per_call": t * 1e3, "gcell_updates_per_s": upd / t / 1e9,
+            "problems": len(probs), "shots": shots, "cell_updates": upd, "waves": nwaves,
+            "graph_launches_per_call": 1, "gpu_launches": launches, "first_call_s": t_first, "clocks": clk,
             "plain_fp64_sample": {"gcell_updates_per_s": s_upd / s_t / 1e9,
                                   "sample": "1 shot of problems 0, 12, 24, 36, plain per-shot FP64 form",
                                   "speedup_fp32_over_plain_fp64": (upd / t) / (s_upd / s_t)}}
+
+
+def cfg4_line():
+    r = cfg4_leg()
+    line = {"metric": "cfg4: 48 uneven radar gradients, shot-gradients/s & Gcell-upd/s, 1 B200",
+            "value": r["shot_gradients_per_s"], "unit": "shot-gradients/s", "n_gpus": 1, "steps": 1, "warmup": 1,
+            "ms_per_step": r["ms_per_call"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded blob / layer models, observed traces modelled on the device)",
+            "config": {"workload": r["workload"], "problems": r["problems"], "shots": r["shots"],
+                       "cell_updates": r["cell_updates"], "waves": r["waves"], "first_call_s": r["first_call_s"]},
+            "gcell_updates_per_s": r["gcell_updates_per_s"], "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+            "plain_fp64_sample": r["plain_fp64_sample"]}
     print(json.dumps(line), flush=True)
 
 
@@ -497,7 +515,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.cfg4:
-        return cfg4_leg(args)
+        return cfg4_line()
     if args.dc_only:
         from gerjoii_b200 import _native as N
         ctx = N.Context(0)
@@ -721,6 +739,8 @@ def main():
         if not args.no_dc:
             line["dc"] = dc_leg(ctx)
         line["cfg3"] = cfg3_leg(ctx)
+        if not args.no_cfg4:
+            line["cfg4"] = cfg4_leg(ctx)
         # CPU baseline (oracle) on the host cores, bounded sample
         threads = min(os.cpu_count() or 1, 32)
         nt_s = max(50, min(args.nt, 150))
