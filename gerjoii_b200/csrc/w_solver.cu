@@ -1586,11 +1586,11 @@ class WSolver : public WSolverBase {
     }
     return GJ_OK;
   }
-  // Pool bytes plan_buffers carves with all shots in one group and
-  // checkpoint interval Kc (Kc >= nt: the whole history kept).
-  size_t pool_need(int Kc, bool exact) const {
+  // Pool bytes plan_buffers carves with groups of `shots` shots (0: all in
+  // one group) and checkpoint interval Kc (Kc >= nt: the whole history kept).
+  size_t pool_need(int Kc, bool exact, int shots = 0) const {
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t Gs = size_t(nshots), sz = sizeof(T), bs = exact ? size_t(w.bsz) : 0;
+    const size_t Gs = size_t(shots > 0 ? shots : nshots), sz = sizeof(T), bs = exact ? size_t(w.bsz) : 0;
     const bool full = Kc >= g.nt;
     const size_t nseg = full ? 0 : size_t((g.nt + Kc - 1) / Kc);
     const size_t slots = full ? size_t(g.nt + 1) : size_t(Kc + 4);
@@ -2012,6 +2012,7 @@ struct WBatch : WBatchBase {
   std::vector<std::string> keys;
   std::vector<std::unique_ptr<WSolver<T>>> plans;
   std::vector<int> kc;  // checkpoint interval per problem (nt: whole history)
+  std::vector<int> gs;  // shots per group per problem (0: all shots in one launch)
   DevBuf pool;
   std::vector<std::vector<int>> waves;
   cudaGraphExec_t exec = nullptr;  // every wave, one after the other, in one graph
@@ -2079,13 +2080,34 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
     GJ_CUDA(err, cudaMemGetInfo(&free_b, &total_b));
     const size_t avail = free_b > owned ? free_b - owned : 0;
     const size_t budget = o0.mem_budget_bytes ? o0.mem_budget_bytes : size_t(0.8 * double(avail));
-    std::vector<size_t> nmin(np), nfull(np);
+    // Per problem, one of: (a) all shots in one launch, checkpointed (pool
+    // nmin; the cheapest in memory, one recompute pass), upgraded to the whole
+    // history when its wave has room; (b) the whole history in shot groups of
+    // gs shots run one after the other (no recompute pass), for a problem whose
+    // whole history takes more than a quarter of the budget, when groups of at
+    // least 4 shots (or all) fit it.
+    std::vector<size_t> nmin(np), nfull(np), need(np);
     std::vector<int> kmin(np);
+    B->gs.assign(np, 0);
     for (int p = 0; p < np; ++p) {
-      kmin[p] = B->plans[p]->best_k(exact);
-      nmin[p] = B->plans[p]->pool_need(kmin[p], exact);
-      nfull[p] = B->plans[p]->pool_need(B->plans[p]->g.nt, exact);
-      if (nmin[p] > budget) return err.set(GJ_ENOMEM, "problem %d needs %zu bytes, above the budget %zu", p, nmin[p], budget);
+      const WSolver<T>& q = *B->plans[p];
+      kmin[p] = q.best_k(exact);
+      nmin[p] = q.pool_need(kmin[p], exact);
+      nfull[p] = q.pool_need(q.g.nt, exact);
+      need[p] = nmin[p];
+      if (nfull[p] > budget / 4) {
+        const int ns = q.nshots;
+        int G = 0;
+        for (int t = ns; t >= std::min(ns, 4); --t)
+          if (q.pool_need(q.g.nt, exact, t) <= budget) { G = t; break; }
+        if (G > 0) {
+          const int ng = (ns + G - 1) / G;  // balanced groups
+          G = (ns + ng - 1) / ng;
+          B->gs[p] = G;
+          need[p] = q.pool_need(q.g.nt, exact, G);
+        }
+      }
+      if (need[p] > budget) return err.set(GJ_ENOMEM, "problem %d needs %zu bytes, above the budget %zu", p, need[p], budget);
     }
     // pack by work, largest first
     std::vector<int> order(np);
@@ -2097,29 +2119,43 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
     std::vector<int> cur;
     size_t used = 0;
     for (int p : order) {
-      if (!cur.empty() && used + nmin[p] > budget) {
+      if (!cur.empty() && used + need[p] > budget) {
         B->waves.push_back(cur);
         cur.clear();
         used = 0;
       }
       cur.push_back(p);
-      used += nmin[p];
+      used += need[p];
     }
     if (!cur.empty()) B->waves.push_back(cur);
-    // spare memory of a wave: whole histories first for the cheapest upgrades,
-    // then longer checkpoint intervals for the rest
+    // spare memory of a wave: whole histories for the checkpointed problems,
+    // the cheapest upgrades first
     B->kc = kmin;
+    for (int p = 0; p < np; ++p)
+      if (B->gs[p] > 0) B->kc[p] = B->plans[p]->g.nt;
     size_t pool = 0;
     for (auto& wv : B->waves) {
       size_t u = 0;
-      for (int p : wv) u += nmin[p];
-      std::vector<int> up(wv);
+      for (int p : wv) u += need[p];
+      std::vector<int> up;
+      for (int p : wv)
+        if (B->gs[p] == 0) up.push_back(p);
       std::sort(up.begin(), up.end(), [&](int a, int b) { return nfull[a] - nmin[a] < nfull[b] - nmin[b]; });
       for (int p : up)
         if (u - nmin[p] + nfull[p] <= budget) { u += nfull[p] - nmin[p]; B->kc[p] = B->plans[p]->g.nt; }
       pool = std::max(pool, u);
     }
     GJ_TRY(B->pool.alloc(err, pool));
+    if (getenv("GJ_BATCH_VERBOSE")) {
+      for (size_t wi = 0; wi < B->waves.size(); ++wi)
+        for (int p : B->waves[wi])
+          fprintf(stderr, "gerjoii_b200 batch wave %zu problem %d: %d shots (groups of %d), %s, pool %.1f MB\n",
+                  wi, p, B->plans[p]->nshots, B->gs[p] > 0 ? B->gs[p] : B->plans[p]->nshots,
+                  B->gs[p] > 0 ? "whole history in shot groups"
+                               : (B->kc[p] >= B->plans[p]->g.nt ? "whole history" : "checkpointed"),
+                  double(B->gs[p] > 0 ? need[p] : (B->kc[p] >= B->plans[p]->g.nt ? nfull[p] : nmin[p])) / 1e6);
+      fprintf(stderr, "gerjoii_b200 batch pool %.1f MB of budget %.1f MB\n", double(pool) / 1e6, double(budget) / 1e6);
+    }
   }
   if (nwaves_out) *nwaves_out = int(B->waves.size());
   if (!B->exec) {
@@ -2137,7 +2173,7 @@ static gj_status gradient_batch_t(Ctx& c, const gj_w_problem* pr, int np, gj_adj
       for (int p : wv) {
         WSolver<T>& q = *B->plans[p];
         gj_w_opts op = o0;
-        op.shots_per_launch = q.nshots;
+        op.shots_per_launch = B->gs[p] > 0 ? B->gs[p] : q.nshots;
         op.ckpt_every = B->kc[p] >= q.g.nt ? 0 : B->kc[p];
         op.mem_budget_bytes = B->kc[p] >= q.g.nt ? size_t(-1) / 4 : 0;
         q.pool_p = cursor;

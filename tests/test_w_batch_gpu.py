@@ -98,3 +98,35 @@ def test_release_frees_the_batch_pool(gpu_ctx, problems):
     for a, b in zip(r1, r2):
         assert rel_l2(a["g_eps"], b["g_eps"]) < 1e-12
         assert rel_l2(a["g_sig"], b["g_sig"]) < 1e-12
+
+
+@pytest.fixture(scope="module")
+def grouped(oracle):
+    """One problem whose whole history is large against the pool (8 shots,
+    400 steps) beside two small ones."""
+    specs = [dict(m=40, n=60, pml=8, nt=400, nsrc=8, nrec=8, seed=61),
+             dict(m=20, n=30, pml=6, nt=200, nsrc=2, nrec=5, seed=62),
+             dict(m=24, n=28, pml=6, nt=240, nsrc=3, nrec=6, seed=63)]
+    out = []
+    for sp in specs:
+        p = synth.small(**sp)
+        dobs = [oracle.forward(p.grid, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
+        out.append((p, dobs))
+    return out
+
+
+@pytest.mark.parametrize("budget_mb", [128, 256])
+def test_batch_shot_groups_equal_single_calls(gpu_ctx, grouped, budget_mb):
+    """Pool budgets under which the 8-shot problem (whole history about 220 MB
+    in FP64) runs its whole history in two groups of 4 shots one after the other
+    (128 MB) or in one group (256 MB): every gradient equals its own
+    gj_w_gradient call (FP64)."""
+    o = N.OptsC()
+    o.mem_budget_bytes = budget_mb << 20
+    probs = [(p.grid, p.eps0, p.sig0, p.shots, d) for p, d in grouped]
+    res, _ = gpu_ctx.w_gradient_batch(probs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=o)
+    for (p, d), r in zip(grouped, res):
+        ref = gpu_ctx.w_gradient(p.grid, p.eps0, p.sig0, p.shots, d, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64)
+        assert rel_l2(r["g_eps"], ref["g_eps"]) < 1e-11
+        assert rel_l2(r["g_sig"], ref["g_sig"]) < 1e-11
+        assert np.allclose(r["misfit"], ref["misfit"], rtol=1e-12)
