@@ -14,7 +14,9 @@ edge cells, and returns the epsilon and sigma gradients.
 
 The timed region runs with kernel timing off; the per-kernel figures and the
 roofline come from one more step run afterwards with sampled CUDA events on.
-A cfg3 leg times the checkpointed single-shot gradient on the 2000 x 800 grid
+A forward leg times the same acquisition's forward solve alone (temporally
+blocked passes against the one-step ring kernels), a cfg3 leg the checkpointed
+single-shot gradient on the 2000 x 800 grid
 (8000 steps, checkpoints every 90 steps), a cfg4 leg the 48 uneven problems in
 one gj_w_gradient_batch call (--no-cfg4 skips it; --cfg4 prints it as a line of
 its own), and a dc leg the 2.5D DC survey (--no-dc).
@@ -405,6 +407,77 @@ def cfg3_leg(ctx):
             "kernels": per}
 
 
+def forward_leg(ctx, p):
+    """The benchmark acquisition's forward solve alone (the plain-forward
+    workload: 30 shots x 6000 steps on the 1000 x 400 model, traces of 200
+    receivers, FP32), through gj_w_forward with host buffers.  The library's
+    tuner picks the temporally blocked passes (k_fwd_tb, D steps per launch on
+    shared-memory tiles) or the one-step ring kernels; the ring kernels are
+    timed beside it (GJ_TB_DEPTH=0), and the FP32 traces of one shot are
+    compared with FP64.  Device time per launch from sampled CUDA events
+    (a separate instrumented call); algorithmic bytes per blocked pass: the
+    state read and written once (24 B per padded cell) + Ceze, Cezhy (8 B) +
+    the split fields of the PML band (16 B per band node), per shot, for D steps."""
+    import torch
+    from gerjoii_b200 import _native as N
+    g = p.grid
+    cells = g.NX * g.NY
+    bnodes, _ = band_counts(g)
+    pk, pk_src = peaks()
+
+    def timed(kind):
+        ctx.set_kernel_timing(False)
+        ctx.w_forward(g, p.eps0, p.sig0, p.shots, precision=N.GJ_F32)  # plans (and tunes)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = ctx.w_forward(g, p.eps0, p.sig0, p.shots, precision=N.GJ_F32)
+        t = time.perf_counter() - t0
+        launches = ctx.last_launch_count
+        ctx.set_kernel_timing(True)
+        ctx.w_forward(g, p.eps0, p.sig0, p.shots, precision=N.GJ_F32)
+        kt = ctx.kernel_time(kind)
+        ctx.set_kernel_timing(False)
+        dev_s = kt["avg_us"] * kt["launches"] / 1e6
+        return out, t, launches, kt, dev_s
+
+    os.environ.pop("GJ_TB_DEPTH", None)
+    out, t, launches, kt, dev_s = timed("tb_pass")
+    ns = len(p.shots)
+    upd = ns * g.nt * cells
+    res = {"workload": f"radar forward, {ns} shots x {len(p.shots[0].rec)} receivers, {g.n}x{g.m} model "
+                       f"(padded {g.NX}x{g.NY}), {g.nt} steps, FP32, traces only (gj_w_forward, host buffers)",
+           "e2e_shot_forwards_per_s": ns / t, "e2e_s": t, "gpu_launches": launches}
+    if kt["launches"] > 0:
+        steps_per_pass = g.nt / kt["launches"]
+        b = ns * (cells * 32.0 + bnodes * 16.0)
+        res.update({
+            "kernel": "k_fwd_tb<float,D> (interior and PML tiles of a pass)",
+            "steps_per_pass": steps_per_pass, "passes": kt["launches"], "avg_pass_us": kt["avg_us"],
+            "device_s": dev_s, "gcell_updates_per_s": upd / dev_s / 1e9,
+            "roofline": {"bound": "hbm", "achieved": b / (kt["avg_us"] / 1e6) / 1e9, "peak": pk["hbm_gbs"],
+                         "unit": "GB/s", "frac": b / (kt["avg_us"] / 1e6) / 1e9 / pk["hbm_gbs"],
+                         "peak_source": pk_src, "algorithmic_bytes_per_pass": b,
+                         "step_equivalent_gbs": steps_per_pass * b / (kt["avg_us"] / 1e6) / 1e9,
+                         "units": "per shot and pass: 32 B x NX*NY (state once in and out, Ceze/Cezhy) + 16 B x "
+                                  "PML band nodes; step_equivalent: the bytes one-step-per-launch kernels move "
+                                  "for the same steps"}})
+    os.environ["GJ_TB_DEPTH"] = "0"
+    try:
+        out_r, t_r, _, kt_r, dev_r = timed("fwd_step")
+    finally:
+        os.environ.pop("GJ_TB_DEPTH", None)
+    res["ring_one_step_per_launch"] = {"e2e_s": t_r, "device_s": dev_r, "avg_step_us": kt_r["avg_us"],
+                                       "gcell_updates_per_s": upd / dev_r / 1e9 if dev_r > 0 else None}
+    if kt["launches"] > 0 and dev_r > 0:
+        res["speedup_device_over_ring"] = dev_r / dev_s
+    rel = lambda a, b_: float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
+    res["traces_rel_l2_blocked_vs_ring"] = max(rel(a, b_) for a, b_ in zip(out["d"], out_r["d"]))
+    d64 = ctx.w_forward(g, p.eps0, p.sig0, p.shots[:1], precision=N.GJ_F64)["d"][0]
+    res["traces_rel_l2_fp32_vs_fp64_shot0"] = rel(out["d"][0], d64)
+    ctx.release()
+    return res
+
+
 def cfg4_leg(ctx=None):
     """cfg4: 48 uneven problems (grids 256..1536 x 128..512, dx 0.02..0.05 m,
     1500..5000 steps, 4..24 shots; blob / layer models), FP32 exact gradients
@@ -738,6 +811,7 @@ def main():
         # solve of the oracle on one source
         if not args.no_dc:
             line["dc"] = dc_leg(ctx)
+        line["forward"] = forward_leg(ctx, p)
         line["cfg3"] = cfg3_leg(ctx)
         if not args.no_cfg4:
             line["cfg4"] = cfg4_leg(ctx)

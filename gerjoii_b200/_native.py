@@ -216,7 +216,7 @@ class Context:
         return int(self.lib.gj_last_launch_count(self.h))
 
     KERNEL_KINDS = {"fwd_step": 0, "ref_step": 1, "adj_step": 2, "io": 3, "plain": 4, "dc_factor": 5, "image": 6,
-                    "dc_precond": 7}
+                    "dc_precond": 7, "tb_pass": 8}
 
     def set_kernel_timing(self, on: bool):
         self._check(self.lib.gj_set_kernel_timing(self.h, int(bool(on))))

@@ -72,7 +72,7 @@ gj_status gj_set_kernel_timing(gj_ctx* ctx, int on) {
 
 gj_status gj_kernel_time(const gj_ctx* ctx, int kind, double* ms, long* sampled, long* launches,
                          long* shot_launches) {
-  if (!ctx || kind < 0 || kind >= 8) return GJ_EINVAL;
+  if (!ctx || kind < 0 || kind >= gj::KK_NKINDS) return GJ_EINVAL;
   const gj::KernelTimer& t = ctx->c.timer;
   if (ms) *ms = t.ms[kind];
   if (sampled) *sampled = t.sampled[kind];

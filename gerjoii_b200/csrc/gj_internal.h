@@ -101,7 +101,7 @@ class WBatchBase {
 // Kernel kinds reported by gj_kernel_time().
 enum KernelKind {
   KK_FWD_STEP = 0, KK_REF_STEP = 1, KK_ADJ_STEP = 2, KK_IO = 3, KK_PLAIN = 4, KK_DC_FACTOR = 5, KK_IMAGE = 6,
-  KK_DC_PRECOND = 7
+  KK_DC_PRECOND = 7, KK_TB_PASS = 8, KK_NKINDS = 9
 };
 
 // Optional per-kernel device timing: CUDA events around sampled launches of
@@ -119,19 +119,19 @@ struct Marks {
   std::vector<cudaEvent_t> ev;            // owned events, in pairs
   std::vector<int> kind;                  // per pair (-1: dropped run)
   std::vector<int> count;                 // per pair: launches inside it
-  long launches[8] = {0};                 // every launch of each kind in this sequence
-  long shot_launches[8] = {0};            // sum of shots over those launches
+  long launches[KK_NKINDS] = {0};         // every launch of each kind in this sequence
+  long shot_launches[KK_NKINDS] = {0};    // sum of shots over those launches
   ~Marks() { for (auto e : ev) cudaEventDestroy(e); }
 };
 
 struct KernelTimer {
   bool on = false;
   int stride = 16, span = 8;
-  double ms[8] = {0};
-  long sampled[8] = {0};
-  long launches[8] = {0};
-  long shot_launches[8] = {0};
-  long seen[8] = {0};
+  double ms[KK_NKINDS] = {0};
+  long sampled[KK_NKINDS] = {0};
+  long launches[KK_NKINDS] = {0};
+  long shot_launches[KK_NKINDS] = {0};
+  long seen[KK_NKINDS] = {0};
   Marks* cur = nullptr;  // list receiving new marks
   int open = -1;         // kind of the run being timed, or -1
   int open_n = 0;        // launches in it so far
@@ -153,7 +153,7 @@ struct KernelTimer {
       open = -1;
     }
     if (open == kind) return true;
-    const int every = (kind == KK_DC_FACTOR || kind == KK_DC_PRECOND) ? 1 : stride;
+    const int every = (kind == KK_DC_FACTOR || kind == KK_DC_PRECOND) ? 1 : kind == KK_TB_PASS ? 4 : stride;
     if ((seen[kind]++ % every) != 0) return false;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
@@ -190,11 +190,11 @@ struct KernelTimer {
         sampled[m.kind[q]] += m.count[q];
       }
     }
-    for (int k = 0; k < 8; ++k) { launches[k] += m.launches[k]; shot_launches[k] += m.shot_launches[k]; }
+    for (int k = 0; k < KK_NKINDS; ++k) { launches[k] += m.launches[k]; shot_launches[k] += m.shot_launches[k]; }
     cudaGetLastError();
   }
   void reset() {
-    for (int k = 0; k < 8; ++k) { ms[k] = 0; sampled[k] = 0; launches[k] = 0; shot_launches[k] = 0; seen[k] = 0; }
+    for (int k = 0; k < KK_NKINDS; ++k) { ms[k] = 0; sampled[k] = 0; launches[k] = 0; shot_launches[k] = 0; seen[k] = 0; }
     open = -1;
   }
 };

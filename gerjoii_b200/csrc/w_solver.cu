@@ -14,6 +14,7 @@
 #include "w_kernels.cuh"
 #include "w_kernels_vec.cuh"
 #include "w_kernels_ring.cuh"
+#include "w_tblock.cuh"
 #include "w_misfit.cuh"
 #include "w_condition.cuh"
 #include "w_band.cuh"
@@ -348,6 +349,8 @@ class WSolver : public WSolverBase {
     ring_nth = 0;
     tasks.clear();
     tuned.clear();
+    tb_tiles.clear();
+    tb_tuned.clear();
     if constexpr (VT<T>::V * sizeof(T) == 16) {
       int dev = 0;
       GJ_CUDA(err, cudaGetDevice(&dev));
@@ -728,6 +731,204 @@ class WSolver : public WSolverBase {
     return GJ_OK;
   }
 
+  // ------------------------------------------------ temporal blocking
+  // Forward passes that keep no history (gj_w_forward without u, the misfit
+  // and trial-misfit calls) can advance D = 1..4 Yee steps per launch with the
+  // tiled kernels of w_tblock.cuh.  TbCfg: depth D (0 = the one-step ring
+  // kernels), tile shape (tb_shape_G / tb_shape_RC) and shots per CTA.  The
+  // tuner (tb_tune) times the ring kernels and the blocked candidates on this
+  // grid at the launch size and keeps the fastest; GJ_TB_DEPTH, GJ_TB_SHAPE
+  // and GJ_TB_SPB fix a configuration instead (GJ_TB_DEPTH=0: ring kernels).
+  struct TbCfg {
+    int D = 0, shape = 1, spb = 1;
+    bool operator==(const TbCfg& o) const { return D == o.D && shape == o.shape && spb == o.spb; }
+  };
+  std::map<int, TbCfg> tb_tuned;
+  struct TbTiles { DevBuf buf; int nI = 0, nP = 0; };  // interior tiles first, then PML tiles
+  std::map<int, std::unique_ptr<TbTiles>> tb_tiles;    // key D * 16 + shape
+  float tb_us = 0.f;                                   // tuned time per step (tb_tune), us
+
+  // Tiles of depth D and a tile shape: owned TR x TC blocks over the
+  // (NX+1) x (NY+1) nodes, classified interior when every node that a step
+  // updates in the staged region (owned + D halo) uses the interior formulas.
+  gj_status tb_prepare(Err& err, int D, int shape) {
+    const int key = D * 16 + shape;
+    if (tb_tiles.count(key)) return GJ_OK;
+    const int G = tb_shape_G(shape), RC = tb_shape_RC(shape), RR = 32 * G;
+    const int TR = RR - 2 * D, TC = RC - 2 * D;
+    for (int pml = 0; pml < 2; ++pml) {
+      const size_t sm = tb_smem(shape, pml, sizeof(T));
+      if (sm > size_t(maxsm_dyn)) return err.set(GJ_EINVAL, "tile shape %d needs %zu B of shared memory", shape, sm);
+      GJ_CUDA(err, cudaFuncSetAttribute(tb_kernel<T>(D, shape, pml), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(sm)));
+    }
+    std::vector<int2> ti, tp;
+    for (int c0 = 0; c0 <= NY; c0 += TC)
+      for (int r0 = 0; r0 <= NX; r0 += TR) {
+        bool interior = true;
+        for (int col = 0; col < RC && interior; ++col) {
+          const int j = c0 - D + col;
+          if (j < 0 || j > NY) continue;
+          for (int row = 0; row < RR; ++row) {
+            const int i = r0 - D + row;
+            if (i < 0 || i > NX) continue;
+            const bool hx = j <= NY - 1 && col < RC - 1, hy = i <= NX - 1 && row < RR - 1;
+            const bool e = i >= 1 && i <= NX - 1 && j >= 1 && j <= NY - 1 && row >= 1 && col >= 1;
+            if ((hx && !(j >= w.hxj0 && j <= w.hxj1)) || (hy && !(i >= w.hyi0 && i <= w.hyi1)) ||
+                (e && !(i >= w.ei0 && i <= w.ei1 && j >= w.ej0 && j <= w.ej1))) {
+              interior = false;
+              break;
+            }
+          }
+        }
+        (interior ? ti : tp).push_back(make_int2(r0, c0));
+      }
+    auto tt = std::make_unique<TbTiles>();
+    tt->nI = int(ti.size());
+    tt->nP = int(tp.size());
+    ti.insert(ti.end(), tp.begin(), tp.end());
+    GJ_TRY(tt->buf.alloc(err, ti.size() * sizeof(int2)));
+    GJ_CUDA(err, cudaMemcpy(tt->buf.p, ti.data(), ti.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    tb_tiles.emplace(key, std::move(tt));
+    return GJ_OK;
+  }
+  // nd <= q.D forward steps it .. it+nd-1 of gn shots (A -> B); traces of the
+  // steps into d ([shot][nrr][nt]) and Jz into jz when given.  PML tiles on
+  // the side stream, interior tiles on st.
+  gj_status launch_fwd_tb(Err& err, const T* A, T* B, int it, int nd, int gn, const TbCfg& q, T* d, T* jz,
+                          cudaStream_t st) {
+    GJ_TRY(tb_prepare(err, q.D, q.shape));
+    const TbTiles& tt = *tb_tiles.at(q.D * 16 + q.shape);
+    TbArgs<T> a{};
+    a.A = A; a.B = B; a.fstride = fstride; a.sstride = sstride; a.gn = gn; a.spb = std::max(q.spb, 1);
+    a.it = it; a.nd = nd; a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.shot0 = 0;
+    a.nrr = std::max(nr, 1);
+    a.rs = rsbuf.as<int>(); a.nrs = nrsbuf.as<int>();
+    a.d = nr > 0 ? d : nullptr; a.jz = jz;
+    const int gy = (gn + a.spb - 1) / a.spb;
+    const int2* tl = tt.buf.template as<int2>();
+    const int nth = 32 * TB_WARPS;
+    last_kernels = (tt.nI > 0) + (tt.nP > 0);
+    const bool fork = side && tt.nP > 0 && tt.nI > 0;
+    if (fork) {
+      GJ_CUDA(err, cudaEventRecord(ev_fork, st));
+      GJ_CUDA(err, cudaStreamWaitEvent(side, ev_fork, 0));
+    }
+    if (tt.nP > 0)
+      tb_kernel<T>(q.D, q.shape, true)<<<dim3(tt.nP, gy), nth, tb_smem(q.shape, true, sizeof(T)), fork ? side : st>>>(
+          w, a, tl + tt.nI);
+    if (tt.nI > 0)
+      tb_kernel<T>(q.D, q.shape, false)<<<dim3(tt.nI, gy), nth, tb_smem(q.shape, false, sizeof(T)), st>>>(w, a, tl);
+    if (fork) {
+      GJ_CUDA(err, cudaEventRecord(ev_join, side));
+      GJ_CUDA(err, cudaStreamWaitEvent(st, ev_join, 0));
+    }
+    return GJ_OK;
+  }
+  // The configuration for forward-only passes of gn shots: the environment's,
+  // else the tuned one (timed on first use), else the ring kernels.
+  gj_status tb_select(Err& err, int gn, cudaStream_t st, TbCfg& out) {
+    TbCfg e;
+    bool fixed = false;
+    auto env = [&](const char* k, int& v, int lo, int hi) {
+      if (const char* x = getenv(k)) { v = std::min(std::max(atoi(x), lo), hi); fixed = true; }
+    };
+    env("GJ_TB_DEPTH", e.D, 0, 4);
+    env("GJ_TB_SHAPE", e.shape, 0, TB_NSHAPE - 1);
+    env("GJ_TB_SPB", e.spb, 1, 8);
+    if (fixed) {
+      if (e.D > 0 && tb_smem(e.shape, true, sizeof(T)) > size_t(maxsm_dyn)) e.shape = 0;
+      out = e;
+      return GJ_OK;
+    }
+    if (const char* x = getenv("GJ_AUTOTUNE"))
+      if (atoi(x) == 0) { out = TbCfg{}; return GJ_OK; }
+    auto itc = tb_tuned.find(gn);
+    if (itc == tb_tuned.end()) {
+      GJ_TRY(tb_tune(err, gn, st));
+      itc = tb_tuned.find(gn);
+    }
+    out = itc->second;
+    return GJ_OK;
+  }
+  // Times forward passes of gn zeroed shots (24 steps, receivers recorded,
+  // the least of three runs after a warm-up run) for the ring kernels and for
+  // every depth 1..4 x tile shape x shots per CTA (1, 2), and keeps the fastest.
+  gj_status tb_tune(Err& err, int gn, cudaStream_t st) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GJ_CUDA(err, cudaEventCreate(&e0));
+    GJ_CUDA(err, cudaEventCreate(&e1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } guard{e0, e1};
+    const int nsteps = 24, trials = 3;
+    const char* vb = getenv("GJ_AUTOTUNE_VERBOSE");
+    const bool every = vb && atoi(vb) >= 2;
+    auto run = [&](const TbCfg& q) -> gj_status {
+      T* A = fwdA.as<T>() + ld;
+      T* B = fwdB.as<T>() + ld;
+      for (int it = 0; it < nsteps;) {
+        if (q.D == 0) {
+          StepArgs<T> a = step_args(A, B, it % g.nt);
+          GJ_TRY(launch_fwd(err, a, gn, st));
+          k_record<T><<<dim3(1, gn), 128, 0, st>>>(B, sstride, recbuf.as<long>(), std::max(nr, 1),
+                                                   nrsbuf.as<int>(), it % g.nt, g.nt, dbuf.as<T>(), d_src,
+                                                   static_cast<T*>(nullptr), gn);
+          ++it;
+        } else {
+          const int nd = std::min(q.D, nsteps - it);
+          GJ_TRY(launch_fwd_tb(err, A, B, it % g.nt, std::min(nd, g.nt - it % g.nt), gn, q, dbuf.as<T>(), nullptr,
+                               st));
+          it += nd;
+        }
+        std::swap(A, B);
+      }
+      return GJ_OK;
+    };
+    auto time_cfg = [&](const TbCfg& q, float& ms) -> gj_status {
+      GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_TRY(run(q));  // warm-up
+      for (int trial = 0; trial < trials; ++trial) {
+        GJ_CUDA(err, cudaEventRecord(e0, st));
+        GJ_TRY(run(q));
+        GJ_CUDA(err, cudaEventRecord(e1, st));
+        GJ_CUDA(err, cudaEventSynchronize(e1));
+        float t = 0.f;
+        GJ_CUDA(err, cudaEventElapsedTime(&t, e0, e1));
+        ms = trial ? std::min(ms, t) : t;
+      }
+      GJ_CUDA(err, cudaGetLastError());
+      if (every)
+        fprintf(stderr, "gerjoii_b200 tb candidate D=%d shape=%d spb=%d %.2f us/step\n", q.D, q.shape, q.spb,
+                1e3f * ms / nsteps);
+      return GJ_OK;
+    };
+    std::vector<TbCfg> cands;
+    if (ring_nth > 0) cands.push_back(TbCfg{});
+    for (int D = 1; D <= 4; ++D)
+      for (int sh = 0; sh < TB_NSHAPE; ++sh)
+        for (int spb : {1, 2}) {
+          if (tb_smem(sh, true, sizeof(T)) > size_t(maxsm_dyn)) continue;
+          if (spb > gn) continue;
+          TbCfg q; q.D = D; q.shape = sh; q.spb = spb;
+          cands.push_back(q);
+        }
+    TbCfg best = cands.front();
+    float tbest = 0.f;
+    GJ_TRY(time_cfg(best, tbest));  // clocks up before the first timing
+    GJ_TRY(time_cfg(best, tbest));
+    for (size_t k = 1; k < cands.size(); ++k) {
+      float t = 0.f;
+      GJ_TRY(time_cfg(cands[k], t));
+      if (t < 0.98f * tbest) { tbest = t; best = cands[k]; }
+    }
+    tb_tuned[gn] = best;
+    tb_us = 1e3f * tbest / nsteps;
+    if (vb)
+      fprintf(stderr, "gerjoii_b200 tb autotune %dx%d, %d shots/launch: D=%d shape=%d spb=%d %.2f us/step\n", NX, NY,
+              gn, best.D, best.shape, best.spb, tb_us);
+    return GJ_OK;
+  }
+
   // Coefficients from the model (host doubles or device T / double).
   template <class TM>
   gj_status build(Err& err, Ctx& c, const TM* eps_dev, const TM* sig_dev, cudaStream_t st) {
@@ -772,6 +973,11 @@ class WSolver : public WSolverBase {
     GJ_CUDA(err, cudaMemcpy(mh.as<double>(), eps, mn * sizeof(double), cudaMemcpyHostToDevice));
     GJ_CUDA(err, cudaMemcpy(mh.as<double>() + mn, sig, mn * sizeof(double), cudaMemcpyHostToDevice));
     GJ_TRY(build<double>(err, c, mh.as<double>(), mh.as<double>() + mn, st));
+    ring_on = ring_nth > 0;
+    select_cfg(nshots);
+    GJ_TRY(prepare_tasks(err, nshots));
+    TbCfg tq;  // several steps per launch when no history is kept
+    if (!u_out) GJ_TRY(tb_select(err, nshots, st, tq));
     GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
     GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
     T* A = fwdA.as<T>() + ld;
@@ -780,21 +986,39 @@ class WSolver : public WSolverBase {
     DevBuf jzb, ub;
     if (jz_out) GJ_TRY(jzb.alloc(err, size_t(nshots) * g.nt * sizeof(T)));
     if (u_out) GJ_TRY(ub.alloc(err, size_t(nshots) * dn * (g.nt + 1) * sizeof(T)));
-    ring_on = ring_nth > 0;
-    select_cfg(nshots);
-    GJ_TRY(prepare_tasks(err, nshots));
-    for (int it = 0; it < g.nt; ++it) {
-      StepArgs<T> a = step_args(A, B, it);
-      if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * dn; a.hstride = dn; }
-      GJ_TRY(launch_fwd(err, a, nshots, st));
-      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
-                                                   g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
-                                                   nshots);
-      c.launches += 1 + last_kernels;
+    Marks tbm;  // per-launch device time when kernel timing is on
+    struct CurGuard { KernelTimer& t; ~CurGuard() { t.cur = nullptr; t.open = -1; } } cg{c.timer};
+    c.timer.cur = &tbm;
+    for (int it = 0; tq.D > 0 && it < g.nt; it += tq.D) {
+      const bool tm = c.timer.begin(KK_TB_PASS, st, nshots);
+      GJ_TRY(launch_fwd_tb(err, A, B, it, std::min(tq.D, g.nt - it), nshots, tq, dbuf.as<T>(),
+                           jz_out ? jzb.as<T>() : nullptr, st));
+      c.timer.end(tm, st);
+      c.launches += last_kernels;
       std::swap(A, B);
     }
+    c.timer.close(st);
+    for (int it = 0; tq.D == 0 && it < g.nt; ++it) {
+      StepArgs<T> a = step_args(A, B, it);
+      if (u_out) { a.hist = ub.as<T>() + size_t(it) * nshots * dn; a.hstride = dn; }
+      // receivers recorded inside the ring step unless Jz is wanted too
+      const bool fused = ring_on && nr > 0 && !jz_out;
+      RecArgs<T> ra = rec_args(0);
+      if (fused) { ra.d = dbuf.as<T>(); ra.it = it; }
+      const bool tm = c.timer.begin(KK_FWD_STEP, st, nshots);
+      GJ_TRY(launch_fwd(err, a, nshots, st, ra));
+      if (!fused)
+        k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
+                                                     g.nt, dbuf.as<T>(), d_src, jz_out ? jzb.as<T>() : nullptr,
+                                                     nshots);
+      c.timer.end(tm, st);
+      c.launches += (fused ? 0 : 1) + last_kernels;
+      std::swap(A, B);
+    }
+    c.timer.close(st);
     GJ_CUDA(err, cudaGetLastError());
     GJ_CUDA(err, cudaDeviceSynchronize());
+    c.timer.collect(tbm);
     // copy out (per shot nt x nr, time fastest)
     std::vector<T> hd(size_t(nshots) * nrr * g.nt);
     GJ_CUDA(err, cudaMemcpy(hd.data(), dbuf.p, hd.size() * sizeof(T), cudaMemcpyDeviceToHost));
@@ -903,24 +1127,44 @@ class WSolver : public WSolverBase {
   gj_status misfit(Err& err, Ctx& c, const double* eps, const double* sig, const double* dobs, gj_misfit_kind mk,
                    double* misfit_out, cudaStream_t st, const gj_w_opts* opts = nullptr) {
     GJ_TRY(stage_inputs(err, c, eps, sig, false, dobs, false, st));
-    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
-    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     ring_on = ring_nth > 0;
     select_cfg(nshots);
     GJ_TRY(prepare_tasks(err, nshots));
+    TbCfg tq;  // several steps per launch
+    GJ_TRY(tb_select(err, nshots, st, tq));
+    GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, nshots * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
     T* A = fwdA.as<T>() + ld;
     T* B = fwdB.as<T>() + ld;
     const int nrr = std::max(nr, 1);
     const size_t tr = size_t(nrr) * g.nt;
-    for (int it = 0; it < g.nt; ++it) {
-      StepArgs<T> a = step_args(A, B, it);
-      GJ_TRY(launch_fwd(err, a, nshots, st));
-      k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it, g.nt,
-                                                   dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
-      c.launches += 1 + last_kernels;
+    Marks tbm;  // per-launch device time when kernel timing is on
+    struct CurGuard { KernelTimer& t; ~CurGuard() { t.cur = nullptr; t.open = -1; } } cg{c.timer};
+    c.timer.cur = &tbm;
+    for (int it = 0; tq.D > 0 && it < g.nt; it += tq.D) {
+      const bool tm = c.timer.begin(KK_TB_PASS, st, nshots);
+      GJ_TRY(launch_fwd_tb(err, A, B, it, std::min(tq.D, g.nt - it), nshots, tq, dbuf.as<T>(), nullptr, st));
+      c.timer.end(tm, st);
+      c.launches += last_kernels;
       std::swap(A, B);
     }
+    c.timer.close(st);
+    for (int it = 0; tq.D == 0 && it < g.nt; ++it) {
+      StepArgs<T> a = step_args(A, B, it);
+      const bool fused = ring_on && nr > 0;  // receivers recorded inside the ring step
+      RecArgs<T> ra = rec_args(0);
+      if (fused) { ra.d = dbuf.as<T>(); ra.it = it; }
+      const bool tm = c.timer.begin(KK_FWD_STEP, st, nshots);
+      GJ_TRY(launch_fwd(err, a, nshots, st, ra));
+      if (!fused)
+        k_record<T><<<dim3(1, nshots), 128, 0, st>>>(B, sstride, recbuf.as<long>(), nrr, nrsbuf.as<int>(), it,
+                                                     g.nt, dbuf.as<T>(), d_src, static_cast<T*>(nullptr), nshots);
+      c.timer.end(tm, st);
+      c.launches += (fused ? 0 : 1) + last_kernels;
+      std::swap(A, B);
+    }
+    c.timer.close(st);
     if (opts && opts->filt_high > opts->filt_low) {
       GJ_TRY(filt_traces(err, c, *opts, dbuf.as<T>(), nshots, st));
       GJ_TRY(filt_traces(err, c, *opts, dobsbuf.as<T>(), nshots, st));
@@ -936,6 +1180,7 @@ class WSolver : public WSolverBase {
     std::vector<double> hs(2 * nshots);
     GJ_CUDA(err, cudaMemcpyAsync(hs.data(), sums.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     GJ_CUDA(err, cudaStreamSynchronize(st));
+    c.timer.collect(tbm);
     int nbad = 0;
     for (int q = 0; q < nshots; ++q) {
       misfit_out[q] = hs[2 * q + 1] > 0 ? 0.5 * hs[2 * q] / hs[2 * q + 1] : 0.5 * hs[2 * q];

@@ -383,7 +383,9 @@ long gj_last_launch_count(const gj_ctx* ctx);
  * and around every launch of the DC factor and substitution.
  * kind: 0 forward Yee step, 1 reference-adjoint step, 2 exact-adjoint step,
  * 3 receiver I/O, 4 plain kernels, 5 DC band factor, 6 radar imaging,
- * 7 DC band substitution (preconditioner apply).  gj_kernel_time returns the
+ * 7 DC band substitution (preconditioner apply), 8 temporally blocked forward
+ * pass (one launch advancing up to 4 steps; every 4th pass timed, both tile
+ * kernels of the pass inside the bracket).  gj_kernel_time returns the
  * summed milliseconds of the timed launches, their number (ms / sampled is
  * the average launch duration), the number of launches of that kind, and the sum over
  * those launches of the shots each one advanced.  No counterpart in the

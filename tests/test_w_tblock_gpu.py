@@ -1,0 +1,130 @@
+"""Temporally blocked forward passes (k_fwd_tb: D = 1..4 Yee steps per launch
+on shared-memory tiles with a D-node halo) against the oracle and against the
+one-step ring kernels, through the C ABI.  The grids span several tiles in
+both directions, the step counts are not multiples of D (a shorter last
+pass), and receivers sit on tile boundaries, in the PML and on the grid's
+PEC corners."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from gerjoii_b200 import synth
+from gerjoii_b200 import _native as N
+from gerjoii_b200.geometry import Shot
+
+pytestmark = pytest.mark.gpu
+
+
+def _with_receivers(p, extra):
+    g = p.grid
+    NX1 = g.NX + 1
+    lin = [i + j * NX1 for i, j in extra]
+    p.shots = [Shot(sh.src_i, sh.src_j, sh.wavelet, np.concatenate([np.asarray(sh.rec, np.int64), lin]))
+               for sh in p.shots]
+    p.corner0 = [sh.nr - len(lin) for sh in p.shots]  # first of the four corner receivers
+    return p
+
+
+def _extra_nodes(g):
+    """Nodes on tile edges of every tile shape (rows 27-34, 55-66, 119-126;
+    columns 27-30, 55-62), in the bottom and side PML, and the four corners."""
+    pts = [(0, 0), (g.NX, g.NY), (g.NX, 0), (0, g.NY), (g.NX - 3, g.NY // 2), (g.NX // 2, 2), (g.NX // 2, g.NY - 2)]
+    for i in (27, 28, 33, 34, 55, 56, 61, 62, 65, 66, 119, 120, 125, 126):
+        for j in (27, 28, 29, 30, 55, 56, 61, 62):
+            if i < g.NX and j < g.NY:
+                pts.append((i, j))
+    return pts
+
+
+@pytest.fixture(scope="module")
+def multi_ft():
+    p = synth.small(m=130, n=150, pml=10, nt=157, free_top=True, seed=41, nsrc=3, nrec=20)
+    return _with_receivers(p, _extra_nodes(p.grid))
+
+
+@pytest.fixture(scope="module")
+def multi_ref():
+    p = synth.small(m=110, n=90, pml=12, nt=103, free_top=False, seed=42, nsrc=2, nrec=10)
+    return _with_receivers(p, _extra_nodes(p.grid))
+
+
+@pytest.fixture(scope="module")
+def oracle_out(oracle, multi_ft, multi_ref):
+    out = {}
+    for name, p in (("ft", multi_ft), ("ref", multi_ref)):
+        out[name] = [oracle.forward(p.grid, p.eps0, p.sig0, sh) for sh in p.shots]
+    return out
+
+
+CFGS = [(D, shape, spb) for D in (1, 2, 3, 4) for shape in (0, 1, 2) for spb in (1, 2)]
+
+
+def _set(monkeypatch, D, shape, spb):
+    monkeypatch.setenv("GJ_TB_DEPTH", str(D))
+    monkeypatch.setenv("GJ_TB_SHAPE", str(shape))
+    monkeypatch.setenv("GJ_TB_SPB", str(spb))
+
+
+@pytest.mark.parametrize("D,shape,spb", CFGS)
+def test_blocked_forward_f64_matches_oracle(gpu_ctx, multi_ft, oracle_out, monkeypatch, D, shape, spb):
+    p = multi_ft
+    _set(monkeypatch, D, shape, spb)
+    out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F64, want_jz=True)
+    for k in range(len(p.shots)):
+        d, jz, _ = oracle_out["ft"][k]
+        assert rel_l2(out["d"][k], d) < 1e-12
+        assert rel_l2(out["jz"][k], jz) < 1e-12
+        c0 = p.corner0[k]
+        assert np.all(out["d"][k][:, c0:c0 + 4] == 0)  # the four PEC corners
+
+
+@pytest.mark.parametrize("D,shape", [(1, 0), (2, 1), (3, 2), (4, 1)])
+def test_blocked_forward_reference_layout_f64(gpu_ctx, multi_ref, oracle_out, monkeypatch, D, shape):
+    p = multi_ref
+    _set(monkeypatch, D, shape, 1)
+    out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F64, want_jz=True)
+    for k in range(len(p.shots)):
+        d, jz, _ = oracle_out["ref"][k]
+        assert rel_l2(out["d"][k], d) < 1e-12
+        assert rel_l2(out["jz"][k], jz) < 1e-12
+
+
+@pytest.mark.parametrize("D,shape,spb", [(1, 1, 1), (2, 1, 2), (3, 0, 1), (4, 2, 2)])
+def test_blocked_forward_f32_traces(gpu_ctx, multi_ft, oracle_out, monkeypatch, D, shape, spb):
+    """FP32 traces within 1e-5 rel-L2 of the FP64 oracle and of the FP32 ring
+    kernels (one step per launch)."""
+    p = multi_ft
+    monkeypatch.setenv("GJ_TB_DEPTH", "0")
+    ring = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F32)
+    _set(monkeypatch, D, shape, spb)
+    out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F32)
+    for k in range(len(p.shots)):
+        d, _, _ = oracle_out["ft"][k]
+        assert rel_l2(out["d"][k], d) < 1e-5
+        assert rel_l2(out["d"][k], ring["d"][k]) < 1e-5
+
+
+def test_blocked_misfit_equals_ring_misfit(gpu_ctx, multi_ft, oracle, monkeypatch):
+    p = multi_ft
+    dobs = [oracle.forward(p.grid, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
+    monkeypatch.setenv("GJ_TB_DEPTH", "0")
+    ring = gpu_ctx.w_misfit(p.grid, p.eps0, p.sig0, p.shots, dobs, precision=N.GJ_F64)
+    for D in (2, 4):
+        _set(monkeypatch, D, 1, 1)
+        tb = gpu_ctx.w_misfit(p.grid, p.eps0, p.sig0, p.shots, dobs, precision=N.GJ_F64)
+        assert np.allclose(tb, ring, rtol=1e-12, atol=0)
+        trials = gpu_ctx.w_misfit_trials(p.grid, [p.eps0, p.eps_true], [p.sig0, p.sig_true], p.shots, dobs,
+                                         precision=N.GJ_F64)
+        assert np.allclose(trials[0], ring, rtol=1e-12, atol=0)
+        assert np.all(trials[1] < 1e-20)
+
+
+def test_tuned_forward_matches_oracle(gpu_ctx, multi_ft, oracle_out, monkeypatch):
+    """No configuration fixed: the tuner picks one (the ring kernels or a
+    blocked depth) and the traces still equal the oracle's."""
+    p = multi_ft
+    for k in ("GJ_TB_DEPTH", "GJ_TB_SHAPE", "GJ_TB_SPB", "GJ_AUTOTUNE"):
+        monkeypatch.delenv(k, raising=False)
+    out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F64)
+    for k in range(len(p.shots)):
+        assert rel_l2(out["d"][k], oracle_out["ft"][k][0]) < 1e-12
