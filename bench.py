@@ -15,7 +15,8 @@ edge cells, and returns the epsilon and sigma gradients.
 The timed region runs with kernel timing off; the per-kernel figures and the
 roofline come from one more step run afterwards with sampled CUDA events on.
 A forward leg times the same acquisition's forward solve alone (temporally
-blocked passes against the one-step ring kernels), a cfg3 leg the checkpointed
+blocked passes against the one-step ring kernels), a cfg1 leg the plain FP64
+small-size gradient (GPU plain FP64, GPU FP32 and the oracle), a cfg3 leg the checkpointed
 single-shot gradient on the 2000 x 800 grid
 (8000 steps, checkpoints every 90 steps), a cfg4 leg the 48 uneven problems in
 one gj_w_gradient_batch call (--no-cfg4 skips it; --cfg4 prints it as a line of
@@ -405,6 +406,74 @@ def cfg3_leg(ctx):
                          "units": "per shot-step 32 B x NX*NY (forward, recompute, adjoint) + per model cell 4 B "
                                   "(u slot, adjoint ring) + 8 B per imaged step + 36 B per imaging pass"},
             "kernels": per}
+
+
+def _cfg1_worker(k):
+    """One shot of the small-size workload's FP64 exact gradient on the oracle
+    (one worker process per shot, the reference's parfor)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from gerjoii_b200 import synth
+    p = synth.cfg1()
+    g, sh = p.grid, p.shots[k]
+    dobs = pyoracle.forward(g, p.eps_true, p.sig_true, sh)[0]
+    t0 = time.perf_counter()
+    ge, gs, mis = pyoracle.gradient_batch(g, p.eps0, p.sig0, [sh], dobs.T[None], mode="exact", precision="f64",
+                                          threads=1)
+    return time.perf_counter() - t0, np.asarray(ge), np.asarray(gs)
+
+
+def cfg1_leg(ctx):
+    """The plain FP64 small-size workload (100 x 200 model, 20 PML cells, free
+    top, 2000 steps, 5 shots x 50 receivers) in full: the exact gradient of
+    the 5 shots as the plain per-shot FP64 GPU form, as the batched FP32 GPU
+    form, and on the oracle in FP64 with one host process per shot; the GPU
+    gradients against the oracle's."""
+    import multiprocessing as mp
+    import torch
+    from gerjoii_b200 import synth
+    from gerjoii_b200 import _native as N
+    p = synth.cfg1()
+    g = p.grid
+    dobs = ctx.w_forward(g, p.eps_true, p.sig_true, p.shots, precision=N.GJ_F64)["d"]
+    o_pl = N.OptsC()
+    o_pl.plain = 1
+
+    def timed(prec, o):
+        ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=prec, opts=o)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=prec, opts=o)
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    r64, t64 = timed(N.GJ_F64, o_pl)
+    r32, t32 = timed(N.GJ_F32, None)
+    ctx.release()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    pyoracle.build()
+    with mp.get_context("spawn").Pool(len(p.shots)) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_cfg1_worker, range(len(p.shots)), chunksize=1)
+        t_cpu = time.perf_counter() - t0
+    ge = sum(r[1] for r in res)
+    gs = sum(r[2] for r in res)
+    rel = lambda a, b: float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+    cos = lambda a, b: float(np.ravel(a) @ np.ravel(b) / (np.linalg.norm(a) * np.linalg.norm(b)))
+    ns = len(p.shots)
+    upd = 2 * ns * g.nt * g.NX * g.NY
+    return {"workload": f"plain FP64 small-size gradient, {g.n}x{g.m} model (padded {g.NX}x{g.NY}), {ns} shots x "
+                        f"{len(p.shots[0].rec)} receivers, {g.nt} steps, exact adjoint",
+            "gpu_plain_fp64": {"shot_gradients_per_s": ns / t64, "gcell_updates_per_s": upd / t64 / 1e9,
+                               "g_eps_rel_l2_vs_oracle": rel(r64["g_eps"], ge),
+                               "g_sig_rel_l2_vs_oracle": rel(r64["g_sig"], gs)},
+            "gpu_fp32_batched": {"shot_gradients_per_s": ns / t32, "gcell_updates_per_s": upd / t32 / 1e9,
+                                 "g_eps_rel_l2_vs_oracle": rel(r32["g_eps"], ge),
+                                 "g_eps_cosine_vs_oracle": cos(r32["g_eps"], ge),
+                                 "g_sig_rel_l2_vs_oracle": rel(r32["g_sig"], gs)},
+            "cpu_oracle_fp64": {"shot_gradients_per_s": ns / t_cpu, "cores": ns, "kind": "port",
+                                "sample": f"all {ns} shots, full {g.nt} steps, one process per shot"}}
 
 
 def forward_leg(ctx, p):
@@ -812,6 +881,7 @@ def main():
         if not args.no_dc:
             line["dc"] = dc_leg(ctx)
         line["forward"] = forward_leg(ctx, p)
+        line["cfg1"] = cfg1_leg(ctx)
         line["cfg3"] = cfg3_leg(ctx)
         if not args.no_cfg4:
             line["cfg4"] = cfg4_leg(ctx)

@@ -733,27 +733,45 @@ class WSolver : public WSolverBase {
 
   // ------------------------------------------------ temporal blocking
   // Forward passes that keep no history (gj_w_forward without u, the misfit
-  // and trial-misfit calls) can advance D = 1..4 Yee steps per launch with the
-  // tiled kernels of w_tblock.cuh.  TbCfg: depth D (0 = the one-step ring
-  // kernels), tile shape (tb_shape_G / tb_shape_RC) and shots per CTA.  The
-  // tuner (tb_tune) times the ring kernels and the blocked candidates on this
-  // grid at the launch size and keeps the fastest; GJ_TB_DEPTH, GJ_TB_SHAPE
-  // and GJ_TB_SPB fix a configuration instead (GJ_TB_DEPTH=0: ring kernels).
+  // and trial-misfit calls) can advance D = 1..4 Yee steps per launch
+  // (w_tblock.cuh).  TbCfg: depth D (0 = the one-step ring kernels), tile
+  // shape (tb_shape_G / tb_shape_RC), shots per tile CTA, and the streaming
+  // mode: the interior rows and columns run as streaming warp tasks
+  // (k_fwd_tbs, column chunks of lc) and only the rest of the grid as tiles.
+  // The tuner (tb_tune) times the ring kernels and the blocked candidates on
+  // this grid at the launch size and keeps the fastest; GJ_TB_DEPTH,
+  // GJ_TB_SHAPE, GJ_TB_SPB, GJ_TB_STREAM and GJ_TB_CHUNK fix a configuration
+  // instead (GJ_TB_DEPTH=0: ring kernels).
   struct TbCfg {
-    int D = 0, shape = 1, spb = 1;
-    bool operator==(const TbCfg& o) const { return D == o.D && shape == o.shape && spb == o.spb; }
+    int D = 0, shape = 1, spb = 1, stream = 0, lc = 32, ss = 6;  // ss: ring stages of the streaming tasks
+    bool operator==(const TbCfg& o) const {
+      return D == o.D && shape == o.shape && spb == o.spb && stream == o.stream && lc == o.lc && ss == o.ss;
+    }
   };
   std::map<int, TbCfg> tb_tuned;
-  struct TbTiles { DevBuf buf; int nI = 0, nP = 0; };  // interior tiles first, then PML tiles
-  std::map<int, std::unique_ptr<TbTiles>> tb_tiles;    // key D * 16 + shape
-  float tb_us = 0.f;                                   // tuned time per step (tb_tune), us
+  // Partition of one pass: tiles (interior tiles first, then PML tiles) and,
+  // in streaming mode, the streaming tasks of gn shots.
+  struct TbTiles {
+    DevBuf buf; int nI = 0, nP = 0;
+    DevBuf sbuf; int nS = 0;
+  };
+  std::map<long, std::unique_ptr<TbTiles>> tb_tiles;
+  float tb_us = 0.f;  // tuned time per step (tb_tune), us
+  static long tb_key(const TbCfg& q, int gn) {
+    return (((((long(q.D) * 8 + q.shape) * 2 + (q.stream ? 1 : 0)) * 1024 + (q.stream ? q.lc : 0)) * 8 +
+             (q.stream ? q.ss : 0)) << 24) | long(q.stream ? gn : 0);
+  }
 
-  // Tiles of depth D and a tile shape: owned TR x TC blocks over the
-  // (NX+1) x (NY+1) nodes, classified interior when every node that a step
-  // updates in the staged region (owned + D halo) uses the interior formulas.
-  gj_status tb_prepare(Err& err, int D, int shape) {
-    const int key = D * 16 + shape;
+  // The partition of a pass of depth D for gn shots.  Streaming rows: tasks
+  // of 32 V loaded rows at R = R0 + k stride whose rows R-1 .. R+32V are all
+  // interior (fast) rows, columns [ej0 + D - 1, ej1 - D + 1] in chunks of lc;
+  // every other node belongs to a clipped tile of TR x TC owned nodes,
+  // classified interior when every node that a step updates in its staged
+  // region (owned + D halo) uses the interior formulas.
+  gj_status tb_prepare(Err& err, const TbCfg& q, int gn) {
+    const long key = tb_key(q, gn);
     if (tb_tiles.count(key)) return GJ_OK;
+    const int D = q.D, shape = q.shape;
     const int G = tb_shape_G(shape), RC = tb_shape_RC(shape), RR = 32 * G;
     const int TR = RR - 2 * D, TC = RC - 2 * D;
     for (int pml = 0; pml < 2; ++pml) {
@@ -762,54 +780,132 @@ class WSolver : public WSolverBase {
       GJ_CUDA(err, cudaFuncSetAttribute(tb_kernel<T>(D, shape, pml), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         int(sm)));
     }
-    std::vector<int2> ti, tp;
-    for (int c0 = 0; c0 <= NY; c0 += TC)
-      for (int r0 = 0; r0 <= NX; r0 += TR) {
-        bool interior = true;
-        for (int col = 0; col < RC && interior; ++col) {
-          const int j = c0 - D + col;
-          if (j < 0 || j > NY) continue;
-          for (int row = 0; row < RR; ++row) {
-            const int i = r0 - D + row;
-            if (i < 0 || i > NX) continue;
-            const bool hx = j <= NY - 1 && col < RC - 1, hy = i <= NX - 1 && row < RR - 1;
-            const bool e = i >= 1 && i <= NX - 1 && j >= 1 && j <= NY - 1 && row >= 1 && col >= 1;
-            if ((hx && !(j >= w.hxj0 && j <= w.hxj1)) || (hy && !(i >= w.hyi0 && i <= w.hyi1)) ||
-                (e && !(i >= w.ei0 && i <= w.ei1 && j >= w.ej0 && j <= w.ej1))) {
-              interior = false;
-              break;
+    auto tt = std::make_unique<TbTiles>();
+    // streaming region
+    int rs_lo = 0, rs_hi = 0, cs_lo = 0, cs_hi = -1;
+    std::vector<int> Rs;
+    if (q.stream) {
+      constexpr int V = VT<T>::V, RW = 32 * V;
+      const int stride = V * ((RW + 2 - 2 * D) / V);
+      auto eligible = [&](int R) {
+        if (R + RW > NX - 1) return false;
+        for (int I = std::max(R - 1, 0); I <= R + RW; ++I)
+          if (!fast_row(I)) return false;
+        return true;
+      };
+      // owned rows per task: [R + D - 1, R + D - 1 + stride) (from 0 when R = 0),
+      // and a last task aligned to the last eligible row that owns the rest
+      // of its exact rows [.., R + RW - D + 1)
+      std::vector<std::pair<int, int>> own;
+      int R = 0;
+      while (R + RW <= NX - 1 && !eligible(R)) R += V;
+      for (; eligible(R); R += stride) {
+        Rs.push_back(R);
+        own.push_back({R == 0 ? 0 : R + D - 1, R + D - 1 + stride});
+      }
+      if (!Rs.empty()) {
+        int Rx = Rs.back() + stride - V;
+        while (Rx > Rs.back() && !eligible(Rx)) Rx -= V;
+        if (Rx > Rs.back() && Rx + RW - D + 1 > own.back().second) {
+          Rs.push_back(Rx);
+          own.push_back({own.back().second, Rx + RW - D + 1});
+        }
+      }
+      cs_lo = w.ej0 + D - 1;
+      cs_hi = w.ej1 - D + 1;
+      if (Rs.empty() || cs_hi - cs_lo + 1 < 1 || NY >= 65536 || NX >= 65536) {
+        Rs.clear();
+        cs_hi = cs_lo - 1;
+      } else {
+        rs_lo = own.front().first;
+        rs_hi = own.back().second;
+      }
+      std::vector<int4> ts;
+      for (int z = 0; z < gn; ++z)
+        for (size_t k = 0; k < Rs.size(); ++k)
+          for (int c0 = cs_lo; c0 <= cs_hi; c0 += q.lc) {
+            const int c1 = std::min(c0 + q.lc - 1, cs_hi);
+            bool rec = false;  // a receiver of shot z among the task's owned nodes
+            for (int r = 0; r < nrs[z] && !rec; ++r) {
+              const long kk = sh[z].rec[r];
+              const int I = int(kk % ld), J = int(kk / ld);
+              rec = I >= own[k].first && I < own[k].second && J >= c0 && J <= c1;
+            }
+            ts.push_back(make_int4(Rs[k], c0 | (c1 << 16), own[k].first | (own[k].second << 16),
+                                   z | (rec ? TBS_HAS_REC : 0)));
+          }
+      tt->nS = int(ts.size());
+      if (tt->nS) {
+        GJ_TRY(tt->sbuf.alloc(err, ts.size() * sizeof(int4)));
+        GJ_CUDA(err, cudaMemcpy(tt->sbuf.p, ts.data(), ts.size() * sizeof(int4), cudaMemcpyHostToDevice));
+      }
+      if (tbs_smem(q.ss) > size_t(maxsm_dyn)) return err.set(GJ_EINVAL, "streaming stages %d too many", q.ss);
+      GJ_CUDA(err, cudaFuncSetAttribute(tbs_kernel<T>(D, q.ss), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(tbs_smem(q.ss))));
+    }
+    const bool streamed = !Rs.empty();
+    // tiles over [a0, a1] x [b0, b1], clipped
+    std::vector<int4> ti, tp;
+    auto tile_rect = [&](int a0, int a1, int b0, int b1) {
+      for (int c0 = b0; c0 <= b1; c0 += TC)
+        for (int r0 = a0; r0 <= a1; r0 += TR) {
+          const int tr = std::min(TR, a1 - r0 + 1), tc = std::min(TC, b1 - c0 + 1);
+          bool interior = true;
+          for (int col = 0; col < RC && interior; ++col) {
+            const int j = c0 - D + col;
+            if (j < 0 || j > NY) continue;
+            for (int row = 0; row < RR; ++row) {
+              const int i = r0 - D + row;
+              if (i < 0 || i > NX) continue;
+              const bool hx = j <= NY - 1 && col < RC - 1, hy = i <= NX - 1 && row < RR - 1;
+              const bool e = i >= 1 && i <= NX - 1 && j >= 1 && j <= NY - 1 && row >= 1 && col >= 1;
+              if ((hx && !(j >= w.hxj0 && j <= w.hxj1)) || (hy && !(i >= w.hyi0 && i <= w.hyi1)) ||
+                  (e && !(i >= w.ei0 && i <= w.ei1 && j >= w.ej0 && j <= w.ej1))) {
+                interior = false;
+                break;
+              }
             }
           }
+          (interior ? ti : tp).push_back(make_int4(r0, c0, tr, tc));
         }
-        (interior ? ti : tp).push_back(make_int2(r0, c0));
-      }
-    auto tt = std::make_unique<TbTiles>();
+    };
+    if (!streamed) {
+      tile_rect(0, NX, 0, NY);
+    } else {
+      if (rs_lo > 0) tile_rect(0, rs_lo - 1, 0, NY);
+      if (rs_hi <= NX) tile_rect(rs_hi, NX, 0, NY);
+      if (cs_lo > 0) tile_rect(rs_lo, rs_hi - 1, 0, cs_lo - 1);
+      if (cs_hi < NY) tile_rect(rs_lo, rs_hi - 1, cs_hi + 1, NY);
+    }
     tt->nI = int(ti.size());
     tt->nP = int(tp.size());
     ti.insert(ti.end(), tp.begin(), tp.end());
-    GJ_TRY(tt->buf.alloc(err, ti.size() * sizeof(int2)));
-    GJ_CUDA(err, cudaMemcpy(tt->buf.p, ti.data(), ti.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    if (!ti.empty()) {
+      GJ_TRY(tt->buf.alloc(err, ti.size() * sizeof(int4)));
+      GJ_CUDA(err, cudaMemcpy(tt->buf.p, ti.data(), ti.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     tb_tiles.emplace(key, std::move(tt));
     return GJ_OK;
   }
-  // nd <= q.D forward steps it .. it+nd-1 of gn shots (A -> B); traces of the
+  // q.D forward steps it .. it+q.D-1 of gn shots (A -> B); traces of the
   // steps into d ([shot][nrr][nt]) and Jz into jz when given.  PML tiles on
-  // the side stream, interior tiles on st.
-  gj_status launch_fwd_tb(Err& err, const T* A, T* B, int it, int nd, int gn, const TbCfg& q, T* d, T* jz,
+  // the side stream; streaming tasks and interior tiles on st.
+  gj_status launch_fwd_tb(Err& err, const T* A, T* B, int it, int gn, const TbCfg& q, T* d, T* jz,
                           cudaStream_t st) {
-    GJ_TRY(tb_prepare(err, q.D, q.shape));
-    const TbTiles& tt = *tb_tiles.at(q.D * 16 + q.shape);
+    if (q.D < 1 || q.D > 4 || it + q.D > g.nt) return err.set(GJ_EINVAL, "blocked pass of %d steps at %d", q.D, it);
+    GJ_TRY(tb_prepare(err, q, gn));
+    const TbTiles& tt = *tb_tiles.at(tb_key(q, gn));
     TbArgs<T> a{};
     a.A = A; a.B = B; a.fstride = fstride; a.sstride = sstride; a.gn = gn; a.spb = std::max(q.spb, 1);
-    a.it = it; a.nd = nd; a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.shot0 = 0;
+    a.it = it; a.nd = q.D; a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.shot0 = 0;
     a.nrr = std::max(nr, 1);
     a.rs = rsbuf.as<int>(); a.nrs = nrsbuf.as<int>();
     a.d = nr > 0 ? d : nullptr; a.jz = jz;
     const int gy = (gn + a.spb - 1) / a.spb;
-    const int2* tl = tt.buf.template as<int2>();
+    const int4* tl = tt.buf.template as<int4>();
     const int nth = 32 * TB_WARPS;
-    last_kernels = (tt.nI > 0) + (tt.nP > 0);
-    const bool fork = side && tt.nP > 0 && tt.nI > 0;
+    last_kernels = (tt.nI > 0) + (tt.nP > 0) + (tt.nS > 0);
+    const bool fork = side && tt.nP > 0 && (tt.nI > 0 || tt.nS > 0);
     if (fork) {
       GJ_CUDA(err, cudaEventRecord(ev_fork, st));
       GJ_CUDA(err, cudaStreamWaitEvent(side, ev_fork, 0));
@@ -817,6 +913,9 @@ class WSolver : public WSolverBase {
     if (tt.nP > 0)
       tb_kernel<T>(q.D, q.shape, true)<<<dim3(tt.nP, gy), nth, tb_smem(q.shape, true, sizeof(T)), fork ? side : st>>>(
           w, a, tl + tt.nI);
+    if (tt.nS > 0)
+      tbs_kernel<T>(q.D, q.ss)<<<(tt.nS + TBS_WARPS - 1) / TBS_WARPS, 32 * TBS_WARPS, tbs_smem(q.ss), st>>>(
+          w, a, tt.sbuf.template as<int4>(), tt.nS);
     if (tt.nI > 0)
       tb_kernel<T>(q.D, q.shape, false)<<<dim3(tt.nI, gy), nth, tb_smem(q.shape, false, sizeof(T)), st>>>(w, a, tl);
     if (fork) {
@@ -824,6 +923,15 @@ class WSolver : public WSolverBase {
       GJ_CUDA(err, cudaStreamWaitEvent(st, ev_join, 0));
     }
     return GJ_OK;
+  }
+  // A pass of up to q.D steps from step it: the last pass of a run shorter
+  // than q.D uses the same configuration at the remaining depth.
+  gj_status launch_fwd_tb_at(Err& err, const T* A, T* B, int it, int gn, const TbCfg& q, T* d, T* jz,
+                             cudaStream_t st, int& nd) {
+    TbCfg qq = q;
+    qq.D = std::min(q.D, g.nt - it);
+    nd = qq.D;
+    return launch_fwd_tb(err, A, B, it, gn, qq, d, jz, st);
   }
   // The configuration for forward-only passes of gn shots: the environment's,
   // else the tuned one (timed on first use), else the ring kernels.
@@ -836,6 +944,11 @@ class WSolver : public WSolverBase {
     env("GJ_TB_DEPTH", e.D, 0, 4);
     env("GJ_TB_SHAPE", e.shape, 0, TB_NSHAPE - 1);
     env("GJ_TB_SPB", e.spb, 1, 8);
+    env("GJ_TB_STREAM", e.stream, 0, 1);
+    env("GJ_TB_CHUNK", e.lc, 4, 1 << 20);
+    env("GJ_TB_STAGES", e.ss, 3, 6);
+    e.ss = e.ss >= 6 ? 6 : 3;
+    if constexpr (VT<T>::V * sizeof(T) != 16) e.stream = 0;
     if (fixed) {
       if (e.D > 0 && tb_smem(e.shape, true, sizeof(T)) > size_t(maxsm_dyn)) e.shape = 0;
       out = e;
@@ -874,9 +987,8 @@ class WSolver : public WSolverBase {
                                                    static_cast<T*>(nullptr), gn);
           ++it;
         } else {
-          const int nd = std::min(q.D, nsteps - it);
-          GJ_TRY(launch_fwd_tb(err, A, B, it % g.nt, std::min(nd, g.nt - it % g.nt), gn, q, dbuf.as<T>(), nullptr,
-                               st));
+          int nd = 0;
+          GJ_TRY(launch_fwd_tb_at(err, A, B, it % g.nt, gn, q, dbuf.as<T>(), nullptr, st, nd));
           it += nd;
         }
         std::swap(A, B);
@@ -898,8 +1010,8 @@ class WSolver : public WSolverBase {
       }
       GJ_CUDA(err, cudaGetLastError());
       if (every)
-        fprintf(stderr, "gerjoii_b200 tb candidate D=%d shape=%d spb=%d %.2f us/step\n", q.D, q.shape, q.spb,
-                1e3f * ms / nsteps);
+        fprintf(stderr, "gerjoii_b200 tb candidate D=%d shape=%d spb=%d stream=%d lc=%d ss=%d %.2f us/step\n", q.D,
+                q.shape, q.spb, q.stream, q.lc, q.ss, 1e3f * ms / nsteps);
       return GJ_OK;
     };
     std::vector<TbCfg> cands;
@@ -912,6 +1024,15 @@ class WSolver : public WSolverBase {
           TbCfg q; q.D = D; q.shape = sh; q.spb = spb;
           cands.push_back(q);
         }
+    if constexpr (VT<T>::V * sizeof(T) == 16)
+      for (int D = 1; D <= 4; ++D)
+        for (int lc : {16, 32, 64})
+          for (int ss : {3, 6})
+            for (int spb : {1, 2}) {
+              if (spb > gn) continue;
+              TbCfg q; q.D = D; q.shape = 0; q.stream = 1; q.lc = lc; q.ss = ss; q.spb = spb;
+              cands.push_back(q);
+            }
     TbCfg best = cands.front();
     float tbest = 0.f;
     GJ_TRY(time_cfg(best, tbest));  // clocks up before the first timing
@@ -924,8 +1045,8 @@ class WSolver : public WSolverBase {
     tb_tuned[gn] = best;
     tb_us = 1e3f * tbest / nsteps;
     if (vb)
-      fprintf(stderr, "gerjoii_b200 tb autotune %dx%d, %d shots/launch: D=%d shape=%d spb=%d %.2f us/step\n", NX, NY,
-              gn, best.D, best.shape, best.spb, tb_us);
+      fprintf(stderr, "gerjoii_b200 tb autotune %dx%d, %d shots/launch: D=%d shape=%d spb=%d stream=%d lc=%d ss=%d "
+              "%.2f us/step\n", NX, NY, gn, best.D, best.shape, best.spb, best.stream, best.lc, best.ss, tb_us);
     return GJ_OK;
   }
 
@@ -989,10 +1110,9 @@ class WSolver : public WSolverBase {
     Marks tbm;  // per-launch device time when kernel timing is on
     struct CurGuard { KernelTimer& t; ~CurGuard() { t.cur = nullptr; t.open = -1; } } cg{c.timer};
     c.timer.cur = &tbm;
-    for (int it = 0; tq.D > 0 && it < g.nt; it += tq.D) {
+    for (int it = 0, nd = 0; tq.D > 0 && it < g.nt; it += nd) {
       const bool tm = c.timer.begin(KK_TB_PASS, st, nshots);
-      GJ_TRY(launch_fwd_tb(err, A, B, it, std::min(tq.D, g.nt - it), nshots, tq, dbuf.as<T>(),
-                           jz_out ? jzb.as<T>() : nullptr, st));
+      GJ_TRY(launch_fwd_tb_at(err, A, B, it, nshots, tq, dbuf.as<T>(), jz_out ? jzb.as<T>() : nullptr, st, nd));
       c.timer.end(tm, st);
       c.launches += last_kernels;
       std::swap(A, B);
@@ -1142,9 +1262,9 @@ class WSolver : public WSolverBase {
     Marks tbm;  // per-launch device time when kernel timing is on
     struct CurGuard { KernelTimer& t; ~CurGuard() { t.cur = nullptr; t.open = -1; } } cg{c.timer};
     c.timer.cur = &tbm;
-    for (int it = 0; tq.D > 0 && it < g.nt; it += tq.D) {
+    for (int it = 0, nd = 0; tq.D > 0 && it < g.nt; it += nd) {
       const bool tm = c.timer.begin(KK_TB_PASS, st, nshots);
-      GJ_TRY(launch_fwd_tb(err, A, B, it, std::min(tq.D, g.nt - it), nshots, tq, dbuf.as<T>(), nullptr, st));
+      GJ_TRY(launch_fwd_tb_at(err, A, B, it, nshots, tq, dbuf.as<T>(), nullptr, st, nd));
       c.timer.end(tm, st);
       c.launches += last_kernels;
       std::swap(A, B);

@@ -27,9 +27,11 @@ def _with_receivers(p, extra):
 
 def _extra_nodes(g):
     """Nodes on tile edges of every tile shape (rows 27-34, 55-66, 119-126;
-    columns 27-30, 55-62), in the bottom and side PML, and the four corners."""
+    columns 27-30, 55-62) and on streaming-task row edges (rows 60-66,
+    119-130, 240-250), in the bottom and side PML, and the four corners."""
     pts = [(0, 0), (g.NX, g.NY), (g.NX, 0), (0, g.NY), (g.NX - 3, g.NY // 2), (g.NX // 2, 2), (g.NX // 2, g.NY - 2)]
-    for i in (27, 28, 33, 34, 55, 56, 61, 62, 65, 66, 119, 120, 125, 126):
+    for i in (27, 28, 33, 34, 55, 56, 60, 61, 62, 63, 65, 66, 119, 120, 121, 122, 123, 124, 125, 126, 127, 128, 130,
+              240, 243, 244, 245, 246, 247, 250):
         for j in (27, 28, 29, 30, 55, 56, 61, 62):
             if i < g.NX and j < g.NY:
                 pts.append((i, j))
@@ -49,9 +51,16 @@ def multi_ref():
 
 
 @pytest.fixture(scope="module")
-def oracle_out(oracle, multi_ft, multi_ref):
+def tall_ft():
+    """Tall enough for several FP32 streaming row tasks (128 loaded rows each)."""
+    p = synth.small(m=290, n=100, pml=10, nt=91, free_top=True, seed=43, nsrc=2, nrec=12)
+    return _with_receivers(p, _extra_nodes(p.grid))
+
+
+@pytest.fixture(scope="module")
+def oracle_out(oracle, multi_ft, multi_ref, tall_ft):
     out = {}
-    for name, p in (("ft", multi_ft), ("ref", multi_ref)):
+    for name, p in (("ft", multi_ft), ("ref", multi_ref), ("tall", tall_ft)):
         out[name] = [oracle.forward(p.grid, p.eps0, p.sig0, sh) for sh in p.shots]
     return out
 
@@ -104,6 +113,49 @@ def test_blocked_forward_f32_traces(gpu_ctx, multi_ft, oracle_out, monkeypatch, 
         assert rel_l2(out["d"][k], ring["d"][k]) < 1e-5
 
 
+STREAM = [(D, lc, shape, ss) for D in (1, 2, 3, 4) for lc, shape, ss in ((8, 0, 3), (20, 1, 6), (64, 0, 6))]
+
+
+def _set_stream(monkeypatch, D, lc, shape, ss):
+    _set(monkeypatch, D, shape, 1)
+    monkeypatch.setenv("GJ_TB_STREAM", "1")
+    monkeypatch.setenv("GJ_TB_CHUNK", str(lc))
+    monkeypatch.setenv("GJ_TB_STAGES", str(ss))
+
+
+@pytest.mark.parametrize("D,lc,shape,ss", STREAM)
+@pytest.mark.parametrize("which", ["ft", "ref", "tall"])
+def test_streamed_forward_f64_matches_oracle(gpu_ctx, multi_ft, multi_ref, tall_ft, oracle_out, monkeypatch, D, lc,
+                                             shape, ss, which):
+    """Streaming warp tasks over the interior (k_fwd_tbs, D levels in
+    registers) with clipped tiles around them, FP64 against the oracle."""
+    p = {"ft": multi_ft, "ref": multi_ref, "tall": tall_ft}[which]
+    _set_stream(monkeypatch, D, lc, shape, ss)
+    out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F64, want_jz=True)
+    for k in range(len(p.shots)):
+        d, jz, _ = oracle_out[which][k]
+        assert rel_l2(out["d"][k], d) < 1e-12
+        assert rel_l2(out["jz"][k], jz) < 1e-12
+
+
+@pytest.mark.parametrize("D,lc,shape,ss", STREAM)
+@pytest.mark.parametrize("which", ["ft", "tall"])
+def test_streamed_forward_f32_matches_ring(gpu_ctx, multi_ft, tall_ft, oracle_out, monkeypatch, D, lc, shape, ss,
+                                           which):
+    """FP32 streaming passes (128-row tasks) against the FP64 oracle (1e-5)
+    and the FP32 one-step ring kernels."""
+    p = {"ft": multi_ft, "tall": tall_ft}[which]
+    monkeypatch.setenv("GJ_TB_DEPTH", "0")
+    ring = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F32, want_jz=True)
+    _set_stream(monkeypatch, D, lc, shape, ss)
+    out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F32, want_jz=True)
+    for k in range(len(p.shots)):
+        d, jz, _ = oracle_out[which][k]
+        assert rel_l2(out["d"][k], d) < 1e-5
+        assert rel_l2(out["d"][k], ring["d"][k]) < 1e-5
+        assert rel_l2(out["jz"][k], ring["jz"][k]) < 1e-5
+
+
 def test_blocked_misfit_equals_ring_misfit(gpu_ctx, multi_ft, oracle, monkeypatch):
     p = multi_ft
     dobs = [oracle.forward(p.grid, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
@@ -123,7 +175,7 @@ def test_tuned_forward_matches_oracle(gpu_ctx, multi_ft, oracle_out, monkeypatch
     """No configuration fixed: the tuner picks one (the ring kernels or a
     blocked depth) and the traces still equal the oracle's."""
     p = multi_ft
-    for k in ("GJ_TB_DEPTH", "GJ_TB_SHAPE", "GJ_TB_SPB", "GJ_AUTOTUNE"):
+    for k in ("GJ_TB_DEPTH", "GJ_TB_SHAPE", "GJ_TB_SPB", "GJ_TB_STREAM", "GJ_TB_CHUNK", "GJ_TB_STAGES", "GJ_AUTOTUNE"):
         monkeypatch.delenv(k, raising=False)
     out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F64)
     for k in range(len(p.shots)):
