@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--no-cfg4", action="store_true", help="skip the 48-problem batch leg")
     ap.add_argument("--dc-only", action="store_true", help="only the DC leg (JSON line of its own)")
     ap.add_argument("--dc-sources", type=int, default=200, help="DC sources (x 20 wavenumbers)")
+    ap.add_argument("--forward-only", action="store_true",
+                    help="only the forward leg on --nshots x --nt (JSON line of its own; the profiling case)")
     ap.add_argument("--cfg4", action="store_true",
                     help="the 48 uneven problems instead (one gradient call each, vs plain FP64 on a sample)")
     return ap.parse_args()
@@ -408,6 +410,15 @@ def cfg3_leg(ctx):
             "kernels": per}
 
 
+def _leg(fn, *args):
+    """An extra leg of the bench line; its failure is reported in the line
+    instead of losing the line."""
+    try:
+        return fn(*args)
+    except Exception as e:  # reported, not hidden: the key holds the error
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def _cfg1_worker(k):
     """One shot of the small-size workload's FP64 exact gradient on the oracle
     (one worker process per shot, the reference's parfor)."""
@@ -509,7 +520,7 @@ def forward_leg(ctx, p):
         dev_s = kt["avg_us"] * kt["launches"] / 1e6
         return out, t, launches, kt, dev_s
 
-    os.environ.pop("GJ_TB_DEPTH", None)
+    saved = os.environ.get("GJ_TB_DEPTH")  # a depth fixed by the caller (profiling) stays in force
     out, t, launches, kt, dev_s = timed("tb_pass")
     ns = len(p.shots)
     upd = ns * g.nt * cells
@@ -534,7 +545,10 @@ def forward_leg(ctx, p):
     try:
         out_r, t_r, _, kt_r, dev_r = timed("fwd_step")
     finally:
-        os.environ.pop("GJ_TB_DEPTH", None)
+        if saved is None:
+            os.environ.pop("GJ_TB_DEPTH", None)
+        else:
+            os.environ["GJ_TB_DEPTH"] = saved
     res["ring_one_step_per_launch"] = {"e2e_s": t_r, "device_s": dev_r, "avg_step_us": kt_r["avg_us"],
                                        "gcell_updates_per_s": upd / dev_r / 1e9 if dev_r > 0 else None}
     if kt["launches"] > 0 and dev_r > 0:
@@ -658,6 +672,14 @@ def main():
         return run_reference(args)
     if args.cfg4:
         return cfg4_line()
+    if args.forward_only:
+        from gerjoii_b200 import _native as N
+        p, _ = workload(args)
+        ctx = N.Context(0)
+        print(json.dumps({"metric": "radar forward solve, shot-forwards/s, 1 B200", "forward": forward_leg(ctx, p)}),
+              flush=True)
+        ctx.close()
+        return
     if args.dc_only:
         from gerjoii_b200 import _native as N
         ctx = N.Context(0)
@@ -880,8 +902,8 @@ def main():
         # solve of the oracle on one source
         if not args.no_dc:
             line["dc"] = dc_leg(ctx)
-        line["forward"] = forward_leg(ctx, p)
-        line["cfg1"] = cfg1_leg(ctx)
+        line["forward"] = _leg(forward_leg, ctx, p)
+        line["cfg1"] = _leg(cfg1_leg, ctx)
         line["cfg3"] = cfg3_leg(ctx)
         if not args.no_cfg4:
             line["cfg4"] = cfg4_leg(ctx)
