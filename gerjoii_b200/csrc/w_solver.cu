@@ -757,6 +757,17 @@ class WSolver : public WSolverBase {
   };
   std::map<long, std::unique_ptr<TbTiles>> tb_tiles;
   float tb_us = 0.f;  // tuned time per step (tb_tune), us
+  // A batch of models in one blocked run (misfit_trials): tb_spt shots per
+  // model, the coefficient sets tb_cstride elements apart from tb_w's, cezj per
+  // (model, shot), the states and traces in the batch's own buffers; tb_spt = 0
+  // for the plan's one model.
+  int tb_spt = 0;
+  size_t tb_cstride = 0;
+  const WDev<T>* tb_w = nullptr;
+  const T* tb_cezj = nullptr;
+  DevBuf* tb_sA = nullptr;
+  DevBuf* tb_sB = nullptr;
+  DevBuf* tb_d = nullptr;
   static long tb_key(const TbCfg& q, int gn) {
     return (((((long(q.D) * 8 + q.shape) * 2 + (q.stream ? 1 : 0)) * 1024 + (q.stream ? q.lc : 0)) * 8 +
              (q.stream ? q.ss : 0)) << 24) | long(q.stream ? gn : 0);
@@ -826,8 +837,9 @@ class WSolver : public WSolverBase {
           for (int c0 = cs_lo; c0 <= cs_hi; c0 += q.lc) {
             const int c1 = std::min(c0 + q.lc - 1, cs_hi);
             bool rec = false;  // a receiver of shot z among the task's owned nodes
-            for (int r = 0; r < nrs[z] && !rec; ++r) {
-              const long kk = sh[z].rec[r];
+            const int zs = tb_spt > 0 ? z % tb_spt : z;
+            for (int r = 0; r < nrs[zs] && !rec; ++r) {
+              const long kk = sh[zs].rec[r];
               const int I = int(kk % ld), J = int(kk / ld);
               rec = I >= own[k].first && I < own[k].second && J >= c0 && J <= c1;
             }
@@ -901,6 +913,11 @@ class WSolver : public WSolverBase {
     a.nrr = std::max(nr, 1);
     a.rs = rsbuf.as<int>(); a.nrs = nrsbuf.as<int>();
     a.d = nr > 0 ? d : nullptr; a.jz = jz;
+    a.spt = tb_spt > 0 ? tb_spt : gn;
+    a.cstride = tb_cstride;
+    if (tb_cezj) a.cezj = tb_cezj;
+    if (tb_spt > 0 && a.spt % a.spb != 0) a.spb = 1;  // a tile CTA's shots stay in one model
+    const WDev<T>& wd = tb_w ? *tb_w : w;
     const int gy = (gn + a.spb - 1) / a.spb;
     const int4* tl = tt.buf.template as<int4>();
     const int nth = 32 * TB_WARPS;
@@ -912,12 +929,12 @@ class WSolver : public WSolverBase {
     }
     if (tt.nP > 0)
       tb_kernel<T>(q.D, q.shape, true)<<<dim3(tt.nP, gy), nth, tb_smem(q.shape, true, sizeof(T)), fork ? side : st>>>(
-          w, a, tl + tt.nI);
+          wd, a, tl + tt.nI);
     if (tt.nS > 0)
       tbs_kernel<T>(q.D, q.ss)<<<(tt.nS + TBS_WARPS - 1) / TBS_WARPS, 32 * TBS_WARPS, tbs_smem(q.ss), st>>>(
-          w, a, tt.sbuf.template as<int4>(), tt.nS);
+          wd, a, tt.sbuf.template as<int4>(), tt.nS);
     if (tt.nI > 0)
-      tb_kernel<T>(q.D, q.shape, false)<<<dim3(tt.nI, gy), nth, tb_smem(q.shape, false, sizeof(T)), st>>>(w, a, tl);
+      tb_kernel<T>(q.D, q.shape, false)<<<dim3(tt.nI, gy), nth, tb_smem(q.shape, false, sizeof(T)), st>>>(wd, a, tl);
     if (fork) {
       GJ_CUDA(err, cudaEventRecord(ev_join, side));
       GJ_CUDA(err, cudaStreamWaitEvent(st, ev_join, 0));
@@ -975,9 +992,12 @@ class WSolver : public WSolverBase {
     const int nsteps = 24, trials = 3;
     const char* vb = getenv("GJ_AUTOTUNE_VERBOSE");
     const bool every = vb && atoi(vb) >= 2;
+    DevBuf& sA = tb_sA ? *tb_sA : fwdA;
+    DevBuf& sB = tb_sB ? *tb_sB : fwdB;
+    DevBuf& dB = tb_d ? *tb_d : dbuf;
     auto run = [&](const TbCfg& q) -> gj_status {
-      T* A = fwdA.as<T>() + ld;
-      T* B = fwdB.as<T>() + ld;
+      T* A = sA.as<T>() + ld;
+      T* B = sB.as<T>() + ld;
       for (int it = 0; it < nsteps;) {
         if (q.D == 0) {
           StepArgs<T> a = step_args(A, B, it % g.nt);
@@ -988,7 +1008,7 @@ class WSolver : public WSolverBase {
           ++it;
         } else {
           int nd = 0;
-          GJ_TRY(launch_fwd_tb_at(err, A, B, it % g.nt, gn, q, dbuf.as<T>(), nullptr, st, nd));
+          GJ_TRY(launch_fwd_tb_at(err, A, B, it % g.nt, gn, q, dB.as<T>(), nullptr, st, nd));
           it += nd;
         }
         std::swap(A, B);
@@ -996,8 +1016,8 @@ class WSolver : public WSolverBase {
       return GJ_OK;
     };
     auto time_cfg = [&](const TbCfg& q, float& ms) -> gj_status {
-      GJ_CUDA(err, cudaMemsetAsync(fwdA.p, 0, size_t(gn) * sstride * sizeof(T), st));
-      GJ_CUDA(err, cudaMemsetAsync(fwdB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_CUDA(err, cudaMemsetAsync(sA.p, 0, size_t(gn) * sstride * sizeof(T), st));
+      GJ_CUDA(err, cudaMemsetAsync(sB.p, 0, size_t(gn) * sstride * sizeof(T), st));
       GJ_TRY(run(q));  // warm-up
       for (int trial = 0; trial < trials; ++trial) {
         GJ_CUDA(err, cudaEventRecord(e0, st));
@@ -1015,7 +1035,7 @@ class WSolver : public WSolverBase {
       return GJ_OK;
     };
     std::vector<TbCfg> cands;
-    if (ring_nth > 0) cands.push_back(TbCfg{});
+    if (ring_nth > 0 && tb_spt == 0) cands.push_back(TbCfg{});  // the ring kernels run the plan's model only
     for (int D = 1; D <= 4; ++D)
       for (int sh = 0; sh < TB_NSHAPE; ++sh)
         for (int spb : {1, 2}) {
@@ -1306,6 +1326,119 @@ class WSolver : public WSolverBase {
       misfit_out[q] = hs[2 * q + 1] > 0 ? 0.5 * hs[2 * q] / hs[2 * q + 1] : 0.5 * hs[2 * q];
       nbad += std::isfinite(misfit_out[q]) ? 0 : 1;
     }
+    if (nbad) return err.set(GJ_ENUMERIC, "%d non-finite misfits (outputs written)", nbad);
+    return GJ_OK;
+  }
+
+  // All trial models of one step-length search (w_stepparabola_e.m:20-27) as
+  // one blocked forward run: every pass is one launch over the ntrial x nshots
+  // (model, shot) pairs, each model with its own coefficient set; then the
+  // misfits of each model as misfit() computes them.  done = false (nothing
+  // run) when the configuration for the batch is one step per launch: the
+  // ring kernels run the plan's model only, and the caller then runs the
+  // models one by one.
+  gj_status misfit_trials(Err& err, Ctx& c, int ntrial, const double* eps, const double* sig, const double* dobs,
+                          gj_misfit_kind mk, double* out, cudaStream_t st, const gj_w_opts* opts, bool& done) {
+    done = false;
+    if constexpr (VT<T>::V * sizeof(T) != 16) return GJ_OK;
+    if (ntrial < 2 || ring_nth == 0) return GJ_OK;
+    const int gn = ntrial * nshots;
+    const size_t cset = 12 * fstride;  // elements of one coefficient set
+    const int nrr = std::max(nr, 1);
+    const size_t tr = size_t(nrr) * g.nt;
+    GJ_TRY(stage_inputs(err, c, eps, sig, false, dobs, false, st));  // observed traces (and model 0)
+    ring_on = true;
+    select_cfg(nshots);
+    GJ_TRY(prepare_tasks(err, nshots));
+    DevBuf tcoef, tcz, tA, tB, td, mh;
+    GJ_TRY(tcoef.alloc(err, size_t(ntrial) * cset * sizeof(T)));
+    GJ_TRY(tcz.alloc(err, size_t(gn) * sizeof(T)));
+    GJ_TRY(mh.alloc(err, 2 * mn * sizeof(double)));
+    GJ_CUDA(err, cudaMemsetAsync(tcoef.p, 0, size_t(ntrial) * cset * sizeof(T), st));
+    T* base = tcoef.as<T>() + ld;  // one column in, like the plan's arrays
+    {
+      struct Restore {
+        WSolver& s; WDev<T> w0, wr0;
+        ~Restore() { s.w = w0; s.wr = wr0; }
+      } rs{*this, w, wr};
+      for (int t = 0; t < ntrial; ++t) {
+        GJ_CUDA(err, cudaMemcpyAsync(mh.as<double>(), eps + size_t(t) * mn, mn * sizeof(double),
+                                     cudaMemcpyHostToDevice, st));
+        GJ_CUDA(err, cudaMemcpyAsync(mh.as<double>() + mn, sig + size_t(t) * mn, mn * sizeof(double),
+                                     cudaMemcpyHostToDevice, st));
+        T* cb = base + size_t(t) * cset;
+        w.ce = cb; w.chy = cb + fstride; w.ax = cb + 2 * fstride; w.bx = cb + 3 * fstride;
+        w.ay = cb + 4 * fstride; w.by = cb + 5 * fstride; w.hxa = cb + 6 * fstride; w.hxb = cb + 7 * fstride;
+        w.hya = cb + 8 * fstride; w.hyb = cb + 9 * fstride;
+        wr.ce = cb + 10 * fstride; wr.chy = cb + 11 * fstride;
+        GJ_TRY(build<double>(err, c, mh.as<double>(), mh.as<double>() + mn, st));
+        GJ_CUDA(err, cudaMemcpyAsync(tcz.as<T>() + size_t(t) * nshots, d_cezj, nshots * sizeof(T),
+                                     cudaMemcpyDeviceToDevice, st));
+        // mh is rewritten by the next model: its build must have read it
+        GJ_CUDA(err, cudaStreamSynchronize(st));
+      }
+    }
+    WDev<T> wt = w;  // model 0's arrays; model t's lie t * cset further
+    wt.ce = base; wt.chy = base + fstride; wt.ax = base + 2 * fstride; wt.bx = base + 3 * fstride;
+    wt.ay = base + 4 * fstride; wt.by = base + 5 * fstride; wt.hxa = base + 6 * fstride; wt.hxb = base + 7 * fstride;
+    wt.hya = base + 8 * fstride; wt.hyb = base + 9 * fstride;
+    GJ_TRY(tA.alloc(err, size_t(gn) * sstride * sizeof(T)));
+    GJ_TRY(tB.alloc(err, size_t(gn) * sstride * sizeof(T)));
+    GJ_TRY(td.alloc(err, size_t(gn) * tr * sizeof(T)));
+    struct Batch {
+      WSolver& s;
+      ~Batch() {
+        s.tb_spt = 0; s.tb_cstride = 0; s.tb_w = nullptr; s.tb_cezj = nullptr;
+        s.tb_sA = s.tb_sB = s.tb_d = nullptr;
+      }
+    } bg{*this};
+    tb_spt = nshots; tb_cstride = cset; tb_w = &wt; tb_cezj = tcz.as<T>();
+    tb_sA = &tA; tb_sB = &tB; tb_d = &td;
+    TbCfg tq;
+    GJ_TRY(tb_select(err, gn, st, tq));
+    if (tq.D == 0) return GJ_OK;  // one step per launch: the caller runs the models one by one
+    GJ_CUDA(err, cudaMemsetAsync(tA.p, 0, size_t(gn) * sstride * sizeof(T), st));
+    GJ_CUDA(err, cudaMemsetAsync(tB.p, 0, size_t(gn) * sstride * sizeof(T), st));
+    T* A = tA.as<T>() + ld;
+    T* B = tB.as<T>() + ld;
+    Marks tbm;
+    struct CurGuard { KernelTimer& t; ~CurGuard() { t.cur = nullptr; t.open = -1; } } cg{c.timer};
+    c.timer.cur = &tbm;
+    for (int it = 0, nd = 0; it < g.nt; it += nd) {
+      const bool tm = c.timer.begin(KK_TB_PASS, st, gn);
+      GJ_TRY(launch_fwd_tb_at(err, A, B, it, gn, tq, td.as<T>(), nullptr, st, nd));
+      c.timer.end(tm, st);
+      c.launches += last_kernels;
+      std::swap(A, B);
+    }
+    c.timer.close(st);
+    const bool filt = opts && opts->filt_high > opts->filt_low;
+    if (filt) GJ_TRY(filt_traces(err, c, *opts, dobsbuf.as<T>(), nshots, st));
+    int nbad = 0;
+    std::vector<double> hs(2 * nshots);
+    for (int t = 0; t < ntrial; ++t) {
+      GJ_CUDA(err, cudaMemcpyAsync(dbuf.p, td.as<T>() + size_t(t) * nshots * tr, size_t(nshots) * tr * sizeof(T),
+                                   cudaMemcpyDeviceToDevice, st));
+      GJ_CUDA(err, cudaMemsetAsync(sums.p, 0, 2 * nshots * sizeof(double), st));
+      if (filt) GJ_TRY(filt_traces(err, c, *opts, dbuf.as<T>(), nshots, st));
+      if (mk != GJ_MISFIT_L2) {
+        GJ_TRY(env_residual(err, c, 0, nshots, mk, st));
+      } else {
+        k_residual<T><<<dim3(64, nshots), 256, 0, st>>>(dbuf.as<T>(), dobsbuf.as<T>(), ebuf.as<T>(), tr,
+                                                        sums.as<double>());
+        ++c.launches;
+      }
+      GJ_CUDA(err, cudaGetLastError());
+      GJ_CUDA(err, cudaMemcpyAsync(hs.data(), sums.p, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      GJ_CUDA(err, cudaStreamSynchronize(st));
+      for (int q = 0; q < nshots; ++q) {
+        double& m = out[size_t(t) * nshots + q];
+        m = hs[2 * q + 1] > 0 ? 0.5 * hs[2 * q] / hs[2 * q + 1] : 0.5 * hs[2 * q];
+        nbad += std::isfinite(m) ? 0 : 1;
+      }
+    }
+    c.timer.collect(tbm);
+    done = true;
     if (nbad) return err.set(GJ_ENUMERIC, "%d non-finite misfits (outputs written)", nbad);
     return GJ_OK;
   }
@@ -2337,6 +2470,17 @@ gj_status w_misfit(Ctx& c, const gj_w_grid& g, gj_precision prec, const double* 
   if (mk < GJ_MISFIT_L2 || mk > GJ_MISFIT_ENV_LOG) return c.err.set(GJ_EINVAL, "unknown misfit kind");
   if (ntrial < 1) return c.err.set(GJ_EINVAL, "ntrial must be >= 1");
   const size_t mn = size_t(g.m) * size_t(g.n);
+  if (ntrial > 1) {  // all models in one blocked run when the configuration allows it
+    bool done = false;
+    if (prec == GJ_F64) {
+      WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+      GJ_TRY(s->misfit_trials(c.err, c, ntrial, eps, sig, dobs, mk, misfit_out, 0, opts, done));
+    } else {
+      WSolver<float>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));
+      GJ_TRY(s->misfit_trials(c.err, c, ntrial, eps, sig, dobs, mk, misfit_out, 0, opts, done));
+    }
+    if (done) return GJ_OK;
+  }
   for (int t = 0; t < ntrial; ++t) {
     if (prec == GJ_F64) {
       WSolver<double>* s; GJ_TRY(get_solver(c, g, shots, nshots, s));

@@ -39,16 +39,21 @@ struct TbArgs {
   int gn;                // shots in the launch
   int spb;               // shots per CTA (consecutive shots; the coefficients stay in registers)
   int it, nd;            // first step of the pass and steps in it (1..D)
-  const long* src;       // per shot (absolute index) linear source node or -1
-  const T* cezj;         // per shot
-  const T* wav;          // [shot][nt]
+  const long* src;       // per shot (shot0 + zl % spt) linear source node or -1
+  const T* cezj;         // per launch shot (shot0 + zl)
+  const T* wav;          // [shot][nt] (shot0 + zl % spt)
   int nt;
   int shot0;             // absolute index of the launch's first shot (source tables)
-  const int* rs;         // per shot of the launch: nrr x {column J, row I, receiver r}, sorted by column
-  const int* nrs;        // per shot of the launch: receivers
+  const int* rs;         // per shot (zl % spt): nrr x {column J, row I, receiver r}, sorted by column
+  const int* nrs;        // per shot (zl % spt): receivers
   int nrr;
   T* d;                  // traces of the launch's shots, [shot][nrr][nt], or nullptr
   T* jz;                 // Ez at the source node, [shot][nt], or nullptr
+  // batches of models (the trial models of a step-length search): launch shot
+  // zl is shot zl % spt of model zl / spt, whose coefficient arrays lie
+  // (zl / spt) * cstride elements after the WDev ones; cezj is per launch shot
+  int spt;
+  size_t cstride;
 };
 
 // Tile (int4): owned rows [x, x + z), owned columns [y, y + w), z <= TR and
@@ -78,6 +83,8 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
   const size_t fs = a.fstride;
   const int row = 32 * (wid % G) + lane, col0 = wid / G;
   const int i = r0 - D + row;
+  // coefficients of the CTA's model (the host keeps a CTA's shots in one model)
+  const size_t co = size_t(blockIdx.y * a.spb / a.spt) * a.cstride;
   // row classes (fixed for the pass)
   const bool rIn = i >= 0 && i <= NX;
   const bool rHy = i >= 0 && i <= NX - 1 && row < RR - 1;
@@ -115,8 +122,8 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
       rce[q] = T(0); rch[q] = T(0);
       if ((cls(q) & 12u) == 12u) {
         const size_t kk = nidx(i, c0 - D + col0 + CS * q, ld);
-        rce[q] = __ldg(w.ce + kk);
-        rch[q] = __ldg(w.chy + kk);
+        rce[q] = __ldg(w.ce + co + kk);
+        rch[q] = __ldg(w.chy + co + kk);
       }
     }
   }
@@ -136,18 +143,19 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
       if (!(c & 64u)) continue;
       const size_t kk = nidx(i, c0 - D + col0 + CS * q, ld);
       if (c & 4u) {
-        if (c & 8u) { kA[q] = __ldg(w.ce + kk); kB[q] = __ldg(w.chy + kk); }
-        else { kA[q] = __ldg(w.ax + kk); kB[q] = __ldg(w.bx + kk); kC[q] = __ldg(w.ay + kk); kD[q] = __ldg(w.by + kk); }
+        if (c & 8u) { kA[q] = __ldg(w.ce + co + kk); kB[q] = __ldg(w.chy + co + kk); }
+        else { kA[q] = __ldg(w.ax + co + kk); kB[q] = __ldg(w.bx + co + kk); kC[q] = __ldg(w.ay + co + kk); kD[q] = __ldg(w.by + co + kk); }
       }
-      if ((c & 1u) && !(c & 16u)) { kXa[q] = __ldg(w.hxa + kk); kXb[q] = __ldg(w.hxb + kk); }
-      if ((c & 2u) && !rHyInt) { kYa[q] = __ldg(w.hya + kk); kYb[q] = __ldg(w.hyb + kk); }
+      if ((c & 1u) && !(c & 16u)) { kXa[q] = __ldg(w.hxa + co + kk); kXb[q] = __ldg(w.hxb + co + kk); }
+      if ((c & 2u) && !rHyInt) { kYa[q] = __ldg(w.hya + co + kk); kYb[q] = __ldg(w.hyb + co + kk); }
     }
   }
 
   for (int z = 0; z < a.spb; ++z) {
     const int zl = blockIdx.y * a.spb + z;
     if (zl >= a.gn) break;  // uniform over the CTA
-    const int s = a.shot0 + zl;
+    const int sp = zl % a.spt;  // shot of the model
+    const int s = a.shot0 + sp;
     const size_t off = size_t(zl) * a.sstride;
     const T* EzA = a.A + off;
     T* EzB = a.B + off;
@@ -168,12 +176,12 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
     }
     const long src = a.src[s];
     const int srcI = src >= 0 ? int(src % ld) : -1, srcJ = src >= 0 ? int(src / ld) : -1;
-    const T cz = src >= 0 ? a.cezj[s] : T(0);
+    const T cz = src >= 0 ? a.cezj[a.shot0 + zl] : T(0);
     // receivers of this shot whose column lies in the owned columns
     int rlo = 0, rhi = 0;
-    const int* rsz = a.rs + size_t(zl) * a.nrr * 3;
+    const int* rsz = a.rs + size_t(sp) * a.nrr * 3;
     if (a.d) {
-      const int n = a.nrs[zl];
+      const int n = a.nrs[sp];
       int lo = 0, hi = n;
       while (lo < hi) { const int mid = (lo + hi) >> 1; if (rsz[3 * mid] < c0) lo = mid + 1; else hi = mid; }
       rlo = lo; hi = n;
@@ -211,7 +219,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
           if (CACHE) { ha = kXa[CACHE ? q : 0]; hb = kXb[CACHE ? q : 0]; }
           else if (PML && !(c & 16u)) {
             const size_t kk = nidx(i, c0 - D + col, ld);
-            ha = __ldg(w.hxa + kk); hb = __ldg(w.hxb + kk);
+            ha = __ldg(w.hxa + co + kk); hb = __ldg(w.hxb + co + kk);
           }
           sHx[p] = ha * sHx[p] + hb * (sEz[p + RR] - ez);
         }
@@ -220,7 +228,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
           if (CACHE) { ha = kYa[CACHE ? q : 0]; hb = kYb[CACHE ? q : 0]; }
           else if (PML && !rHyInt) {
             const size_t kk = nidx(i, c0 - D + col, ld);
-            ha = __ldg(w.hya + kk); hb = __ldg(w.hyb + kk);
+            ha = __ldg(w.hya + co + kk); hb = __ldg(w.hyb + co + kk);
           }
           sHy[p] = ha * sHy[p] + hb * (sEz[p + 1] - ez);
         }
@@ -242,7 +250,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
           if (CACHE) { ce = kA[CACHE ? q : 0]; ch = kB[CACHE ? q : 0]; }
           else if (PML) {
             const size_t kk = nidx(i, j, ld);
-            ce = __ldg(w.ce + kk); ch = __ldg(w.chy + kk);
+            ce = __ldg(w.ce + co + kk); ch = __ldg(w.chy + co + kk);
           }
           e = ce * sEz[p] + ch * dhy + (rxy * ch) * dhx;
           if (srcRow && j == srcJ) e += sval;
@@ -251,7 +259,7 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
           if (CACHE) { ax_ = kA[CACHE ? q : 0]; bx_ = kB[CACHE ? q : 0]; ay_ = kC[CACHE ? q : 0]; by_ = kD[CACHE ? q : 0]; }
           else {
             const size_t kk = nidx(i, j, ld);
-            ax_ = __ldg(w.ax + kk); bx_ = __ldg(w.bx + kk); ay_ = __ldg(w.ay + kk); by_ = __ldg(w.by + kk);
+            ax_ = __ldg(w.ax + co + kk); bx_ = __ldg(w.bx + co + kk); ay_ = __ldg(w.ay + co + kk); by_ = __ldg(w.by + co + kk);
           }
           const T ex = ax_ * sEx[p] + bx_ * dhy;
           const T ey = ay_ * sEy[p] + by_ * dhx;
@@ -321,6 +329,8 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
   if (t >= ntask) return;  // whole warp; no CTA barrier in this kernel
   const int4 tk = tasks[t];
   const int R = tk.x, c0 = tk.y & 0xffff, c1 = tk.y >> 16, zl = tk.w & (TBS_HAS_REC - 1);
+  const int sp = zl % a.spt;                           // shot of the model
+  const size_t co = size_t(zl / a.spt) * a.cstride;    // coefficients of the model
   const int ld = w.ld;
   const int I0 = R + lane * V;
   const bool upl = lane == 0, dnl = lane == 31;
@@ -332,7 +342,7 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
   T* HxB = EzB + fs;
   T* HyB = EzB + 2 * fs;
   uint4* ring = tbs_ring + size_t(wib) * S * STAGE;
-  const int s = a.shot0 + zl;
+  const int s = a.shot0 + sp;
   const int own_lo = tk.z & 0xffff, own_hi = tk.z >> 16;
   unsigned own = 0;
 #pragma unroll
@@ -343,7 +353,7 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
   const bool srcLane = srcI >= I0 && srcI < I0 + V;
   T sv[D];
 #pragma unroll
-  for (int d = 0; d < D; ++d) sv[d] = srcLane ? a.cezj[s] * a.wav[size_t(s) * a.nt + a.it + d] : T(0);
+  for (int d = 0; d < D; ++d) sv[d] = srcLane ? a.cezj[a.shot0 + zl] * a.wav[size_t(s) * a.nt + a.it + d] : T(0);
   const T chx = w.chxez, chy = w.chyez, rxy = w.rxy;
   const int Js = c0 - D + 1, Je = c1 + D - 1;
   auto issue = [&](int J, int stg) {
@@ -353,8 +363,8 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
     cp16(L + RF_EZN * 32, EzA + k + ld);
     cp16(L + RF_HX * 32, HxA + k);
     cp16(L + RF_HY * 32, HyA + k);
-    cp16(L + RF_CE * 32, w.ce + k);
-    cp16(L + RF_CH * 32, w.chy + k);
+    cp16(L + RF_CE * 32, w.ce + co + k);
+    cp16(L + RF_CH * 32, w.chy + co + k);
     uint4* H = Rg + SLOTS * 32;
     if (dnl) cp16(H + HF_EZDN, EzA + nidx(I0 + V, J, ld));
     if (upl && I0 >= 1) {
@@ -391,8 +401,8 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
   // shot's column-sorted list from the first one at a column >= c0, lane q
   // holding entry q; per level the index of its next receiver and that
   // receiver's column (entries past the window are read from global memory)
-  const int* rsl = a.rs + size_t(zl) * 3 * a.nrr;
-  const int rn = (a.d && (tk.w & TBS_HAS_REC)) ? a.nrs[zl] : 0;
+  const int* rsl = a.rs + size_t(sp) * 3 * a.nrr;
+  const int rn = (a.d && (tk.w & TBS_HAS_REC)) ? a.nrs[sp] : 0;
   const int rp0 = rn ? rec_first(rsl, rn, c0) : 0;
   int wJ = 0x7fffffff, wI = 0, wR = 0;
   if (rp0 + lane < rn) { wJ = rsl[3 * (rp0 + lane)]; wI = rsl[3 * (rp0 + lane) + 1]; wR = rsl[3 * (rp0 + lane) + 2]; }

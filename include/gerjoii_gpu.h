@@ -199,7 +199,11 @@ gj_status gj_w_misfit(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision
  *                  exponent filt_steep, 0 = 8), as w_objs_e.m:33-36 does with
  *                  regu.f_ and regu.f__; the misfit and its d_o'd_o normaliser
  *                  are then those of the filtered traces
- *   misfit_out   : ntrial x nshots misfits, trial-major */
+ *   misfit_out   : ntrial x nshots misfits, trial-major
+ * With ntrial > 1 all models run as one temporally blocked forward run: each
+ * pass is one launch per kernel kind over every (model, shot) pair, each model
+ * with its own coefficient set (unless GJ_TB_DEPTH=0 fixes one step per
+ * launch, which runs the models one by one). */
 gj_status gj_w_misfit_trials(gj_ctx* ctx, const gj_w_grid* grid, gj_precision precision, int ntrial,
                              const double* eps_r, const double* sigma, const gj_w_shot* shots, int nshots,
                              const double* d_obs, gj_misfit_kind misfit, const gj_w_opts* opts,

@@ -394,7 +394,8 @@ def test_misfit_trials_batched_and_band_filtered(gpu_ctx, oracle, small_ft, prec
     assert many.shape == (3, len(p.shots))
     for t, eps in enumerate(models):
         one = gpu_ctx.w_misfit_trials(g, [eps], [p.sig0], p.shots, dobs, precision=prec, filt=band)
-        assert np.allclose(one[0], many[t], rtol=1e-12)
+        # FP32: the batch and the single call may run different kernels (tuned apart)
+        assert np.allclose(one[0], many[t], rtol=1e-12 if prec == N.GJ_F64 else 1e-5)
         for k, sh in enumerate(p.shots):
             d, _, _ = oracle.forward(g, eps, p.sig0, sh)
             fd = npo.filt_gauss(d, g.dt, band[0], band[1], 8)
@@ -402,4 +403,5 @@ def test_misfit_trials_batched_and_band_filtered(gpu_ctx, oracle, small_ft, prec
             ref = 0.5 * np.sum((fd - fo) ** 2) / np.sum(fo ** 2)
             assert abs(many[t, k] - ref) <= tol * ref
     plain = gpu_ctx.w_misfit_trials(g, models, sigs, p.shots, dobs, precision=prec)
-    assert np.allclose(plain[1], gpu_ctx.w_misfit(g, models[1], p.sig0, p.shots, dobs, precision=prec), rtol=1e-12)
+    assert np.allclose(plain[1], gpu_ctx.w_misfit(g, models[1], p.sig0, p.shots, dobs, precision=prec),
+                       rtol=1e-12 if prec == N.GJ_F64 else 1e-5)

@@ -171,6 +171,36 @@ def test_blocked_misfit_equals_ring_misfit(gpu_ctx, multi_ft, oracle, monkeypatc
         assert np.all(trials[1] < 1e-20)
 
 
+@pytest.mark.parametrize("misfit,band", [("L2", None), ("env_L2", None), ("L2", (80e6, 500e6))])
+@pytest.mark.parametrize("cfg", [(3, 16, 0, 3, 2), (2, 0, 1, 0, 1)])
+def test_trial_models_in_one_blocked_run(gpu_ctx, multi_ft, oracle, monkeypatch, misfit, band, cfg):
+    """gj_w_misfit_trials with three models: one blocked run whose every pass
+    is one launch over the 3 x 3 (model, shot) pairs, each model with its own
+    coefficient set, equals the models run one by one with one step per
+    launch (FP64, 1e-11), band-filtered and envelope objectives included."""
+    p = multi_ft
+    g = p.grid
+    dobs = [oracle.forward(g, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
+    models = [p.eps0 * f for f in (0.95, 1.0, 1.05)]
+    sigs = [p.sig0 * f for f in (1.0, 1.2, 0.8)]
+    monkeypatch.setenv("GJ_TB_DEPTH", "0")
+    ref = np.stack([gpu_ctx.w_misfit_trials(g, [e], [s_], p.shots, dobs, misfit=misfit, precision=N.GJ_F64,
+                                            filt=band)[0] for e, s_ in zip(models, sigs)])
+    D, lc, shape, ss, stream = cfg
+    _set(monkeypatch, D, shape, 2)
+    monkeypatch.setenv("GJ_TB_STREAM", str(stream))
+    monkeypatch.setenv("GJ_TB_CHUNK", str(max(lc, 4)))
+    monkeypatch.setenv("GJ_TB_STAGES", str(max(ss, 3)))
+    got = gpu_ctx.w_misfit_trials(g, models, sigs, p.shots, dobs, misfit=misfit, precision=N.GJ_F64, filt=band)
+    launches = gpu_ctx.last_launch_count
+    assert got.shape == (3, len(p.shots))
+    assert np.allclose(got, ref, rtol=1e-11, atol=0)
+    # at most three launches per pass for all three models together (three
+    # models run one by one would take at least six per pass)
+    passes = -(-g.nt // D)
+    assert launches < 5 * passes
+
+
 def test_tuned_forward_matches_oracle(gpu_ctx, multi_ft, oracle_out, monkeypatch):
     """No configuration fixed: the tuner picks one (the ring kernels or a
     blocked depth) and the traces still equal the oracle's."""
