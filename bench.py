@@ -537,6 +537,10 @@ def forward_leg(ctx, p):
             "roofline": {"bound": "hbm", "achieved": b / (kt["avg_us"] / 1e6) / 1e9, "peak": pk["hbm_gbs"],
                          "unit": "GB/s", "frac": b / (kt["avg_us"] / 1e6) / 1e9 / pk["hbm_gbs"],
                          "peak_source": pk_src, "algorithmic_bytes_per_pass": b,
+                         # DRAM bytes per pass from the ncu capture of a 3-step pass, scaled per shot-cell
+                         "traffic": (traffic_per_unit("k_fwd_tb+k_fwd_tbs<float,3>") * ns * cells
+                                     if round(steps_per_pass) == 3 and traffic_per_unit("k_fwd_tb+k_fwd_tbs<float,3>")
+                                     else None),
                          "step_equivalent_gbs": steps_per_pass * b / (kt["avg_us"] / 1e6) / 1e9,
                          "units": "per shot and pass: 32 B x NX*NY (state once in and out, Ceze/Cezhy) + 16 B x "
                                   "PML band nodes; step_equivalent: the bytes one-step-per-launch kernels move "
