@@ -1346,6 +1346,12 @@ class WSolver : public WSolverBase {
     const size_t cset = 12 * fstride;  // elements of one coefficient set
     const int nrr = std::max(nr, 1);
     const size_t tr = size_t(nrr) * g.nt;
+    {  // the batch's states, traces and coefficient sets must fit; else one model at a time
+      size_t fr = 0, tot = 0;
+      GJ_CUDA(err, cudaMemGetInfo(&fr, &tot));
+      const size_t need = (size_t(gn) * (2 * sstride + tr) + size_t(ntrial) * cset) * sizeof(T);
+      if (need > fr / 10 * 8) return GJ_OK;
+    }
     GJ_TRY(stage_inputs(err, c, eps, sig, false, dobs, false, st));  // observed traces (and model 0)
     ring_on = true;
     select_cfg(nshots);
