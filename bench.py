@@ -764,8 +764,11 @@ def main():
     for _ in range(isteps):
         step()
     torch.cuda.synchronize()
-    ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step", "image")}
+    ktimes = {k: ctx.kernel_time(k) for k in ("fwd_step", "ref_step", "adj_step", "image", "tb_pass")}
     ktimes = {k: v for k, v in ktimes.items() if v["launches"] > 0}
+    # a temporally blocked forward (whole history kept) runs every step of every
+    # shot in passes of several steps: its shot-steps are the acquisition's
+    tb_steps = args.nshots * g.nt * isteps if "tb_pass" in ktimes else 0
     ctx.set_kernel_timing(False)
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -778,7 +781,8 @@ def main():
     bnodes, bsz = band_counts(g)
     # cell-updates in the timed region: every forward, recompute and adjoint
     # launch (counted per step in the instrumented pass, which runs the same plan)
-    upd = sum(ktimes[k]["shot_launches"] for k in ktimes if k != "image") / isteps * args.steps * cells * world
+    upd = ((sum(ktimes[k]["shot_launches"] for k in ktimes if k not in ("image", "tb_pass")) + tb_steps) / isteps
+           * args.steps * cells * world)
     gcell = upd / (ms / 1e3) / 1e9
     # Algorithmic DRAM bytes of each kernel kind over the timed region.
     #  fwd_step (k_fwdw): read Ez, Hx, Hy, Ceze, Cezhy + write Ez, Hx, Hy = 32 B per
@@ -802,11 +806,14 @@ def main():
         "adj_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 4.0 + bnodes * 16.0 + bz * 4.0),
         "image": lambda k: adj_sl * (mn + bz) * 8.0 + k["shot_launches"] * (mn * 36.0 + bz * 20.0),
         "ref_step": lambda k: k["shot_launches"] * (cells * 32.0 + mn * 48.0),
+        # per shot and pass the state once in and out with Ceze/Cezhy, the split
+        # fields of the band; per shot-step the history and band-history writes
+        "tb_pass": lambda k: k["shot_launches"] * (cells * 32.0 + bnodes * 16.0) + tb_steps * (mn * 4.0 + bz * 4.0),
     }
     # (a forward or adjoint "launch" is one step: the fast-only and the general
     # ring kernel of that step together)
     kname = {"fwd_step": "k_fwdw<float,2>", "adj_step": "k_adjw<float,2>", "image": "k_image<float>",
-             "ref_step": "k_stepv<float,1>"}
+             "ref_step": "k_stepv<float,1>", "tb_pass": "k_fwd_tb+k_fwd_tbs<float,3>"}
     pk, pk_src = peaks()
     kern = {}
     for kk, kt in ktimes.items():
@@ -834,7 +841,9 @@ def main():
                                   "x PML band nodes + 4 B x band-frame entries (adjoint band ring)",
                       "image": "per imaged shot-step 8 B x (m*n + band-frame entries), per shot-launch 36 B x m*n + "
                                "20 B x band-frame entries",
-                      "ref_step": "per shot: 32 B x NX*NY cells + 48 B x m*n (4 history reads, 4 sums r/w)"}[dom],
+                      "ref_step": "per shot: 32 B x NX*NY cells + 48 B x m*n (4 history reads, 4 sums r/w)",
+                      "tb_pass": "per shot and pass (several steps): 32 B x NX*NY + 16 B x PML band nodes; per shot-step "
+                                 "4 B x m*n history + 4 B x band-frame entries"}[dom],
             "kernel_share_of_step": kt["avg_us"] * kt["launches"] / 1e3 / isteps / (ms / args.steps),
             "pass": "separate instrumented step after the timed region (CUDA events around runs of 8 consecutive "
                     "launches of each step kernel, one run per 16 launches, also inside the graphs; runs that the "

@@ -749,6 +749,9 @@ class WSolver : public WSolverBase {
     }
   };
   std::map<int, TbCfg> tb_tuned;
+  // the gradient's forward with the whole history kept: blocked passes per
+  // launch size when the tuner chose them (GJ_TB_GRAD=0: one step per launch)
+  std::map<int, TbCfg> tb_grad;
   // Partition of one pass: tiles (interior tiles first, then PML tiles) and,
   // in streaming mode, the streaming tasks of gn shots.
   struct TbTiles {
@@ -822,6 +825,13 @@ class WSolver : public WSolverBase {
           own.push_back({own.back().second, Rx + RW - D + 1});
         }
       }
+      // rows from bR0 down belong to the band frame of the exact adjoint, whose
+      // history the tiles write: the streamed rows stop above it
+      while (!own.empty() && own.back().second > w.bR0) {
+        own.back().second = w.bR0;
+        if (own.back().second <= own.back().first) { own.pop_back(); Rs.pop_back(); }
+        else break;
+      }
       cs_lo = w.ej0 + D - 1;
       cs_hi = w.ej1 - D + 1;
       if (Rs.empty() || cs_hi - cs_lo + 1 < 1 || NY >= 65536 || NX >= 65536) {
@@ -831,20 +841,25 @@ class WSolver : public WSolverBase {
         rs_lo = own.front().first;
         rs_hi = own.back().second;
       }
+      // per (row task, chunk): a receiver of any shot among its owned nodes (so
+      // the table serves every shot group of the same size)
+      const int nch = (cs_hi - cs_lo + q.lc) / q.lc;
+      std::vector<char> recf(Rs.size() * std::max(nch, 0), 0);
+      for (int zs = 0; zs < nshots; ++zs)
+        for (int r = 0; r < nrs[zs]; ++r) {
+          const long kk = sh[zs].rec[r];
+          const int I = int(kk % ld), J = int(kk / ld);
+          if (J < cs_lo || J > cs_hi) continue;
+          for (size_t k = 0; k < Rs.size(); ++k)
+            if (I >= own[k].first && I < own[k].second) recf[k * nch + (J - cs_lo) / q.lc] = 1;
+        }
       std::vector<int4> ts;
       for (int z = 0; z < gn; ++z)
         for (size_t k = 0; k < Rs.size(); ++k)
-          for (int c0 = cs_lo; c0 <= cs_hi; c0 += q.lc) {
+          for (int c0 = cs_lo, ch = 0; c0 <= cs_hi; c0 += q.lc, ++ch) {
             const int c1 = std::min(c0 + q.lc - 1, cs_hi);
-            bool rec = false;  // a receiver of shot z among the task's owned nodes
-            const int zs = tb_spt > 0 ? z % tb_spt : z;
-            for (int r = 0; r < nrs[zs] && !rec; ++r) {
-              const long kk = sh[zs].rec[r];
-              const int I = int(kk % ld), J = int(kk / ld);
-              rec = I >= own[k].first && I < own[k].second && J >= c0 && J <= c1;
-            }
             ts.push_back(make_int4(Rs[k], c0 | (c1 << 16), own[k].first | (own[k].second << 16),
-                                   z | (rec ? TBS_HAS_REC : 0)));
+                                   z | (recf[k * nch + ch] ? TBS_HAS_REC : 0)));
           }
       tt->nS = int(ts.size());
       if (tt->nS) {
@@ -903,15 +918,18 @@ class WSolver : public WSolverBase {
   // steps into d ([shot][nrr][nt]) and Jz into jz when given.  PML tiles on
   // the side stream; streaming tasks and interior tiles on st.
   gj_status launch_fwd_tb(Err& err, const T* A, T* B, int it, int gn, const TbCfg& q, T* d, T* jz,
-                          cudaStream_t st) {
+                          cudaStream_t st, int shot0 = 0, T* hist = nullptr, size_t hslot = 0, T* band = nullptr,
+                          size_t bslot = 0) {
     if (q.D < 1 || q.D > 4 || it + q.D > g.nt) return err.set(GJ_EINVAL, "blocked pass of %d steps at %d", q.D, it);
     GJ_TRY(tb_prepare(err, q, gn));
     const TbTiles& tt = *tb_tiles.at(tb_key(q, gn));
     TbArgs<T> a{};
     a.A = A; a.B = B; a.fstride = fstride; a.sstride = sstride; a.gn = gn; a.spb = std::max(q.spb, 1);
-    a.it = it; a.nd = q.D; a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.shot0 = 0;
+    a.it = it; a.nd = q.D; a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.shot0 = shot0;
     a.nrr = std::max(nr, 1);
-    a.rs = rsbuf.as<int>(); a.nrs = nrsbuf.as<int>();
+    a.rs = rsbuf.as<int>() + size_t(shot0) * a.nrr * 3; a.nrs = nrsbuf.as<int>() + shot0;
+    a.hist = hist; a.hstride = dn; a.hslot = hslot;
+    a.band = band; a.bslot = bslot;
     a.d = nr > 0 ? d : nullptr; a.jz = jz;
     a.spt = tb_spt > 0 ? tb_spt : gn;
     a.cstride = tb_cstride;
@@ -1839,7 +1857,26 @@ class WSolver : public WSolverBase {
     if (full) GJ_CUDA(err, cudaMemsetAsync(H, 0, gn * hs * sizeof(T), st));  // slot 0 = zero state
     if (full && band_on) GJ_CUDA(err, cudaMemsetAsync(BH, 0, gn * size_t(w.bsz) * sizeof(T), st));
     size_t segi = 0;
-    for (int it = 0; it < nt; ++it) {
+    // whole history kept and blocked passes chosen: D steps per launch, the
+    // history and band history of every step written by the pass
+    const TbCfg* tgc = nullptr;
+    if (full && ring_on) {
+      auto itg = tb_grad.find(gn);
+      if (itg != tb_grad.end() && itg->second.D > 0) tgc = &itg->second;
+    }
+    for (int it = 0, nd = 0; tgc && it < nt; it += nd) {
+      TbCfg qq = *tgc;
+      qq.D = std::min(tgc->D, nt - it);
+      nd = qq.D;
+      if (!tb_tiles.count(tb_key(qq, gn))) return err.set(GJ_ECUDA, "blocked pass tables were not prepared");
+      const bool tm = c.timer.begin(KK_TB_PASS, st, gn);
+      GJ_TRY(launch_fwd_tb(err, A, B, it, gn, qq, nr > 0 ? dgrp : nullptr, nullptr, st, g0, slot_ptr(it + 1, 0),
+                           size_t(gn) * hs, band_on ? bslot(it + 1, 0) : nullptr, size_t(gn) * size_t(w.bsz)));
+      c.timer.end(tm, st);
+      nl += last_kernels;
+      std::swap(A, B);
+    }
+    for (int it = 0; !tgc && it < nt; ++it) {
       if (!full && segi < segs.size() && it == segs[segi].first) {
         GJ_CUDA(err, cudaMemcpyAsync(ckpt.as<T>() + segi * gn * sstride, A - ld, gn * sstride * sizeof(T),
                                      cudaMemcpyDeviceToDevice, st));
@@ -2069,6 +2106,23 @@ class WSolver : public WSolverBase {
       GJ_TRY(autotune(err, G, st));
       if (nshots % G) GJ_TRY(autotune(err, nshots % G, st));
     }
+    const std::map<int, TbCfg> tb_prev = tb_grad;
+    tb_grad.clear();
+    const char* tg = getenv("GJ_TB_GRAD");
+    if (ring_on && full && !(tg && atoi(tg) == 0)) {
+      // tuned (and the pass tables built) here, outside any graph capture
+      for (int gn : {G, nshots % G}) {
+        if (gn < 1 || tb_grad.count(gn)) continue;
+        TbCfg q;
+        GJ_TRY(tb_select(err, gn, st, q));
+        if (q.D > 0) {
+          GJ_TRY(tb_prepare(err, q, gn));
+          if (g.nt % q.D) { TbCfg r = q; r.D = g.nt % q.D; GJ_TRY(tb_prepare(err, r, gn)); }
+        }
+        tb_grad[gn] = q;
+      }
+    }
+    if (!(tb_grad == tb_prev)) drop_graphs();  // captured forwards of another pass configuration
     segs_ = segs;
     full_ = full;
     return GJ_OK;

@@ -26,6 +26,7 @@
 // in L2).  The arithmetic is k_step's, node for node.
 #pragma once
 #include "w_kernels_ring.cuh"
+#include "w_band.cuh"
 
 namespace gj {
 
@@ -54,6 +55,12 @@ struct TbArgs {
   // (zl / spt) * cstride elements after the WDev ones; cezj is per launch shot
   int spt;
   size_t cstride;
+  // gradient forward: the u history (domain-node layout, per shot hstride;
+  // step it + d's slot at hist + d hslot) and the band history of the exact
+  // adjoint (band frame, per shot w.bsz; step it + d's slot at band + d
+  // bslot), the slots of step it + 1 given; nullptr when not kept
+  T* hist; size_t hstride, hslot;
+  T* band; size_t bslot;
 };
 
 // Tile (int4): owned rows [x, x + z), owned columns [y, y + w), z <= TR and
@@ -278,6 +285,42 @@ __global__ void __launch_bounds__(32 * TB_WARPS, 2) k_fwd_tb(const WDev<T> w, co
       }
       if (a.jz && ownSrc && threadIdx.x == 0)
         a.jz[size_t(zl) * a.nt + itd] = sEz[(srcJ - c0 + D) * RR + (srcI - r0 + D)];
+      // u history and band history of the step (owned nodes; as the ring kernels write them)
+      if (a.hist || a.band) {
+        const bool hrow = a.hist && drow(w, i);
+        const bool brow = a.band && i < w.bRB;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          if (!(cls(q) & 128u)) continue;
+          const int col = col0 + CS * q, j = c0 - D + col;
+          const int p = col * RR + row;
+          if (hrow && j >= w.dj0 && j < w.dj0 + w.n)
+            a.hist[size_t(d) * a.hslot + size_t(zl) * a.hstride + dnode(w, i, j)] = sEz[p];
+          if (brow) {
+            T* bs = a.band + size_t(d) * a.bslot + size_t(zl) * w.bsz;
+            const long oe = band_off_e(w, i, j, 0);
+            if (oe >= 0) {
+              const bool bn = PML && ez_bandnode(w, i, j);
+              bs[oe] = bn ? sEx[p] : T(0);
+              bs[oe + (i >= w.bR0 ? w.bBsz : w.bLsz)] = bn ? sEy[p] : T(0);
+            }
+            const long ox = band_off_hx(w, i, j);
+            if (ox >= 0) bs[ox] = sHx[p];
+            const long oy = band_off_hy(w, i, j);
+            if (oy >= 0) bs[oy] = sHy[p];
+            if (i == NX) {  // the frame's rows below the grid hold zeros (no tile owns them)
+              for (int r2 = NX + 1; r2 < w.bRB; ++r2) {
+                const long o2 = band_off_e(w, r2, j, 0);
+                if (o2 >= 0) { bs[o2] = T(0); bs[o2 + (r2 >= w.bR0 ? w.bBsz : w.bLsz)] = T(0); }
+                const long x2 = band_off_hx(w, r2, j);
+                if (x2 >= 0) bs[x2] = T(0);
+                const long y2 = band_off_hy(w, r2, j);
+                if (y2 >= 0) bs[y2] = T(0);
+              }
+            }
+          }
+        }
+      }
     }
     // owned tile at level n + nd
 #pragma unroll
@@ -435,6 +478,19 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
       a.jz[size_t(zl) * a.nt + a.it + d] = val;
     }
   };
+  // u history of level d at column K (owned rows; the layout's rows as the ring kernels write them)
+  const bool hlane = a.hist && own && drow(w, I0);
+  auto hist_store = [&](int d, int K, const T (&E)[V]) {
+    if (!hlane || K < c0 || K > c1 || K < w.dj0 || K >= w.dj0 + w.n) return;
+    T* hp = a.hist + size_t(d) * a.hslot + size_t(zl) * a.hstride + dnode(w, I0, K);
+    if (own == (1u << V) - 1u) {
+      vst(hp, E);
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        if ((own >> v) & 1u) hp[v] = E[v];
+    }
+  };
   for (int J = Js; J <= Je; ++J) {
     const int it = J - Js;
     if (J + S - 1 <= Je) issue(J + S - 1, (it + S - 1) % S);
@@ -474,6 +530,7 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
           if (srcI == I0 + v) E[v] += sv[0];
       }
       record(0, J, E);
+      hist_store(0, J, E);
 #pragma unroll
       for (int v = 0; v < V; ++v) { hx1[v] = HX[v]; ez_c[v] = ez_n[v]; }
     }
@@ -504,6 +561,7 @@ __global__ void __launch_bounds__(32 * TBS_WARPS) k_fwd_tbs(const WDev<T> w, con
           if (srcI == I0 + v) E2[v] += sv[d];
       }
       record(d, K, E2);
+      hist_store(d, K, E2);
 #pragma unroll
       for (int v = 0; v < V; ++v) {
         hxp[d][v] = HX2[v];

@@ -58,10 +58,12 @@ def test_ring_exact_gradient_matches_oracle(gpu_ctx, oracle, tall, ckpt):
     o.ckpt_every = ckpt
     res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F64, opts=o)
     # the eps imaging sums l (E^k - E^{k-1}): cancellation between consecutive
-    # fields puts the FP64 agreement near 1e-10 on this 150-row grid
+    # fields puts the FP64 agreement near 1e-10 on this 150-row grid; the edge
+    # cells (band terms, stronger cancellation) near 1e-9, with the rounding of
+    # whichever forward kernels the tuner chose (one step or several per launch)
     assert rel_l2(res["g_eps"], ge) < 1e-9
     assert rel_l2(res["g_sig"], gs) < 1e-9
-    assert rel_l2(edge_cells(res["g_eps"]), edge_cells(ge)) < 1e-9
+    assert rel_l2(edge_cells(res["g_eps"]), edge_cells(ge)) < 3e-9
 
 
 def test_ring_forward_api_matches_oracle(gpu_ctx, oracle, tall):
@@ -185,13 +187,17 @@ def test_kernel_timing_counts_runs(gpu_ctx, oracle, tall):
         t0 = time.perf_counter()
         gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=N.GJ_ADJ_EXACT, precision=N.GJ_F32)
         wall_ms = 1e3 * (time.perf_counter() - t0)
-        kt = {k: gpu_ctx.kernel_time(k) for k in ("fwd_step", "adj_step", "image")}
+        kt = {k: gpu_ctx.kernel_time(k) for k in ("fwd_step", "adj_step", "image", "tb_pass")}
     finally:
         gpu_ctx.set_kernel_timing(False)
-    for k in ("fwd_step", "adj_step"):
-        assert kt[k]["launches"] >= g.nt
+    # the forward runs one step per launch, or (whole history kept, blocked
+    # passes tuned in) up to 4 steps per launch
+    fwd = "tb_pass" if kt["tb_pass"]["launches"] > 0 else "fwd_step"
+    assert kt[fwd]["launches"] >= (g.nt if fwd == "fwd_step" else -(-g.nt // 4))
+    assert kt["adj_step"]["launches"] >= g.nt
+    for k in (fwd, "adj_step"):
         assert 0 < kt[k]["sampled"] <= kt[k]["launches"]
-        assert 0 < kt[k]["avg_us"] < 1e3 * wall_ms / g.nt
+        assert 0 < kt[k]["avg_us"] < 1e3 * wall_ms / kt[k]["launches"]
     assert kt["image"]["launches"] >= 1
 
 

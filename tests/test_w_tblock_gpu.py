@@ -201,11 +201,54 @@ def test_trial_models_in_one_blocked_run(gpu_ctx, multi_ft, oracle, monkeypatch,
     assert launches < 5 * passes
 
 
+@pytest.mark.parametrize("mode", [N.GJ_ADJ_EXACT, N.GJ_ADJ_REFERENCE])
+@pytest.mark.parametrize("cfg", [(3, 1, 16, 3), (2, 0, 0, 3), (4, 1, 64, 6), (1, 1, 8, 3)])
+@pytest.mark.parametrize("which", ["ft", "tall"])
+def test_gradient_with_blocked_forward(gpu_ctx, multi_ft, tall_ft, oracle, monkeypatch, mode, cfg, which):
+    """The gradient's forward (whole u history kept) as blocked passes that
+    write the u history and the band history of the exact adjoint at every
+    step: FP64 gradients of every model cell (edge cells included) equal the
+    oracle's to 1e-10 and the one-step ring kernels' (GJ_TB_GRAD=0) to 1e-12."""
+    p = {"ft": multi_ft, "tall": tall_ft}[which]
+    g = p.grid
+    dobs = [oracle.forward(g, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
+    ge, gs, mis = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]),
+                                        mode="exact" if mode == N.GJ_ADJ_EXACT else "reference")
+    D, stream, lc, ss = cfg
+    _set(monkeypatch, D, 0, 1)
+    monkeypatch.setenv("GJ_TB_STREAM", str(stream))
+    monkeypatch.setenv("GJ_TB_CHUNK", str(max(lc, 4)))
+    monkeypatch.setenv("GJ_TB_STAGES", str(ss))
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64)
+    assert rel_l2(res["g_eps"], ge) < 1e-10 and rel_l2(res["g_sig"], gs) < 1e-10
+    assert np.allclose(res["misfit"], mis, rtol=1e-10)
+    monkeypatch.setenv("GJ_TB_GRAD", "0")
+    ring = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F64)
+    assert rel_l2(res["g_eps"], ring["g_eps"]) < 1e-12 and rel_l2(res["g_sig"], ring["g_sig"]) < 1e-12
+
+
+@pytest.mark.parametrize("mode", [N.GJ_ADJ_EXACT, N.GJ_ADJ_REFERENCE])
+def test_gradient_with_blocked_forward_f32(gpu_ctx, multi_ft, oracle, monkeypatch, mode):
+    """FP32 gradient with the blocked forward: 1e-4 rel-L2 and cosine >= 1 - 1e-4
+    against the FP64 oracle."""
+    from conftest import cosine
+    p = multi_ft
+    g = p.grid
+    dobs = [oracle.forward(g, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
+    ge, gs, _ = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]),
+                                      mode="exact" if mode == N.GJ_ADJ_EXACT else "reference")
+    _set_stream(monkeypatch, 3, 16, 0, 3)
+    res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F32)
+    for a_, b_ in ((res["g_eps"], ge), (res["g_sig"], gs)):
+        assert rel_l2(a_, b_) < 1e-4 and cosine(a_, b_) > 1 - 1e-4
+
+
 def test_tuned_forward_matches_oracle(gpu_ctx, multi_ft, oracle_out, monkeypatch):
     """No configuration fixed: the tuner picks one (the ring kernels or a
     blocked depth) and the traces still equal the oracle's."""
     p = multi_ft
-    for k in ("GJ_TB_DEPTH", "GJ_TB_SHAPE", "GJ_TB_SPB", "GJ_TB_STREAM", "GJ_TB_CHUNK", "GJ_TB_STAGES", "GJ_AUTOTUNE"):
+    for k in ("GJ_TB_DEPTH", "GJ_TB_SHAPE", "GJ_TB_SPB", "GJ_TB_STREAM", "GJ_TB_CHUNK", "GJ_TB_STAGES", "GJ_TB_GRAD",
+              "GJ_AUTOTUNE"):
         monkeypatch.delenv(k, raising=False)
     out = gpu_ctx.w_forward(p.grid, p.eps0, p.sig0, p.shots, precision=N.GJ_F64)
     for k in range(len(p.shots)):
