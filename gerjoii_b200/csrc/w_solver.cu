@@ -922,7 +922,9 @@ class WSolver : public WSolverBase {
                           size_t bslot = 0) {
     if (q.D < 1 || q.D > 4 || it + q.D > g.nt) return err.set(GJ_EINVAL, "blocked pass of %d steps at %d", q.D, it);
     GJ_TRY(tb_prepare(err, q, gn));
-    const TbTiles& tt = *tb_tiles.at(tb_key(q, gn));
+    auto itt = tb_tiles.find(tb_key(q, gn));
+    if (itt == tb_tiles.end()) return err.set(GJ_ECUDA, "blocked pass tables missing");
+    const TbTiles& tt = *itt->second;
     TbArgs<T> a{};
     a.A = A; a.B = B; a.fstride = fstride; a.sstride = sstride; a.gn = gn; a.spb = std::max(q.spb, 1);
     a.it = it; a.nd = q.D; a.src = d_src; a.cezj = d_cezj; a.wav = d_wav; a.nt = g.nt; a.shot0 = shot0;
@@ -1003,6 +1005,11 @@ class WSolver : public WSolverBase {
   // the least of three runs after a warm-up run) for the ring kernels and for
   // every depth 1..4 x tile shape x shots per CTA (1, 2), and keeps the fastest.
   gj_status tb_tune(Err& err, int gn, cudaStream_t st) {
+    // the ring candidate runs the ring configuration (and task tables) of gn shots
+    if (ring_nth > 0 && tb_spt == 0) {
+      select_cfg(gn);
+      GJ_TRY(prepare_tasks(err, gn));
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     GJ_CUDA(err, cudaEventCreate(&e0));
     GJ_CUDA(err, cudaEventCreate(&e1));
