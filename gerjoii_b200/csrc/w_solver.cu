@@ -750,7 +750,7 @@ class WSolver : public WSolverBase {
   };
   std::map<int, TbCfg> tb_tuned;
   // the gradient's forward with the whole history kept: blocked passes per
-  // launch size when the tuner chose them (GJ_TB_GRAD=0: one step per launch)
+  // launch size when GJ_TB_GRAD=1 and the tuner chose them (else one step per launch)
   std::map<int, TbCfg> tb_grad;
   // Partition of one pass: tiles (interior tiles first, then PML tiles) and,
   // in streaming mode, the streaming tasks of gn shots.
@@ -2115,8 +2115,10 @@ class WSolver : public WSolverBase {
     }
     const std::map<int, TbCfg> tb_prev = tb_grad;
     tb_grad.clear();
+    // off unless GJ_TB_GRAD=1: on the benchmark grid the passes' history and
+    // band-history stores made a blocked step slower than a ring step
     const char* tg = getenv("GJ_TB_GRAD");
-    if (ring_on && full && !(tg && atoi(tg) == 0)) {
+    if (ring_on && full && tg && atoi(tg) != 0) {
       // tuned (and the pass tables built) here, outside any graph capture
       for (int gn : {G, nshots % G}) {
         if (gn < 1 || tb_grad.count(gn)) continue;

@@ -205,16 +205,18 @@ def test_trial_models_in_one_blocked_run(gpu_ctx, multi_ft, oracle, monkeypatch,
 @pytest.mark.parametrize("cfg", [(3, 1, 16, 3), (2, 0, 0, 3), (4, 1, 64, 6), (1, 1, 8, 3)])
 @pytest.mark.parametrize("which", ["ft", "tall"])
 def test_gradient_with_blocked_forward(gpu_ctx, multi_ft, tall_ft, oracle, monkeypatch, mode, cfg, which):
-    """The gradient's forward (whole u history kept) as blocked passes that
-    write the u history and the band history of the exact adjoint at every
-    step: FP64 gradients of every model cell (edge cells included) equal the
-    oracle's to 1e-10 and the one-step ring kernels' (GJ_TB_GRAD=0) to 1e-12."""
+    """The gradient's forward (whole u history kept) as blocked passes
+    (GJ_TB_GRAD=1) that write the u history and the band history of the exact
+    adjoint at every step: FP64 gradients of every model cell (edge cells
+    included) equal the oracle's to 1e-10 and the one-step ring kernels'
+    (GJ_TB_GRAD=0) to 1e-12."""
     p = {"ft": multi_ft, "tall": tall_ft}[which]
     g = p.grid
     dobs = [oracle.forward(g, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
     ge, gs, mis = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]),
                                         mode="exact" if mode == N.GJ_ADJ_EXACT else "reference")
     D, stream, lc, ss = cfg
+    monkeypatch.setenv("GJ_TB_GRAD", "1")
     _set(monkeypatch, D, 0, 1)
     monkeypatch.setenv("GJ_TB_STREAM", str(stream))
     monkeypatch.setenv("GJ_TB_CHUNK", str(max(lc, 4)))
@@ -237,6 +239,7 @@ def test_gradient_with_blocked_forward_f32(gpu_ctx, multi_ft, oracle, monkeypatc
     dobs = [oracle.forward(g, p.eps_true, p.sig_true, sh)[0] for sh in p.shots]
     ge, gs, _ = oracle.gradient_batch(g, p.eps0, p.sig0, p.shots, np.stack([d.T for d in dobs]),
                                       mode="exact" if mode == N.GJ_ADJ_EXACT else "reference")
+    monkeypatch.setenv("GJ_TB_GRAD", "1")
     _set_stream(monkeypatch, 3, 16, 0, 3)
     res = gpu_ctx.w_gradient(g, p.eps0, p.sig0, p.shots, dobs, mode=mode, precision=N.GJ_F32)
     for a_, b_ in ((res["g_eps"], ge), (res["g_sig"], gs)):
