@@ -15,6 +15,7 @@
 #include "w_kernels_vec.cuh"
 #include "w_kernels_ring.cuh"
 #include "w_tblock.cuh"
+#include "w_tblock_plan.h"
 #include "w_misfit.cuh"
 #include "w_condition.cuh"
 #include "w_band.cuh"
@@ -786,8 +787,7 @@ class WSolver : public WSolverBase {
     const long key = tb_key(q, gn);
     if (tb_tiles.count(key)) return GJ_OK;
     const int D = q.D, shape = q.shape;
-    const int G = tb_shape_G(shape), RC = tb_shape_RC(shape), RR = 32 * G;
-    const int TR = RR - 2 * D, TC = RC - 2 * D;
+    const int G = tb_shape_G(shape), RC = tb_shape_RC(shape);
     for (int pml = 0; pml < 2; ++pml) {
       const size_t sm = tb_smem(shape, pml, sizeof(T));
       if (sm > size_t(maxsm_dyn)) return err.set(GJ_EINVAL, "tile shape %d needs %zu B of shared memory", shape, sm);
@@ -795,118 +795,45 @@ class WSolver : public WSolverBase {
                                         int(sm)));
     }
     auto tt = std::make_unique<TbTiles>();
-    // streaming region
-    int rs_lo = 0, rs_hi = 0, cs_lo = 0, cs_hi = -1;
-    std::vector<int> Rs;
-    if (q.stream) {
-      constexpr int V = VT<T>::V, RW = 32 * V;
-      const int stride = V * ((RW + 2 - 2 * D) / V);
-      auto eligible = [&](int R) {
-        if (R + RW > NX - 1) return false;
-        for (int I = std::max(R - 1, 0); I <= R + RW; ++I)
-          if (!fast_row(I)) return false;
-        return true;
-      };
-      // owned rows per task: [R + D - 1, R + D - 1 + stride) (from 0 when R = 0),
-      // and a last task aligned to the last eligible row that owns the rest
-      // of its exact rows [.., R + RW - D + 1)
-      std::vector<std::pair<int, int>> own;
-      int R = 0;
-      while (R + RW <= NX - 1 && !eligible(R)) R += V;
-      for (; eligible(R); R += stride) {
-        Rs.push_back(R);
-        own.push_back({R == 0 ? 0 : R + D - 1, R + D - 1 + stride});
-      }
-      if (!Rs.empty()) {
-        int Rx = Rs.back() + stride - V;
-        while (Rx > Rs.back() && !eligible(Rx)) Rx -= V;
-        if (Rx > Rs.back() && Rx + RW - D + 1 > own.back().second) {
-          Rs.push_back(Rx);
-          own.push_back({own.back().second, Rx + RW - D + 1});
-        }
-      }
-      // rows from bR0 down belong to the band frame of the exact adjoint, whose
-      // history the tiles write: the streamed rows stop above it
-      while (!own.empty() && own.back().second > w.bR0) {
-        own.back().second = w.bR0;
-        if (own.back().second <= own.back().first) { own.pop_back(); Rs.pop_back(); }
-        else break;
-      }
-      cs_lo = w.ej0 + D - 1;
-      cs_hi = w.ej1 - D + 1;
-      if (Rs.empty() || cs_hi - cs_lo + 1 < 1 || NY >= 65536 || NX >= 65536) {
-        Rs.clear();
-        cs_hi = cs_lo - 1;
-      } else {
-        rs_lo = own.front().first;
-        rs_hi = own.back().second;
-      }
+    TbGeom gm{};
+    gm.NX = NX; gm.NY = NY; gm.ei0 = w.ei0; gm.ei1 = w.ei1; gm.ej0 = w.ej0; gm.ej1 = w.ej1;
+    gm.hyi0 = w.hyi0; gm.hyi1 = w.hyi1; gm.hxj0 = w.hxj0; gm.hxj1 = w.hxj1; gm.pml_top = g.pml_top; gm.bR0 = w.bR0;
+    const TbPlan pl = tb_plan(gm, D, G, RC, q.stream != 0, VT<T>::V);
+    if (!pl.rows.empty()) {
+      const int cs_lo = pl.cs_lo, cs_hi = pl.cs_hi;
       // per (row task, chunk): a receiver of any shot among its owned nodes (so
       // the table serves every shot group of the same size)
       const int nch = (cs_hi - cs_lo + q.lc) / q.lc;
-      std::vector<char> recf(Rs.size() * std::max(nch, 0), 0);
+      std::vector<char> recf(pl.rows.size() * size_t(nch), 0);
       for (int zs = 0; zs < nshots; ++zs)
         for (int r = 0; r < nrs[zs]; ++r) {
           const long kk = sh[zs].rec[r];
           const int I = int(kk % ld), J = int(kk / ld);
           if (J < cs_lo || J > cs_hi) continue;
-          for (size_t k = 0; k < Rs.size(); ++k)
-            if (I >= own[k].first && I < own[k].second) recf[k * nch + (J - cs_lo) / q.lc] = 1;
+          for (size_t k = 0; k < pl.rows.size(); ++k)
+            if (I >= pl.rows[k].own_lo && I < pl.rows[k].own_hi) recf[k * nch + (J - cs_lo) / q.lc] = 1;
         }
       std::vector<int4> ts;
       for (int z = 0; z < gn; ++z)
-        for (size_t k = 0; k < Rs.size(); ++k)
+        for (size_t k = 0; k < pl.rows.size(); ++k)
           for (int c0 = cs_lo, ch = 0; c0 <= cs_hi; c0 += q.lc, ++ch) {
             const int c1 = std::min(c0 + q.lc - 1, cs_hi);
-            ts.push_back(make_int4(Rs[k], c0 | (c1 << 16), own[k].first | (own[k].second << 16),
+            ts.push_back(make_int4(pl.rows[k].R, c0 | (c1 << 16), pl.rows[k].own_lo | (pl.rows[k].own_hi << 16),
                                    z | (recf[k * nch + ch] ? TBS_HAS_REC : 0)));
           }
       tt->nS = int(ts.size());
-      if (tt->nS) {
-        GJ_TRY(tt->sbuf.alloc(err, ts.size() * sizeof(int4)));
-        GJ_CUDA(err, cudaMemcpy(tt->sbuf.p, ts.data(), ts.size() * sizeof(int4), cudaMemcpyHostToDevice));
-      }
+      GJ_TRY(tt->sbuf.alloc(err, ts.size() * sizeof(int4)));
+      GJ_CUDA(err, cudaMemcpy(tt->sbuf.p, ts.data(), ts.size() * sizeof(int4), cudaMemcpyHostToDevice));
       if (tbs_smem(q.ss) > size_t(maxsm_dyn)) return err.set(GJ_EINVAL, "streaming stages %d too many", q.ss);
       GJ_CUDA(err, cudaFuncSetAttribute(tbs_kernel<T>(D, q.ss), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         int(tbs_smem(q.ss))));
     }
-    const bool streamed = !Rs.empty();
-    // tiles over [a0, a1] x [b0, b1], clipped
-    std::vector<int4> ti, tp;
-    auto tile_rect = [&](int a0, int a1, int b0, int b1) {
-      for (int c0 = b0; c0 <= b1; c0 += TC)
-        for (int r0 = a0; r0 <= a1; r0 += TR) {
-          const int tr = std::min(TR, a1 - r0 + 1), tc = std::min(TC, b1 - c0 + 1);
-          bool interior = true;
-          for (int col = 0; col < RC && interior; ++col) {
-            const int j = c0 - D + col;
-            if (j < 0 || j > NY) continue;
-            for (int row = 0; row < RR; ++row) {
-              const int i = r0 - D + row;
-              if (i < 0 || i > NX) continue;
-              const bool hx = j <= NY - 1 && col < RC - 1, hy = i <= NX - 1 && row < RR - 1;
-              const bool e = i >= 1 && i <= NX - 1 && j >= 1 && j <= NY - 1 && row >= 1 && col >= 1;
-              if ((hx && !(j >= w.hxj0 && j <= w.hxj1)) || (hy && !(i >= w.hyi0 && i <= w.hyi1)) ||
-                  (e && !(i >= w.ei0 && i <= w.ei1 && j >= w.ej0 && j <= w.ej1))) {
-                interior = false;
-                break;
-              }
-            }
-          }
-          (interior ? ti : tp).push_back(make_int4(r0, c0, tr, tc));
-        }
-    };
-    if (!streamed) {
-      tile_rect(0, NX, 0, NY);
-    } else {
-      if (rs_lo > 0) tile_rect(0, rs_lo - 1, 0, NY);
-      if (rs_hi <= NX) tile_rect(rs_hi, NX, 0, NY);
-      if (cs_lo > 0) tile_rect(rs_lo, rs_hi - 1, 0, cs_lo - 1);
-      if (cs_hi < NY) tile_rect(rs_lo, rs_hi - 1, cs_hi + 1, NY);
+    // tiles: interior ones first, then PML ones
+    std::vector<int4> ti;
+    for (const TbTile& t : pl.tiles) {
+      ti.push_back(make_int4(t.r0, t.c0, t.tr, t.tc));
+      (t.interior ? tt->nI : tt->nP) += 1;
     }
-    tt->nI = int(ti.size());
-    tt->nP = int(tp.size());
-    ti.insert(ti.end(), tp.begin(), tp.end());
     if (!ti.empty()) {
       GJ_TRY(tt->buf.alloc(err, ti.size() * sizeof(int4)));
       GJ_CUDA(err, cudaMemcpy(tt->buf.p, ti.data(), ti.size() * sizeof(int4), cudaMemcpyHostToDevice));
