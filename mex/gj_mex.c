@@ -186,6 +186,33 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     check(gj_w_misfit(ctx(), &g, prec, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, dobs, mk, mxGetPr(plhs[0])));
     for (int k = 0; k < ns; ++k) mxFree(recs[k]);
     mxFree(recs); mxFree(shots); mxFree(dobs);
+  } else if (!strcmp(cmd, "w_misfit_trials")) {
+    /* E = gj_mex('w_misfit_trials', EPS, SIG, grid, S (ns x 2), Mcell, wavelet, dobs_cell, obj_FNC, band)
+       (the nparabo trial objectives of one w_stepparabola_e.m search, w_objs_e.m:24-65 for every trial
+        model, in one call: EPS and SIG hold the trial models (m x n x ntrial); band = [f_low f_high steep]
+        band-filters both trace sets first as w_objs_e.m:33-36 does; E is ns x ntrial) */
+    gj_w_grid g = wgrid(prhs[3]);
+    long** recs;
+    double* dobs;
+    int ns;
+    gj_w_shot* shots = pack_shots(prhs[4], prhs[5], prhs[6], prhs[7], g.nt, &recs, &dobs, &ns);
+    const gj_misfit_kind mk = nrhs > 8 ? misfit_kind(prhs[8]) : GJ_MISFIT_L2;
+    const size_t mn = (size_t)g.m * (size_t)g.n;
+    const int ntrial = (int)(mxGetNumberOfElements(prhs[1]) / mn);
+    if (ntrial < 1 || mxGetNumberOfElements(prhs[2]) != (size_t)ntrial * mn)
+      mexErrMsgIdAndTxt("gerjoii:arg", "EPS and SIG must hold the same number of m x n trial models");
+    gj_w_opts o;
+    memset(&o, 0, sizeof o);
+    if (nrhs > 9 && mxGetNumberOfElements(prhs[9]) >= 2) {
+      o.filt_low = mxGetPr(prhs[9])[0];
+      o.filt_high = mxGetPr(prhs[9])[1];
+      if (mxGetNumberOfElements(prhs[9]) >= 3) o.filt_steep = (int)mxGetPr(prhs[9])[2];
+    }
+    plhs[0] = mxCreateDoubleMatrix(ns, ntrial, mxREAL);
+    check(gj_w_misfit_trials(ctx(), &g, prec, ntrial, mxGetPr(prhs[1]), mxGetPr(prhs[2]), shots, ns, dobs, mk, &o,
+                             mxGetPr(plhs[0])));
+    for (int k = 0; k < ns; ++k) mxFree(recs[k]);
+    mxFree(recs); mxFree(shots); mxFree(dobs);
   } else if (!strcmp(cmd, "dc_fwd2_5d") || !strcmp(cmd, "dc_gradient2_5d")) {
     /* [d, u, u_k] = gj_mex('dc_fwd2_5d', sigma_robin, dcgrid, AB (ns x 2, 1-based), I, MNcell, kyw_cell,
                             alpha_cell)   (u_k: (n*m) x n_ky x ns, gerjoii_.dc.u_k of dc_fwd2_5d.m:61)
