@@ -21,9 +21,13 @@
 //
 // Interior tiles (PML = false: every updated node of the staged region is an
 // interior Ez node, an interior Hx column and an interior Hy row, as the host
-// classifies them) stage three fields; PML tiles stage five and read the strip
-// and split-field coefficients per step (they are shared by all shots and stay
-// in L2).  The arithmetic is k_step's, node for node.
+// classifies them, w_tblock_plan.h) stage three fields; PML tiles stage five
+// and keep the strip and split-field coefficients of their nodes in registers
+// for the pass (narrow tiles) or read them per step from L2 (wider tiles).
+// The gradient's forward (when asked for) also writes the u history and the
+// band history of the exact adjoint of every step.  The arithmetic is
+// k_step's, node for node.  The streaming interior tasks (k_fwd_tbs, below)
+// cover the interior of large grids; these tiles then cover the rest.
 #pragma once
 #include "w_kernels_ring.cuh"
 #include "w_band.cuh"
