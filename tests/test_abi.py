@@ -57,3 +57,20 @@ def test_python_constants_match_the_header_enums():
         assert getattr(N, name) == int(m.group(1)), name
     assert set(N.MISFIT_KINDS.values()) == {0, 1, 2, 3, 4}
     assert N.misfit_kind("env_LOG") == N.GJ_MISFIT_ENV_LOG and N.misfit_kind(3) == 3
+
+
+def test_kernel_kinds_match_the_library_enum():
+    """The ctypes binding's kernel-timing kinds carry the numbers the library's
+    KernelKind enum gives them (gj_kernel_time's `kind`), the blocked forward
+    pass included."""
+    from gerjoii_b200 import _native as N
+    txt = open(os.path.join(ROOT, "gerjoii_b200", "csrc", "gj_internal.h")).read()
+    body = re.search(r"enum KernelKind\s*\{(.*?)\};", txt, flags=re.S).group(1)
+    enum = {k: int(v) for k, v in re.findall(r"\b(KK_[A-Z0-9_]+)\s*=\s*(\d+)", body)}
+    names = {"fwd_step": "KK_FWD_STEP", "ref_step": "KK_REF_STEP", "adj_step": "KK_ADJ_STEP", "io": "KK_IO",
+             "plain": "KK_PLAIN", "dc_factor": "KK_DC_FACTOR", "image": "KK_IMAGE", "dc_precond": "KK_DC_PRECOND",
+             "tb_pass": "KK_TB_PASS"}
+    assert set(N.Context.KERNEL_KINDS) == set(names)
+    for py, c in names.items():
+        assert N.Context.KERNEL_KINDS[py] == enum[c], py
+    assert enum["KK_NKINDS"] == len(names)
